@@ -1,0 +1,331 @@
+"""B200 (sm_100a) implementation of the per-design-iteration hot path of
+natashahirt/AlgorithmEngineering_AltProject (`top3d_xl_cli GLOBAL`).
+
+The compute lives in the in-tree CUDA library ``libt3d_b200.so`` (C-ABI: include/t3d_b200.h).
+This module is a thin ctypes binding that mirrors the reference's operator API
+(cpp/include/fea.hpp, solver.hpp, multigrid/multigrid.hpp, filter.hpp, driver.hpp) with the
+reference's array layouts.  There is no Python or CPU fallback: importing works without a GPU,
+but every compute call needs the native library and a CUDA device and raises otherwise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+__all__ = ["Problem", "T3DError", "library", "IterRecord", "Params", "LIB_PATH", "HEADER_PATH"]
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "libt3d_b200.so")
+HEADER_PATH = os.path.join(os.path.dirname(PKG_DIR), "include", "t3d_b200.h")
+
+T3D_OK, T3D_ERR_INVALID, T3D_ERR_CUDA, T3D_ERR_OOM, T3D_ERR_NO_DEVICE, T3D_ERR_UNSUPPORTED, T3D_ERR_NUMERIC = range(7)
+T3D_SUM_REFERENCE, T3D_SUM_FP64 = 0, 1
+T3D_FP64, T3D_MIXED = 0, 1
+
+_f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+
+
+class T3DError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("t3d error %d: %s" % (code, msg))
+        self.code = code
+
+
+class Params(C.Structure):
+    _fields_ = [("E0", C.c_float), ("Emin", C.c_float), ("nu", C.c_float), ("penal", C.c_float),
+                ("cg_tol", C.c_float), ("cg_max_it", C.c_int), ("mg_nondyadic", C.c_int),
+                ("mg_max_levels", C.c_int), ("mg_weight", C.c_float), ("filter_rmin", C.c_float),
+                ("oc_sum_order", C.c_int), ("precision", C.c_int), ("device", C.c_int),
+                ("reserved", C.c_int * 7)]
+
+
+class Info(C.Structure):
+    _fields_ = [("res", C.c_int64 * 3), ("orig", C.c_int64 * 3), ("num_elements", C.c_int64),
+                ("num_nodes", C.c_int64), ("num_free", C.c_int64), ("num_levels", C.c_int64),
+                ("levels", (C.c_int64 * 4) * 8), ("coarse_n", C.c_int64), ("coarse_cholesky_ok", C.c_int64),
+                ("device_bytes", C.c_int64)]
+
+
+class IterRecord(C.Structure):
+    _fields_ = [("loop", C.c_int), ("pcg_iters", C.c_int), ("obj", C.c_double), ("vol", C.c_float),
+                ("sharp", C.c_float), ("cons", C.c_float), ("change", C.c_float), ("lmid", C.c_float),
+                ("bisections", C.c_int), ("t_total", C.c_double), ("t_cg", C.c_double), ("t_opt", C.c_double),
+                ("t_filter", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_CTX = C.c_void_p
+# name -> (restype, argtypes); every function declared in include/t3d_b200.h
+_SIGS = {
+    "t3d_params_default": (C.c_int, [C.POINTER(Params)]),
+    "t3d_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(Params), C.POINTER(_CTX)]),
+    "t3d_destroy": (C.c_int, [_CTX]),
+    "t3d_get_info": (C.c_int, [_CTX, C.POINTER(Info)]),
+    "t3d_last_error": (C.c_char_p, []),
+    "t3d_get_ke": (C.c_int, [_CTX, _f64p]),
+    "t3d_set_ke": (C.c_int, [_CTX, _f64p]),
+    "t3d_get_element_map": (C.c_int, [_CTX, _i32p]),
+    "t3d_get_free_dofs": (C.c_int, [_CTX, _i32p]),
+    "t3d_get_load": (C.c_int, [_CTX, _f64p]),
+    "t3d_matvec": (C.c_int, [_CTX, _f64p, _f64p, _f64p]),
+    "t3d_mg_setup": (C.c_int, [_CTX, _f64p]),
+    "t3d_vcycle": (C.c_int, [_CTX, _f64p, _f64p]),
+    "t3d_pcg": (C.c_int, [_CTX, _f64p, _f64p, _f64p, C.c_double, C.c_int, C.POINTER(C.c_int)]),
+    "t3d_compliance": (C.c_int, [_CTX, _f64p, _f64p, _f64p, C.POINTER(C.c_double)]),
+    "t3d_mg_get_diag": (C.c_int, [_CTX, C.c_int, _f64p]),
+    "t3d_mg_get_mask": (C.c_int, [_CTX, C.c_int, _u8p]),
+    "t3d_mg_coarse_matrix": (C.c_int, [_CTX, _f64p, _f64p]),
+    "t3d_filter_apply": (C.c_int, [_CTX, _f32p, _f32p]),
+    "t3d_filter_get_state": (C.c_int, [_CTX, _f64p, _f64p, _f64p]),
+    "t3d_filter_set_state": (C.c_int, [_CTX, _f64p, _f64p]),
+    "t3d_simp": (C.c_int, [_CTX, _f32p, _f64p]),
+    "t3d_sensitivity": (C.c_int, [_CTX, _f32p, _f64p, C.c_double, _f32p]),
+    "t3d_dc_scale": (C.c_int, [_CTX, _f32p, _f32p, _f32p]),
+    "t3d_oc_update": (C.c_int, [_CTX, _f32p, _f32p, C.c_float, _f32p, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                C.POINTER(C.c_int)]),
+    "t3d_design_init": (C.c_int, [_CTX, C.c_float, C.POINTER(C.c_double)]),
+    "t3d_design_step": (C.c_int, [_CTX, C.POINTER(IterRecord)]),
+    "t3d_design_step_host": (C.c_int, [_CTX, _f32p, _f32p, C.POINTER(IterRecord)]),
+    "t3d_get_density": (C.c_int, [_CTX, _f32p]),
+    "t3d_set_density": (C.c_int, [_CTX, _f32p]),
+    "t3d_run_global": (C.c_int, [_CTX, C.c_float, C.c_int, C.POINTER(C.c_double), C.POINTER(IterRecord),
+                                 C.POINTER(C.c_int), _f32p]),
+    "t3d_synchronize": (C.c_int, [_CTX]),
+}
+
+_lib = None
+
+
+def library():
+    """Load libt3d_b200.so (raises if it has not been built; there is no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise T3DError(T3D_ERR_UNSUPPORTED, "native library %s not built; run "
+                           "`python -m algorithmengineering_altproject_b200._build`" % LIB_PATH)
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(rc):
+    if rc != T3D_OK:
+        raise T3DError(rc, library().t3d_last_error().decode())
+
+
+def default_params(**kw):
+    p = Params()
+    _check(library().t3d_params_default(C.byref(p)))
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+class Problem:
+    """One cantilever design on one GPU: the reference's `Problem` + MG hierarchy + PDE filter.
+
+    Constructed like ``CreateVoxelFEAmodel_Cuboid(pb, nely, nelx, nelz); ApplyBoundaryConditions(pb);
+    mg::build_static_once(...); SetupPDEFilter(pb, rMin)`` (fea.cpp:181-447, preconditioner.cpp:19,
+    filter.cpp:9).  Methods keep the reference's names and array layouts.
+    """
+
+    def __init__(self, nely, nelx, nelz, **params):
+        self._lib = library()
+        self.params = default_params(**params)
+        h = _CTX()
+        _check(self._lib.t3d_create(nely, nelx, nelz, C.byref(self.params), C.byref(h)))
+        self._h = h
+        info = Info()
+        _check(self._lib.t3d_get_info(self._h, C.byref(info)))
+        self.res = tuple(int(v) for v in info.res)
+        self.ne = int(info.num_elements)
+        self.nn = int(info.num_nodes)
+        self.nf = int(info.num_free)
+        self.nlev = int(info.num_levels)
+        self.levels = [tuple(int(v) for v in info.levels[l]) for l in range(self.nlev)]
+        self.coarse_n = int(info.coarse_n)
+        self.device_bytes = int(info.device_bytes)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.t3d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def info(self):
+        info = Info()
+        _check(self._lib.t3d_get_info(self._h, C.byref(info)))
+        return info
+
+    def level_nodes(self, l):
+        nx, ny, nz, _ = self.levels[l]
+        return (nx + 1) * (ny + 1) * (nz + 1)
+
+    # ---- model data
+    def ke(self):
+        out = np.zeros(576)
+        _check(self._lib.t3d_get_ke(self._h, out))
+        return out.reshape(24, 24)
+
+    def set_ke(self, Ke):
+        _check(self._lib.t3d_set_ke(self._h, _f64(Ke).ravel()))
+
+    def ele_map_back(self):
+        out = np.zeros(self.ne, dtype=np.int32)
+        _check(self._lib.t3d_get_element_map(self._h, out))
+        return out
+
+    def free_dofs(self):
+        out = np.zeros(self.nf, dtype=np.int32)
+        _check(self._lib.t3d_get_free_dofs(self._h, out))
+        return out
+
+    def bfree(self):
+        out = np.zeros(self.nf)
+        _check(self._lib.t3d_get_load(self._h, out))
+        return out
+
+    # ---- operators (reference names)
+    def K_times_u_finest(self, eleE, uFree):
+        y = np.zeros(self.nf)
+        _check(self._lib.t3d_matvec(self._h, _f64(eleE), _f64(uFree), y))
+        return y
+
+    def make_diagonal_preconditioner_from_static(self, eleE):
+        _check(self._lib.t3d_mg_setup(self._h, _f64(eleE)))
+
+    def vcycle(self, rFree):
+        z = np.zeros(self.nf)
+        _check(self._lib.t3d_vcycle(self._h, _f64(rFree), z))
+        return z
+
+    def PCG_free(self, eleE, bFree, xFree, tol=None, maxIt=800):
+        tol = float(np.float32(1e-3)) if tol is None else float(tol)
+        x = np.array(xFree, dtype=np.float64, copy=True)
+        its = C.c_int()
+        _check(self._lib.t3d_pcg(self._h, _f64(eleE), _f64(bFree), x, C.c_double(tol), int(maxIt), C.byref(its)))
+        return x, int(its.value)
+
+    def ComputeCompliance(self, eleE, uFree):
+        ce = np.zeros(self.ne)
+        Cv = C.c_double()
+        _check(self._lib.t3d_compliance(self._h, _f64(eleE), _f64(uFree), ce, C.byref(Cv)))
+        return float(Cv.value), ce
+
+    def mg_diag(self, level):
+        out = np.zeros(3 * self.level_nodes(level))
+        _check(self._lib.t3d_mg_get_diag(self._h, level, out))
+        return out
+
+    def mg_mask(self, level):
+        out = np.zeros(3 * self.level_nodes(level), dtype=np.uint8)
+        _check(self._lib.t3d_mg_get_mask(self._h, level, out))
+        return out
+
+    def coarse_matrix(self, eleE):
+        n = self.coarse_n
+        out = np.zeros(n * n)
+        _check(self._lib.t3d_mg_coarse_matrix(self._h, _f64(eleE), out))
+        return out.reshape(n, n)
+
+    def ApplyPDEFilter(self, src):
+        dst = np.zeros(self.ne, dtype=np.float32)
+        _check(self._lib.t3d_filter_apply(self._h, _f32(src), dst))
+        return dst
+
+    def filter_state(self):
+        lx, lr, dg = np.zeros(self.nn), np.zeros(self.nn), np.zeros(self.nn)
+        _check(self._lib.t3d_filter_get_state(self._h, lx, lr, dg))
+        return lx, lr, dg
+
+    def filter_set_state(self, lastx, lastrhs):
+        _check(self._lib.t3d_filter_set_state(self._h, _f64(lastx), _f64(lastrhs)))
+
+    def simp(self, xPhys):
+        E = np.zeros(self.ne)
+        _check(self._lib.t3d_simp(self._h, _f32(xPhys), E))
+        return E
+
+    def sensitivity(self, xPhys, ce, csolid):
+        dc = np.zeros(self.ne, dtype=np.float32)
+        _check(self._lib.t3d_sensitivity(self._h, _f32(xPhys), _f64(ce), C.c_double(csolid), dc))
+        return dc
+
+    def dc_scale(self, dcf, x):
+        dc = np.zeros(self.ne, dtype=np.float32)
+        _check(self._lib.t3d_dc_scale(self._h, _f32(dcf), _f32(x), dc))
+        return dc
+
+    def oc_update(self, x, dc, V0):
+        xn = np.zeros(self.ne, dtype=np.float32)
+        ch, lm, nb = C.c_float(), C.c_float(), C.c_int()
+        _check(self._lib.t3d_oc_update(self._h, _f32(x), _f32(dc), C.c_float(V0), xn, C.byref(ch), C.byref(lm),
+                                       C.byref(nb)))
+        return xn, float(ch.value), float(lm.value), int(nb.value)
+
+    # ---- design loop
+    def design_init(self, V0):
+        cs = C.c_double()
+        _check(self._lib.t3d_design_init(self._h, C.c_float(V0), C.byref(cs)))
+        return float(cs.value)
+
+    def design_step(self):
+        rec = IterRecord()
+        _check(self._lib.t3d_design_step(self._h, C.byref(rec)))
+        return rec.as_dict()
+
+    def design_step_host(self, x_in):
+        rec = IterRecord()
+        xo = np.zeros(self.ne, dtype=np.float32)
+        _check(self._lib.t3d_design_step_host(self._h, _f32(x_in), xo, C.byref(rec)))
+        return xo, rec.as_dict()
+
+    def density(self):
+        x = np.zeros(self.ne, dtype=np.float32)
+        _check(self._lib.t3d_get_density(self._h, x))
+        return x
+
+    def set_density(self, x):
+        _check(self._lib.t3d_set_density(self._h, _f32(x)))
+
+    def run_global(self, V0, nLoop):
+        """TOP3D_XL_GLOBAL for one simulation (driver.cpp:23-218): (Csolid, records, final x)."""
+        recs = (IterRecord * max(1, nLoop))()
+        n = C.c_int()
+        cs = C.c_double()
+        x = np.zeros(self.ne, dtype=np.float32)
+        _check(self._lib.t3d_run_global(self._h, C.c_float(V0), int(nLoop), C.byref(cs), recs, C.byref(n), x))
+        return float(cs.value), [recs[i].as_dict() for i in range(n.value)], x
+
+    def synchronize(self):
+        _check(self._lib.t3d_synchronize(self._h))

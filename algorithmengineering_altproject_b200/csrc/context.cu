@@ -1,0 +1,1010 @@
+// Host runtime of the B200 library: one context = one cantilever design on one GPU.  Owns every
+// device buffer (allocated once at creation, none afterwards on the design-loop path), orchestrates
+// the kernels of the design iteration on one stream, captures the PCG iteration in CUDA graphs and
+// implements the C-ABI declared in include/t3d_b200.h.
+#include "t3d_b200.h"
+#include "kernels.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <memory>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace t3d {
+
+namespace {
+thread_local std::string g_err;
+}
+
+int set_error(int code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+int set_cuda_error(cudaError_t e, const char* what, const char* file, int line) {
+    char buf[512];
+    std::snprintf(buf, sizeof buf, "%s failed: %s (%s:%d)", what, cudaGetErrorString(e), file, line);
+    g_err = buf;
+    return e == cudaErrorMemoryAllocation ? T3D_ERR_OOM : T3D_ERR_CUDA;
+}
+
+// ------------------------------------------------------------------ host-side model constants
+// Unit-modulus hex8 stiffness (fea.cpp:117-179): 2x2x2 Gauss, Voigt [xx,yy,zz,yz,xz,xy],
+// local DOF 3a+c with the natural-coordinate node order (-,-,-),(+,-,-),(+,+,-),(-,+,-), then +z.
+static void hex8_stiffness(double nu, double h, double* Ke) {
+    const double lam = nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
+    const double mu = 1.0 / (2.0 * (1.0 + nu));
+    double D[6][6] = {{0}};
+    for (int i = 0; i < 3; ++i) {
+        for (int j = 0; j < 3; ++j) D[i][j] = lam;
+        D[i][i] = lam + 2.0 * mu;
+        D[3 + i][3 + i] = mu;
+    }
+    static const double sg[8] = {-1, 1, 1, -1, -1, 1, 1, -1};
+    static const double tg[8] = {-1, -1, 1, 1, -1, -1, 1, 1};
+    static const double pg[8] = {-1, -1, -1, -1, 1, 1, 1, 1};
+    const double gq = 1.0 / std::sqrt(3.0);
+    const double detJ = (h * h * h) / 8.0, sc = 2.0 / h;
+    std::memset(Ke, 0, 576 * sizeof(double));
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b)
+            for (int c = 0; c < 2; ++c) {
+                const double s = a ? gq : -gq, t = b ? gq : -gq, q = c ? gq : -gq;
+                double B[6][24] = {{0}};
+                for (int n = 0; n < 8; ++n) {
+                    const double dx = 0.125 * sg[n] * (1 + tg[n] * t) * (1 + pg[n] * q) * sc;
+                    const double dy = 0.125 * tg[n] * (1 + sg[n] * s) * (1 + pg[n] * q) * sc;
+                    const double dz = 0.125 * pg[n] * (1 + sg[n] * s) * (1 + tg[n] * t) * sc;
+                    B[0][3 * n] = dx; B[1][3 * n + 1] = dy; B[2][3 * n + 2] = dz;
+                    B[3][3 * n + 1] = dz; B[3][3 * n + 2] = dy;
+                    B[4][3 * n] = dz; B[4][3 * n + 2] = dx;
+                    B[5][3 * n] = dy; B[5][3 * n + 1] = dx;
+                }
+                double DB[6][24];
+                for (int i = 0; i < 6; ++i)
+                    for (int j = 0; j < 24; ++j) {
+                        double acc = 0.0;
+                        for (int k = 0; k < 6; ++k) acc += D[i][k] * B[k][j];
+                        DB[i][j] = acc;
+                    }
+                for (int i = 0; i < 24; ++i)
+                    for (int j = 0; j < 24; ++j) {
+                        double acc = 0.0;
+                        for (int k = 0; k < 6; ++k) acc += B[k][i] * DB[k][j];
+                        Ke[i * 24 + j] += acc * detJ;
+                    }
+            }
+}
+
+// PDE-filter 8x8 kernel r^2 KEF0 + KEF1 (filter.cpp:11-54) followed by its 8 row sums (:56-62)
+static void filter_kernel(float rmin, double* kf) {
+    static const double sg[8] = {-1, 1, 1, -1, -1, 1, 1, -1};
+    static const double tg[8] = {-1, -1, 1, 1, -1, -1, 1, 1};
+    static const double pg[8] = {-1, -1, -1, -1, 1, 1, 1, 1};
+    double N[8][8], dS[24][8];
+    for (int g = 0; g < 8; ++g) {
+        const double s = sg[g] / std::sqrt(3.0), t = tg[g] / std::sqrt(3.0), q = pg[g] / std::sqrt(3.0);
+        for (int a = 0; a < 8; ++a) {
+            N[g][a] = 0.125 * (1 + sg[a] * s) * (1 + tg[a] * t) * (1 + pg[a] * q);
+            dS[3 * g + 0][a] = 0.125 * sg[a] * (1 + tg[a] * t) * (1 + pg[a] * q);
+            dS[3 * g + 1][a] = 0.125 * tg[a] * (1 + sg[a] * s) * (1 + pg[a] * q);
+            dS[3 * g + 2][a] = 0.125 * pg[a] * (1 + sg[a] * s) * (1 + tg[a] * t);
+        }
+    }
+    const double rr = ((double)rmin * 1.0) / (2.0 * std::sqrt(3.0));
+    for (int i = 0; i < 8; ++i)
+        for (int j = 0; j < 8; ++j) {
+            double k0 = 0.0, k1 = 0.0;
+            for (int k = 0; k < 24; ++k) k0 += dS[k][i] * dS[k][j];
+            for (int g = 0; g < 8; ++g) k1 += N[g][i] * (1.0 / 8.0) * N[g][j];
+            kf[i * 8 + j] = rr * rr * k0 + k1;
+        }
+    for (int a = 0; a < 8; ++a) {
+        double s = 0.0;
+        for (int b = 0; b < 8; ++b) s += kf[a * 8 + b];
+        kf[64 + a] = s;
+    }
+}
+
+static int pad_levels(uint64_t nvox) {   // padding.hpp:23-33
+    int L = 0;
+    while (nvox >= 50000u) { ++L; nvox = (nvox + 4u) / 8u; }
+    return L < 3 ? 3 : L;
+}
+static int pad_dim(int n, int L) {
+    const int s = 1 << L;
+    return ((n + s - 1) / s) * s;
+}
+
+// ------------------------------------------------------------------ context
+struct Context {
+    t3d_params prm{};
+    Grid g{};
+    Cuboid cub{};
+    int dev = 0;
+    cudaStream_t st = nullptr;
+    int nlev = 0;
+    MgLevel lv[8]{};
+    int Nc = 0;                 // dense coarsest size (0: Jacobi coarsest)
+    int64_t ne = 0;             // solid elements
+    size_t bytes = 0;
+    std::vector<void*> allocs;
+
+    double* Ke = nullptr;       // 576
+    double* kf = nullptr;       // 72
+    double Ke_h[576];
+    uint8_t* solid = nullptr;   // cells
+    uint8_t* mask0 = nullptr;   // nodes
+    double *E = nullptr, *ce = nullptr;                       // cells
+    float *x = nullptr, *xnew = nullptr, *dc = nullptr, *xdc = nullptr, *dcf = nullptr;   // cells
+    double *b = nullptr, *u = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *Ap = nullptr;  // 3 NN
+    PcgScalars* S = nullptr;
+    FilterScalars* FS = nullptr;
+    OcState* OC = nullptr;
+    double* scal = nullptr;     // [0] C, [1] Csolid, [2] objective
+    RedSlot slot[4]{};
+    double *Kce = nullptr, *Kc = nullptr, *LT = nullptr, *Lrow = nullptr;
+    int* chol_status = nullptr;
+    double *frhs = nullptr, *fx = nullptr, *fr = nullptr, *fz = nullptr, *fp = nullptr, *fAp = nullptr,
+           *flastx = nullptr, *flastrhs = nullptr, *fdiag = nullptr;
+    // lazily built maps between the reference's layouts and the grid
+    int32_t* morton = nullptr;          // [ne] cell index of the k-th element in Morton order
+    std::vector<int32_t> morton_h;
+    int32_t* free_d = nullptr;
+    std::vector<int32_t> free_h;
+    double* stage = nullptr;            // staging buffer for host<->device conversions
+    size_t stage_n = 0;
+    // pinned host mirror of small device state
+    PcgScalars* S_h = nullptr;
+    OcState* OC_h = nullptr;
+    FilterScalars* FS_h = nullptr;
+    double* scal_h = nullptr;
+    int* flag_h = nullptr;              // two done-flag slots for pipelined polling
+    // CUDA graph of a chunk of PCG iterations
+    cudaGraphExec_t pcg_graph = nullptr;
+    int pcg_graph_len = 0;
+    bool use_graph = true;
+    // design state
+    bool mg_ready = false;
+    bool design_ready = false;
+    float V0 = 0.0f;
+    int loop = 0;
+    cudaEvent_t ev[8]{};
+
+    template <class T>
+    int alloc(T** ptr, size_t n) {
+        void* q = nullptr;
+        const size_t nb = std::max<size_t>(n, 1) * sizeof(T);
+        cudaError_t e = cudaMalloc(&q, nb);
+        if (e != cudaSuccess) return set_cuda_error(e, "cudaMalloc", __FILE__, __LINE__);
+        allocs.push_back(q);
+        bytes += nb;
+        *ptr = static_cast<T*>(q);
+        return T3D_OK;
+    }
+
+    ~Context() {
+        if (pcg_graph) cudaGraphExecDestroy(pcg_graph);
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+        for (void* q : allocs) cudaFree(q);
+        if (S_h) cudaFreeHost(S_h);
+        if (OC_h) cudaFreeHost(OC_h);
+        if (FS_h) cudaFreeHost(FS_h);
+        if (scal_h) cudaFreeHost(scal_h);
+        if (flag_h) cudaFreeHost(flag_h);
+        if (st) cudaStreamDestroy(st);
+    }
+};
+
+#define CHECK(call)                       \
+    do {                                  \
+        int rc_ = (call);                 \
+        if (rc_ != T3D_OK) return rc_;    \
+    } while (0)
+
+static int launch_check(const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_cuda_error(e, what, __FILE__, __LINE__);
+    return T3D_OK;
+}
+
+static int sync(Context* c) {
+    T3D_CUDA_OK(cudaStreamSynchronize(c->st));
+    return T3D_OK;
+}
+
+// ------------------------------------------------------------------ creation
+static int build_levels(Context* c) {
+    // hierarchy.cpp:84-138: span 4 first (non-dyadic), then 2, exact divisibility, stop at min dim <= 2
+    int nx = c->g.nx, ny = c->g.ny, nz = c->g.nz;
+    c->nlev = 0;
+    MgLevel& L0 = c->lv[c->nlev++];
+    L0.nx = nx; L0.ny = ny; L0.nz = nz; L0.span = 1;
+    for (int li = 1; li < c->prm.mg_max_levels && li < 8; ++li) {
+        const int s = (li == 1 && c->prm.mg_nondyadic) ? 4 : 2;
+        if (nx % s || ny % s || nz % s) break;
+        if (nx / s < 1 || ny / s < 1 || nz / s < 1) break;
+        nx /= s; ny /= s; nz /= s;
+        MgLevel& L = c->lv[c->nlev++];
+        L.nx = nx; L.ny = ny; L.nz = nz; L.span = s;
+        if (std::min(nx, std::min(ny, nz)) <= 2) break;
+    }
+    if (c->nlev < 2) return set_error(T3D_ERR_UNSUPPORTED, "grid admits no coarse multigrid level");
+    for (int l = 0; l < c->nlev; ++l) {
+        MgLevel& L = c->lv[l];
+        L.nn = (int64_t)(L.nx + 1) * (L.ny + 1) * (L.nz + 1);
+        CHECK(c->alloc(&L.diag, 3 * L.nn));
+        if (l == 0) L.mask = c->mask0;
+        else {
+            CHECK(c->alloc(&L.mask, L.nn));
+            CHECK(c->alloc(&L.r, 3 * L.nn));
+            CHECK(c->alloc(&L.x, 3 * L.nn));
+        }
+    }
+    const int N = (int)(3 * c->lv[c->nlev - 1].nn);
+    c->Nc = (N <= 1000) ? N : 0;   // NlimitDofs (preconditioner.cpp:52-54)
+    if (c->Nc) {
+        const MgLevel& Lc = c->lv[c->nlev - 1];
+        CHECK(c->alloc(&c->Kce, (size_t)Lc.nx * Lc.ny * Lc.nz * 576));
+        CHECK(c->alloc(&c->Kc, (size_t)N * N));
+        CHECK(c->alloc(&c->LT, (size_t)N * N));
+        CHECK(c->alloc(&c->Lrow, (size_t)N * N));
+    }
+    CHECK(c->alloc(&c->chol_status, 1));
+    T3D_CUDA_OK(cudaMemsetAsync(c->chol_status, 0, sizeof(int), c->st));
+    for (int l = 0; l + 1 < c->nlev; ++l) launch_mask_restrict(c->lv[l + 1], c->lv[l], c->st);
+    return launch_check("mask restriction");
+}
+
+static int create(int nely, int nelx, int nelz, const t3d_params* prm, Context* c) {
+    if (nely <= 0 || nelx <= 0 || nelz <= 0) return set_error(T3D_ERR_INVALID, "element counts must be positive");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return set_error(T3D_ERR_NO_DEVICE, "no CUDA device available (the library has no CPU path)");
+    }
+    if (prm) c->prm = *prm;
+    else t3d_params_default(&c->prm);
+    if (c->prm.device < 0 || c->prm.device >= ndev) return set_error(T3D_ERR_NO_DEVICE, "device index out of range");
+    if (c->prm.precision != T3D_FP64) return set_error(T3D_ERR_UNSUPPORTED, "only T3D_FP64 precision is built");
+    c->dev = c->prm.device;
+    T3D_CUDA_OK(cudaSetDevice(c->dev));
+    T3D_CUDA_OK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+    for (auto& e : c->ev) T3D_CUDA_OK(cudaEventCreate(&e));
+    c->use_graph = std::getenv("T3D_NO_GRAPH") == nullptr;
+
+    // padding (padding.hpp:42-53, fea.cpp:189-197)
+    const uint64_t nvox = (uint64_t)nelx * nely * nelz;
+    const int L = pad_levels(nvox);
+    const int nx = pad_dim(nelx, L), ny = pad_dim(nely, L), nz = pad_dim(nelz, L);
+    if ((int64_t)(nx + 1) * (ny + 1) * (nz + 1) * 3 >= (int64_t)INT32_MAX)
+        return set_error(T3D_ERR_UNSUPPORTED, "grid too large for 32-bit DOF indices");
+    c->g = make_grid(nx, ny, nz);
+    c->cub = Cuboid{nelx, nely, nelz};
+    c->ne = (int64_t)nelx * nely * nelz;
+    const Grid& g = c->g;
+
+    CHECK(c->alloc(&c->Ke, 576));
+    CHECK(c->alloc(&c->kf, 72));
+    CHECK(c->alloc(&c->solid, g.NE));
+    CHECK(c->alloc(&c->mask0, g.NN));
+    CHECK(c->alloc(&c->E, g.NE));
+    CHECK(c->alloc(&c->ce, g.NE));
+    CHECK(c->alloc(&c->x, g.NE));
+    CHECK(c->alloc(&c->xnew, g.NE));
+    CHECK(c->alloc(&c->dc, g.NE));
+    CHECK(c->alloc(&c->xdc, g.NE));
+    CHECK(c->alloc(&c->dcf, g.NE));
+    for (double** v : {&c->b, &c->u, &c->r, &c->z, &c->p, &c->Ap}) CHECK(c->alloc(v, 3 * g.NN));
+    for (double** v : {&c->frhs, &c->fx, &c->fr, &c->fz, &c->fp, &c->fAp, &c->flastx, &c->flastrhs, &c->fdiag})
+        CHECK(c->alloc(v, g.NN));
+    CHECK(c->alloc(&c->S, 1));
+    CHECK(c->alloc(&c->FS, 1));
+    CHECK(c->alloc(&c->OC, 1));
+    CHECK(c->alloc(&c->scal, 8));
+    double* part = nullptr;
+    unsigned int* cnt = nullptr;
+    CHECK(c->alloc(&part, 4 * RED_BLOCKS));
+    CHECK(c->alloc(&cnt, 4));
+    T3D_CUDA_OK(cudaMemsetAsync(cnt, 0, 4 * sizeof(unsigned int), c->st));
+    for (int i = 0; i < 4; ++i) c->slot[i] = RedSlot{part + i * RED_BLOCKS, cnt + i};
+    T3D_CUDA_OK(cudaMallocHost(&c->S_h, sizeof(PcgScalars)));
+    T3D_CUDA_OK(cudaMallocHost(&c->OC_h, sizeof(OcState)));
+    T3D_CUDA_OK(cudaMallocHost(&c->FS_h, sizeof(FilterScalars)));
+    T3D_CUDA_OK(cudaMallocHost(&c->scal_h, 8 * sizeof(double)));
+    T3D_CUDA_OK(cudaMallocHost(&c->flag_h, 2 * sizeof(int)));
+
+    // element stiffness (fea.cpp:345 passes nu = 0.3 literally) and filter kernel
+    hex8_stiffness(0.3, 1.0, c->Ke_h);
+    T3D_CUDA_OK(cudaMemcpyAsync(c->Ke, c->Ke_h, sizeof c->Ke_h, cudaMemcpyHostToDevice, c->st));
+    double kf[72];
+    filter_kernel(c->prm.filter_rmin, kf);
+    T3D_CUDA_OK(cudaMemcpyAsync(c->kf, kf, sizeof kf, cudaMemcpyHostToDevice, c->st));
+
+    // zero every array once: ghost cells and non-solid cells stay exactly zero from here on
+    T3D_CUDA_OK(cudaMemsetAsync(c->E, 0, g.NE * sizeof(double), c->st));
+    T3D_CUDA_OK(cudaMemsetAsync(c->ce, 0, g.NE * sizeof(double), c->st));
+    for (float* v : {c->x, c->xnew, c->dc, c->xdc, c->dcf})
+        T3D_CUDA_OK(cudaMemsetAsync(v, 0, g.NE * sizeof(float), c->st));
+    for (double* v : {c->b, c->u, c->r, c->z, c->p, c->Ap})
+        T3D_CUDA_OK(cudaMemsetAsync(v, 0, 3 * g.NN * sizeof(double), c->st));
+    for (double* v : {c->frhs, c->fx, c->fr, c->fz, c->fp, c->fAp, c->flastx, c->flastrhs})
+        T3D_CUDA_OK(cudaMemsetAsync(v, 0, g.NN * sizeof(double), c->st));
+    T3D_CUDA_OK(cudaMemsetAsync(c->S, 0, sizeof(PcgScalars), c->st));
+    T3D_CUDA_OK(cudaMemsetAsync(c->scal, 0, 8 * sizeof(double), c->st));
+
+    // model: solid cells, fixed DOFs, load (fea.cpp:181-447)
+    launch_setup_cells(g, c->cub, c->solid, c->st);
+    launch_setup_mask0(g, c->solid, c->mask0, c->st);
+    {
+        const int ix_load = std::min(nelx, g.nnx - 1);
+        const int iz_max = std::max(1, nz / 6);
+        const int count = (iz_max + 1) * g.nny;
+        launch_setup_load(g, ix_load, iz_max, -1.0 / (double)count, c->mask0, c->b, c->st);
+    }
+    CHECK(launch_check("model set-up"));
+    CHECK(build_levels(c));
+    launch_filter_diag(g, c->solid, c->kf, c->fdiag, c->st);
+    CHECK(launch_check("filter set-up"));
+    return sync(c);
+}
+
+// ------------------------------------------------------------------ lazily built layout maps
+// Morton order of the solid elements (fea.cpp:289-317): octree walk visiting children in key order
+// (x bit most significant, then y, then z), emitting grid cell indices.
+static void morton_walk(const Context* c, int x0, int y0, int z0, int h, std::vector<int32_t>& out) {
+    const Cuboid& q = c->cub;
+    if (x0 >= q.nelx || y0 >= q.nely || z0 >= q.nelz) return;
+    if (h == 1) {
+        out.push_back((int32_t)c->g.cell(x0, c->g.ny - 1 - y0, z0));
+        return;
+    }
+    const int m = h / 2;
+    for (int k = 0; k < 8; ++k) morton_walk(c, x0 + ((k >> 2) & 1) * m, y0 + ((k >> 1) & 1) * m, z0 + (k & 1) * m, m, out);
+}
+
+static int ensure_morton(Context* c) {
+    if (c->morton) return T3D_OK;
+    int h = 1;
+    while (h < std::max(c->cub.nelx, std::max(c->cub.nely, c->cub.nelz))) h *= 2;
+    c->morton_h.clear();
+    c->morton_h.reserve(c->ne);
+    morton_walk(c, 0, 0, 0, h, c->morton_h);
+    CHECK(c->alloc(&c->morton, c->ne));
+    T3D_CUDA_OK(cudaMemcpy(c->morton, c->morton_h.data(), c->ne * sizeof(int32_t), cudaMemcpyHostToDevice));
+    return T3D_OK;
+}
+
+static int ensure_free(Context* c) {
+    if (c->free_d) return T3D_OK;
+    std::vector<uint8_t> m(c->g.NN);
+    T3D_CUDA_OK(cudaMemcpy(m.data(), c->mask0, c->g.NN, cudaMemcpyDeviceToHost));
+    c->free_h.clear();
+    for (int64_t n = 0; n < c->g.NN; ++n)
+        for (int k = 0; k < 3; ++k)
+            if (!((m[n] >> k) & 1)) c->free_h.push_back((int32_t)(3 * n + k));
+    CHECK(c->alloc(&c->free_d, c->free_h.size()));
+    T3D_CUDA_OK(cudaMemcpy(c->free_d, c->free_h.data(), c->free_h.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    return T3D_OK;
+}
+
+static int ensure_stage(Context* c) {
+    CHECK(ensure_free(c));
+    CHECK(ensure_morton(c));
+    const size_t need = std::max(c->free_h.size(), (size_t)c->ne);
+    if (c->stage_n >= need) return T3D_OK;
+    CHECK(c->alloc(&c->stage, need));
+    c->stage_n = need;
+    return T3D_OK;
+}
+
+// host free vector -> device grid vector (fixed DOFs zero)
+static int upload_free(Context* c, const double* h, double* grid) {
+    CHECK(ensure_stage(c));
+    const int64_t nf = (int64_t)c->free_h.size();
+    T3D_CUDA_OK(cudaMemsetAsync(grid, 0, 3 * c->g.NN * sizeof(double), c->st));
+    T3D_CUDA_OK(cudaMemcpyAsync(c->stage, h, nf * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    launch_scatter_free(nf, c->free_d, c->stage, c->g.NN, grid, c->st);
+    return launch_check("scatter_free");
+}
+static int download_free(Context* c, const double* grid, double* h) {
+    CHECK(ensure_stage(c));
+    const int64_t nf = (int64_t)c->free_h.size();
+    launch_gather_free(nf, c->free_d, grid, c->g.NN, c->stage, c->st);
+    CHECK(launch_check("gather_free"));
+    T3D_CUDA_OK(cudaMemcpyAsync(h, c->stage, nf * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    return sync(c);
+}
+static int upload_cells_f64(Context* c, const double* h, double* cells) {
+    CHECK(ensure_stage(c));
+    T3D_CUDA_OK(cudaMemsetAsync(cells, 0, c->g.NE * sizeof(double), c->st));
+    T3D_CUDA_OK(cudaMemcpyAsync(c->stage, h, c->ne * sizeof(double), cudaMemcpyHostToDevice, c->st));
+    launch_cells_from_morton_f64(c->ne, c->morton, c->stage, cells, c->st);
+    return launch_check("cells_from_morton");
+}
+static int download_cells_f64(Context* c, const double* cells, double* h) {
+    CHECK(ensure_stage(c));
+    launch_cells_to_morton_f64(c->ne, c->morton, cells, c->stage, c->st);
+    CHECK(launch_check("cells_to_morton"));
+    T3D_CUDA_OK(cudaMemcpyAsync(h, c->stage, c->ne * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    return sync(c);
+}
+static int upload_cells_f32(Context* c, const float* h, float* cells) {
+    CHECK(ensure_stage(c));
+    float* st = reinterpret_cast<float*>(c->stage);
+    T3D_CUDA_OK(cudaMemsetAsync(cells, 0, c->g.NE * sizeof(float), c->st));
+    T3D_CUDA_OK(cudaMemcpyAsync(st, h, c->ne * sizeof(float), cudaMemcpyHostToDevice, c->st));
+    launch_cells_from_morton_f32(c->ne, c->morton, st, cells, c->st);
+    return launch_check("cells_from_morton");
+}
+static int download_cells_f32(Context* c, const float* cells, float* h) {
+    CHECK(ensure_stage(c));
+    float* st = reinterpret_cast<float*>(c->stage);
+    launch_cells_to_morton_f32(c->ne, c->morton, cells, st, c->st);
+    CHECK(launch_check("cells_to_morton"));
+    T3D_CUDA_OK(cudaMemcpyAsync(h, st, c->ne * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+    return sync(c);
+}
+
+// ------------------------------------------------------------------ multigrid
+// make_diagonal_preconditioner_from_static for the moduli in c->E (preconditioner.cpp:38-79)
+static int mg_setup(Context* c) {
+    launch_diag0(c->g, c->Ke, c->E, c->mask0, c->lv[0].diag, c->st);
+    for (int l = 0; l + 1 < c->nlev; ++l) launch_diag_coarsen(c->lv[l + 1], c->lv[l], c->st);
+    if (c->Nc) {
+        const MgLevel& Lc = c->lv[c->nlev - 1];
+        launch_coarse_element_matrices(c->g, Lc, c->mask0, c->E, c->Ke, (double)c->prm.Emin, c->Kce, c->st);
+        launch_coarse_assemble(Lc, c->Kce, c->Kc, c->st);
+        launch_cholesky(c->Kc, c->LT, c->Lrow, c->Nc, c->chol_status, c->st);
+    }
+    c->mg_ready = true;
+    return launch_check("mg set-up");
+}
+
+// z = M r for grid vectors; with S, r.z goes to S (rz / beta)
+static void vcycle(Context* c, const double* r, double* z, PcgScalars* S, RedSlot dot) {
+    const int L = c->nlev;
+    for (int l = 0; l + 1 < L; ++l)
+        launch_restrict(c->lv[l + 1], c->lv[l], l == 0 ? r : c->lv[l].r, c->lv[l + 1].r, S, c->st);
+    launch_coarse_solve(c->lv[L - 1], c->Lrow, c->LT, c->Nc, c->chol_status, S, c->st);
+    for (int l = L - 2; l >= 1; --l)
+        launch_prolong_smooth(c->lv[l + 1], c->lv[l], c->lv[l + 1].x, c->lv[l].r, c->lv[l].x,
+                              (double)c->prm.mg_weight, S, c->st);
+    launch_prolong_smooth0(c->lv[1], c->lv[0], c->lv[1].x, r, z, (double)c->prm.mg_weight, dot, S, c->st);
+}
+
+// ------------------------------------------------------------------ PCG (solver.cpp:87-217)
+static void pcg_iteration(Context* c) {
+    launch_matvec64(c->g, c->Ke, c->E, c->mask0, c->p, c->Ap, c->slot[0], c->S, c->st);
+    launch_pcg_update(c->g, c->u, c->r, c->p, c->Ap, c->slot[1], c->S, c->st);
+    vcycle(c, c->r, c->z, c->S, c->slot[2]);
+    launch_pcg_direction(c->g, c->z, c->p, c->S, c->st);
+}
+
+static constexpr int PCG_CHUNK = 16;
+
+static int ensure_pcg_graph(Context* c) {
+    if (!c->use_graph || c->pcg_graph) return T3D_OK;
+    cudaGraph_t graph;
+    T3D_CUDA_OK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < PCG_CHUNK; ++k) pcg_iteration(c);
+    T3D_CUDA_OK(cudaStreamEndCapture(c->st, &graph));
+    cudaError_t e = cudaGraphInstantiate(&c->pcg_graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return set_cuda_error(e, "cudaGraphInstantiate", __FILE__, __LINE__);
+    c->pcg_graph_len = PCG_CHUNK;
+    return T3D_OK;
+}
+
+// Solves K(E) u = b on device-resident c->E, c->b, warm start c->u.  Returns the PCG_free
+// iteration count in *iters.
+static int pcg_solve(Context* c, double tol, int maxit, int* iters) {
+    if (!c->mg_ready) return set_error(T3D_ERR_INVALID, "multigrid preconditioner not set up");
+    CHECK(ensure_pcg_graph(c));
+    launch_matvec64(c->g, c->Ke, c->E, c->mask0, c->u, c->Ap, RedSlot{nullptr, nullptr}, nullptr, c->st);
+    launch_pcg_init(c->g, c->b, c->Ap, c->r, c->slot[1], c->S, tol, c->st);
+    vcycle(c, c->r, c->z, c->S, c->slot[2]);
+    launch_pcg_start(c->g, c->z, c->p, c->st);
+    CHECK(launch_check("pcg start"));
+    int queued = 0, chunk = 0;
+    bool done = false;
+    while (queued < maxit && !done) {
+        const int n = std::min(PCG_CHUNK, maxit - queued);
+        if (c->use_graph && n == PCG_CHUNK) {
+            T3D_CUDA_OK(cudaGraphLaunch(c->pcg_graph, c->st));
+        } else {
+            for (int k = 0; k < n; ++k) pcg_iteration(c);
+            CHECK(launch_check("pcg iteration"));
+        }
+        queued += n;
+        const int slot = chunk & 1;
+        T3D_CUDA_OK(cudaMemcpyAsync(&c->flag_h[slot], &c->S->done, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+        T3D_CUDA_OK(cudaEventRecord(c->ev[slot], c->st));
+        if (chunk >= 1) {   // poll the previous chunk while this one runs
+            T3D_CUDA_OK(cudaEventSynchronize(c->ev[slot ^ 1]));
+            done = c->flag_h[slot ^ 1] != 0;
+        }
+        ++chunk;
+    }
+    T3D_CUDA_OK(cudaMemcpyAsync(c->S_h, c->S, sizeof(PcgScalars), cudaMemcpyDeviceToHost, c->st));
+    CHECK(sync(c));
+    *iters = c->S_h->done ? c->S_h->result : maxit;
+    return T3D_OK;
+}
+
+// ------------------------------------------------------------------ PDE filter (filter.cpp:175-275)
+static int filter_apply(Context* c, const float* src_cells, float* dst_cells) {
+    const Grid& g = c->g;
+    launch_filter_rhs(g, c->solid, src_cells, c->frhs, c->st);
+    launch_filter_norms(g, c->frhs, c->flastrhs, c->slot[0], c->slot[1], c->FS, c->st);
+    launch_filter_x0(g, c->flastx, c->fx, c->FS, c->st);
+    launch_filter_matvec(g, c->solid, c->kf, c->fx, c->fAp, RedSlot{nullptr, nullptr}, c->FS, c->st);
+    launch_filter_r0(g, c->frhs, c->fAp, c->fdiag, c->fr, c->fz, c->fp, c->slot[0], c->slot[1], c->FS, c->st);
+    CHECK(launch_check("filter start"));
+    for (int it = 0; it < 80; it += 8) {
+        for (int k = 0; k < 8 && it + k < 80; ++k) {
+            launch_filter_matvec(g, c->solid, c->kf, c->fp, c->fAp, c->slot[2], c->FS, c->st);
+            launch_filter_update(g, c->fx, c->fr, c->fp, c->fAp, c->slot[3], c->FS, c->st);
+            launch_filter_precond(g, c->fr, c->fdiag, c->fz, c->slot[0], c->FS, c->st);
+            launch_filter_direction(g, c->fz, c->fp, c->FS, c->st);
+        }
+        CHECK(launch_check("filter iteration"));
+        T3D_CUDA_OK(cudaMemcpyAsync(c->flag_h, &c->FS->done, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+        CHECK(sync(c));
+        if (c->flag_h[0]) break;
+    }
+    launch_filter_to_cells(g, c->solid, c->fx, dst_cells, c->st);
+    T3D_CUDA_OK(cudaMemcpyAsync(c->flastx, c->fx, g.NN * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+    T3D_CUDA_OK(cudaMemcpyAsync(c->flastrhs, c->frhs, g.NN * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+    return launch_check("filter finish");
+}
+
+// ------------------------------------------------------------------ OC (driver.cpp:170-189)
+static constexpr int OC_MAX_PASSES = 400;
+
+static int oc_update(Context* c, float V0) {
+    const int fp64 = c->prm.oc_sum_order == T3D_SUM_FP64;
+    if (!fp64) CHECK(ensure_morton(c));
+    launch_oc_init(c->OC, c->st);
+    int passes = 0;
+    for (;;) {
+        for (int k = 0; k < 16; ++k) {
+            launch_oc_pass(c->g, c->solid, c->x, c->dc, c->xnew, c->OC, fp64, V0, c->ne, c->slot[0], c->st);
+            if (!fp64) launch_oc_vec8_vol(c->ne, c->morton, c->xnew, c->OC, V0, c->st);
+        }
+        CHECK(launch_check("oc pass"));
+        passes += 16;
+        T3D_CUDA_OK(cudaMemcpyAsync(c->flag_h, &c->OC->done, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+        CHECK(sync(c));
+        if (c->flag_h[0]) break;
+        if (passes >= OC_MAX_PASSES) return set_error(T3D_ERR_NUMERIC, "OC bisection did not terminate");
+    }
+    launch_oc_finish(c->g, c->solid, c->x, c->xnew, c->OC, fp64, c->ne, c->slot[0], c->slot[1], c->st);
+    if (!fp64) launch_oc_vec8_stats(c->ne, c->morton, c->x, c->OC, c->st);
+    CHECK(launch_check("oc finish"));
+    T3D_CUDA_OK(cudaMemcpyAsync(c->OC_h, c->OC, sizeof(OcState), cudaMemcpyDeviceToHost, c->st));
+    return sync(c);
+}
+
+// ------------------------------------------------------------------ design loop (driver.cpp:60-216)
+static int fill_cells(Context* c, float v) {
+    std::vector<float> h((size_t)c->ne, v);
+    return upload_cells_f32(c, h.data(), c->x);
+}
+
+static int design_init(Context* c, float V0, double* Csolid) {
+    CHECK(ensure_morton(c));
+    c->V0 = V0;
+    c->loop = 0;
+    CHECK(fill_cells(c, V0));
+    {   // eleMod = E0 for every element for the solid reference solve (driver.cpp:67, 85-103)
+        std::vector<double> e((size_t)c->ne, (double)c->prm.E0);
+        CHECK(upload_cells_f64(c, e.data(), c->E));
+    }
+    T3D_CUDA_OK(cudaMemsetAsync(c->u, 0, 3 * c->g.NN * sizeof(double), c->st));
+    T3D_CUDA_OK(cudaMemsetAsync(c->flastx, 0, c->g.NN * sizeof(double), c->st));
+    T3D_CUDA_OK(cudaMemsetAsync(c->flastrhs, 0, c->g.NN * sizeof(double), c->st));
+    CHECK(mg_setup(c));
+    int its = 0;
+    CHECK(pcg_solve(c, (double)c->prm.cg_tol, c->prm.cg_max_it, &its));
+    launch_compliance64(c->g, c->Ke, c->E, c->u, c->ce, c->slot[0], c->scal + 1, c->st);
+    CHECK(launch_check("solid compliance"));
+    T3D_CUDA_OK(cudaMemcpyAsync(c->scal_h, c->scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CHECK(sync(c));
+    if (Csolid) *Csolid = c->scal_h[1];
+    c->design_ready = true;
+    return T3D_OK;
+}
+
+static int design_step(Context* c, t3d_iter_record* rec) {
+    if (!c->design_ready) return set_error(T3D_ERR_INVALID, "t3d_design_init not called");
+    const Grid& g = c->g;
+    const t3d_params& P = c->prm;
+    ++c->loop;
+    cudaEvent_t e0 = c->ev[2], e1 = c->ev[3], e2 = c->ev[4], e3 = c->ev[5], e4 = c->ev[6];
+    T3D_CUDA_OK(cudaEventRecord(e0, c->st));
+    launch_simp(g, c->solid, c->x, P.E0, P.Emin, P.penal, c->E, c->st);
+    if (c->loop == 1 || c->loop % 5 == 0) CHECK(mg_setup(c));
+    int its = 0;
+    CHECK(pcg_solve(c, (double)P.cg_tol, P.cg_max_it, &its));
+    T3D_CUDA_OK(cudaEventRecord(e1, c->st));
+    launch_compliance64(g, c->Ke, c->E, c->u, c->ce, c->slot[0], c->scal + 0, c->st);
+    launch_objective(g, c->E, c->ce, c->scal + 1, c->slot[1], c->scal + 2, c->st);
+    launch_sens(g, c->solid, c->x, c->ce, c->scal + 1, P.E0, P.Emin, P.penal, c->dc, c->xdc, c->st);
+    CHECK(launch_check("sensitivities"));
+    T3D_CUDA_OK(cudaEventRecord(e2, c->st));
+    CHECK(filter_apply(c, c->xdc, c->dcf));
+    T3D_CUDA_OK(cudaEventRecord(e3, c->st));
+    launch_dc_scale(g, c->solid, c->dcf, c->x, c->dc, c->st);
+    CHECK(oc_update(c, c->V0));
+    T3D_CUDA_OK(cudaEventRecord(e4, c->st));
+    T3D_CUDA_OK(cudaMemcpyAsync(c->scal_h, c->scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CHECK(sync(c));
+    if (rec) {
+        float tcg = 0, topt1 = 0, tf = 0, topt2 = 0;
+        cudaEventElapsedTime(&tcg, e0, e1);
+        cudaEventElapsedTime(&topt1, e1, e2);
+        cudaEventElapsedTime(&tf, e2, e3);
+        cudaEventElapsedTime(&topt2, e3, e4);
+        rec->loop = c->loop;
+        rec->pcg_iters = its;
+        rec->obj = c->scal_h[2];
+        rec->vol = c->OC_h->volfrac;
+        rec->sharp = c->OC_h->sharp;
+        rec->cons = c->OC_h->volfrac - c->V0;
+        rec->change = c->OC_h->change;
+        rec->lmid = c->OC_h->lmid;
+        rec->bisections = c->OC_h->passes;
+        rec->t_cg = tcg * 1e-3;
+        rec->t_filter = tf * 1e-3;
+        rec->t_opt = (topt1 + tf + topt2) * 1e-3;
+        rec->t_total = (tcg + topt1 + tf + topt2) * 1e-3;
+    }
+    return T3D_OK;
+}
+
+}  // namespace t3d
+
+// ====================================================================== C-ABI
+struct t3d_context : public t3d::Context {};
+
+#define API_GUARD(ctx)                                                                  \
+    if (!(ctx)) return t3d::set_error(T3D_ERR_INVALID, "null context");                \
+    if (cudaSetDevice((ctx)->dev) != cudaSuccess) return t3d::set_error(T3D_ERR_CUDA, "cudaSetDevice failed")
+
+extern "C" {
+
+int t3d_params_default(t3d_params* p) {
+    if (!p) return t3d::set_error(T3D_ERR_INVALID, "null params");
+    std::memset(p, 0, sizeof *p);
+    p->E0 = 1.0f; p->Emin = 1.0e-6f; p->nu = 0.3f; p->penal = 3.0f;     // core.hpp:28-31
+    p->cg_tol = 1.0e-3f; p->cg_max_it = 800;                             // core.hpp:35-36
+    p->mg_nondyadic = 1; p->mg_max_levels = 5; p->mg_weight = 0.6f;      // driver.cpp:54
+    p->filter_rmin = std::sqrt(3.0f);                                    // top3d_cli.cpp:33
+    p->oc_sum_order = T3D_SUM_REFERENCE;
+    p->precision = T3D_FP64;
+    p->device = 0;
+    return T3D_OK;
+}
+
+const char* t3d_last_error(void) { return t3d::g_err.c_str(); }
+
+int t3d_create(int nely, int nelx, int nelz, const t3d_params* p, t3d_context** out) {
+    if (!out) return t3d::set_error(T3D_ERR_INVALID, "null output pointer");
+    *out = nullptr;
+    t3d_context* c = new (std::nothrow) t3d_context();
+    if (!c) return t3d::set_error(T3D_ERR_OOM, "host allocation failed");
+    int rc = t3d::create(nely, nelx, nelz, p, c);
+    if (rc != T3D_OK) {
+        delete c;
+        return rc;
+    }
+    *out = c;
+    return T3D_OK;
+}
+
+int t3d_destroy(t3d_context* ctx) {
+    if (!ctx) return T3D_OK;
+    cudaSetDevice(ctx->dev);
+    cudaStreamSynchronize(ctx->st);
+    delete ctx;
+    return T3D_OK;
+}
+
+int t3d_get_info(const t3d_context* ctx, t3d_info* info) {
+    if (!ctx || !info) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    std::memset(info, 0, sizeof *info);
+    info->res[0] = ctx->g.nx; info->res[1] = ctx->g.ny; info->res[2] = ctx->g.nz;
+    info->orig[0] = ctx->cub.nelx; info->orig[1] = ctx->cub.nely; info->orig[2] = ctx->cub.nelz;
+    info->num_elements = ctx->ne;
+    info->num_nodes = ctx->g.NN;
+    // free DOFs of the cantilever: nodes used by a solid element and not on the x=0 face
+    {
+        const int64_t ux = ctx->cub.nelx + 1, uy = ctx->cub.nely + 1, uz = ctx->cub.nelz + 1;
+        info->num_free = 3 * (ux - 1) * uy * uz;
+    }
+    info->num_levels = ctx->nlev;
+    for (int l = 0; l < ctx->nlev; ++l) {
+        info->levels[l][0] = ctx->lv[l].nx; info->levels[l][1] = ctx->lv[l].ny;
+        info->levels[l][2] = ctx->lv[l].nz; info->levels[l][3] = ctx->lv[l].span;
+    }
+    info->coarse_n = ctx->Nc;
+    int st = 0;
+    if (ctx->Nc && ctx->mg_ready) cudaMemcpy(&st, ctx->chol_status, sizeof(int), cudaMemcpyDeviceToHost);
+    info->coarse_cholesky_ok = st;
+    info->device_bytes = (int64_t)ctx->bytes;
+    return T3D_OK;
+}
+
+int t3d_get_ke(const t3d_context* ctx, double* ke) {
+    if (!ctx || !ke) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    std::memcpy(ke, ctx->Ke_h, sizeof ctx->Ke_h);
+    return T3D_OK;
+}
+
+int t3d_set_ke(t3d_context* ctx, const double* ke) {
+    API_GUARD(ctx);
+    if (!ke) return t3d::set_error(T3D_ERR_INVALID, "null Ke");
+    std::memcpy(ctx->Ke_h, ke, sizeof ctx->Ke_h);
+    T3D_CUDA_OK(cudaMemcpy(ctx->Ke, ctx->Ke_h, sizeof ctx->Ke_h, cudaMemcpyHostToDevice));
+    return T3D_OK;
+}
+
+int t3d_get_element_map(t3d_context* ctx, int32_t* out) {
+    API_GUARD(ctx);
+    if (!out) return t3d::set_error(T3D_ERR_INVALID, "null output");
+    CHECK(t3d::ensure_morton(ctx));
+    const t3d::Grid& g = ctx->g;
+    for (int64_t k = 0; k < ctx->ne; ++k) {   // grid cell -> reference full index ny*nx*ez + ny*ex + (ny-1-ey)
+        const int64_t ci = ctx->morton_h[k];
+        const int cx = (int)(ci % g.ex) - 1, cy = (int)((ci / g.ex) % g.ey) - 1, cz = (int)(ci / ((int64_t)g.ex * g.ey)) - 1;
+        out[k] = (int32_t)((int64_t)g.ny * g.nx * cz + (int64_t)g.ny * cx + cy);
+    }
+    return T3D_OK;
+}
+
+int t3d_get_free_dofs(t3d_context* ctx, int32_t* out) {
+    API_GUARD(ctx);
+    if (!out) return t3d::set_error(T3D_ERR_INVALID, "null output");
+    CHECK(t3d::ensure_free(ctx));
+    std::memcpy(out, ctx->free_h.data(), ctx->free_h.size() * sizeof(int32_t));
+    return T3D_OK;
+}
+
+int t3d_get_load(t3d_context* ctx, double* b) {
+    API_GUARD(ctx);
+    if (!b) return t3d::set_error(T3D_ERR_INVALID, "null output");
+    return t3d::download_free(ctx, ctx->b, b);
+}
+
+int t3d_matvec(t3d_context* ctx, const double* E, const double* u, double* y) {
+    API_GUARD(ctx);
+    if (!E || !u || !y) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    CHECK(t3d::upload_cells_f64(ctx, E, ctx->E));
+    CHECK(t3d::upload_free(ctx, u, ctx->p));
+    t3d::launch_matvec64(ctx->g, ctx->Ke, ctx->E, ctx->mask0, ctx->p, ctx->Ap, t3d::RedSlot{nullptr, nullptr},
+                         nullptr, ctx->st);
+    CHECK(t3d::launch_check("matvec"));
+    return t3d::download_free(ctx, ctx->Ap, y);
+}
+
+int t3d_mg_setup(t3d_context* ctx, const double* E) {
+    API_GUARD(ctx);
+    if (!E) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    CHECK(t3d::upload_cells_f64(ctx, E, ctx->E));
+    CHECK(t3d::mg_setup(ctx));
+    return t3d::sync(ctx);
+}
+
+int t3d_vcycle(t3d_context* ctx, const double* r, double* z) {
+    API_GUARD(ctx);
+    if (!r || !z) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    if (!ctx->mg_ready) return t3d::set_error(T3D_ERR_INVALID, "t3d_mg_setup not called");
+    CHECK(t3d::upload_free(ctx, r, ctx->r));
+    T3D_CUDA_OK(cudaMemsetAsync(ctx->S, 0, sizeof(t3d::PcgScalars), ctx->st));
+    t3d::vcycle(ctx, ctx->r, ctx->z, ctx->S, ctx->slot[2]);
+    CHECK(t3d::launch_check("vcycle"));
+    return t3d::download_free(ctx, ctx->z, z);
+}
+
+int t3d_pcg(t3d_context* ctx, const double* E, const double* b, double* x, double tol, int max_it, int* iters) {
+    API_GUARD(ctx);
+    if (!E || !b || !x || max_it < 0) return t3d::set_error(T3D_ERR_INVALID, "bad argument");
+    if (!ctx->mg_ready) return t3d::set_error(T3D_ERR_INVALID, "t3d_mg_setup not called");
+    // the preconditioner keeps the moduli it was built with; the operator uses E
+    CHECK(t3d::upload_cells_f64(ctx, E, ctx->E));
+    CHECK(t3d::upload_free(ctx, b, ctx->b));
+    CHECK(t3d::upload_free(ctx, x, ctx->u));
+    int its = 0;
+    CHECK(t3d::pcg_solve(ctx, tol, max_it, &its));
+    if (iters) *iters = its;
+    CHECK(t3d::download_free(ctx, ctx->u, x));
+    // restore the cantilever load for later design iterations
+    T3D_CUDA_OK(cudaMemsetAsync(ctx->b, 0, 3 * ctx->g.NN * sizeof(double), ctx->st));
+    {
+        const int ix_load = std::min(ctx->cub.nelx, ctx->g.nnx - 1);
+        const int iz_max = std::max(1, ctx->g.nz / 6);
+        t3d::launch_setup_load(ctx->g, ix_load, iz_max, -1.0 / (double)((iz_max + 1) * ctx->g.nny), ctx->mask0,
+                               ctx->b, ctx->st);
+    }
+    return t3d::sync(ctx);
+}
+
+int t3d_compliance(t3d_context* ctx, const double* E, const double* u, double* ce, double* C) {
+    API_GUARD(ctx);
+    if (!E || !u) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    CHECK(t3d::upload_cells_f64(ctx, E, ctx->E));
+    CHECK(t3d::upload_free(ctx, u, ctx->u));
+    t3d::launch_compliance64(ctx->g, ctx->Ke, ctx->E, ctx->u, ctx->ce, ctx->slot[0], ctx->scal + 3, ctx->st);
+    CHECK(t3d::launch_check("compliance"));
+    if (ce) CHECK(t3d::download_cells_f64(ctx, ctx->ce, ce));
+    T3D_CUDA_OK(cudaMemcpyAsync(ctx->scal_h, ctx->scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+    CHECK(t3d::sync(ctx));
+    if (C) *C = ctx->scal_h[3];
+    return T3D_OK;
+}
+
+int t3d_mg_get_diag(t3d_context* ctx, int level, double* out) {
+    API_GUARD(ctx);
+    if (!out || level < 0 || level >= ctx->nlev) return t3d::set_error(T3D_ERR_INVALID, "bad level");
+    const t3d::MgLevel& L = ctx->lv[level];
+    std::vector<double> soa(3 * L.nn);
+    T3D_CUDA_OK(cudaMemcpy(soa.data(), L.diag, soa.size() * sizeof(double), cudaMemcpyDeviceToHost));
+    for (int64_t n = 0; n < L.nn; ++n)
+        for (int c = 0; c < 3; ++c) out[3 * n + c] = soa[c * L.nn + n];
+    return T3D_OK;
+}
+
+int t3d_mg_get_mask(t3d_context* ctx, int level, uint8_t* out) {
+    API_GUARD(ctx);
+    if (!out || level < 0 || level >= ctx->nlev) return t3d::set_error(T3D_ERR_INVALID, "bad level");
+    const t3d::MgLevel& L = ctx->lv[level];
+    std::vector<uint8_t> m(L.nn);
+    T3D_CUDA_OK(cudaMemcpy(m.data(), L.mask, L.nn, cudaMemcpyDeviceToHost));
+    for (int64_t n = 0; n < L.nn; ++n)
+        for (int c = 0; c < 3; ++c) out[3 * n + c] = (m[n] >> c) & 1;
+    return T3D_OK;
+}
+
+int t3d_mg_coarse_matrix(t3d_context* ctx, const double* E, double* Kc) {
+    API_GUARD(ctx);
+    if (!E || !Kc) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    if (!ctx->Nc) return t3d::set_error(T3D_ERR_UNSUPPORTED, "coarsest level uses the Jacobi fallback");
+    CHECK(t3d::upload_cells_f64(ctx, E, ctx->E));
+    CHECK(t3d::mg_setup(ctx));
+    T3D_CUDA_OK(cudaMemcpyAsync(Kc, ctx->Kc, (size_t)ctx->Nc * ctx->Nc * sizeof(double), cudaMemcpyDeviceToHost,
+                                ctx->st));
+    return t3d::sync(ctx);
+}
+
+int t3d_filter_apply(t3d_context* ctx, const float* src, float* dst) {
+    API_GUARD(ctx);
+    if (!src || !dst) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    CHECK(t3d::upload_cells_f32(ctx, src, ctx->xdc));
+    CHECK(t3d::filter_apply(ctx, ctx->xdc, ctx->dcf));
+    return t3d::download_cells_f32(ctx, ctx->dcf, dst);
+}
+
+int t3d_filter_get_state(t3d_context* ctx, double* last_x, double* last_rhs, double* diag) {
+    API_GUARD(ctx);
+    const size_t nb = ctx->g.NN * sizeof(double);
+    if (last_x) T3D_CUDA_OK(cudaMemcpy(last_x, ctx->flastx, nb, cudaMemcpyDeviceToHost));
+    if (last_rhs) T3D_CUDA_OK(cudaMemcpy(last_rhs, ctx->flastrhs, nb, cudaMemcpyDeviceToHost));
+    if (diag) T3D_CUDA_OK(cudaMemcpy(diag, ctx->fdiag, nb, cudaMemcpyDeviceToHost));
+    return T3D_OK;
+}
+
+int t3d_filter_set_state(t3d_context* ctx, const double* last_x, const double* last_rhs) {
+    API_GUARD(ctx);
+    if (!last_x || !last_rhs) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    const size_t nb = ctx->g.NN * sizeof(double);
+    T3D_CUDA_OK(cudaMemcpy(ctx->flastx, last_x, nb, cudaMemcpyHostToDevice));
+    T3D_CUDA_OK(cudaMemcpy(ctx->flastrhs, last_rhs, nb, cudaMemcpyHostToDevice));
+    return T3D_OK;
+}
+
+int t3d_simp(t3d_context* ctx, const float* xphys, double* E) {
+    API_GUARD(ctx);
+    if (!xphys || !E) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    CHECK(t3d::upload_cells_f32(ctx, xphys, ctx->x));
+    t3d::launch_simp(ctx->g, ctx->solid, ctx->x, ctx->prm.E0, ctx->prm.Emin, ctx->prm.penal, ctx->E, ctx->st);
+    CHECK(t3d::launch_check("simp"));
+    return t3d::download_cells_f64(ctx, ctx->E, E);
+}
+
+int t3d_sensitivity(t3d_context* ctx, const float* xphys, const double* ce, double c_solid, float* dc) {
+    API_GUARD(ctx);
+    if (!xphys || !ce || !dc) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    CHECK(t3d::upload_cells_f32(ctx, xphys, ctx->x));
+    CHECK(t3d::upload_cells_f64(ctx, ce, ctx->ce));
+    T3D_CUDA_OK(cudaMemcpy(ctx->scal + 4, &c_solid, sizeof(double), cudaMemcpyHostToDevice));
+    t3d::launch_sens(ctx->g, ctx->solid, ctx->x, ctx->ce, ctx->scal + 4, ctx->prm.E0, ctx->prm.Emin, ctx->prm.penal,
+                     ctx->dc, ctx->xdc, ctx->st);
+    CHECK(t3d::launch_check("sensitivity"));
+    return t3d::download_cells_f32(ctx, ctx->dc, dc);
+}
+
+int t3d_dc_scale(t3d_context* ctx, const float* dcf, const float* x, float* dc) {
+    API_GUARD(ctx);
+    if (!dcf || !x || !dc) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    CHECK(t3d::upload_cells_f32(ctx, dcf, ctx->dcf));
+    CHECK(t3d::upload_cells_f32(ctx, x, ctx->x));
+    t3d::launch_dc_scale(ctx->g, ctx->solid, ctx->dcf, ctx->x, ctx->dc, ctx->st);
+    CHECK(t3d::launch_check("dc_scale"));
+    return t3d::download_cells_f32(ctx, ctx->dc, dc);
+}
+
+int t3d_oc_update(t3d_context* ctx, const float* x, const float* dc, float V0, float* xnew, float* change,
+                  float* lmid, int* bis) {
+    API_GUARD(ctx);
+    if (!x || !dc || !xnew) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    CHECK(t3d::upload_cells_f32(ctx, x, ctx->x));
+    CHECK(t3d::upload_cells_f32(ctx, dc, ctx->dc));
+    CHECK(t3d::oc_update(ctx, V0));
+    if (change) *change = ctx->OC_h->change;
+    if (lmid) *lmid = ctx->OC_h->lmid;
+    if (bis) *bis = ctx->OC_h->passes;
+    return t3d::download_cells_f32(ctx, ctx->x, xnew);
+}
+
+int t3d_design_init(t3d_context* ctx, float V0, double* c_solid) {
+    API_GUARD(ctx);
+    return t3d::design_init(ctx, V0, c_solid);
+}
+
+int t3d_design_step(t3d_context* ctx, t3d_iter_record* rec) {
+    API_GUARD(ctx);
+    return t3d::design_step(ctx, rec);
+}
+
+int t3d_design_step_host(t3d_context* ctx, const float* x_in, float* x_out, t3d_iter_record* rec) {
+    API_GUARD(ctx);
+    if (!x_in || !x_out) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    CHECK(t3d::upload_cells_f32(ctx, x_in, ctx->x));
+    CHECK(t3d::design_step(ctx, rec));
+    return t3d::download_cells_f32(ctx, ctx->x, x_out);
+}
+
+int t3d_get_density(t3d_context* ctx, float* x) {
+    API_GUARD(ctx);
+    if (!x) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    return t3d::download_cells_f32(ctx, ctx->x, x);
+}
+
+int t3d_set_density(t3d_context* ctx, const float* x) {
+    API_GUARD(ctx);
+    if (!x) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    CHECK(t3d::upload_cells_f32(ctx, x, ctx->x));
+    return t3d::sync(ctx);
+}
+
+int t3d_run_global(t3d_context* ctx, float V0, int n_loop, double* c_solid, t3d_iter_record* records, int* n_records,
+                   float* x_final) {
+    API_GUARD(ctx);
+    CHECK(t3d::design_init(ctx, V0, c_solid));
+    float change = 1.0f, sharp = 1.0f;
+    int n = 0;
+    while (n < n_loop && change > 1e-4 && sharp > 0.01) {   // driver.cpp:112
+        t3d_iter_record rec;
+        CHECK(t3d::design_step(ctx, &rec));
+        change = rec.change;
+        sharp = rec.sharp;
+        if (records) records[n] = rec;
+        ++n;
+    }
+    if (n_records) *n_records = n;
+    if (x_final) CHECK(t3d::download_cells_f32(ctx, ctx->x, x_final));
+    return T3D_OK;
+}
+
+int t3d_synchronize(t3d_context* ctx) {
+    API_GUARD(ctx);
+    return t3d::sync(ctx);
+}
+
+}  // extern "C"

@@ -1,0 +1,128 @@
+// Host-side launchers of the B200 kernels.  All launches go to the given stream; none allocates.
+#pragma once
+#include "t3d_common.cuh"
+
+namespace t3d {
+
+struct Cuboid {          // solid region of the padded grid (fea.cpp:204-215)
+    int nelx, nely, nelz;
+};
+
+int set_cuda_error(cudaError_t e, const char* what, const char* file, int line);
+
+struct MgLevel {         // one structured multigrid level (hierarchy.cpp:45-81)
+    int nx, ny, nz, span;
+    int64_t nn;          // nodes
+    double* r;           // 3 SoA planes (level 0: not used, the PCG vectors are passed directly)
+    double* x;
+    double* diag;        // 3 SoA planes
+    uint8_t* mask;       // per node, bit c = fixed
+};
+
+// ---- model set-up (fea.cpp:181-447)
+void launch_setup_cells(const Grid& g, Cuboid c, uint8_t* solid, cudaStream_t s);
+void launch_setup_mask0(const Grid& g, const uint8_t* solid, uint8_t* mask, cudaStream_t s);
+void launch_setup_load(const Grid& g, int ix_load, int iz_max, double fz, const uint8_t* mask, double* b,
+                       cudaStream_t s);
+
+// ---- FEA operators
+void launch_matvec64(const Grid& g, const double* Ke, const double* E, const uint8_t* mask, const double* u,
+                     double* y, RedSlot dot, PcgScalars* S, cudaStream_t s);
+void launch_compliance64(const Grid& g, const double* Ke, const double* E, const double* u, double* ce,
+                         RedSlot red, double* C, cudaStream_t s);
+void launch_simp(const Grid& g, const uint8_t* solid, const float* x, float E0, float Emin, float penal, double* E,
+                 cudaStream_t s);
+void launch_sens(const Grid& g, const uint8_t* solid, const float* x, const double* ce, const double* Csolid,
+                 float E0, float Emin, float penal, float* dc, float* xdc, cudaStream_t s);
+void launch_objective(const Grid& g, const double* E, const double* ce, const double* Csolid, RedSlot red,
+                      double* obj, cudaStream_t s);
+
+// ---- multigrid (hierarchy.cpp, masks.cpp, diagonal.cpp, transfers.cpp, coarsest.cpp, preconditioner.cpp)
+void launch_diag0(const Grid& g, const double* Ke, const double* E, const uint8_t* mask, double* diag,
+                  cudaStream_t s);
+void launch_mask_restrict(const MgLevel& Lc, const MgLevel& Lf, cudaStream_t s);
+void launch_diag_coarsen(const MgLevel& Lc, const MgLevel& Lf, cudaStream_t s);
+void launch_restrict(const MgLevel& Lc, const MgLevel& Lf, const double* rf, double* rc, const PcgScalars* S,
+                     cudaStream_t s);
+void launch_coarse_jacobi(const MgLevel& L, const PcgScalars* S, cudaStream_t s);
+void launch_prolong_smooth(const MgLevel& Lc, const MgLevel& Lf, const double* xc, const double* rf, double* xf,
+                           double weight, const PcgScalars* S, cudaStream_t s);
+void launch_prolong_smooth0(const MgLevel& Lc, const MgLevel& Lf, const double* xc, const double* r, double* z,
+                            double weight, RedSlot dot, PcgScalars* S, cudaStream_t s);
+// coarsest dense Galerkin matrix, Cholesky factor and triangular solves (coarsest.cpp, preconditioner.cpp:47-78)
+void launch_coarse_element_matrices(const Grid& g0, const MgLevel& Lc, const uint8_t* mask0, const double* E,
+                                    const double* Ke, double emin, double* Kce, cudaStream_t s);
+void launch_coarse_assemble(const MgLevel& Lc, const double* Kce, double* Kc, cudaStream_t s);
+void launch_cholesky(const double* A, double* LT, double* Lrow, int N, int* status, cudaStream_t s);
+// Cholesky solve when *status == 1, else the Jacobi fallback (preconditioner.cpp:76-77, 195-215)
+void launch_coarse_solve(const MgLevel& L, const double* Lrow, const double* LT, int N, const int* status,
+                         const PcgScalars* S, cudaStream_t s);
+
+// ---- PCG vector steps (solver.cpp:87-217)
+void launch_pcg_init(const Grid& g, const double* b, const double* Ax, double* r, RedSlot red, PcgScalars* S,
+                     double tol, cudaStream_t s);
+void launch_pcg_start(const Grid& g, const double* z, double* p, cudaStream_t s);
+void launch_pcg_update(const Grid& g, double* x, double* r, const double* p, const double* Ap, RedSlot red,
+                       PcgScalars* S, cudaStream_t s);
+void launch_pcg_direction(const Grid& g, const double* z, double* p, PcgScalars* S, cudaStream_t s);
+
+// ---- PDE filter (filter.cpp)
+struct FilterScalars {
+    double nr2, df2;          // |rhs|^2, |rhs - lastRhs|^2
+    double rz, den, beta;
+    int warm, done, it, pad;
+};
+// kf: 64 kernel entries followed by the 8 row sums (filter.cpp:53-70)
+void launch_filter_diag(const Grid& g, const uint8_t* solid, const double* kf, double* fdiag, cudaStream_t s);
+void launch_filter_rhs(const Grid& g, const uint8_t* solid, const float* src, double* rhs, cudaStream_t s);
+void launch_filter_norms(const Grid& g, const double* rhs, const double* lastrhs, RedSlot r1, RedSlot r2,
+                         FilterScalars* F, cudaStream_t s);
+void launch_filter_x0(const Grid& g, const double* lastx, double* x, const FilterScalars* F, cudaStream_t s);
+void launch_filter_matvec(const Grid& g, const uint8_t* solid, const double* kf, const double* x, double* y,
+                          RedSlot dot, FilterScalars* F, cudaStream_t s);
+void launch_filter_r0(const Grid& g, const double* rhs, const double* Ax, const double* fdiag, double* r, double* z,
+                      double* p, RedSlot r1, RedSlot r2, FilterScalars* F, cudaStream_t s);
+void launch_filter_update(const Grid& g, double* x, double* r, const double* p, const double* Ap, RedSlot red,
+                          FilterScalars* F, cudaStream_t s);
+void launch_filter_precond(const Grid& g, const double* r, const double* fdiag, double* z, RedSlot red,
+                           FilterScalars* F, cudaStream_t s);
+void launch_filter_direction(const Grid& g, const double* z, double* p, const FilterScalars* F, cudaStream_t s);
+void launch_filter_to_cells(const Grid& g, const uint8_t* solid, const double* x, float* dst, cudaStream_t s);
+
+// ---- generic canonical reductions over node arrays (ncomp SoA planes of NN values)
+void launch_dot(const Grid& g, int ncomp, const double* a, const double* b, RedSlot red, double* out, cudaStream_t s);
+void launch_diffnorm(const Grid& g, const double* a, const double* b, RedSlot red, double* out_a2, double* out_d2,
+                     cudaStream_t s);
+
+// ---- layout conversion between the reference's layouts and the device grid
+void launch_scatter_free(int64_t nf, const int32_t* free_dofs, const double* vfree, int64_t NN, double* grid,
+                         cudaStream_t s);
+void launch_gather_free(int64_t nf, const int32_t* free_dofs, const double* grid, int64_t NN, double* vfree,
+                        cudaStream_t s);
+void launch_cells_from_morton_f64(int64_t ne, const int32_t* cell_of, const double* v, double* cells, cudaStream_t s);
+void launch_cells_to_morton_f64(int64_t ne, const int32_t* cell_of, const double* cells, double* v, cudaStream_t s);
+void launch_cells_from_morton_f32(int64_t ne, const int32_t* cell_of, const float* v, float* cells, cudaStream_t s);
+void launch_cells_to_morton_f32(int64_t ne, const int32_t* cell_of, const float* cells, float* v, cudaStream_t s);
+
+// ---- OC (driver.cpp:160-189)
+struct OcState {
+    float l1, l2, lmid, vol;
+    float change, sharp, volfrac, pad;
+    int passes, done, pad1, pad2;
+};
+void launch_dc_scale(const Grid& g, const uint8_t* solid, const float* dcf, const float* x, float* dc,
+                     cudaStream_t s);
+void launch_oc_init(OcState* st, cudaStream_t s);
+// one bisection pass: xnew for lmid; fp64_sum: canonical FP64 volume sum + l1/l2 update in the same kernel
+void launch_oc_pass(const Grid& g, const uint8_t* solid, const float* x, const float* dc, float* xnew, OcState* st,
+                    int fp64_sum, float V0, int64_t ne, RedSlot red, cudaStream_t s);
+// reference-order volume sum (8-lane vectorised std::accumulate over Morton order) + l1/l2 update
+void launch_oc_vec8_vol(int64_t ne, const int32_t* morton_cells, const float* xnew, OcState* st, float V0,
+                        cudaStream_t s);
+// change = max|xnew-x|, x = xnew; fp64_sum: sharpness and volume fraction by canonical FP64 sums
+void launch_oc_finish(const Grid& g, const uint8_t* solid, float* x, const float* xnew, OcState* st, int fp64_sum,
+                      int64_t ne, RedSlot r1, RedSlot r2, cudaStream_t s);
+// reference-order sharpness and volume fraction
+void launch_oc_vec8_stats(int64_t ne, const int32_t* morton_cells, const float* x, OcState* st, cudaStream_t s);
+
+}  // namespace t3d

@@ -1,0 +1,140 @@
+/* t3d_b200 -- C-ABI of the B200 (sm_100a) implementation of the per-design-iteration hot path of
+ * natashahirt/AlgorithmEngineering_AltProject (`top3d_xl_cli GLOBAL`): the matrix-free hex8
+ * K(rho)u product inside PCG, the geometric-multigrid V-cycle preconditioner, the PDE filter and
+ * the OC update.
+ *
+ * Conventions shared by every entry point:
+ *   - plain pointers to HOST memory, sizes as int64; no CUDA or C++ types cross the boundary;
+ *   - every call returns an int status (T3D_OK = 0); t3d_last_error() gives the message;
+ *   - element arrays use the reference's compact element order (64-bit Morton order of the
+ *     element indices, fea.cpp:289-317), length num_elements;
+ *   - free-DOF vectors use the reference's order (ascending global DOF 3*node+c over free DOFs,
+ *     fea.cpp:420-421), length num_free;
+ *   - node arrays use the reference's lexicographic nodes (fea.cpp:253-255), length num_nodes;
+ *   - all device state (moduli, displacement, MG hierarchy, filter warm start) lives in the
+ *     context; a context is bound to one GPU and is not thread-safe (like the reference's
+ *     Preconditioner closure and PDEFilter, preconditioner.cpp:82-88, filter.hpp:8-14).
+ * The library needs a CUDA device; there is no CPU fallback: without one t3d_create fails with
+ * T3D_ERR_NO_DEVICE.
+ */
+#ifndef T3D_B200_H
+#define T3D_B200_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    T3D_OK = 0,
+    T3D_ERR_INVALID = 1,       /* bad argument or call order */
+    T3D_ERR_CUDA = 2,          /* CUDA runtime error */
+    T3D_ERR_OOM = 3,           /* device allocation failed */
+    T3D_ERR_NO_DEVICE = 4,     /* no CUDA device / device index out of range */
+    T3D_ERR_UNSUPPORTED = 5,   /* configuration the library does not handle */
+    T3D_ERR_NUMERIC = 6        /* non-finite value or non-converging bisection */
+};
+
+enum { T3D_SUM_REFERENCE = 0, T3D_SUM_FP64 = 1 };   /* OC volume / sharpness summation order */
+enum { T3D_FP64 = 0, T3D_MIXED = 1 };              /* solver precision */
+
+typedef struct t3d_params {
+    float E0, Emin, nu, penal;    /* GlobalParams core.hpp:26-33 (Ke always uses nu = 0.3, fea.cpp:345) */
+    float cg_tol;                 /* core.hpp:35 */
+    int   cg_max_it;              /* core.hpp:36 */
+    int   mg_nondyadic;           /* MGPrecondConfig multigrid.hpp:9-13 as set in driver.cpp:54 */
+    int   mg_max_levels;
+    float mg_weight;
+    float filter_rmin;            /* top3d_cli.cpp:33: sqrt(3) cells */
+    int   oc_sum_order;           /* T3D_SUM_REFERENCE (bit-identical bisection) or T3D_SUM_FP64 */
+    int   precision;              /* T3D_FP64 */
+    int   device;                 /* CUDA device ordinal */
+    int   reserved[7];
+} t3d_params;
+
+typedef struct t3d_info {
+    int64_t res[3];               /* padded element counts resX,resY,resZ (padding.hpp:42-53) */
+    int64_t orig[3];              /* original nelx, nely, nelz */
+    int64_t num_elements;         /* solid elements */
+    int64_t num_nodes;
+    int64_t num_free;
+    int64_t num_levels;           /* multigrid levels (hierarchy.cpp:84-138) */
+    int64_t levels[8][4];         /* per level resX,resY,resZ,span */
+    int64_t coarse_n;             /* dense coarsest system size, 0 = Jacobi coarsest */
+    int64_t coarse_cholesky_ok;   /* 1 when the last MG set-up factorised the coarsest matrix */
+    int64_t device_bytes;         /* device memory held by the context */
+} t3d_info;
+
+typedef struct t3d_iter_record {  /* one design iteration (driver.cpp:205-216) */
+    int    loop;
+    int    pcg_iters;
+    double obj;                   /* Cdisp */
+    float  vol, sharp, cons, change;
+    float  lmid;
+    int    bisections;
+    double t_total, t_cg, t_opt, t_filter;  /* seconds, CUDA-event timed */
+} t3d_iter_record;
+
+/* --------------------------------------------------------------- lifecycle */
+int  t3d_params_default(t3d_params* p);
+/* CreateVoxelFEAmodel_Cuboid + ApplyBoundaryConditions + mg::build_static_once + SetupPDEFilter
+ * (fea.cpp:181-447, preconditioner.cpp:19-34, filter.cpp:9-75) for the built-in cantilever. */
+int  t3d_create(int nely, int nelx, int nelz, const t3d_params* p, struct t3d_context** out);
+int  t3d_destroy(struct t3d_context* ctx);
+int  t3d_get_info(const struct t3d_context* ctx, t3d_info* info);
+const char* t3d_last_error(void);
+
+/* --------------------------------------------------------------- model data (reference layouts) */
+int  t3d_get_ke(const struct t3d_context* ctx, double* ke576);            /* ComputeVoxelKe fea.cpp:117 */
+int  t3d_set_ke(struct t3d_context* ctx, const double* ke576);
+int  t3d_get_element_map(struct t3d_context* ctx, int32_t* ele_map_back); /* mesh.eleMapBack core.hpp:60 */
+int  t3d_get_free_dofs(struct t3d_context* ctx, int32_t* free_dofs);      /* Problem::freeDofIndex core.hpp:88 */
+int  t3d_get_load(struct t3d_context* ctx, double* b_free);               /* restrict_to_free(F) solver.cpp:12 */
+
+/* --------------------------------------------------------------- operators (host buffers) */
+/* K_times_u_finest (fea.hpp:42-45, fea.cpp:763-837) */
+int  t3d_matvec(struct t3d_context* ctx, const double* ele_E, const double* u_free, double* y_free);
+/* mg::make_diagonal_preconditioner_from_static (multigrid.hpp:66-68, preconditioner.cpp:38-79) */
+int  t3d_mg_setup(struct t3d_context* ctx, const double* ele_E);
+/* the preconditioner closure z = M^-1 r (preconditioner.cpp:88-265) */
+int  t3d_vcycle(struct t3d_context* ctx, const double* r_free, double* z_free);
+/* PCG_free (solver.hpp:24-27, solver.cpp:87-217) with the preconditioner of t3d_mg_setup;
+ * x_free is the warm start on entry and the solution on return */
+int  t3d_pcg(struct t3d_context* ctx, const double* ele_E, const double* b_free, double* x_free, double tol,
+             int max_it, int* iters);
+/* ComputeCompliance (fea.hpp:47, fea.cpp:851-864): ce per element, returns C */
+int  t3d_compliance(struct t3d_context* ctx, const double* ele_E, const double* u_free, double* ce, double* C);
+/* MG internals for inspection: per-level Jacobi diagonal / BC mask (interleaved 3n+c), coarsest matrix */
+int  t3d_mg_get_diag(struct t3d_context* ctx, int level, double* diag);
+int  t3d_mg_get_mask(struct t3d_context* ctx, int level, uint8_t* mask);
+int  t3d_mg_coarse_matrix(struct t3d_context* ctx, const double* ele_E, double* Kc);
+/* ApplyPDEFilter (filter.hpp:28, filter.cpp:175-275); warm-start state lives in the context */
+int  t3d_filter_apply(struct t3d_context* ctx, const float* src, float* dst);
+int  t3d_filter_get_state(struct t3d_context* ctx, double* last_x, double* last_rhs, double* diag_precond);
+int  t3d_filter_set_state(struct t3d_context* ctx, const double* last_x, const double* last_rhs);
+/* SIMP moduli (driver.cpp:117-121) and sensitivities (driver.cpp:151-157) */
+int  t3d_simp(struct t3d_context* ctx, const float* x_phys, double* ele_E);
+int  t3d_sensitivity(struct t3d_context* ctx, const float* x_phys, const double* ce, double c_solid, float* dc);
+/* dc_filt / max(1e-3, x) (driver.cpp:166) and the OC bisection (driver.cpp:170-184) */
+int  t3d_dc_scale(struct t3d_context* ctx, const float* dc_filt, const float* x, float* dc);
+int  t3d_oc_update(struct t3d_context* ctx, const float* x, const float* dc, float V0, float* x_new, float* change,
+                   float* lmid, int* bisections);
+
+/* --------------------------------------------------------------- device-resident design loop */
+/* x = V0, solid reference solve (driver.cpp:60-103); *c_solid = compliance of the solid domain */
+int  t3d_design_init(struct t3d_context* ctx, float V0, double* c_solid);
+/* one design iteration (driver.cpp:112-216) on device-resident state */
+int  t3d_design_step(struct t3d_context* ctx, t3d_iter_record* rec);
+/* the same iteration through host buffers: x_in -> device, step, device -> x_out (Morton order) */
+int  t3d_design_step_host(struct t3d_context* ctx, const float* x_in, float* x_out, t3d_iter_record* rec);
+int  t3d_get_density(struct t3d_context* ctx, float* x);
+int  t3d_set_density(struct t3d_context* ctx, const float* x);
+/* TOP3D_XL_GLOBAL (driver.hpp:4, driver.cpp:23-280) for one simulation: records[nLoop], x_final[num_elements] */
+int  t3d_run_global(struct t3d_context* ctx, float V0, int n_loop, double* c_solid, t3d_iter_record* records,
+                    int* n_records, float* x_final);
+int  t3d_synchronize(struct t3d_context* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -31,7 +31,7 @@ class OrcParams(C.Structure):
     _fields_ = [("E0", C.c_float), ("Emin", C.c_float), ("nu", C.c_float), ("penal", C.c_float),
                 ("cg_tol", C.c_float), ("cg_max_it", C.c_int), ("mg_nondyadic", C.c_int),
                 ("mg_max_levels", C.c_int), ("mg_weight", C.c_float), ("pow_mode", C.c_int),
-                ("vol_mode", C.c_int), ("approx_mode", C.c_int)]
+                ("vol_mode", C.c_int), ("approx_mode", C.c_int), ("red_mode", C.c_int)]
 
 
 class OrcIterRecord(C.Structure):
@@ -182,6 +182,8 @@ class Oracle(_Common):
             L.orc_pcg.restype = C.c_int
             L.orc_compliance.argtypes = [C.c_void_p, _f64p, _f64p, _f64p]
             L.orc_compliance.restype = C.c_double
+            L.orc_objective.argtypes = [C.c_void_p, _f64p, _f64p, C.c_double]
+            L.orc_objective.restype = C.c_double
             L.orc_filter_setup.argtypes = [C.c_void_p, C.c_float]
             L.orc_filter_apply.argtypes = [C.c_void_p, _f32p, _f32p]
             L.orc_filter_state.argtypes = [C.c_void_p, _f64p, _f64p, _f64p]
@@ -202,7 +204,7 @@ class Oracle(_Common):
             cls._lib = L
         return cls._lib
 
-    def __init__(self, nely, nelx, nelz, emin=None, max_levels=5, pow_mode=0, vol_mode=0, approx_mode=0,
+    def __init__(self, nely, nelx, nelz, emin=None, max_levels=5, pow_mode=0, vol_mode=0, approx_mode=0, red_mode=0,
                  penal=None):
         L = self.lib()
         p = OrcParams()
@@ -215,6 +217,7 @@ class Oracle(_Common):
         p.pow_mode = pow_mode
         p.vol_mode = vol_mode
         p.approx_mode = approx_mode
+        p.red_mode = red_mode
         self.params = p
         self.h = C.c_void_p(L.orc_create(nely, nelx, nelz, C.byref(p)))
         self._info = L.orc_info
@@ -259,6 +262,10 @@ class Oracle(_Common):
         n = self.lib().orc_oc(self.h, np.ascontiguousarray(x, np.float32), np.ascontiguousarray(dc, np.float32),
                               C.c_float(V0), xnew, C.byref(ch), C.byref(lm))
         return xnew, float(ch.value), float(lm.value), int(n)
+
+    def objective(self, E, ce, csolid):
+        return float(self.lib().orc_objective(self.h, np.ascontiguousarray(E, np.float64),
+                                              np.ascontiguousarray(ce, np.float64), C.c_double(csolid)))
 
     def dc_scale(self, dcf, x):
         dc = np.zeros(self.ne, dtype=np.float32)

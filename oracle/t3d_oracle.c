@@ -64,6 +64,10 @@ struct orc_problem {
     int filter_ready;
 };
 
+typedef double (*canon_step)(double part, int64_t item, const void* ctx);
+static double canon_fold(int64_t nitems, canon_step step, const void* ctx);
+static int32_t* cell_to_element(const orc_problem* P);
+
 static void* xcalloc(size_t n, size_t sz) {
     void* p = calloc(n ? n : 1, sz);
     if (!p) { fprintf(stderr, "oracle: out of memory\n"); abort(); }
@@ -76,7 +80,7 @@ void orc_params_default(orc_params* p) {
     p->E0 = 1.0f; p->Emin = 1.0e-6f; p->nu = 0.3f; p->penal = 3.0f;
     p->cg_tol = 1.0e-3f; p->cg_max_it = 800;
     p->mg_nondyadic = 1; p->mg_max_levels = 5; p->mg_weight = 0.6f;
-    p->pow_mode = 0; p->vol_mode = 0; p->approx_mode = 0;
+    p->pow_mode = 0; p->vol_mode = 0; p->approx_mode = 0; p->red_mode = 0;
 }
 
 /* ------------------------------------------------------------------ padding
@@ -276,6 +280,20 @@ void orc_matvec(orc_problem* P, const double* E, const double* u, double* y) {
 
 /* fea.cpp:587-677, 851-864: ce_e = ue' Ke ue (0 when E <= 1e-16), C = sum E ce.
  * u is a free vector; fixed DOFs read as 0 (scatter_from_free into zeroed U). */
+typedef struct { const int32_t* cell2e; const double* w; const double* v; double scale; } cell_sum_ctx;
+static double step_cell_wv(double part, int64_t k, const void* vctx) {   /* part + w*v over live cells */
+    const cell_sum_ctx* c = (const cell_sum_ctx*)vctx;
+    const int e = c->cell2e[k];
+    if (e < 0 || c->w[e] <= 1.0e-16) return part;
+    return part + c->w[e] * c->v[e];
+}
+static double step_cell_obj(double part, int64_t k, const void* vctx) {  /* part + E*(ce*rc) */
+    const cell_sum_ctx* c = (const cell_sum_ctx*)vctx;
+    const int e = c->cell2e[k];
+    if (e < 0 || c->w[e] == 0.0) return part;
+    return part + c->w[e] * (c->v[e] * c->scale);
+}
+
 double orc_compliance(orc_problem* P, const double* E, const double* u, double* ce) {
     double C = 0.0;
     for (int e = 0; e < P->ne; ++e) {
@@ -295,7 +313,27 @@ double orc_compliance(orc_problem* P, const double* E, const double* u, double* 
         ce[e] = s;
         C += E[e] * s;
     }
+    if (P->p.red_mode == 1) {
+        int32_t* m = cell_to_element(P);
+        cell_sum_ctx c = {m, E, ce, 1.0};
+        C = canon_fold((int64_t)P->nx * P->ny * P->nz, step_cell_wv, &c);
+        free(m);
+    }
     return C;
+}
+
+/* printed objective Cdisp (driver.cpp:144-150) */
+double orc_objective(const orc_problem* P, const double* E, const double* ce, double Csolid) {
+    if (P->p.red_mode == 1) {
+        int32_t* m = cell_to_element(P);
+        cell_sum_ctx c = {m, E, ce, 1.0 / Csolid};
+        const double s = canon_fold((int64_t)P->nx * P->ny * P->nz, step_cell_obj, &c);
+        free(m);
+        return Csolid > 0 ? s * Csolid : s;
+    }
+    double cobj = 0.0;
+    for (int e = 0; e < P->ne; ++e) cobj += E[e] * (ce[e] / Csolid);
+    return Csolid > 0 ? cobj * Csolid : cobj;
 }
 
 /* ------------------------------------------------------------------ multigrid hierarchy
@@ -704,6 +742,106 @@ static double dot(const double* a, const double* b, int64_t n) {
     return s;
 }
 
+/* ------------------------------------------------------------------ canonical reduction order
+ * Emulates the CUDA path's deterministic reductions: item i (a node or a cell) belongs to thread
+ * gid = i mod (RB*RT); each thread folds its items in increasing order into a partial starting at 0
+ * through `step`; the 32 partials of a warp are combined by an xor butterfly (offsets 16..1), the 8
+ * warp sums of a block by the same butterfly padded with zeros, and the RB block partials by a last
+ * pass where thread t sums partials t, t+RT, ... in order, followed by the two butterflies. */
+#define RB 1184
+#define RT 256
+
+static double butterfly32(double* v) {
+    double t[32];
+    for (int off = 16; off > 0; off >>= 1) {
+        for (int l = 0; l < 32; ++l) t[l] = v[l] + v[l ^ off];
+        memcpy(v, t, sizeof t);
+    }
+    return v[0];
+}
+
+static double fold_block(const double* lanes /* RT */) {
+    double w[8];
+    for (int k = 0; k < 8; ++k) {
+        double v[32];
+        memcpy(v, lanes + 32 * k, sizeof v);
+        w[k] = butterfly32(v);
+    }
+    double v[32];
+    for (int l = 0; l < 32; ++l) v[l] = l < 8 ? w[l] : 0.0;
+    return butterfly32(v);
+}
+
+static double canon_fold(int64_t nitems, canon_step step, const void* ctx) {
+    static double partial[RB];
+    double lanes[RT];
+    const int64_t stride = (int64_t)RB * RT;
+    for (int b = 0; b < RB; ++b) {
+        if ((int64_t)b * RT >= nitems) {   /* threads without items: the butterflies of +0 give +0 */
+            partial[b] = 0.0;
+            continue;
+        }
+        for (int t = 0; t < RT; ++t) {
+            double p = 0.0;
+            for (int64_t i = (int64_t)b * RT + t; i < nitems; i += stride) p = step(p, i, ctx);
+            lanes[t] = p;
+        }
+        partial[b] = fold_block(lanes);
+    }
+    for (int t = 0; t < RT; ++t) {
+        double s = 0.0;
+        for (int i = t; i < RB; i += RT) s = s + partial[i];
+        lanes[t] = s;
+    }
+    return fold_block(lanes);
+}
+
+/* node-item step: sum over the three DOFs of node i of a*b (free vectors; fixed DOFs read 0) */
+typedef struct { const orc_problem* P; const double* a; const double* b; } node_dot_ctx;
+static double step_node_dot(double part, int64_t n, const void* vctx) {
+    const node_dot_ctx* c = (const node_dot_ctx*)vctx;
+    for (int d = 0; d < 3; ++d) {
+        const int f = c->P->dof2free[3 * n + d];
+        const double av = f >= 0 ? c->a[f] : 0.0, bv = f >= 0 ? c->b[f] : 0.0;
+        part = part + av * bv;
+    }
+    return part;
+}
+
+/* inner product of two free-DOF vectors in the selected order */
+static double free_dot(const orc_problem* P, const double* a, const double* b) {
+    if (P->p.red_mode == 0) return dot(a, b, P->nf);
+    node_dot_ctx c = {P, a, b};
+    return canon_fold(P->nn, step_node_dot, &c);
+}
+
+/* inner product of two node vectors (filter) in the selected order */
+typedef struct { const double* a; const double* b; } vec_dot_ctx;
+static double step_vec_dot(double part, int64_t n, const void* vctx) {
+    const vec_dot_ctx* c = (const vec_dot_ctx*)vctx;
+    return part + c->a[n] * c->b[n];
+}
+static double node_dot(const orc_problem* P, const double* a, const double* b) {
+    if (P->p.red_mode == 0) return dot(a, b, P->nn);
+    vec_dot_ctx c = {a, b};
+    return canon_fold(P->nn, step_vec_dot, &c);
+}
+
+/* canonical cell order: k = (cz*ny + cy)*nx + cx over the padded grid; cell2e maps k to the
+   compact (Morton) element or -1 for a void cell */
+static int32_t* cell_to_element(const orc_problem* P) {
+    const int64_t ncell = (int64_t)P->nx * P->ny * P->nz;
+    int32_t* m = xcalloc((size_t)ncell, sizeof(int32_t));
+    for (int64_t k = 0; k < ncell; ++k) m[k] = -1;
+    for (int e = 0; e < P->ne; ++e) {
+        const int full = P->ele_full[e];   /* ny*nx*cz + ny*cx + cy */
+        const int cz = full / (P->nx * P->ny), rem = full % (P->nx * P->ny);
+        const int cx = rem / P->ny, cy = rem % P->ny;
+        m[((int64_t)cz * P->ny + cy) * P->nx + cx] = e;
+    }
+    return m;
+}
+
 /* PCG_free (solver.cpp:87-217) with the multigrid preconditioner built by orc_mg_build */
 int orc_pcg(orc_problem* P, const double* E, const double* b, double* x, double tol, int maxit) {
     const int64_t n = P->nf;
@@ -711,13 +849,13 @@ int orc_pcg(orc_problem* P, const double* E, const double* b, double* x, double 
     orc_matvec(P, E, x, Ap);
     for (int64_t i = 0; i < n; ++i) r[i] = b[i] - Ap[i];
     orc_vcycle(P, r, z);
-    double rz = dot(r, z, n);
+    double rz = free_dot(P, r, z);
     memcpy(p, z, (size_t)n * sizeof(double));
-    const double nb = sqrt(dot(b, b, n));
+    const double nb = sqrt(free_dot(P, b, b));
     const double stop = (nb > 1.0e-30 ? nb : 1.0e-30) * tol;
     for (int it = 0; it < maxit; ++it) {
         orc_matvec(P, E, p, Ap);
-        const double den = dot(p, Ap, n);
+        const double den = free_dot(P, p, Ap);
         const double alpha = rz / (den > 1.0e-30 ? den : 1.0e-30);
         double rn2 = 0.0;
         for (int64_t i = 0; i < n; ++i) {
@@ -725,9 +863,10 @@ int orc_pcg(orc_problem* P, const double* E, const double* b, double* x, double 
             r[i] -= alpha * Ap[i];
             rn2 += r[i] * r[i];
         }
+        if (P->p.red_mode == 1) rn2 = free_dot(P, r, r);
         if (sqrt(rn2) < stop) return it + 1;
         orc_vcycle(P, r, z);
-        const double rzn = dot(r, z, n);
+        const double rzn = free_dot(P, r, z);
         const double beta = rzn / (rz > 1.0e-30 ? rz : 1.0e-30);
         rz = rzn;
         for (int64_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
@@ -826,6 +965,13 @@ void orc_filter_apply(orc_problem* P, const float* src, float* dst) {
         nr += rhs[i] * rhs[i];
         df += d * d;
     }
+    if (P->p.red_mode == 1) {
+        double* dv = xcalloc((size_t)nn, sizeof(double));
+        for (int64_t i = 0; i < nn; ++i) dv[i] = rhs[i] - P->flastrhs[i];
+        nr = node_dot(P, rhs, rhs);
+        df = node_dot(P, dv, dv);
+        free(dv);
+    }
     nr = sqrt(nr);
     df = sqrt(df);
     const int warm = (nr > 0.0) && (df / (nr > 1.0e-30 ? nr : 1.0e-30) < 1000.0);
@@ -843,23 +989,25 @@ void orc_filter_apply(orc_problem* P, const float* src, float* dst) {
         z[i] = P->fdiag[i] * r[i];
         rz += r[i] * z[i];
     }
+    if (P->p.red_mode == 1) rz = node_dot(P, r, z);
     if (rz == 0) rz = 1.0;
     memcpy(p, z, (size_t)nn * sizeof(double));
-    const double rn0 = sqrt(dot(r, r, nn));
+    const double rn0 = sqrt(node_dot(P, r, r));
     if (!(rn0 < 1.0e-2)) {
         for (int it = 0; it < 80; ++it) {
             filter_matvec(P, p, Ap);
-            const double den = dot(p, Ap, nn);
+            const double den = node_dot(P, p, Ap);
             const double alpha = rz / (den > 1.0e-30 ? den : 1.0e-30);
             for (int64_t i = 0; i < nn; ++i) x[i] += alpha * p[i];
             for (int64_t i = 0; i < nn; ++i) r[i] -= alpha * Ap[i];
-            const double rn = sqrt(dot(r, r, nn));
+            const double rn = sqrt(node_dot(P, r, r));
             if (rn < 1e-3) break;
             double rzn = 0.0;
             for (int64_t i = 0; i < nn; ++i) {
                 z[i] = P->fdiag[i] * r[i];
                 rzn += r[i] * z[i];
             }
+            if (P->p.red_mode == 1) rzn = node_dot(P, r, z);
             const double beta = rzn / (rz > 1.0e-30 ? rz : 1.0e-30);
             for (int64_t i = 0; i < nn; ++i) p[i] = z[i] + beta * p[i];
             rz = rzn;
@@ -992,16 +1140,37 @@ static float seq_sum(const float* t, int n) {
     return s;
 }
 
+typedef struct { const int32_t* cell2e; const float* x; int sharp; } cell_f_ctx;
+static double step_cell_f(double part, int64_t k, const void* vctx) {
+    const cell_f_ctx* c = (const cell_f_ctx*)vctx;
+    const int e = c->cell2e[k];
+    if (e < 0) return part;
+    const float v = c->x[e];
+    return part + (double)(c->sharp ? v * (1.0f - v) : v);
+}
+/* FP64 sum of x (or x(1-x)) over the elements: canonical cell order when red_mode = 1 */
+static double fp64_sum(const orc_problem* P, const float* x, int sharp) {
+    if (P->p.red_mode == 1) {
+        int32_t* m = cell_to_element(P);
+        cell_f_ctx c = {m, x, sharp};
+        const double s = canon_fold((int64_t)P->nx * P->ny * P->nz, step_cell_f, &c);
+        free(m);
+        return s;
+    }
+    double s = 0.0;
+    for (int i = 0; i < P->ne; ++i) s += (double)(sharp ? x[i] * (1.0f - x[i]) : x[i]);
+    return s;
+}
+
 float orc_vol_sum(const orc_problem* P, const float* x, int n) {
     if (P->p.vol_mode == 0) return vec8_sum(x, n);
     if (P->p.vol_mode == 1) return seq_sum(x, n);
-    double s = 0.0;
-    for (int i = 0; i < n; ++i) s += (double)x[i];
-    return (float)s;
+    return (float)fp64_sum(P, x, 0);
 }
 
 /* sharpness 4*sum(x(1-x))/ne (driver.cpp:188) */
 float orc_sharpness(const orc_problem* P, const float* x, int n) {
+    if (P->p.vol_mode == 2) return 4.0f * (float)fp64_sum(P, x, 1) / (float)n;
     float* t = xcalloc((size_t)n, sizeof(float));
     for (int i = 0; i < n; ++i) t[i] = x[i] * (1.0f - x[i]);
     const float s = P->p.vol_mode == 0 ? vec8_sum(t, n) : seq_sum(t, n);
@@ -1151,9 +1320,7 @@ int orc_design_loop(orc_problem* P, float V0, int nLoop, float rMin, double* Cso
         if (loop == 1 || loop % 5 == 0) orc_mg_build(P, E);
         const int its = orc_pcg(P, E, b, u, tol, P->p.cg_max_it);
         orc_compliance(P, E, u, ce);
-        double cobj = 0.0;
-        for (int e = 0; e < ne; ++e) cobj += E[e] * (ce[e] / Csolid);
-        const double Cdisp = Csolid > 0 ? cobj * Csolid : cobj;
+        const double Cdisp = orc_objective(P, E, ce, Csolid);
         orc_sens(P, x, ce, Csolid, dc);
         for (int e = 0; e < ne; ++e) xdc[e] = x[e] * dc[e];
         orc_filter_apply(P, xdc, dcf);

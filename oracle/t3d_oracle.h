@@ -41,6 +41,10 @@ typedef struct orc_params {
                                            Newton step for dc/max(1e-3,x) (driver.cpp:166), both on 8/4-wide
                                            blocks with exact IEEE ops on the last 0..3 elements.  Their bits
                                            depend on the x86 CPU's rsqrt/rcp approximation tables. */
+    int   red_mode;                 /* inner products and sums: 0 = sequential in the reference's loop order;
+                                       1 = the CUDA path's canonical deterministic order (grid-stride over
+                                           nodes/cells with 1184 x 256 threads, warp and block butterflies),
+                                           so that the two can be compared bit for bit */
 } orc_params;
 
 typedef struct orc_iter_record {    /* one line of driver.cpp:205-211 */
@@ -75,6 +79,7 @@ int    orc_coarse_matrix(orc_problem* P, const double* E, double* out);
 void   orc_vcycle(orc_problem* P, const double* r, double* z);
 int    orc_pcg(orc_problem* P, const double* E, const double* b, double* x, double tol, int maxit);
 double orc_compliance(orc_problem* P, const double* E, const double* u, double* ce);
+double orc_objective(const orc_problem* P, const double* E, const double* ce, double Csolid);
 
 void orc_filter_setup(orc_problem* P, float rmin);
 void orc_filter_apply(orc_problem* P, const float* src, float* dst);
