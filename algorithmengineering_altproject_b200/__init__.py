@@ -48,7 +48,7 @@ class Info(C.Structure):
     _fields_ = [("res", C.c_int64 * 3), ("orig", C.c_int64 * 3), ("num_elements", C.c_int64),
                 ("num_nodes", C.c_int64), ("num_free", C.c_int64), ("num_levels", C.c_int64),
                 ("levels", (C.c_int64 * 4) * 8), ("coarse_n", C.c_int64), ("coarse_cholesky_ok", C.c_int64),
-                ("device_bytes", C.c_int64)]
+                ("device_bytes", C.c_int64), ("kernel_launches", C.c_int64)]
 
 
 class IterRecord(C.Structure):
@@ -98,7 +98,9 @@ _SIGS = {
     "t3d_run_global": (C.c_int, [_CTX, C.c_float, C.c_int, C.POINTER(C.c_double), C.POINTER(IterRecord),
                                  C.POINTER(C.c_int), _f32p]),
     "t3d_synchronize": (C.c_int, [_CTX]),
+    "t3d_profile": (C.c_int, [_CTX, C.c_int, C.c_int, C.POINTER(C.c_double)]),
 }
+T3D_PROFILE_MATVEC, T3D_PROFILE_VCYCLE = 0, 1
 
 _lib = None
 
@@ -329,3 +331,12 @@ class Problem:
 
     def synchronize(self):
         _check(self._lib.t3d_synchronize(self._h))
+
+    def profile(self, what, reps):
+        """mean ms per launch of the matvec (what=0) or V-cycle (what=1), CUDA events on the library stream"""
+        ms = C.c_double()
+        _check(self._lib.t3d_profile(self._h, int(what), int(reps), C.byref(ms)))
+        return float(ms.value)
+
+    def kernel_launches(self):
+        return int(self.info().kernel_launches)

@@ -147,7 +147,9 @@ struct Context {
     OcState* OC = nullptr;
     double* scal = nullptr;     // [0] C, [1] Csolid, [2] objective
     RedSlot slot[4]{};
-    double *Kce = nullptr, *Kc = nullptr, *LT = nullptr, *Lrow = nullptr;
+    double *Kce = nullptr, *Kc = nullptr, *LT = nullptr, *Lrow = nullptr, *Xc = nullptr;
+    double* ra1[8]{};           // separable-restriction pass buffers per level transition
+    double* ra2[8]{};
     int* chol_status = nullptr;
     double *frhs = nullptr, *fx = nullptr, *fr = nullptr, *fz = nullptr, *fp = nullptr, *fAp = nullptr,
            *flastx = nullptr, *flastrhs = nullptr, *fdiag = nullptr;
@@ -174,6 +176,7 @@ struct Context {
     float V0 = 0.0f;
     int loop = 0;
     cudaEvent_t ev[8]{};
+    int64_t launches = 0;   // kernels launched (graph replays counted per node)
 
     template <class T>
     int alloc(T** ptr, size_t n) {
@@ -254,6 +257,12 @@ static int build_levels(Context* c) {
         CHECK(c->alloc(&c->Kc, (size_t)N * N));
         CHECK(c->alloc(&c->LT, (size_t)N * N));
         CHECK(c->alloc(&c->Lrow, (size_t)N * N));
+        CHECK(c->alloc(&c->Xc, (size_t)N * N));
+    }
+    for (int l = 0; l + 1 < c->nlev; ++l) {
+        const MgLevel &Lf = c->lv[l], &Lc = c->lv[l + 1];
+        CHECK(c->alloc(&c->ra1[l], (size_t)3 * (Lf.nz + 1) * (Lf.ny + 1) * (Lc.nx + 1)));
+        CHECK(c->alloc(&c->ra2[l], (size_t)3 * (Lf.nz + 1) * (Lc.ny + 1) * (Lc.nx + 1)));
     }
     CHECK(c->alloc(&c->chol_status, 1));
     T3D_CUDA_OK(cudaMemsetAsync(c->chol_status, 0, sizeof(int), c->st));
@@ -454,6 +463,7 @@ static int download_cells_f32(Context* c, const float* cells, float* h) {
 // ------------------------------------------------------------------ multigrid
 // make_diagonal_preconditioner_from_static for the moduli in c->E (preconditioner.cpp:38-79)
 static int mg_setup(Context* c) {
+    c->launches += 1 + (c->nlev - 1) + (c->Nc ? 4 : 0);
     launch_diag0(c->g, c->Ke, c->E, c->mask0, c->lv[0].diag, c->st);
     for (int l = 0; l + 1 < c->nlev; ++l) launch_diag_coarsen(c->lv[l + 1], c->lv[l], c->st);
     if (c->Nc) {
@@ -461,6 +471,7 @@ static int mg_setup(Context* c) {
         launch_coarse_element_matrices(c->g, Lc, c->mask0, c->E, c->Ke, (double)c->prm.Emin, c->Kce, c->st);
         launch_coarse_assemble(Lc, c->Kce, c->Kc, c->st);
         launch_cholesky(c->Kc, c->LT, c->Lrow, c->Nc, c->chol_status, c->st);
+        launch_coarse_inverse(c->Lrow, c->Nc, c->chol_status, c->Xc, c->st);
     }
     c->mg_ready = true;
     return launch_check("mg set-up");
@@ -469,9 +480,11 @@ static int mg_setup(Context* c) {
 // z = M r for grid vectors; with S, r.z goes to S (rz / beta)
 static void vcycle(Context* c, const double* r, double* z, PcgScalars* S, RedSlot dot) {
     const int L = c->nlev;
+    c->launches += 4 * (L - 1) + 1;
     for (int l = 0; l + 1 < L; ++l)
-        launch_restrict(c->lv[l + 1], c->lv[l], l == 0 ? r : c->lv[l].r, c->lv[l + 1].r, S, c->st);
-    launch_coarse_solve(c->lv[L - 1], c->Lrow, c->LT, c->Nc, c->chol_status, S, c->st);
+        launch_restrict(c->lv[l + 1], c->lv[l], l == 0 ? r : c->lv[l].r, c->lv[l + 1].r, c->ra1[l], c->ra2[l], S,
+                        c->st);
+    launch_coarse_solve(c->lv[L - 1], c->Xc, c->Nc, c->chol_status, S, c->st);
     for (int l = L - 2; l >= 1; --l)
         launch_prolong_smooth(c->lv[l + 1], c->lv[l], c->lv[l + 1].x, c->lv[l].r, c->lv[l].x,
                               (double)c->prm.mg_weight, S, c->st);
@@ -480,6 +493,7 @@ static void vcycle(Context* c, const double* r, double* z, PcgScalars* S, RedSlo
 
 // ------------------------------------------------------------------ PCG (solver.cpp:87-217)
 static void pcg_iteration(Context* c) {
+    c->launches += 3;
     launch_matvec64(c->g, c->Ke, c->E, c->mask0, c->p, c->Ap, c->slot[0], c->S, c->st);
     launch_pcg_update(c->g, c->u, c->r, c->p, c->Ap, c->slot[1], c->S, c->st);
     vcycle(c, c->r, c->z, c->S, c->slot[2]);
@@ -508,6 +522,7 @@ static int pcg_solve(Context* c, double tol, int maxit, int* iters) {
     CHECK(ensure_pcg_graph(c));
     launch_matvec64(c->g, c->Ke, c->E, c->mask0, c->u, c->Ap, RedSlot{nullptr, nullptr}, nullptr, c->st);
     launch_pcg_init(c->g, c->b, c->Ap, c->r, c->slot[1], c->S, tol, c->st);
+    c->launches += 2;
     vcycle(c, c->r, c->z, c->S, c->slot[2]);
     launch_pcg_start(c->g, c->z, c->p, c->st);
     CHECK(launch_check("pcg start"));
@@ -517,6 +532,7 @@ static int pcg_solve(Context* c, double tol, int maxit, int* iters) {
         const int n = std::min(PCG_CHUNK, maxit - queued);
         if (c->use_graph && n == PCG_CHUNK) {
             T3D_CUDA_OK(cudaGraphLaunch(c->pcg_graph, c->st));
+            c->launches += (int64_t)PCG_CHUNK * (3 + 4 * (c->nlev - 1) + 1);
         } else {
             for (int k = 0; k < n; ++k) pcg_iteration(c);
             CHECK(launch_check("pcg iteration"));
@@ -548,6 +564,7 @@ static int filter_apply(Context* c, const float* src_cells, float* dst_cells) {
     CHECK(launch_check("filter start"));
     for (int it = 0; it < 80; it += 8) {
         for (int k = 0; k < 8 && it + k < 80; ++k) {
+            c->launches += 4;
             launch_filter_matvec(g, c->solid, c->kf, c->fp, c->fAp, c->slot[2], c->FS, c->st);
             launch_filter_update(g, c->fx, c->fr, c->fp, c->fAp, c->slot[3], c->FS, c->st);
             launch_filter_precond(g, c->fr, c->fdiag, c->fz, c->slot[0], c->FS, c->st);
@@ -559,6 +576,7 @@ static int filter_apply(Context* c, const float* src_cells, float* dst_cells) {
         if (c->flag_h[0]) break;
     }
     launch_filter_to_cells(g, c->solid, c->fx, dst_cells, c->st);
+    c->launches += 6;
     T3D_CUDA_OK(cudaMemcpyAsync(c->flastx, c->fx, g.NN * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
     T3D_CUDA_OK(cudaMemcpyAsync(c->flastrhs, c->frhs, g.NN * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
     return launch_check("filter finish");
@@ -574,6 +592,7 @@ static int oc_update(Context* c, float V0) {
     int passes = 0;
     for (;;) {
         for (int k = 0; k < 16; ++k) {
+            c->launches += fp64 ? 1 : 2;
             launch_oc_pass(c->g, c->solid, c->x, c->dc, c->xnew, c->OC, fp64, V0, c->ne, c->slot[0], c->st);
             if (!fp64) launch_oc_vec8_vol(c->ne, c->morton, c->xnew, c->OC, V0, c->st);
         }
@@ -585,6 +604,7 @@ static int oc_update(Context* c, float V0) {
         if (passes >= OC_MAX_PASSES) return set_error(T3D_ERR_NUMERIC, "OC bisection did not terminate");
     }
     launch_oc_finish(c->g, c->solid, c->x, c->xnew, c->OC, fp64, c->ne, c->slot[0], c->slot[1], c->st);
+    c->launches += 3 + (fp64 ? 0 : 1);
     if (!fp64) launch_oc_vec8_stats(c->ne, c->morton, c->x, c->OC, c->st);
     CHECK(launch_check("oc finish"));
     T3D_CUDA_OK(cudaMemcpyAsync(c->OC_h, c->OC, sizeof(OcState), cudaMemcpyDeviceToHost, c->st));
@@ -629,6 +649,7 @@ static int design_step(Context* c, t3d_iter_record* rec) {
     cudaEvent_t e0 = c->ev[2], e1 = c->ev[3], e2 = c->ev[4], e3 = c->ev[5], e4 = c->ev[6];
     T3D_CUDA_OK(cudaEventRecord(e0, c->st));
     launch_simp(g, c->solid, c->x, P.E0, P.Emin, P.penal, c->E, c->st);
+    c->launches += 5;   // simp, compliance, objective, sensitivities, dc scale
     if (c->loop == 1 || c->loop % 5 == 0) CHECK(mg_setup(c));
     int its = 0;
     CHECK(pcg_solve(c, (double)P.cg_tol, P.cg_max_it, &its));
@@ -738,6 +759,7 @@ int t3d_get_info(const t3d_context* ctx, t3d_info* info) {
     if (ctx->Nc && ctx->mg_ready) cudaMemcpy(&st, ctx->chol_status, sizeof(int), cudaMemcpyDeviceToHost);
     info->coarse_cholesky_ok = st;
     info->device_bytes = (int64_t)ctx->bytes;
+    info->kernel_launches = ctx->launches;
     return T3D_OK;
 }
 
@@ -1005,6 +1027,32 @@ int t3d_run_global(t3d_context* ctx, float V0, int n_loop, double* c_solid, t3d_
 int t3d_synchronize(t3d_context* ctx) {
     API_GUARD(ctx);
     return t3d::sync(ctx);
+}
+
+int t3d_profile(t3d_context* ctx, int what, int reps, double* ms) {
+    API_GUARD(ctx);
+    if (reps <= 0 || !ms || (what != T3D_PROFILE_MATVEC && what != T3D_PROFILE_VCYCLE))
+        return t3d::set_error(T3D_ERR_INVALID, "bad profile request");
+    if (what == T3D_PROFILE_VCYCLE && !ctx->mg_ready) return t3d::set_error(T3D_ERR_INVALID, "MG not set up");
+    T3D_CUDA_OK(cudaMemsetAsync(ctx->S, 0, sizeof(t3d::PcgScalars), ctx->st));
+    auto once = [&]() {
+        if (what == T3D_PROFILE_MATVEC) {
+            t3d::launch_matvec64(ctx->g, ctx->Ke, ctx->E, ctx->mask0, ctx->p, ctx->Ap, ctx->slot[0], ctx->S, ctx->st);
+            ctx->launches += 1;
+        } else {
+            t3d::vcycle(ctx, ctx->r, ctx->z, ctx->S, ctx->slot[2]);
+        }
+    };
+    once();
+    T3D_CUDA_OK(cudaEventRecord(ctx->ev[6], ctx->st));
+    for (int k = 0; k < reps; ++k) once();
+    T3D_CUDA_OK(cudaEventRecord(ctx->ev[7], ctx->st));
+    CHECK(t3d::launch_check("profile"));
+    T3D_CUDA_OK(cudaEventSynchronize(ctx->ev[7]));
+    float t = 0;
+    T3D_CUDA_OK(cudaEventElapsedTime(&t, ctx->ev[6], ctx->ev[7]));
+    *ms = (double)t / reps;
+    return T3D_OK;
 }
 
 }  // extern "C"

@@ -63,7 +63,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_matvec64(Grid g, const double* 
                                                           const uint8_t* __restrict__ mask,
                                                           const double* __restrict__ u, double* __restrict__ y,
                                                           RedSlot dot, PcgScalars* S) {
-    __shared__ double Ke[576];
+    __shared__ __align__(16) double Ke[576];
     __shared__ double sh[32];
     if (S != nullptr && S->done) return;
     for (int i = threadIdx.x; i < 576; i += blockDim.x) Ke[i] = Keg[i];
@@ -94,13 +94,17 @@ __global__ void __launch_bounds__(RED_THREADS) k_matvec64(Grid g, const double* 
                 ue[3 * b + 1] = u1[m];
                 ue[3 * b + 2] = u2[m];
             }
-            const double* K0 = Ke + (3 * a) * 24;
+            const double2* K0 = reinterpret_cast<const double2*>(Ke + (3 * a) * 24);
             double f0 = 0.0, f1 = 0.0, f2 = 0.0;
 #pragma unroll
-            for (int j = 0; j < 24; ++j) {
-                f0 = fma(K0[j], ue[j], f0);
-                f1 = fma(K0[24 + j], ue[j], f1);
-                f2 = fma(K0[48 + j], ue[j], f2);
+            for (int j = 0; j < 24; j += 2) {
+                const double2 k0 = K0[j / 2], k1 = K0[12 + j / 2], k2 = K0[24 + j / 2];
+                f0 = fma(k0.x, ue[j], f0);
+                f0 = fma(k0.y, ue[j + 1], f0);
+                f1 = fma(k1.x, ue[j], f1);
+                f1 = fma(k1.y, ue[j + 1], f1);
+                f2 = fma(k2.x, ue[j], f2);
+                f2 = fma(k2.y, ue[j + 1], f2);
             }
             y0 = fma(f0, Ee, y0);
             y1 = fma(f1, Ee, y1);

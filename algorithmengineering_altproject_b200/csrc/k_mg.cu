@@ -5,6 +5,8 @@
 #include "kernels.hpp"
 #include "red.cuh"
 
+#include <algorithm>
+
 namespace t3d {
 
 namespace {
@@ -109,36 +111,90 @@ __global__ void k_diag_coarsen(MgLevel Lc, MgLevel Lf) {
 }
 
 // ------------------------------------------------------------------ restriction (transfers.cpp:449-533)
-// valSum*(1/wSum) over the clipped window, then the coarse BC mask (preconditioner.cpp:183-191)
-__global__ void k_restrict(MgLevel Lc, MgLevel Lf, const double* __restrict__ rf, double* __restrict__ rc,
-                           const PcgScalars* S) {
+// The normalised hat-weighted window average, evaluated separably in three passes (x sums for each
+// fine (z,y) row, then y, then z; each sum in increasing index order from 0; weight sum = product
+// of the exact 1D sums), then scaled by 1/wSum and masked (preconditioner.cpp:183-191).  The CPU
+// oracle's canonical mode evaluates the same order.
+__global__ void k_restrict_x(MgLevel Lc, MgLevel Lf, const double* __restrict__ rf, double* __restrict__ a1,
+                             const PcgScalars* S) {
+    if (S != nullptr && S->done) return;
+    const int cnx = Lc.nx + 1, fnx = Lf.nx + 1, fny = Lf.ny + 1, fnz = Lf.nz + 1;
+    const int64_t total = (int64_t)fnz * fny * cnx;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const int cx = (int)(t % cnx);
+    const int64_t row = t / cnx;   // fz*fny + fy
+    const int s = Lc.span, ws = 2 * s - 1;
+    const int64_t fNN = Lf.nn;
+    const double* __restrict__ src = rf + row * fnx;
+    double v0 = 0.0, v1 = 0.0, v2 = 0.0;
+    for (int ix = 0; ix < ws; ++ix) {
+        const int fx = cx * s + ix - (s - 1);
+        if (fx < 0 || fx >= fnx) continue;
+        const double w = hat(ix, s);
+        v0 = v0 + w * src[fx];
+        v1 = v1 + w * src[fNN + fx];
+        v2 = v2 + w * src[2 * fNN + fx];
+    }
+    a1[t] = v0;
+    a1[total + t] = v1;
+    a1[2 * total + t] = v2;
+}
+
+__global__ void k_restrict_y(MgLevel Lc, MgLevel Lf, const double* __restrict__ a1, double* __restrict__ a2,
+                             const PcgScalars* S) {
+    if (S != nullptr && S->done) return;
+    const int cnx = Lc.nx + 1, cny = Lc.ny + 1, fny = Lf.ny + 1, fnz = Lf.nz + 1;
+    const int64_t total = (int64_t)fnz * cny * cnx, total1 = (int64_t)fnz * fny * cnx;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const int cx = (int)(t % cnx);
+    const int cy = (int)((t / cnx) % cny);
+    const int fz = (int)(t / ((int64_t)cnx * cny));
+    const int s = Lc.span, ws = 2 * s - 1;
+    double v0 = 0.0, v1 = 0.0, v2 = 0.0;
+    for (int iy = 0; iy < ws; ++iy) {
+        const int fy = cy * s + iy - (s - 1);
+        if (fy < 0 || fy >= fny) continue;
+        const double w = hat(iy, s);
+        const int64_t i = ((int64_t)fz * fny + fy) * cnx + cx;
+        v0 = v0 + w * a1[i];
+        v1 = v1 + w * a1[total1 + i];
+        v2 = v2 + w * a1[2 * total1 + i];
+    }
+    a2[t] = v0;
+    a2[total + t] = v1;
+    a2[2 * total + t] = v2;
+}
+
+__global__ void k_restrict_z(MgLevel Lc, MgLevel Lf, const double* __restrict__ a2, double* __restrict__ rc,
+                             const PcgScalars* S) {
     if (S != nullptr && S->done) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= Lc.nn) return;
-    const LevelIdx C(Lc), F(Lf);
-    const int cx = n % C.nnx, cy = (n / C.nnx) % C.nny, cz = n / (C.nnx * C.nny);
+    const int cnx = Lc.nx + 1, cny = Lc.ny + 1;
+    const int fnx = Lf.nx + 1, fny = Lf.ny + 1, fnz = Lf.nz + 1;
+    const int cx = n % cnx, cy = (n / cnx) % cny, cz = n / (cnx * cny);
     const int s = Lc.span, ws = 2 * s - 1;
-    const int64_t fNN = Lf.nn;
-    double v0 = 0.0, v1 = 0.0, v2 = 0.0, wsum = 0.0;
+    const int64_t total2 = (int64_t)fnz * cny * cnx;
+    double swx = 0.0, swy = 0.0, swz = 0.0;
+    for (int i = 0; i < ws; ++i) {
+        const int fx = cx * s + i - (s - 1), fy = cy * s + i - (s - 1);
+        if (fx >= 0 && fx < fnx) swx = swx + hat(i, s);
+        if (fy >= 0 && fy < fny) swy = swy + hat(i, s);
+    }
+    double v0 = 0.0, v1 = 0.0, v2 = 0.0;
     for (int iz = 0; iz < ws; ++iz) {
         const int fz = cz * s + iz - (s - 1);
-        if (fz < 0 || fz >= F.nnz) continue;
-        for (int iy = 0; iy < ws; ++iy) {
-            const int fy = cy * s + iy - (s - 1);
-            if (fy < 0 || fy >= F.nny) continue;
-            const double wzy = hat(iz, s) * hat(iy, s);
-            for (int ix = 0; ix < ws; ++ix) {
-                const int fx = cx * s + ix - (s - 1);
-                if (fx < 0 || fx >= F.nnx) continue;
-                const double w = wzy * hat(ix, s);
-                const int f = F.node(fx, fy, fz);
-                v0 = v0 + rf[f] * w;
-                v1 = v1 + rf[fNN + f] * w;
-                v2 = v2 + rf[2 * fNN + f] * w;
-                wsum = wsum + w;
-            }
-        }
+        if (fz < 0 || fz >= fnz) continue;
+        swz = swz + hat(iz, s);
+        const double w = hat(iz, s);
+        const int64_t i = ((int64_t)fz * cny + cy) * cnx + cx;
+        v0 = v0 + w * a2[i];
+        v1 = v1 + w * a2[total2 + i];
+        v2 = v2 + w * a2[2 * total2 + i];
     }
+    const double wsum = swz * swy * swx;
     double o0 = 0.0, o1 = 0.0, o2 = 0.0;
     if (wsum > 1e-12) {
         const double iw = 1.0 / wsum;
@@ -371,18 +427,39 @@ __global__ void __launch_bounds__(1024) k_cholesky(const double* __restrict__ A,
     if (threadIdx.x == 0) *status = 1;
 }
 
-// Coarsest solve L L' x = r (coarsest.cpp:92-122) in the exact operation order of the row-oriented
-// forward and column-oriented backward substitutions: thread i owns x_i; step j publishes x_j.
-// Without a factor (*status != 1) the coarsest level falls back to x = r/max(1e-30,D)
-// (preconditioner.cpp:199-214).  The result is masked (preconditioner.cpp:217-227).
-__global__ void __launch_bounds__(1024) k_coarse_solve(MgLevel L, const double* __restrict__ Lrow,
-                                                       const double* __restrict__ LT, int N,
-                                                       const int* __restrict__ status, const PcgScalars* S) {
-    __shared__ double xs[2];
+// Coarsest inverse for the canonical coarsest solve: column j of X = L'^-1 L^-1 e_j computed by
+// thread j with the reference's substitution order (coarsest.cpp:92-122); column j is stored
+// contiguously (X[j*N + i]).  Runs at each MG set-up after a successful factorisation.
+__global__ void k_coarse_inverse(const double* __restrict__ Lrow, int N, const int* __restrict__ status,
+                                 double* __restrict__ X) {
+    if (*status != 1) return;
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= N) return;
+    double* x = X + (int64_t)j * N;
+    for (int i = 0; i < N; ++i) x[i] = (i == j) ? 1.0 : 0.0;
+    for (int i = 0; i < N; ++i) {
+        double s = x[i];
+        const double* Li = Lrow + (int64_t)i * N;
+        for (int k = 0; k < i; ++k) s = s - Li[k] * x[k];
+        x[i] = s / Li[i];
+    }
+    for (int i = N - 1; i >= 0; --i) {
+        const double* Li = Lrow + (int64_t)i * N;
+        x[i] = x[i] / Li[i];
+        const double xi = x[i];
+        for (int k = 0; k < i; ++k) x[k] = x[k] - Li[k] * xi;
+    }
+}
+
+// Coarsest solve x_i = sum_j X[i][j] r_j (sequential in j) when the factorisation succeeded, else
+// the Jacobi fallback x = r/max(1e-30,D) (preconditioner.cpp:195-215); masked (:217-227).
+__global__ void __launch_bounds__(128) k_coarse_solve(MgLevel L, const double* __restrict__ X, int N,
+                                                      const int* __restrict__ status, const PcgScalars* S) {
+    extern __shared__ double rs[];
     if (S != nullptr && S->done) return;
     const int64_t nn = L.nn;
     if (*status != 1) {
-        for (int n = threadIdx.x; n < nn; n += blockDim.x) {
+        for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x) {
             const int m = L.mask[n];
             for (int c = 0; c < 3; ++c) {
                 const double d = L.diag[c * nn + n];
@@ -392,31 +469,14 @@ __global__ void __launch_bounds__(1024) k_coarse_solve(MgLevel L, const double* 
         }
         return;
     }
-    const int i = threadIdx.x;
-    const bool own = i < N;
-    const int ni = i / 3, ci = i % 3;
-    double xi = own ? L.r[ci * nn + ni] : 0.0;
-    for (int j = 0; j < N; ++j) {
-        if (i == j) {
-            xi = xi / LT[(int64_t)j * N + j];
-            xs[j & 1] = xi;
-        }
-        __syncthreads();
-        if (own && i > j) xi = xi - LT[(int64_t)j * N + i] * xs[j & 1];
-    }
+    for (int j = threadIdx.x; j < N; j += blockDim.x) rs[j] = L.r[(j % 3) * nn + j / 3];
     __syncthreads();
-    for (int k = N - 1; k >= 0; --k) {
-        if (i == k) {
-            xi = xi / Lrow[(int64_t)k * N + k];
-            xs[k & 1] = xi;
-        }
-        __syncthreads();
-        if (own && i < k) xi = xi - Lrow[(int64_t)k * N + i] * xs[k & 1];
-    }
-    if (own) {
-        const int m = L.mask[ni];
-        L.x[ci * nn + ni] = ((m >> ci) & 1) ? 0.0 : xi;
-    }
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double acc = 0.0;
+    for (int j = 0; j < N; ++j) acc = acc + X[(int64_t)j * N + i] * rs[j];
+    const int ni = i / 3, ci = i % 3;
+    L.x[ci * nn + ni] = ((L.mask[ni] >> ci) & 1) ? 0.0 : acc;
 }
 
 inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
@@ -429,9 +489,13 @@ void launch_mask_restrict(const MgLevel& Lc, const MgLevel& Lf, cudaStream_t s) 
 void launch_diag_coarsen(const MgLevel& Lc, const MgLevel& Lf, cudaStream_t s) {
     k_diag_coarsen<<<blocks_for(Lc.nn, 128), 128, 0, s>>>(Lc, Lf);
 }
-void launch_restrict(const MgLevel& Lc, const MgLevel& Lf, const double* rf, double* rc, const PcgScalars* S,
-                     cudaStream_t s) {
-    k_restrict<<<blocks_for(Lc.nn, 128), 128, 0, s>>>(Lc, Lf, rf, rc, S);
+void launch_restrict(const MgLevel& Lc, const MgLevel& Lf, const double* rf, double* rc, double* a1, double* a2,
+                     const PcgScalars* S, cudaStream_t s) {
+    const int64_t n1 = (int64_t)(Lf.nz + 1) * (Lf.ny + 1) * (Lc.nx + 1);
+    const int64_t n2 = (int64_t)(Lf.nz + 1) * (Lc.ny + 1) * (Lc.nx + 1);
+    k_restrict_x<<<blocks_for(n1, 256), 256, 0, s>>>(Lc, Lf, rf, a1, S);
+    k_restrict_y<<<blocks_for(n2, 256), 256, 0, s>>>(Lc, Lf, a1, a2, S);
+    k_restrict_z<<<blocks_for(Lc.nn, 128), 128, 0, s>>>(Lc, Lf, a2, rc, S);
 }
 void launch_coarse_jacobi(const MgLevel& L, const PcgScalars* S, cudaStream_t s) {
     k_coarse_jacobi<<<blocks_for(L.nn, 128), 128, 0, s>>>(L, S);
@@ -456,9 +520,14 @@ void launch_coarse_assemble(const MgLevel& Lc, const double* Kce, double* Kc, cu
 void launch_cholesky(const double* A, double* LT, double* Lrow, int N, int* status, cudaStream_t s) {
     k_cholesky<<<1, 1024, 0, s>>>(A, LT, Lrow, N, status);
 }
-void launch_coarse_solve(const MgLevel& L, const double* Lrow, const double* LT, int N, const int* status,
-                         const PcgScalars* S, cudaStream_t s) {
-    k_coarse_solve<<<1, 1024, 0, s>>>(L, Lrow, LT, N, status, S);
+void launch_coarse_inverse(const double* Lrow, int N, const int* status, double* X, cudaStream_t s) {
+    k_coarse_inverse<<<blocks_for(N, 32), 32, 0, s>>>(Lrow, N, status, X);
+}
+void launch_coarse_solve(const MgLevel& L, const double* X, int N, const int* status, const PcgScalars* S,
+                         cudaStream_t s) {
+    const int64_t work = N > 0 ? N : L.nn;
+    const unsigned blocks = (unsigned)std::max<int64_t>(1, (work + 127) / 128);
+    k_coarse_solve<<<blocks, 128, (size_t)std::max(N, 1) * sizeof(double), s>>>(L, X, N, status, S);
 }
 
 }  // namespace t3d

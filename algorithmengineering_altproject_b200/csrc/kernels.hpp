@@ -26,6 +26,7 @@ void launch_setup_load(const Grid& g, int ix_load, int iz_max, double fz, const 
                        cudaStream_t s);
 
 // ---- FEA operators
+// Ke: device pointer to the 576 stiffness coefficients
 void launch_matvec64(const Grid& g, const double* Ke, const double* E, const uint8_t* mask, const double* u,
                      double* y, RedSlot dot, PcgScalars* S, cudaStream_t s);
 void launch_compliance64(const Grid& g, const double* Ke, const double* E, const double* u, double* ce,
@@ -42,8 +43,9 @@ void launch_diag0(const Grid& g, const double* Ke, const double* E, const uint8_
                   cudaStream_t s);
 void launch_mask_restrict(const MgLevel& Lc, const MgLevel& Lf, cudaStream_t s);
 void launch_diag_coarsen(const MgLevel& Lc, const MgLevel& Lf, cudaStream_t s);
-void launch_restrict(const MgLevel& Lc, const MgLevel& Lf, const double* rf, double* rc, const PcgScalars* S,
-                     cudaStream_t s);
+// separable restriction; a1, a2: pass buffers of 3*(fnz*fny*cnx) and 3*(fnz*cny*cnx) doubles
+void launch_restrict(const MgLevel& Lc, const MgLevel& Lf, const double* rf, double* rc, double* a1, double* a2,
+                     const PcgScalars* S, cudaStream_t s);
 void launch_coarse_jacobi(const MgLevel& L, const PcgScalars* S, cudaStream_t s);
 void launch_prolong_smooth(const MgLevel& Lc, const MgLevel& Lf, const double* xc, const double* rf, double* xf,
                            double weight, const PcgScalars* S, cudaStream_t s);
@@ -54,9 +56,11 @@ void launch_coarse_element_matrices(const Grid& g0, const MgLevel& Lc, const uin
                                     const double* Ke, double emin, double* Kce, cudaStream_t s);
 void launch_coarse_assemble(const MgLevel& Lc, const double* Kce, double* Kc, cudaStream_t s);
 void launch_cholesky(const double* A, double* LT, double* Lrow, int N, int* status, cudaStream_t s);
-// Cholesky solve when *status == 1, else the Jacobi fallback (preconditioner.cpp:76-77, 195-215)
-void launch_coarse_solve(const MgLevel& L, const double* Lrow, const double* LT, int N, const int* status,
-                         const PcgScalars* S, cudaStream_t s);
+// canonical coarsest solve: inverse columns from the factor, then x = X r (Jacobi fallback when
+// *status != 1, preconditioner.cpp:76-77, 195-215)
+void launch_coarse_inverse(const double* Lrow, int N, const int* status, double* X, cudaStream_t s);
+void launch_coarse_solve(const MgLevel& L, const double* X, int N, const int* status, const PcgScalars* S,
+                         cudaStream_t s);
 
 // ---- PCG vector steps (solver.cpp:87-217)
 void launch_pcg_init(const Grid& g, const double* b, const double* Ax, double* r, RedSlot red, PcgScalars* S,

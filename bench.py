@@ -1,0 +1,307 @@
+"""Benchmark of the B200 design iteration (SIMP -> MG-preconditioned PCG -> compliance ->
+sensitivities -> PDE filter -> OC) on the reference's cantilever.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--config c2]
+
+Prints ONE JSON line (rank 0).  A step is one design iteration.  `value` = design iterations/s
+over the whole job, timed on the device (CUDA events recorded by the library on its stream; max
+over ranks); `e2e` = the same metric through the host-buffer C-ABI call t3d_design_step_host
+(H2D of the design field, D2H of the updated field, wall clock).  Multi-GPU runs are independent
+replicas (one design per GPU, no collective on the data path).
+
+--impl reference times the reference's own CPU implementation (oracle/_ref/libt3d_ref.so, the
+unmodified reference sources) on this host's cores with a bounded sample of the same workload:
+design iterations with PCG capped at a few iterations, extrapolated to the iteration count of a
+full solve.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+# workloads: element counts, V0, MG level cap
+CONFIGS = {
+    "c0": dict(nely=30, nelx=60, nelz=30, V0=0.12, max_levels=5,
+               name="cantilever 30x60x30 (54,000 elements, 172,980 free DOF)"),
+    "c1": dict(nely=96, nelx=192, nelz=96, V0=0.12, max_levels=5,
+               name="cantilever 96x192x96 (1,769,472 elements, 5,419,584 free DOF)"),
+    "c2": dict(nely=256, nelx=512, nelz=256, V0=0.08, max_levels=6,
+               name="cantilever 256x512x256 (33,554,432 elements, 101,451,264 free DOF)"),
+}
+DEFAULT_CONFIG = "c2"
+METRIC = "design iterations/s"
+MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC_NOTE = os.path.join(ROOT, "profiles", "matvec_fp64_traffic.md")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--config", default=DEFAULT_CONFIG, choices=sorted(CONFIGS))
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("LOCAL_RANK", "0"))
+
+
+# ---------------------------------------------------------------- clocks sampling
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples every 200 ms while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join("/tmp", "t3d_clocks_%d_%d.csv" % (os.getpid(), index))
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        busy = [s for s in sm if s > 600] or sm
+        return {"sm_mhz": statistics.median(busy) if busy else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def hbm_peak():
+    try:
+        d = json.load(open(MEASURED_PEAKS))
+        return float(d["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def traffic_per_launch():
+    """dram read+write bytes per matvec launch from the committed ncu summary, if present."""
+    try:
+        m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(TRAFFIC_NOTE).read())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+# ---------------------------------------------------------------- CPU baseline / reference arm
+def reference_sample(cfg, steps, warmup, n_pcg, threads):
+    """Bounded sample of the reference's CPU design iteration: `steps` iterations with PCG capped at
+    3 iterations (after `warmup` untimed ones), extrapolated to n_pcg PCG iterations per design
+    iteration with the per-iteration PCG cost measured from caps of 1 and 3."""
+    from oracle.bindings import Reference, reference_available
+    if reference_available():
+        Reference.set_threads(threads)
+        r = Reference(cfg["nely"], cfg["nelx"], cfg["nelz"], max_levels=cfg["max_levels"])
+        kind, cores = "reference", threads
+    else:
+        raise RuntimeError("reference build oracle/_ref/libt3d_ref.so is not present")
+    V0 = cfg["V0"]
+    for k in range(max(1, warmup)):
+        r.sample_iteration(V0, 1, k == 0)
+    per_iter = []
+    rest = []
+    for k in range(max(1, steps)):
+        _, a = r.sample_iteration(V0, 1, False)
+        _, b = r.sample_iteration(V0, 3, False)
+        per_iter.append((b[2] - a[2]) / 2.0)
+        rest.append(b[0] + b[3] + b[4] + b[5] + a[1])
+    _, mg = r.sample_iteration(V0, 1, True)
+    t_iter = statistics.median(per_iter)
+    t_pcg_full = max(t_iter, 0.0) * n_pcg
+    t_design = t_pcg_full + statistics.median(rest) + mg[1] / 5.0
+    return dict(value=1.0 / t_design, seconds_per_design_iteration=t_design, pcg_iteration_s=t_iter,
+                kind=kind, cores=cores,
+                sample="%d reference design iterations with PCG capped at 1 and 3 iterations "
+                       "(per-PCG-iteration cost %.3f s); extrapolated to %d PCG iterations per design iteration "
+                       "plus the measured SIMP/compliance/filter/OC time and 1/5 of an MG rebuild"
+                       % (2 * max(1, steps), t_iter, n_pcg))
+
+
+def run_reference_arm(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    cfg = CONFIGS[args.config]
+    threads = os.cpu_count() or 1
+    n_pcg = 800   # cgMaxIt (core.hpp:36): the reference's solves hit the cap at these sizes
+    t0 = time.time()
+    s = reference_sample(cfg, args.steps, args.warmup, n_pcg, threads)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": s["value"], "unit": "design iter/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * s["seconds_per_design_iteration"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (built-in cantilever load case)",
+        "config": {"workload": cfg["name"], "V0": cfg["V0"], "mg_max_levels": cfg["max_levels"],
+                   "precision": "fp64 (reference OpenMP CPU path)", "pcg_iterations_assumed": n_pcg},
+        "cpu_baseline": {"value": s["value"], "unit": "design iter/s", "cores": s["cores"], "kind": s["kind"],
+                         "sample": s["sample"]},
+        "e2e": {"value": s["value"], "unit": "design iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "wall_s": time.time() - t0,
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- B200 arm
+def run_b200(args):
+    import torch
+    import algorithmengineering_altproject_b200 as t3d
+
+    rank, world, local = dist_env()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    dev = local
+    torch.cuda.set_device(dev)
+    cfg = CONFIGS[args.config]
+
+    P = t3d.Problem(cfg["nely"], cfg["nelx"], cfg["nelz"], device=dev, mg_max_levels=cfg["max_levels"],
+                    oc_sum_order=t3d.T3D_SUM_FP64)
+    P.design_init(cfg["V0"])
+    for _ in range(args.warmup):
+        P.design_step()
+
+    def barrier():
+        torch.cuda.synchronize(dev)
+        if world > 1:
+            torch.distributed.barrier()
+
+    clocks = ClockSampler(dev)
+    clocks.start()
+    barrier()
+    launches0 = P.kernel_launches()
+    t_wall0 = time.perf_counter()
+    recs = [P.design_step() for _ in range(args.steps)]
+    t_wall = time.perf_counter() - t_wall0
+    launches = P.kernel_launches() - launches0
+    barrier()
+    clk = clocks.stop()
+    dev_time = sum(r["t_total"] for r in recs)
+
+    # roofline of the dominant kernel (K(E)p with fused p.Ap), CUDA events on the library stream
+    mv_ms = P.profile(t3d.T3D_PROFILE_MATVEC, 20)
+    vc_ms = P.profile(t3d.T3D_PROFILE_VCYCLE, 10)
+
+    # end to end through host buffers
+    e2e = None
+    if not args.no_e2e:
+        x = torch.empty(P.ne, dtype=torch.float32, pin_memory=True).numpy()
+        x[:] = P.density()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            xo, _ = P.design_step_host(x)
+            x[:] = xo
+        e2e_t = time.perf_counter() - t0
+        barrier()
+        e2e = e2e_t
+
+    times = torch.tensor([dev_time, t_wall, e2e if e2e is not None else 0.0], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(times, op=torch.distributed.ReduceOp.MAX)
+    dev_time, t_wall, e2e = [float(v) for v in times.cpu()]
+
+    if rank == 0:
+        w = 8
+        ne, nf = P.ne, P.nf
+        alg_bytes = w * (2 * nf + ne)              # read p, write Ap (free DOFs), read E
+        achieved = alg_bytes / (mv_ms * 1e-3) / 1e9
+        peak, peak_kind = hbm_peak()
+        pcg_its = [r["pcg_iters"] for r in recs]
+        line = {
+            "metric": METRIC, "value": world * args.steps / dev_time, "unit": "design iter/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * dev_time / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (the reference's built-in cantilever load case; no dataset involved)",
+            "config": {"workload": cfg["name"], "V0": cfg["V0"], "mg_max_levels": cfg["max_levels"],
+                       "mg_levels": P.nlev, "coarse_dofs": P.coarse_n, "precision": "fp64 (plain GPU form)",
+                       "oc_volume_sum": "fp64", "parallelism": "replicas" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (node vectors %.0f MB each)" % (3 * P.nn * 8 / 1e6)},
+            "pcg_iterations": pcg_its,
+            "per_kernel_ms": {"matvec": mv_ms, "vcycle": vc_ms,
+                              "pcg_iteration": 1000.0 * sum(r["t_cg"] for r in recs) / max(1, sum(pcg_its))},
+            "throughput": {"dof_matvecs_per_s": nf / (mv_ms * 1e-3), "vcycles_per_s": 1.0 / (vc_ms * 1e-3)},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic_per_launch(), "peak_source": peak_kind,
+                         "kernel": "k_matvec64 (K(E)p + p.Ap)", "algorithmic_bytes_per_launch": alg_bytes,
+                         "fp64_flops_per_launch": 1152 * ne,
+                         "fp64_tflops": 1152 * ne / (mv_ms * 1e-3) / 1e12},
+            "clocks": clk,
+            "gpu_launches": launches,
+            "wall_s_timed": t_wall,
+        }
+        if e2e:
+            line["e2e"] = {"value": world * args.steps / e2e, "unit": "design iter/s",
+                           "h2d_bytes_per_step": 4 * ne, "d2h_bytes_per_step": 4 * ne + 64}
+        if not args.no_cpu_baseline and world == 1:
+            try:
+                s = reference_sample(CONFIGS[args.config], 1, 1, int(round(statistics.mean(pcg_its))),
+                                     os.cpu_count() or 1)
+                line["cpu_baseline"] = {"value": s["value"], "unit": "design iter/s", "cores": s["cores"],
+                                        "kind": s["kind"], "sample": s["sample"]}
+            except Exception as e:  # baseline is reported, never required for the GPU number
+                line["cpu_baseline"] = {"value": None, "unit": "design iter/s", "cores": 0, "kind": "reference",
+                                        "sample": "unavailable: %s" % e}
+        print(json.dumps(line), flush=True)
+    P.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

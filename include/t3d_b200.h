@@ -63,6 +63,7 @@ typedef struct t3d_info {
     int64_t coarse_n;             /* dense coarsest system size, 0 = Jacobi coarsest */
     int64_t coarse_cholesky_ok;   /* 1 when the last MG set-up factorised the coarsest matrix */
     int64_t device_bytes;         /* device memory held by the context */
+    int64_t kernel_launches;      /* kernels launched by this context so far (graph nodes included) */
 } t3d_info;
 
 typedef struct t3d_iter_record {  /* one design iteration (driver.cpp:205-216) */
@@ -133,6 +134,14 @@ int  t3d_set_density(struct t3d_context* ctx, const float* x);
 int  t3d_run_global(struct t3d_context* ctx, float V0, int n_loop, double* c_solid, t3d_iter_record* records,
                     int* n_records, float* x_final);
 int  t3d_synchronize(struct t3d_context* ctx);
+
+/* --------------------------------------------------------------- profiling (no reference counterpart)
+ * Times `reps` back-to-back launches of one device-resident kernel sequence with CUDA events on the
+ * context's stream, after one untimed launch: T3D_PROFILE_MATVEC = K(E)p with the fused p.Ap,
+ * T3D_PROFILE_VCYCLE = one V-cycle z = M r.  Operates on the current device state (E, p, r) and
+ * overwrites Ap / z; *ms = mean milliseconds per launch. */
+enum { T3D_PROFILE_MATVEC = 0, T3D_PROFILE_VCYCLE = 1 };
+int  t3d_profile(struct t3d_context* ctx, int what, int reps, double* ms);
 
 #ifdef __cplusplus
 }

@@ -324,6 +324,8 @@ class Reference(_Common):
             L.ref_filter_set_state.argtypes = [C.c_void_p, _f64p, _f64p]
             L.ref_set_threads.argtypes = [C.c_int]
             L.ref_max_threads.restype = C.c_int
+            L.ref_sample_iteration.argtypes = [C.c_void_p, C.c_float, C.c_int, C.c_int, _f64p]
+            L.ref_sample_iteration.restype = C.c_int
             L.ref_run_global.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, C.c_float, C.c_char_p]
             cls._lib = L
         return cls._lib
@@ -348,6 +350,12 @@ class Reference(_Common):
         self._fs, self._fa, self._fst, self._fss = (L.ref_filter_setup, L.ref_filter_apply, L.ref_filter_state,
                                                     L.ref_filter_set_state)
         self._setup_info()
+
+    def sample_iteration(self, V0, pcg_max, rebuild_mg):
+        """one reference design iteration with PCG capped at pcg_max; returns (iters, times[6])"""
+        t = np.zeros(6)
+        it = self.lib().ref_sample_iteration(self.h, C.c_float(V0), int(pcg_max), int(bool(rebuild_mg)), t)
+        return int(it), t
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -24,8 +24,12 @@
 #include "multigrid/detail/coarsest.hpp"
 #include "multigrid/detail/transfers.hpp"
 
+#include <algorithm>
+#include <chrono>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
+#include <numeric>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -40,6 +44,10 @@ namespace {
 
 struct RefCtx {
     Problem pb;
+    // design state of ref_sample_iteration (driver.cpp:60-84 initialisation)
+    std::vector<float> x;
+    std::vector<double> uWarm, bFree;
+    bool sampleReady = false;
     mg::MGPrecondConfig cfg;
     mg::MGHierarchy H;
     std::vector<std::vector<uint8_t>> masks;
@@ -349,6 +357,74 @@ void ref_filter_set_state(void* h, const double* lastx, const double* lastrhs) {
     const size_t nn = c->pb.mesh.numNodes;
     c->pf.lastXNode.assign(lastx, lastx + nn);
     c->pf.lastRhsNode.assign(lastrhs, lastrhs + nn);
+}
+
+// One design iteration of the reference (driver.cpp:115-189) with PCG capped at pcg_max
+// iterations, for bounded CPU-baseline samples: the reference's own PCG_free, ComputeCompliance,
+// make_diagonal_preconditioner_from_static and ApplyPDEFilter, with the driver's inline SIMP,
+// sensitivity and OC loops restated here and compiled with the reference's flags.
+// times[0..5] = seconds in SIMP, MG rebuild, PCG, compliance+sensitivities, filter, OC;
+// returns the PCG iteration count.
+int ref_sample_iteration(void* h, float V0, int pcg_max, int rebuild_mg, double* times) {
+    auto* c = static_cast<RefCtx*>(h);
+    using clk = std::chrono::steady_clock;
+    auto secs = [](clk::time_point a, clk::time_point b) { return std::chrono::duration<double>(b - a).count(); };
+    const int ne = c->pb.mesh.numElements;
+    if (!c->sampleReady) {
+        c->x.assign(ne, V0);
+        restrict_to_free(c->pb, c->pb.F, c->bFree);
+        c->uWarm.assign(c->bFree.size(), 0.0);
+        if (!c->filterReady) { c->pf = SetupPDEFilter(c->pb, std::sqrt(3.0f)); c->filterReady = true; }
+        c->sampleReady = true;
+    }
+    const auto& P = c->pb.params;
+    std::vector<double> E(ne), ce;
+    auto t0 = clk::now();
+    for (int e = 0; e < ne; e++) {
+        float rho = std::clamp(c->x[e], 0.0f, 1.0f);
+        float powp = static_cast<float>(std::pow(rho, P.simpPenalty));
+        E[e] = P.youngsModulusMin + powp * (P.youngsModulus - P.youngsModulusMin);
+    }
+    auto t1 = clk::now();
+    if (rebuild_mg || !c->M) c->M = mg::make_diagonal_preconditioner_from_static(c->pb, c->H, c->masks, E, c->cfg);
+    auto t2 = clk::now();
+    int it = PCG_free(c->pb, E, c->bFree, c->uWarm, P.cgTol, pcg_max, c->M, c->pws);
+    auto t3 = clk::now();
+    DOFData U;
+    U.ux.assign(c->pb.mesh.numNodes, 0.0); U.uy.assign(c->pb.mesh.numNodes, 0.0); U.uz.assign(c->pb.mesh.numNodes, 0.0);
+    scatter_from_free(c->pb, c->uWarm, U);
+    double C = ComputeCompliance(c->pb, E, U, ce);
+    std::vector<float> dc(ne), xdc(ne), dcf;
+    for (int e = 0; e < ne; e++) {
+        float rho = std::clamp(c->x[e], 0.0f, 1.0f);
+        float dEdrho = P.simpPenalty * static_cast<float>(std::pow(rho, P.simpPenalty - 1.0f)) *
+                       (P.youngsModulus - P.youngsModulusMin);
+        dc[e] = -dEdrho * static_cast<float>(ce[e] / C);
+        xdc[e] = c->x[e] * dc[e];
+    }
+    auto t4 = clk::now();
+    ApplyPDEFilter(c->pb, c->pf, xdc, dcf, c->fws);
+    auto t5 = clk::now();
+    for (int e = 0; e < ne; e++) dc[e] = dcf[e] / std::max(1.0e-3f, c->x[e]);
+    float l1 = 0.0f, l2 = 1e9f, move = 0.2f;
+    std::vector<float> xnew(ne);
+    while ((l2 - l1) / (l1 + l2) > 1e-6) {
+        float lmid = 0.5f * (l1 + l2);
+        for (int e = 0; e < ne; e++) {
+            float val = std::sqrt(std::max(1e-30f, -dc[e] / lmid));
+            float xe = std::clamp(c->x[e] * val, c->x[e] - move, c->x[e] + move);
+            xe = std::clamp(xe, 0.0f, 1.0f);
+            xnew[e] = std::max(1.0e-3f, xe);
+        }
+        float vol = std::accumulate(xnew.begin(), xnew.end(), 0.0f, [](float s, float v) { return s + v; }) /
+                    static_cast<float>(ne);
+        if (vol - V0 > 0) l1 = lmid; else l2 = lmid;
+    }
+    c->x.swap(xnew);
+    auto t6 = clk::now();
+    times[0] = secs(t0, t1); times[1] = secs(t1, t2); times[2] = secs(t2, t3);
+    times[3] = secs(t3, t4); times[4] = secs(t4, t5); times[5] = secs(t5, t6);
+    return it;
 }
 
 }  // extern "C"

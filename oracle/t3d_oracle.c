@@ -52,6 +52,7 @@ struct orc_problem {
     int nlev;
     orc_level lv[8];
     double* Lc;                    /* coarsest Cholesky factor, row-major, lower */
+    double* Xc;                    /* red_mode 1: coarsest inverse, column j = solve(L L', e_j) */
     int Nc;                        /* 0 -> Jacobi coarsest */
     double* tmpf;                  /* [3*nn0] prolongation scratch */
     double *r, *z, *pp, *Ap;       /* PCG workspace [nf] */
@@ -413,6 +414,54 @@ static void restrict_nodes(const orc_level* Lc, const orc_level* Lf, const doubl
             }
 }
 
+/* Canonical (red_mode 1) restriction: the same normalised hat average evaluated separably,
+ * first along x for every fine (z,y) row of the window, then along y, then along z, each sum in
+ * increasing index order from 0; the weight sum (exact in binary) is the product of the 1D sums. */
+static void restrict_nodes_separable(const orc_level* Lc, const orc_level* Lf, const double* rf, double* rc) {
+    const int s = Lc->span, ws = 2 * s - 1;
+    const double inv = 1.0 / s;
+    double W[8];
+    for (int i = 0; i < ws; ++i) W[i] = 1.0 - fabs((double)(i - (s - 1))) * inv;
+    const int fnx = Lf->nx + 1, fny = Lf->ny + 1, fnz = Lf->nz + 1;
+    const int cnx = Lc->nx + 1, cny = Lc->ny + 1, cnz = Lc->nz + 1;
+    for (int cz = 0; cz < cnz; ++cz)
+        for (int cy = 0; cy < cny; ++cy)
+            for (int cx = 0; cx < cnx; ++cx) {
+                double vz[3] = {0, 0, 0}, swz = 0.0, swy = 0.0, swx = 0.0;
+                for (int ix = 0; ix < ws; ++ix) {
+                    const int fx = cx * s + ix - (s - 1);
+                    if (fx >= 0 && fx < fnx) swx = swx + W[ix];
+                }
+                for (int iy = 0; iy < ws; ++iy) {
+                    const int fy = cy * s + iy - (s - 1);
+                    if (fy >= 0 && fy < fny) swy = swy + W[iy];
+                }
+                for (int iz = 0; iz < ws; ++iz) {
+                    const int fz = cz * s + iz - (s - 1);
+                    if (fz < 0 || fz >= fnz) continue;
+                    swz = swz + W[iz];
+                    double vy[3] = {0, 0, 0};
+                    for (int iy = 0; iy < ws; ++iy) {
+                        const int fy = cy * s + iy - (s - 1);
+                        if (fy < 0 || fy >= fny) continue;
+                        double vx[3] = {0, 0, 0};
+                        for (int ix = 0; ix < ws; ++ix) {
+                            const int fx = cx * s + ix - (s - 1);
+                            if (fx < 0 || fx >= fnx) continue;
+                            const int64_t f = ((int64_t)fz * fny + fy) * fnx + fx;
+                            for (int c = 0; c < 3; ++c) vx[c] = vx[c] + W[ix] * rf[f * 3 + c];
+                        }
+                        for (int c = 0; c < 3; ++c) vy[c] = vy[c] + W[iy] * vx[c];
+                    }
+                    for (int c = 0; c < 3; ++c) vz[c] = vz[c] + W[iz] * vy[c];
+                }
+                const double wsum = swz * swy * swx;
+                const int64_t ci = ((int64_t)cz * cny + cy) * cnx + cx;
+                const double iw = 1.0 / wsum;
+                for (int c = 0; c < 3; ++c) rc[ci * 3 + c] = wsum > 1e-12 ? vz[c] * iw : 0.0;
+            }
+}
+
 /* Trilinear interpolation from the coarse cell floor(f/s), clamped to the last cell
  * (transfers.cpp:378-445). */
 static void prolongate_nodes(const orc_level* Lc, const orc_level* Lf, const double* xc, double* xf) {
@@ -684,6 +733,20 @@ void orc_mg_build(orc_problem* P, const double* E) {
         if (cholesky_lower(K, N)) { P->Lc = K; P->Nc = N; }
         else free(K);
     }
+    free(P->Xc);
+    P->Xc = NULL;
+    if (P->Nc && P->p.red_mode == 1) {
+        /* canonical coarsest solve: X[:,j] = L'^-1 L^-1 e_j by the reference's substitutions */
+        const int n = P->Nc;
+        P->Xc = xcalloc((size_t)n * n, sizeof(double));
+        double* e = xcalloc((size_t)n, sizeof(double));
+        for (int j = 0; j < n; ++j) {
+            memset(e, 0, (size_t)n * sizeof(double));
+            e[j] = 1.0;
+            cholesky_solve(P->Lc, e, P->Xc + (int64_t)j * n, n);   /* column j stored contiguously */
+        }
+        free(e);
+    }
 }
 
 int orc_mg_coarse_n(const orc_problem* P) { return P->Nc; }
@@ -706,12 +769,20 @@ void orc_vcycle(orc_problem* P, const double* r, double* z) {
             double dd = Lf->diag[d] > 1.0e-30 ? Lf->diag[d] : 1.0e-30;
             Lf->x[d] = Lf->mask[d] ? 0.0 : w * Lf->r[d] / dd;
         }
-        restrict_nodes(Lc, Lf, Lf->r, 3, 0, Lc->r);
+        if (P->p.red_mode == 1) restrict_nodes_separable(Lc, Lf, Lf->r, Lc->r);
+        else restrict_nodes(Lc, Lf, Lf->r, 3, 0, Lc->r);
         for (int64_t d = 0; d < 3 * Lc->nn; ++d)
             if (Lc->mask[d]) Lc->r[d] = 0.0;
     }
     orc_level* LL = &P->lv[P->nlev - 1];
-    if (P->Nc > 0 && P->Nc == 3 * LL->nn) {
+    if (P->Nc > 0 && P->Nc == 3 * LL->nn && P->Xc) {
+        const int n = P->Nc;
+        for (int i = 0; i < n; ++i) {
+            double acc = 0.0;
+            for (int j = 0; j < n; ++j) acc = acc + P->Xc[(int64_t)j * n + i] * LL->r[j];
+            LL->x[i] = acc;
+        }
+    } else if (P->Nc > 0 && P->Nc == 3 * LL->nn) {
         cholesky_solve(P->Lc, LL->r, LL->x, P->Nc);
     } else {
         for (int64_t d = 0; d < 3 * LL->nn; ++d) {
@@ -772,20 +843,19 @@ static double fold_block(const double* lanes /* RT */) {
     return butterfly32(v);
 }
 
-static double canon_fold(int64_t nitems, canon_step step, const void* ctx) {
+/* per-thread partial of thread t of block b; `active` says whether block b has any work */
+typedef double (*canon_thread)(int b, int t, const void* ctx);
+typedef int (*canon_active)(int b, const void* ctx);
+
+static double canon_fold_threads(canon_thread part_of, canon_active active, const void* ctx) {
     static double partial[RB];
     double lanes[RT];
-    const int64_t stride = (int64_t)RB * RT;
     for (int b = 0; b < RB; ++b) {
-        if ((int64_t)b * RT >= nitems) {   /* threads without items: the butterflies of +0 give +0 */
+        if (!active(b, ctx)) {   /* threads without items: the butterflies of +0 give +0 */
             partial[b] = 0.0;
             continue;
         }
-        for (int t = 0; t < RT; ++t) {
-            double p = 0.0;
-            for (int64_t i = (int64_t)b * RT + t; i < nitems; i += stride) p = step(p, i, ctx);
-            lanes[t] = p;
-        }
+        for (int t = 0; t < RT; ++t) lanes[t] = part_of(b, t, ctx);
         partial[b] = fold_block(lanes);
     }
     for (int t = 0; t < RT; ++t) {
@@ -794,6 +864,21 @@ static double canon_fold(int64_t nitems, canon_step step, const void* ctx) {
         lanes[t] = s;
     }
     return fold_block(lanes);
+}
+
+/* item i of a linear grid-stride loop belongs to thread (b,t) with i = b*RT + t (mod RB*RT) */
+typedef struct { int64_t nitems; canon_step step; const void* ctx; } linear_ctx;
+static double linear_part(int b, int t, const void* vctx) {
+    const linear_ctx* c = (const linear_ctx*)vctx;
+    double p = 0.0;
+    for (int64_t i = (int64_t)b * RT + t; i < c->nitems; i += (int64_t)RB * RT) p = c->step(p, i, c->ctx);
+    return p;
+}
+static int linear_active(int b, const void* vctx) { return (int64_t)b * RT < ((const linear_ctx*)vctx)->nitems; }
+
+static double canon_fold(int64_t nitems, canon_step step, const void* ctx) {
+    linear_ctx c = {nitems, step, ctx};
+    return canon_fold_threads(linear_part, linear_active, &c);
 }
 
 /* node-item step: sum over the three DOFs of node i of a*b (free vectors; fixed DOFs read 0) */
@@ -1367,7 +1452,7 @@ void orc_destroy(orc_problem* P) {
     free(P->ele_full); free(P->enod); free(P->bucket); free(P->isfree); free(P->free_dofs);
     free(P->dof2free); free(P->F);
     for (int l = 0; l < P->nlev; ++l) { free(P->lv[l].mask); free(P->lv[l].diag); free(P->lv[l].r); free(P->lv[l].x); }
-    free(P->Lc); free(P->tmpf); free(P->r); free(P->z); free(P->pp); free(P->Ap);
+    free(P->Lc); free(P->Xc); free(P->tmpf); free(P->r); free(P->z); free(P->pp); free(P->Ap);
     free(P->fdiag); free(P->flastx); free(P->flastrhs); free(P->frhs); free(P->fx); free(P->fr); free(P->fz);
     free(P->fp); free(P->fAp);
     free(P);
