@@ -99,6 +99,8 @@ _SIGS = {
                                  C.POINTER(C.c_int), _f32p]),
     "t3d_synchronize": (C.c_int, [_CTX]),
     "t3d_profile": (C.c_int, [_CTX, C.c_int, C.c_int, C.POINTER(C.c_double)]),
+    "t3d_compliance_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, _f64p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_void_p]),
 }
 T3D_PROFILE_MATVEC, T3D_PROFILE_VCYCLE = 0, 1
 

@@ -1,5 +1,7 @@
 // Host-side launchers of the B200 kernels.  All launches go to the given stream; none allocates.
 #pragma once
+#include <string>
+
 #include "t3d_common.cuh"
 
 namespace t3d {
@@ -9,6 +11,7 @@ struct Cuboid {          // solid region of the padded grid (fea.cpp:204-215)
 };
 
 int set_cuda_error(cudaError_t e, const char* what, const char* file, int line);
+int set_error(int code, const std::string& msg);
 
 struct MgLevel {         // one structured multigrid level (hierarchy.cpp:45-81)
     int nx, ny, nz, span;

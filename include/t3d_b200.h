@@ -143,6 +143,25 @@ int  t3d_synchronize(struct t3d_context* ctx);
 enum { T3D_PROFILE_MATVEC = 0, T3D_PROFILE_VCYCLE = 1 };
 int  t3d_profile(struct t3d_context* ctx, int what, int reps, double* ms);
 
+/* --------------------------------------------------------------- allocation-free compliance
+ * No counterpart in the reference.  For callers that cannot allocate device memory (a host that owns
+ * the device heap, a serving loop that must not enter the allocator, a caller without a context):
+ * ComputeCompliance on DEVICE pointers in the library's grid layout, with no cudaMalloc and no context.
+ *   d_E, d_ce : (nx+2)*(ny+2)*(nz+2) doubles, padded grid with a zero ghost ring; cell (cx,cy,cz) at
+ *               ((cz+1)*(ny+2)+cy+1)*(nx+2)+cx+1 is reference element (cx, ny-1-cy, cz); E = 0 off the
+ *               cuboid; d_ce is written for the nx*ny*nz interior cells;
+ *   d_u       : 3 planes of (nx+1)*(ny+1)*(nz+1) doubles, node (ix,iy,iz) of component c at
+ *               c*NN + (iz*(ny+1)+iy)*(nx+1)+ix, zero on fixed DOFs;
+ *   d_C       : one double, sum E*ce;  ke576: HOST pointer to Ke;  stream: a cudaStream_t (0 = default).
+ * nx,ny,nz are the padded counts of t3d_create for (nely,nelx,nelz).  Scratch: a static device array of
+ * 65536+1 doubles (512 KiB per GPU that loads the library, held until exit), one partial per 256
+ * padded cells, so grids above 16,777,216 padded cells are rejected with T3D_ERR_UNSUPPORTED.  The
+ * first call on a device looks up the array's address for that device (do it before any stream
+ * capture).  Every call shares the array: calls that overlap on the GPU race.  Asynchronous on
+ * `stream`. */
+int  t3d_compliance_noalloc(int nely, int nelx, int nelz, const double* ke576, const double* d_E, const double* d_u,
+                            double* d_ce, double* d_C, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
