@@ -95,6 +95,7 @@ _SIGS = {
     "t3d_design_step_host": (C.c_int, [_CTX, _f32p, _f32p, C.POINTER(IterRecord)]),
     "t3d_get_density": (C.c_int, [_CTX, _f32p]),
     "t3d_set_density": (C.c_int, [_CTX, _f32p]),
+    "t3d_get_displacement": (C.c_int, [_CTX, _f64p]),
     "t3d_run_global": (C.c_int, [_CTX, C.c_float, C.c_int, C.POINTER(C.c_double), C.POINTER(IterRecord),
                                  C.POINTER(C.c_int), _f32p]),
     "t3d_synchronize": (C.c_int, [_CTX]),
@@ -102,7 +103,7 @@ _SIGS = {
     "t3d_compliance_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, _f64p, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_void_p]),
 }
-T3D_PROFILE_MATVEC, T3D_PROFILE_VCYCLE = 0, 1
+T3D_PROFILE_MATVEC, T3D_PROFILE_VCYCLE, T3D_PROFILE_MATVEC32, T3D_PROFILE_VCYCLE32 = 0, 1, 2, 3
 
 _lib = None
 
@@ -322,6 +323,12 @@ class Problem:
     def set_density(self, x):
         _check(self._lib.t3d_set_density(self._h, _f32(x)))
 
+    def displacement(self):
+        """the design loop's displacement on the free DOFs (reference order)"""
+        u = np.zeros(self.nf)
+        _check(self._lib.t3d_get_displacement(self._h, u))
+        return u
+
     def run_global(self, V0, nLoop):
         """TOP3D_XL_GLOBAL for one simulation (driver.cpp:23-218): (Csolid, records, final x)."""
         recs = (IterRecord * max(1, nLoop))()
@@ -335,7 +342,8 @@ class Problem:
         _check(self._lib.t3d_synchronize(self._h))
 
     def profile(self, what, reps):
-        """mean ms per launch of the matvec (what=0) or V-cycle (what=1), CUDA events on the library stream"""
+        """mean ms per launch of the FP64 matvec (what=0) or V-cycle (what=1), or of their FP32 forms
+        (2, 3; precision T3D_MIXED only), CUDA events on the library stream"""
         ms = C.c_double()
         _check(self._lib.t3d_profile(self._h, int(what), int(reps), C.byref(ms)))
         return float(ms.value)

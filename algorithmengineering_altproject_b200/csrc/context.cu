@@ -153,6 +153,17 @@ struct Context {
     int* chol_status = nullptr;
     double *frhs = nullptr, *fx = nullptr, *fr = nullptr, *fz = nullptr, *fp = nullptr, *fAp = nullptr,
            *flastx = nullptr, *flastrhs = nullptr, *fdiag = nullptr;
+    // mixed precision (T3D_MIXED): FP32 inner-solve state
+    bool mixed = false;
+    float* Ke32 = nullptr;
+    float* E32 = nullptr;
+    float *r32 = nullptr, *d32 = nullptr, *z32 = nullptr, *p32 = nullptr, *Ap32 = nullptr;
+    MgLevel32 lv32[8]{};
+    float* ra1_32[8]{};
+    float* ra2_32[8]{};
+    PcgScalars* S32 = nullptr;
+    cudaGraphExec_t pcg32_graph = nullptr;
+    int last_outer = 0;
     // lazily built maps between the reference's layouts and the grid
     int32_t* morton = nullptr;          // [ne] cell index of the k-th element in Morton order
     std::vector<int32_t> morton_h;
@@ -192,6 +203,7 @@ struct Context {
 
     ~Context() {
         if (pcg_graph) cudaGraphExecDestroy(pcg_graph);
+        if (pcg32_graph) cudaGraphExecDestroy(pcg32_graph);
         for (auto& e : ev)
             if (e) cudaEventDestroy(e);
         for (void* q : allocs) cudaFree(q);
@@ -270,6 +282,37 @@ static int build_levels(Context* c) {
     return launch_check("mask restriction");
 }
 
+static int build_mixed(Context* c) {
+    const Grid& g = c->g;
+    CHECK(c->alloc(&c->Ke32, 576));
+    CHECK(c->alloc(&c->E32, g.NE));
+    for (float** v : {&c->r32, &c->d32, &c->z32, &c->p32, &c->Ap32}) {
+        CHECK(c->alloc(v, 3 * g.NN));
+        T3D_CUDA_OK(cudaMemsetAsync(*v, 0, 3 * g.NN * sizeof(float), c->st));
+    }
+    CHECK(c->alloc(&c->S32, 1));
+    T3D_CUDA_OK(cudaMemsetAsync(c->S32, 0, sizeof(PcgScalars), c->st));
+    for (int l = 0; l < c->nlev; ++l) {
+        const MgLevel& L = c->lv[l];
+        MgLevel32& M = c->lv32[l];
+        M.nx = L.nx; M.ny = L.ny; M.nz = L.nz; M.span = L.span; M.nn = L.nn; M.mask = L.mask;
+        CHECK(c->alloc(&M.diag, 3 * L.nn));
+        if (l > 0) {
+            CHECK(c->alloc(&M.r, 3 * L.nn));
+            CHECK(c->alloc(&M.x, 3 * L.nn));
+        }
+    }
+    for (int l = 0; l + 1 < c->nlev; ++l) {
+        const MgLevel &Lf = c->lv[l], &Lc = c->lv[l + 1];
+        CHECK(c->alloc(&c->ra1_32[l], (size_t)3 * (Lf.nz + 1) * (Lf.ny + 1) * (Lc.nx + 1)));
+        CHECK(c->alloc(&c->ra2_32[l], (size_t)3 * (Lf.nz + 1) * (Lc.ny + 1) * (Lc.nx + 1)));
+    }
+    float k32[576];
+    for (int i = 0; i < 576; ++i) k32[i] = (float)c->Ke_h[i];
+    T3D_CUDA_OK(cudaMemcpyAsync(c->Ke32, k32, sizeof k32, cudaMemcpyHostToDevice, c->st));
+    return sync(c);
+}
+
 static int create(int nely, int nelx, int nelz, const t3d_params* prm, Context* c) {
     if (nely <= 0 || nelx <= 0 || nelz <= 0) return set_error(T3D_ERR_INVALID, "element counts must be positive");
     int ndev = 0;
@@ -280,7 +323,9 @@ static int create(int nely, int nelx, int nelz, const t3d_params* prm, Context* 
     if (prm) c->prm = *prm;
     else t3d_params_default(&c->prm);
     if (c->prm.device < 0 || c->prm.device >= ndev) return set_error(T3D_ERR_NO_DEVICE, "device index out of range");
-    if (c->prm.precision != T3D_FP64) return set_error(T3D_ERR_UNSUPPORTED, "only T3D_FP64 precision is built");
+    if (c->prm.precision != T3D_FP64 && c->prm.precision != T3D_MIXED)
+        return set_error(T3D_ERR_UNSUPPORTED, "precision must be T3D_FP64 or T3D_MIXED");
+    c->mixed = c->prm.precision == T3D_MIXED;
     c->dev = c->prm.device;
     T3D_CUDA_OK(cudaSetDevice(c->dev));
     T3D_CUDA_OK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
@@ -358,6 +403,7 @@ static int create(int nely, int nelx, int nelz, const t3d_params* prm, Context* 
     }
     CHECK(launch_check("model set-up"));
     CHECK(build_levels(c));
+    if (c->mixed) CHECK(build_mixed(c));
     launch_filter_diag(g, c->solid, c->kf, c->fdiag, c->st);
     CHECK(launch_check("filter set-up"));
     return sync(c);
@@ -473,6 +519,10 @@ static int mg_setup(Context* c) {
         launch_cholesky(c->Kc, c->LT, c->Lrow, c->Nc, c->chol_status, c->st);
         launch_coarse_inverse(c->Lrow, c->Nc, c->chol_status, c->Xc, c->st);
     }
+    if (c->mixed) {
+        for (int l = 0; l < c->nlev; ++l) launch_cast(3 * c->lv[l].nn, c->lv[l].diag, c->lv32[l].diag, c->st);
+        c->launches += c->nlev;
+    }
     c->mg_ready = true;
     return launch_check("mg set-up");
 }
@@ -553,6 +603,113 @@ static int pcg_solve(Context* c, double tol, int maxit, int* iters) {
     return T3D_OK;
 }
 
+// ------------------------------------------------------------------ mixed-precision solve
+static void vcycle32(Context* c, const float* r, float* z, PcgScalars* S, RedSlot dot) {
+    const int L = c->nlev;
+    c->launches += 4 * (L - 1) + 1;
+    for (int l = 0; l + 1 < L; ++l)
+        launch_restrict32(c->lv32[l + 1], c->lv32[l], l == 0 ? r : c->lv32[l].r, c->lv32[l + 1].r, c->ra1_32[l],
+                          c->ra2_32[l], S, c->st);
+    launch_coarse_solve32(c->lv32[L - 1], c->Xc, c->Nc, c->chol_status, S, c->st);
+    for (int l = L - 2; l >= 1; --l)
+        launch_prolong_smooth32(c->lv32[l + 1], c->lv32[l], c->lv32[l + 1].x, c->lv32[l].r, c->lv32[l].x,
+                                c->prm.mg_weight, S, c->st);
+    launch_prolong_smooth0_32(c->lv32[1], c->lv32[0], c->lv32[1].x, r, z, c->prm.mg_weight, dot, S, c->st);
+}
+
+static void pcg32_iteration(Context* c) {
+    c->launches += 3;
+    launch_matvec32(c->g, c->Ke32, c->E32, c->mask0, c->p32, c->Ap32, c->slot[0], c->S32, c->st);
+    launch_pcg_update32(c->g, c->d32, c->r32, c->p32, c->Ap32, c->slot[1], c->S32, c->st);
+    vcycle32(c, c->r32, c->z32, c->S32, c->slot[2]);
+    launch_pcg_direction32(c->g, c->z32, c->p32, c->S32, c->st);
+}
+
+static int ensure_pcg32_graph(Context* c) {
+    if (!c->use_graph || c->pcg32_graph) return T3D_OK;
+    cudaGraph_t graph;
+    const int64_t l0 = c->launches;
+    T3D_CUDA_OK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < PCG_CHUNK; ++k) pcg32_iteration(c);
+    T3D_CUDA_OK(cudaStreamEndCapture(c->st, &graph));
+    c->launches = l0;
+    cudaError_t e = cudaGraphInstantiate(&c->pcg32_graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return set_cuda_error(e, "cudaGraphInstantiate", __FILE__, __LINE__);
+    return T3D_OK;
+}
+
+// Defect correction: r64 = b - K64 u64 (FP64), stop when |r64| < max(1e-30,|b|)*tol (the reference's
+// test, solver.cpp:149,184, applied to the true residual); else solve K32 d = r32 with the FP32
+// MG-PCG (at most the remaining budget of max_it iterations, inner target max(stop, 1e-5|r64|))
+// and add d to u64.  *iters = inner iterations used (max_it when the budget ran out unconverged).
+static int mixed_solve(Context* c, double tol, int maxit, int* iters) {
+    if (!c->mg_ready) return set_error(T3D_ERR_INVALID, "multigrid preconditioner not set up");
+    CHECK(ensure_pcg32_graph(c));
+    const Grid& g = c->g;
+    launch_cast(g.NE, c->E, c->E32, c->st);
+    launch_dot(g, 3, c->b, c->b, c->slot[3], c->scal + 5, c->st);
+    c->launches += 2;
+    T3D_CUDA_OK(cudaMemcpyAsync(c->scal_h + 5, c->scal + 5, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CHECK(sync(c));
+    const double nb = std::sqrt(c->scal_h[5]);
+    const double stop = (1.0e-30 < nb ? nb : 1.0e-30) * tol;
+    int budget = maxit, used = 0, outer = 0;
+    bool converged = false;
+    for (; outer < 64; ++outer) {
+        launch_matvec64(c->g, c->Ke, c->E, c->mask0, c->u, c->Ap, RedSlot{nullptr, nullptr}, nullptr, c->st);
+        launch_mixed_residual(g, c->b, c->Ap, c->r32, c->d32, c->slot[3], c->scal + 6, c->st);
+        c->launches += 2;
+        CHECK(launch_check("mixed residual"));
+        T3D_CUDA_OK(cudaMemcpyAsync(c->scal_h + 6, c->scal + 6, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        CHECK(sync(c));
+        const double rn = std::sqrt(c->scal_h[6]);
+        if (rn < stop) { converged = true; break; }
+        if (budget <= 0) break;
+        PcgScalars init{};
+        init.stop = std::max(stop, 1e-5 * rn);
+        init.tol = tol;
+        init.first = 1;
+        T3D_CUDA_OK(cudaMemcpyAsync(c->S32, &init, sizeof init, cudaMemcpyHostToDevice, c->st));
+        vcycle32(c, c->r32, c->z32, c->S32, c->slot[2]);
+        T3D_CUDA_OK(cudaMemcpyAsync(c->p32, c->z32, 3 * g.NN * sizeof(float), cudaMemcpyDeviceToDevice, c->st));
+        int queued = 0, chunk = 0;
+        bool done = false;
+        while (queued < budget && !done) {
+            const int n = std::min(PCG_CHUNK, budget - queued);
+            if (c->use_graph && n == PCG_CHUNK) {
+                T3D_CUDA_OK(cudaGraphLaunch(c->pcg32_graph, c->st));
+                c->launches += (int64_t)PCG_CHUNK * (3 + 4 * (c->nlev - 1) + 1);
+            } else {
+                for (int k = 0; k < n; ++k) pcg32_iteration(c);
+                CHECK(launch_check("pcg32 iteration"));
+            }
+            queued += n;
+            const int slot = chunk & 1;
+            T3D_CUDA_OK(cudaMemcpyAsync(&c->flag_h[slot], &c->S32->done, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+            T3D_CUDA_OK(cudaEventRecord(c->ev[slot], c->st));
+            if (chunk >= 1) {
+                T3D_CUDA_OK(cudaEventSynchronize(c->ev[slot ^ 1]));
+                done = c->flag_h[slot ^ 1] != 0;
+            }
+            ++chunk;
+        }
+        launch_mixed_accumulate(g, c->u, c->d32, c->st);
+        c->launches += 1;
+        T3D_CUDA_OK(cudaMemcpyAsync(c->S_h, c->S32, sizeof(PcgScalars), cudaMemcpyDeviceToHost, c->st));
+        CHECK(sync(c));
+        used += c->S_h->it;
+        budget -= c->S_h->it;
+    }
+    c->last_outer = outer;
+    *iters = converged ? used : maxit;
+    return T3D_OK;
+}
+
+static int solve(Context* c, double tol, int maxit, int* iters) {
+    return c->mixed ? mixed_solve(c, tol, maxit, iters) : pcg_solve(c, tol, maxit, iters);
+}
+
 // ------------------------------------------------------------------ PDE filter (filter.cpp:175-275)
 static int filter_apply(Context* c, const float* src_cells, float* dst_cells) {
     const Grid& g = c->g;
@@ -631,7 +788,7 @@ static int design_init(Context* c, float V0, double* Csolid) {
     T3D_CUDA_OK(cudaMemsetAsync(c->flastrhs, 0, c->g.NN * sizeof(double), c->st));
     CHECK(mg_setup(c));
     int its = 0;
-    CHECK(pcg_solve(c, (double)c->prm.cg_tol, c->prm.cg_max_it, &its));
+    CHECK(solve(c, (double)c->prm.cg_tol, c->prm.cg_max_it, &its));
     launch_compliance64(c->g, c->Ke, c->E, c->u, c->ce, c->slot[0], c->scal + 1, c->st);
     CHECK(launch_check("solid compliance"));
     T3D_CUDA_OK(cudaMemcpyAsync(c->scal_h, c->scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
@@ -652,7 +809,7 @@ static int design_step(Context* c, t3d_iter_record* rec) {
     c->launches += 5;   // simp, compliance, objective, sensitivities, dc scale
     if (c->loop == 1 || c->loop % 5 == 0) CHECK(mg_setup(c));
     int its = 0;
-    CHECK(pcg_solve(c, (double)P.cg_tol, P.cg_max_it, &its));
+    CHECK(solve(c, (double)P.cg_tol, P.cg_max_it, &its));
     T3D_CUDA_OK(cudaEventRecord(e1, c->st));
     launch_compliance64(g, c->Ke, c->E, c->u, c->ce, c->slot[0], c->scal + 0, c->st);
     launch_objective(g, c->E, c->ce, c->scal + 1, c->slot[1], c->scal + 2, c->st);
@@ -774,6 +931,11 @@ int t3d_set_ke(t3d_context* ctx, const double* ke) {
     if (!ke) return t3d::set_error(T3D_ERR_INVALID, "null Ke");
     std::memcpy(ctx->Ke_h, ke, sizeof ctx->Ke_h);
     T3D_CUDA_OK(cudaMemcpy(ctx->Ke, ctx->Ke_h, sizeof ctx->Ke_h, cudaMemcpyHostToDevice));
+    if (ctx->Ke32) {
+        float k32[576];
+        for (int i = 0; i < 576; ++i) k32[i] = (float)ctx->Ke_h[i];
+        T3D_CUDA_OK(cudaMemcpy(ctx->Ke32, k32, sizeof k32, cudaMemcpyHostToDevice));
+    }
     return T3D_OK;
 }
 
@@ -998,6 +1160,12 @@ int t3d_get_density(t3d_context* ctx, float* x) {
     return t3d::download_cells_f32(ctx, ctx->x, x);
 }
 
+int t3d_get_displacement(t3d_context* ctx, double* u) {
+    API_GUARD(ctx);
+    if (!u) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    return t3d::download_free(ctx, ctx->u, u);
+}
+
 int t3d_set_density(t3d_context* ctx, const float* x) {
     API_GUARD(ctx);
     if (!x) return t3d::set_error(T3D_ERR_INVALID, "null argument");
@@ -1031,16 +1199,30 @@ int t3d_synchronize(t3d_context* ctx) {
 
 int t3d_profile(t3d_context* ctx, int what, int reps, double* ms) {
     API_GUARD(ctx);
-    if (reps <= 0 || !ms || (what != T3D_PROFILE_MATVEC && what != T3D_PROFILE_VCYCLE))
+    if (reps <= 0 || !ms || what < T3D_PROFILE_MATVEC || what > T3D_PROFILE_VCYCLE32)
         return t3d::set_error(T3D_ERR_INVALID, "bad profile request");
-    if (what == T3D_PROFILE_VCYCLE && !ctx->mg_ready) return t3d::set_error(T3D_ERR_INVALID, "MG not set up");
+    if (what != T3D_PROFILE_MATVEC && !ctx->mg_ready) return t3d::set_error(T3D_ERR_INVALID, "MG not set up");
+    if (what >= T3D_PROFILE_MATVEC32 && !ctx->mixed)
+        return t3d::set_error(T3D_ERR_INVALID, "FP32 kernels need precision T3D_MIXED");
     T3D_CUDA_OK(cudaMemsetAsync(ctx->S, 0, sizeof(t3d::PcgScalars), ctx->st));
+    if (ctx->mixed) {   // the FP32 kernels see the FP32 images of the current E, p and r
+        T3D_CUDA_OK(cudaMemsetAsync(ctx->S32, 0, sizeof(t3d::PcgScalars), ctx->st));
+        t3d::launch_cast(ctx->g.NE, ctx->E, ctx->E32, ctx->st);
+        t3d::launch_cast(3 * ctx->g.NN, ctx->p, ctx->p32, ctx->st);
+        t3d::launch_cast(3 * ctx->g.NN, ctx->r, ctx->r32, ctx->st);
+    }
     auto once = [&]() {
         if (what == T3D_PROFILE_MATVEC) {
             t3d::launch_matvec64(ctx->g, ctx->Ke, ctx->E, ctx->mask0, ctx->p, ctx->Ap, ctx->slot[0], ctx->S, ctx->st);
             ctx->launches += 1;
-        } else {
+        } else if (what == T3D_PROFILE_VCYCLE) {
             t3d::vcycle(ctx, ctx->r, ctx->z, ctx->S, ctx->slot[2]);
+        } else if (what == T3D_PROFILE_MATVEC32) {
+            t3d::launch_matvec32(ctx->g, ctx->Ke32, ctx->E32, ctx->mask0, ctx->p32, ctx->Ap32, ctx->slot[0], ctx->S32,
+                                 ctx->st);
+            ctx->launches += 1;
+        } else {
+            t3d::vcycle32(ctx, ctx->r32, ctx->z32, ctx->S32, ctx->slot[2]);
         }
     };
     once();

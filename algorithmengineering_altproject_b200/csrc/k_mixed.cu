@@ -1,0 +1,398 @@
+// Mixed-precision solve: FP32 storage and arithmetic for the inner MG-preconditioned PCG (matvec,
+// smoother, transfers, vector updates) inside an FP64 defect-correction loop.  FP64 is kept for the
+// inner products and alpha/beta (device scalars), the true-residual recompute b - K64 u64 (the FP64
+// matvec), the coarsest-level factor and solve, and the accumulation u64 += d32.  Same algorithm as
+// the FP64 path (solver.cpp:87-217, preconditioner.cpp:88-265); only the storage precision differs.
+#include "kernels.hpp"
+#include "red.cuh"
+
+namespace t3d {
+
+namespace {
+
+__device__ __forceinline__ void node_ijk(const Grid& g, int n, int& ix, int& iy, int& iz) {
+    ix = n % g.nnx;
+    const int t = n / g.nnx;
+    iy = t % g.nny;
+    iz = t / g.nny;
+}
+
+__device__ __forceinline__ float hatf(int i, int s) {   // 1 - |i-(s-1)|/s, exact in binary for s = 2, 4
+    return 1.0f - fabsf((float)(i - (s - 1))) * (1.0f / s);
+}
+
+__global__ void k_cast(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+// r64 = b - A u64; r32 = (float)r64; d32 = 0; |r64|^2 into *rn2 (FP64)
+__global__ void __launch_bounds__(RED_THREADS) k_mixed_residual(Grid g, const double* __restrict__ b,
+                                                                const double* __restrict__ Au,
+                                                                float* __restrict__ r32, float* __restrict__ d32,
+                                                                RedSlot red, double* __restrict__ rn2) {
+    __shared__ double sh[32];
+    const int64_t n3 = 3 * g.NN;
+    double part = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (int64_t)gridDim.x * blockDim.x) {
+        const double rv = b[i] - Au[i];
+        r32[i] = (float)rv;
+        d32[i] = 0.0f;
+        part = fma(rv, rv, part);
+    }
+    double tot;
+    if (grid_fold(part, red, sh, &tot) && threadIdx.x == 0) *rn2 = tot;
+}
+
+// u64 += d32
+__global__ void k_mixed_accumulate(int64_t n3, double* __restrict__ u, const float* __restrict__ d) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (int64_t)gridDim.x * blockDim.x)
+        u[i] = u[i] + (double)d[i];
+}
+
+// ---------------------------------------------------------------- K(E) p in FP32
+// Node-centric gather in the colour order of the FP64 kernel; Ke rows read from shared memory as
+// float4; FP32 FMA chains; p.Ap folded in FP64.
+__global__ void __launch_bounds__(RED_THREADS) k_matvec32(Grid g, const float* __restrict__ Keg,
+                                                          const float* __restrict__ E,
+                                                          const uint8_t* __restrict__ mask,
+                                                          const float* __restrict__ u, float* __restrict__ y,
+                                                          RedSlot dot, PcgScalars* S) {
+    __shared__ __align__(16) float Ke[576];
+    __shared__ double sh[32];
+    if (S != nullptr && S->done) return;
+    for (int i = threadIdx.x; i < 576; i += blockDim.x) Ke[i] = Keg[i];
+    __syncthreads();
+    const int NN = (int)g.NN;
+    const float* __restrict__ u0 = u;
+    const float* __restrict__ u1 = u + NN;
+    const float* __restrict__ u2 = u + 2 * (int64_t)NN;
+    double part = 0.0;
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < NN; n += gridDim.x * blockDim.x) {
+        int ix, iy, iz;
+        node_ijk(g, n, ix, iy, iz);
+        float y0 = 0.0f, y1 = 0.0f, y2 = 0.0f;
+#pragma unroll 1
+        for (int col = 0; col < 8; ++col) {
+            const int cx = (((ix - 1) & 1) == (col & 1)) ? ix - 1 : ix;
+            const int cy = (((g.ny - iy) & 1) == ((col >> 1) & 1)) ? iy - 1 : iy;
+            const int cz = (((iz - 1) & 1) == ((col >> 2) & 1)) ? iz - 1 : iz;
+            const float Ee = E[g.cell(cx, cy, cz)];
+            if (Ee <= 1.0e-16f) continue;
+            const int a = corner_of(ix - cx, iy - cy, iz - cz);
+            float ue[24];
+#pragma unroll
+            for (int b = 0; b < 8; ++b) {
+                const int m = (int)g.node(cx + corner_dx(b), cy + corner_dy(b), cz + corner_dz(b));
+                ue[3 * b + 0] = u0[m];
+                ue[3 * b + 1] = u1[m];
+                ue[3 * b + 2] = u2[m];
+            }
+            const float4* K0 = reinterpret_cast<const float4*>(Ke + (3 * a) * 24);
+            float f0 = 0.0f, f1 = 0.0f, f2 = 0.0f;
+#pragma unroll
+            for (int j = 0; j < 24; j += 4) {
+                const float4 k0 = K0[j / 4], k1 = K0[6 + j / 4], k2 = K0[12 + j / 4];
+                f0 = fmaf(k0.x, ue[j], f0); f0 = fmaf(k0.y, ue[j + 1], f0);
+                f0 = fmaf(k0.z, ue[j + 2], f0); f0 = fmaf(k0.w, ue[j + 3], f0);
+                f1 = fmaf(k1.x, ue[j], f1); f1 = fmaf(k1.y, ue[j + 1], f1);
+                f1 = fmaf(k1.z, ue[j + 2], f1); f1 = fmaf(k1.w, ue[j + 3], f1);
+                f2 = fmaf(k2.x, ue[j], f2); f2 = fmaf(k2.y, ue[j + 1], f2);
+                f2 = fmaf(k2.z, ue[j + 2], f2); f2 = fmaf(k2.w, ue[j + 3], f2);
+            }
+            y0 = fmaf(f0, Ee, y0);
+            y1 = fmaf(f1, Ee, y1);
+            y2 = fmaf(f2, Ee, y2);
+        }
+        const int mk = mask[n];
+        if (mk & 1) y0 = 0.0f;
+        if (mk & 2) y1 = 0.0f;
+        if (mk & 4) y2 = 0.0f;
+        y[n] = y0;
+        y[NN + n] = y1;
+        y[2 * (int64_t)NN + n] = y2;
+        if (dot.partial) {
+            part = fma((double)u0[n], (double)y0, part);
+            part = fma((double)u1[n], (double)y1, part);
+            part = fma((double)u2[n], (double)y2, part);
+        }
+    }
+    if (dot.partial) {
+        double tot;
+        if (grid_fold(part, dot, sh, &tot) && threadIdx.x == 0) S->denom = tot;
+    }
+}
+
+// ---------------------------------------------------------------- V-cycle in FP32
+__global__ void k_restrict_x32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ rf, float* __restrict__ a1,
+                               const PcgScalars* S) {
+    if (S->done) return;
+    const int cnx = Lc.nx + 1, fnx = Lf.nx + 1, fny = Lf.ny + 1, fnz = Lf.nz + 1;
+    const int64_t total = (int64_t)fnz * fny * cnx;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const int cx = (int)(t % cnx);
+    const int64_t row = t / cnx;
+    const int s = Lc.span, ws = 2 * s - 1;
+    const int64_t fNN = Lf.nn;
+    const float* __restrict__ src = rf + row * fnx;
+    float v0 = 0.0f, v1 = 0.0f, v2 = 0.0f;
+    for (int ix = 0; ix < ws; ++ix) {
+        const int fx = cx * s + ix - (s - 1);
+        if (fx < 0 || fx >= fnx) continue;
+        const float w = hatf(ix, s);
+        v0 = fmaf(w, src[fx], v0);
+        v1 = fmaf(w, src[fNN + fx], v1);
+        v2 = fmaf(w, src[2 * fNN + fx], v2);
+    }
+    a1[t] = v0;
+    a1[total + t] = v1;
+    a1[2 * total + t] = v2;
+}
+
+__global__ void k_restrict_y32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ a1, float* __restrict__ a2,
+                               const PcgScalars* S) {
+    if (S->done) return;
+    const int cnx = Lc.nx + 1, cny = Lc.ny + 1, fny = Lf.ny + 1, fnz = Lf.nz + 1;
+    const int64_t total = (int64_t)fnz * cny * cnx, total1 = (int64_t)fnz * fny * cnx;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const int cx = (int)(t % cnx);
+    const int cy = (int)((t / cnx) % cny);
+    const int fz = (int)(t / ((int64_t)cnx * cny));
+    const int s = Lc.span, ws = 2 * s - 1;
+    float v0 = 0.0f, v1 = 0.0f, v2 = 0.0f;
+    for (int iy = 0; iy < ws; ++iy) {
+        const int fy = cy * s + iy - (s - 1);
+        if (fy < 0 || fy >= fny) continue;
+        const float w = hatf(iy, s);
+        const int64_t i = ((int64_t)fz * fny + fy) * cnx + cx;
+        v0 = fmaf(w, a1[i], v0);
+        v1 = fmaf(w, a1[total1 + i], v1);
+        v2 = fmaf(w, a1[2 * total1 + i], v2);
+    }
+    a2[t] = v0;
+    a2[total + t] = v1;
+    a2[2 * total + t] = v2;
+}
+
+__global__ void k_restrict_z32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ a2, float* __restrict__ rc,
+                               const PcgScalars* S) {
+    if (S->done) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= Lc.nn) return;
+    const int cnx = Lc.nx + 1, cny = Lc.ny + 1;
+    const int fnx = Lf.nx + 1, fny = Lf.ny + 1, fnz = Lf.nz + 1;
+    const int cx = n % cnx, cy = (n / cnx) % cny, cz = n / (cnx * cny);
+    const int s = Lc.span, ws = 2 * s - 1;
+    const int64_t total2 = (int64_t)fnz * cny * cnx;
+    float swx = 0.0f, swy = 0.0f, swz = 0.0f;
+    for (int i = 0; i < ws; ++i) {
+        const int fx = cx * s + i - (s - 1), fy = cy * s + i - (s - 1);
+        if (fx >= 0 && fx < fnx) swx += hatf(i, s);
+        if (fy >= 0 && fy < fny) swy += hatf(i, s);
+    }
+    float v0 = 0.0f, v1 = 0.0f, v2 = 0.0f;
+    for (int iz = 0; iz < ws; ++iz) {
+        const int fz = cz * s + iz - (s - 1);
+        if (fz < 0 || fz >= fnz) continue;
+        const float w = hatf(iz, s);
+        swz += w;
+        const int64_t i = ((int64_t)fz * cny + cy) * cnx + cx;
+        v0 = fmaf(w, a2[i], v0);
+        v1 = fmaf(w, a2[total2 + i], v1);
+        v2 = fmaf(w, a2[2 * total2 + i], v2);
+    }
+    const float iw = 1.0f / (swz * swy * swx);
+    const int m = Lc.mask[n];
+    rc[n] = (m & 1) ? 0.0f : v0 * iw;
+    rc[Lc.nn + n] = (m & 2) ? 0.0f : v1 * iw;
+    rc[2 * Lc.nn + n] = (m & 4) ? 0.0f : v2 * iw;
+}
+
+__device__ __forceinline__ void prolong_node32(const MgLevel32& Lc, const float* __restrict__ xc, int fx, int fy,
+                                               int fz, float P[3]) {
+    const int s = Lc.span;
+    const int cnx = Lc.nx + 1, cny = Lc.ny + 1;
+    int cx = fx / s, cy = fy / s, cz = fz / s;
+    int rx = fx % s, ry = fy % s, rz = fz % s;
+    if (cx >= Lc.nx) { cx = Lc.nx - 1; rx = s; }
+    if (cy >= Lc.ny) { cy = Lc.ny - 1; ry = s; }
+    if (cz >= Lc.nz) { cz = Lc.nz - 1; rz = s; }
+    const float inv = 1.0f / s;
+    const float wx1 = rx * inv, wx0 = 1.0f - wx1;
+    const float wy1 = ry * inv, wy0 = 1.0f - wy1;
+    const float wz1 = rz * inv, wz0 = 1.0f - wz1;
+    const int b = (cz * cny + cy) * cnx + cx;
+    const int pz = cnx * cny;
+    for (int c = 0; c < 3; ++c) {
+        const float* X = xc + c * Lc.nn;
+        const float lo = fmaf(wy1, fmaf(wx1, X[b + cnx + 1], wx0 * X[b + cnx]), wy0 * fmaf(wx1, X[b + 1], wx0 * X[b]));
+        const float hi = fmaf(wy1, fmaf(wx1, X[b + pz + cnx + 1], wx0 * X[b + pz + cnx]),
+                              wy0 * fmaf(wx1, X[b + pz + 1], wx0 * X[b + pz]));
+        P[c] = fmaf(wz1, hi, wz0 * lo);
+    }
+}
+
+__global__ void k_prolong_smooth32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ xc,
+                                   const float* __restrict__ rf, float* __restrict__ xf, float w,
+                                   const PcgScalars* S) {
+    if (S->done) return;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= Lf.nn) return;
+    const int fnx = Lf.nx + 1, fny = Lf.ny + 1;
+    const int fx = n % fnx, fy = (n / fnx) % fny, fz = n / (fnx * fny);
+    float P[3];
+    prolong_node32(Lc, xc, fx, fy, fz, P);
+    const int m = Lf.mask[n];
+    for (int c = 0; c < 3; ++c) {
+        const float t = w * rf[c * Lf.nn + n] / fmaxf(1.0e-30f, Lf.diag[c * Lf.nn + n]);
+        xf[c * Lf.nn + n] = ((m >> c) & 1) ? 0.0f : (t + P[c]) + t;
+    }
+}
+
+__global__ void __launch_bounds__(RED_THREADS) k_prolong_smooth0_32(MgLevel32 Lc, MgLevel32 Lf,
+                                                                    const float* __restrict__ xc,
+                                                                    const float* __restrict__ r,
+                                                                    float* __restrict__ z, float w, RedSlot dot,
+                                                                    PcgScalars* S) {
+    __shared__ double sh[32];
+    if (S->done) return;
+    const int NN = (int)Lf.nn;
+    const int fnx = Lf.nx + 1, fny = Lf.ny + 1;
+    double part = 0.0;
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < NN; n += gridDim.x * blockDim.x) {
+        const int fx = n % fnx, fy = (n / fnx) % fny, fz = n / (fnx * fny);
+        float P[3];
+        prolong_node32(Lc, xc, fx, fy, fz, P);
+        const int m = Lf.mask[n];
+        for (int c = 0; c < 3; ++c) {
+            const float rv = r[c * (int64_t)NN + n];
+            const float t = w * rv / fmaxf(1.0e-30f, Lf.diag[c * (int64_t)NN + n]);
+            const float zv = ((m >> c) & 1) ? 0.0f : (t + P[c]) + t;
+            z[c * (int64_t)NN + n] = zv;
+            part = fma((double)rv, (double)zv, part);
+        }
+    }
+    double tot;
+    if (grid_fold(part, dot, sh, &tot) && threadIdx.x == 0) {
+        if (S->first) {
+            S->rz = tot;
+            S->first = 0;
+        } else {
+            const double rz = S->rz;
+            S->beta = tot / (1.0e-30 < rz ? rz : 1.0e-30);
+            S->rz = tot;
+        }
+    }
+}
+
+// coarsest level: FP64 inverse applied to the FP32 residual in FP64, or the Jacobi fallback
+__global__ void __launch_bounds__(128) k_coarse_solve32(MgLevel32 L, const double* __restrict__ X, int N,
+                                                        const int* __restrict__ status, const PcgScalars* S) {
+    extern __shared__ double rs[];
+    if (S->done) return;
+    const int64_t nn = L.nn;
+    if (*status != 1) {
+        for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x) {
+            const int m = L.mask[n];
+            for (int c = 0; c < 3; ++c)
+                L.x[c * nn + n] = ((m >> c) & 1) ? 0.0f : L.r[c * nn + n] / fmaxf(1.0e-30f, L.diag[c * nn + n]);
+        }
+        return;
+    }
+    for (int j = threadIdx.x; j < N; j += blockDim.x) rs[j] = (double)L.r[(j % 3) * nn + j / 3];
+    __syncthreads();
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double acc = 0.0;
+    for (int j = 0; j < N; ++j) acc = fma(X[(int64_t)j * N + i], rs[j], acc);
+    const int ni = i / 3, ci = i % 3;
+    L.x[ci * nn + ni] = ((L.mask[ni] >> ci) & 1) ? 0.0f : (float)acc;
+}
+
+// ---------------------------------------------------------------- PCG vector steps in FP32
+__global__ void __launch_bounds__(RED_THREADS) k_pcg_update32(Grid g, float* __restrict__ x, float* __restrict__ r,
+                                                              const float* __restrict__ p,
+                                                              const float* __restrict__ Ap, RedSlot red,
+                                                              PcgScalars* S) {
+    __shared__ double sh[32];
+    if (S->done) return;
+    const double den = S->denom;
+    const float alpha = (float)(S->rz / (1.0e-30 < den ? den : 1.0e-30));
+    const int64_t n3 = 3 * g.NN;
+    double part = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] = fmaf(alpha, p[i], x[i]);
+        const float rv = fmaf(-alpha, Ap[i], r[i]);
+        r[i] = rv;
+        part = fma((double)rv, (double)rv, part);
+    }
+    double tot;
+    if (grid_fold(part, red, sh, &tot) && threadIdx.x == 0) {
+        S->rnorm2 = tot;
+        S->it = S->it + 1;
+        if (sqrt(tot) < S->stop) {
+            S->done = 1;
+            S->result = S->it;
+        }
+    }
+}
+
+__global__ void k_pcg_direction32(Grid g, const float* __restrict__ z, float* __restrict__ p, PcgScalars* S) {
+    if (S->done) return;
+    const float beta = (float)S->beta;
+    const int64_t n3 = 3 * g.NN;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = fmaf(beta, p[i], z[i]);
+}
+
+inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+void launch_cast(int64_t n, const double* a, float* b, cudaStream_t s) {
+    k_cast<<<RED_BLOCKS, 256, 0, s>>>(n, a, b);
+}
+void launch_mixed_residual(const Grid& g, const double* b, const double* Au, float* r32, float* d32, RedSlot red,
+                           double* rn2, cudaStream_t s) {
+    k_mixed_residual<<<RED_BLOCKS, RED_THREADS, 0, s>>>(g, b, Au, r32, d32, red, rn2);
+}
+void launch_mixed_accumulate(const Grid& g, double* u, const float* d, cudaStream_t s) {
+    k_mixed_accumulate<<<RED_BLOCKS, 256, 0, s>>>(3 * g.NN, u, d);
+}
+void launch_matvec32(const Grid& g, const float* Ke, const float* E, const uint8_t* mask, const float* u, float* y,
+                     RedSlot dot, PcgScalars* S, cudaStream_t s) {
+    k_matvec32<<<RED_BLOCKS, RED_THREADS, 0, s>>>(g, Ke, E, mask, u, y, dot, S);
+}
+void launch_restrict32(const MgLevel32& Lc, const MgLevel32& Lf, const float* rf, float* rc, float* a1, float* a2,
+                       const PcgScalars* S, cudaStream_t s) {
+    const int64_t n1 = (int64_t)(Lf.nz + 1) * (Lf.ny + 1) * (Lc.nx + 1);
+    const int64_t n2 = (int64_t)(Lf.nz + 1) * (Lc.ny + 1) * (Lc.nx + 1);
+    k_restrict_x32<<<blocks_for(n1, 256), 256, 0, s>>>(Lc, Lf, rf, a1, S);
+    k_restrict_y32<<<blocks_for(n2, 256), 256, 0, s>>>(Lc, Lf, a1, a2, S);
+    k_restrict_z32<<<blocks_for(Lc.nn, 128), 128, 0, s>>>(Lc, Lf, a2, rc, S);
+}
+void launch_prolong_smooth32(const MgLevel32& Lc, const MgLevel32& Lf, const float* xc, const float* rf, float* xf,
+                             float w, const PcgScalars* S, cudaStream_t s) {
+    k_prolong_smooth32<<<blocks_for(Lf.nn, 256), 256, 0, s>>>(Lc, Lf, xc, rf, xf, w, S);
+}
+void launch_prolong_smooth0_32(const MgLevel32& Lc, const MgLevel32& Lf, const float* xc, const float* r, float* z,
+                               float w, RedSlot dot, PcgScalars* S, cudaStream_t s) {
+    k_prolong_smooth0_32<<<RED_BLOCKS, RED_THREADS, 0, s>>>(Lc, Lf, xc, r, z, w, dot, S);
+}
+void launch_coarse_solve32(const MgLevel32& L, const double* X, int N, const int* status, const PcgScalars* S,
+                           cudaStream_t s) {
+    const int64_t work = N > 0 ? N : L.nn;
+    const unsigned blocks = (unsigned)((work + 127) / 128 > 0 ? (work + 127) / 128 : 1);
+    k_coarse_solve32<<<blocks, 128, (size_t)(N > 0 ? N : 1) * sizeof(double), s>>>(L, X, N, status, S);
+}
+void launch_pcg_update32(const Grid& g, float* x, float* r, const float* p, const float* Ap, RedSlot red,
+                         PcgScalars* S, cudaStream_t s) {
+    k_pcg_update32<<<RED_BLOCKS, RED_THREADS, 0, s>>>(g, x, r, p, Ap, red, S);
+}
+void launch_pcg_direction32(const Grid& g, const float* z, float* p, PcgScalars* S, cudaStream_t s) {
+    k_pcg_direction32<<<RED_BLOCKS, RED_THREADS, 0, s>>>(g, z, p, S);
+}
+
+}  // namespace t3d

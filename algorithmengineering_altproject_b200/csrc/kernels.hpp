@@ -22,6 +22,15 @@ struct MgLevel {         // one structured multigrid level (hierarchy.cpp:45-81)
     uint8_t* mask;       // per node, bit c = fixed
 };
 
+struct MgLevel32 {       // FP32 copy of a level's vectors for the mixed-precision inner solve
+    int nx, ny, nz, span;
+    int64_t nn;
+    float* r;
+    float* x;
+    float* diag;
+    const uint8_t* mask;  // shared with the FP64 level
+};
+
 // ---- model set-up (fea.cpp:181-447)
 void launch_setup_cells(const Grid& g, Cuboid c, uint8_t* solid, cudaStream_t s);
 void launch_setup_mask0(const Grid& g, const uint8_t* solid, uint8_t* mask, cudaStream_t s);
@@ -131,5 +140,24 @@ void launch_oc_finish(const Grid& g, const uint8_t* solid, float* x, const float
                       int64_t ne, RedSlot r1, RedSlot r2, cudaStream_t s);
 // reference-order sharpness and volume fraction
 void launch_oc_vec8_stats(int64_t ne, const int32_t* morton_cells, const float* x, OcState* st, cudaStream_t s);
+
+// ---- mixed precision (k_mixed.cu)
+void launch_cast(int64_t n, const double* a, float* b, cudaStream_t s);
+void launch_mixed_residual(const Grid& g, const double* b, const double* Au, float* r32, float* d32, RedSlot red,
+                           double* rn2, cudaStream_t s);
+void launch_mixed_accumulate(const Grid& g, double* u, const float* d, cudaStream_t s);
+void launch_matvec32(const Grid& g, const float* Ke, const float* E, const uint8_t* mask, const float* u, float* y,
+                     RedSlot dot, PcgScalars* S, cudaStream_t s);
+void launch_restrict32(const MgLevel32& Lc, const MgLevel32& Lf, const float* rf, float* rc, float* a1, float* a2,
+                       const PcgScalars* S, cudaStream_t s);
+void launch_prolong_smooth32(const MgLevel32& Lc, const MgLevel32& Lf, const float* xc, const float* rf, float* xf,
+                             float w, const PcgScalars* S, cudaStream_t s);
+void launch_prolong_smooth0_32(const MgLevel32& Lc, const MgLevel32& Lf, const float* xc, const float* r, float* z,
+                               float w, RedSlot dot, PcgScalars* S, cudaStream_t s);
+void launch_coarse_solve32(const MgLevel32& L, const double* X, int N, const int* status, const PcgScalars* S,
+                           cudaStream_t s);
+void launch_pcg_update32(const Grid& g, float* x, float* r, const float* p, const float* Ap, RedSlot red,
+                         PcgScalars* S, cudaStream_t s);
+void launch_pcg_direction32(const Grid& g, const float* z, float* p, PcgScalars* S, cudaStream_t s);
 
 }  // namespace t3d

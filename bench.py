@@ -2,8 +2,13 @@
 sensitivities -> PDE filter -> OC) on the reference's cantilever.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--config c2]
+                    [--precision mixed|fp64] [--compare-steps S] [--kernels-only --reps R]
 
-Prints ONE JSON line (rank 0).  A step is one design iteration.  `value` = design iterations/s
+Prints ONE JSON line (rank 0).  A step is one design iteration.  The default form is the mixed-
+precision one (FP32 inner MG-PCG inside FP64 defect correction); before the timed run, S design
+iterations are run by both the mixed and the plain FP64 form from the same densities, and
+`vs_fp64` reports the speed ratio and the compliance / displacement / density errors.
+`value` = design iterations/s
 over the whole job, timed on the device (CUDA events recorded by the library on its stream; max
 over ranks); `e2e` = the same metric through the host-buffer C-ABI call t3d_design_step_host
 (H2D of the design field, D2H of the updated field, wall clock).  Multi-GPU runs are independent
@@ -39,20 +44,29 @@ CONFIGS = {
                name="cantilever 96x192x96 (1,769,472 elements, 5,419,584 free DOF)"),
     "c2": dict(nely=256, nelx=512, nelz=256, V0=0.08, max_levels=6,
                name="cantilever 256x512x256 (33,554,432 elements, 101,451,264 free DOF)"),
+    # kernel-capture size: vectors above L2, a few GB on the device
+    "k1": dict(nely=160, nelx=320, nelz=160, V0=0.08, max_levels=5,
+               name="cantilever 160x320x160 (8,192,000 elements)"),
 }
 DEFAULT_CONFIG = "c2"
 METRIC = "design iterations/s"
 MEASURED_PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
-TRAFFIC_NOTE = os.path.join(ROOT, "profiles", "matvec_fp64_traffic.md")
+TRAFFIC_NOTE = os.path.join(ROOT, "profiles", "matvec_traffic.md")
 
 
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default=DEFAULT_CONFIG, choices=sorted(CONFIGS))
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--compare-steps", type=int, default=2,
+                    help="design iterations run by both forms from the same density (mixed vs FP64 errors)")
+    ap.add_argument("--kernels-only", action="store_true",
+                    help="time the matvec and V-cycle alone on the config's grid (for ncu captures)")
+    ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -119,10 +133,10 @@ def hbm_peak():
         return 6650.0, "fallback"
 
 
-def traffic_per_launch():
-    """dram read+write bytes per matvec launch from the committed ncu summary, if present."""
+def traffic_per_launch(kernel):
+    """dram read+write bytes per full-size launch of `kernel` from the committed ncu summary, if present."""
     try:
-        m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(TRAFFIC_NOTE).read())
+        m = re.search(kernel + r"_traffic_bytes_per_launch:\s*([0-9.eE+]+)", open(TRAFFIC_NOTE).read())
         return float(m.group(1)) if m else None
     except OSError:
         return None
@@ -188,6 +202,71 @@ def run_reference_arm(args):
 
 
 # ---------------------------------------------------------------- B200 arm
+def matvec_roofline(P, mixed, mv_ms):
+    """roofline of K(E)p (+ p.Ap): algorithmic bytes = w*(2 n_free + n_elements), w = 4 (FP32) or 8."""
+    w = 4 if mixed else 8
+    alg_bytes = w * (2 * P.nf + P.ne)
+    achieved = alg_bytes / (mv_ms * 1e-3) / 1e9
+    peak, peak_kind = hbm_peak()
+    flops = 1152 * P.ne
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic_per_launch("matvec32" if mixed else "matvec64"), "peak_source": peak_kind,
+            "kernel": "k_matvec32 (FP32 K(E)p + FP64 p.Ap)" if mixed else "k_matvec64 (K(E)p + p.Ap)",
+            "algorithmic_bytes_per_launch": alg_bytes, "flops_per_launch": flops,
+            "tflops": flops / (mv_ms * 1e-3) / 1e12, "ms": mv_ms}
+
+
+def run_kernels_only(args):
+    """K(E)p and one V-cycle timed alone with CUDA events on a design-like state (E = SIMP of V0)."""
+    import algorithmengineering_altproject_b200 as t3d
+    cfg = CONFIGS[args.config]
+    mixed = args.precision == "mixed"
+    P = t3d.Problem(cfg["nely"], cfg["nelx"], cfg["nelz"], mg_max_levels=cfg["max_levels"],
+                    precision=t3d.T3D_MIXED if mixed else t3d.T3D_FP64)
+    rng = np.random.default_rng(7)
+    E = np.full(P.ne, 1e-9 + cfg["V0"] ** 3 * (1.0 - 1e-9))
+    P.make_diagonal_preconditioner_from_static(E)
+    P.K_times_u_finest(E, rng.standard_normal(P.nf))     # leaves p on the device
+    P.vcycle(rng.standard_normal(P.nf))                  # leaves r on the device
+    mv = P.profile(t3d.T3D_PROFILE_MATVEC32 if mixed else t3d.T3D_PROFILE_MATVEC, args.reps)
+    vc = P.profile(t3d.T3D_PROFILE_VCYCLE32 if mixed else t3d.T3D_PROFILE_VCYCLE, args.reps)
+    print(json.dumps({"config": cfg["name"], "precision": args.precision, "matvec_ms": mv, "vcycle_ms": vc,
+                      "roofline": matvec_roofline(P, mixed, mv)}), flush=True)
+    P.close()
+    return 0
+
+
+def compare_forms(cfg, dev, steps):
+    """Mixed vs plain FP64 on the same designs: both forms run `steps` design iterations, the mixed one
+    starting each iteration from the FP64 one's density.  Returns speeds and relative errors."""
+    import algorithmengineering_altproject_b200 as t3d
+    kw = dict(device=dev, mg_max_levels=cfg["max_levels"], oc_sum_order=t3d.T3D_SUM_FP64)
+    F = t3d.Problem(cfg["nely"], cfg["nelx"], cfg["nelz"], precision=t3d.T3D_FP64, **kw)
+    M = t3d.Problem(cfg["nely"], cfg["nelx"], cfg["nelz"], precision=t3d.T3D_MIXED, **kw)
+    csF, csM = F.design_init(cfg["V0"]), M.design_init(cfg["V0"])
+    out = {"c_solid_rel_err": abs(csM - csF) / abs(csF), "iterations": []}
+    tF = tM = 0.0
+    for _ in range(steps):
+        M.set_density(F.density())
+        rF, rM = F.design_step(), M.design_step()
+        uF, uM = F.displacement(), M.displacement()
+        xF, xM = F.density(), M.density()
+        tF += rF["t_total"]
+        tM += rM["t_total"]
+        out["iterations"].append({
+            "loop": rF["loop"], "pcg_iters_fp64": rF["pcg_iters"], "pcg_iters_mixed": rM["pcg_iters"],
+            "compliance_rel_err": abs(rM["obj"] - rF["obj"]) / abs(rF["obj"]),
+            "displacement_rel_l2_err": float(np.linalg.norm(uM - uF) / np.linalg.norm(uF)),
+            "density_max_abs_err": float(np.max(np.abs(xM.astype(np.float64) - xF))),
+            "s_fp64": rF["t_total"], "s_mixed": rM["t_total"]})
+    out["fp64_design_iter_per_s"] = steps / tF
+    out["mixed_design_iter_per_s"] = steps / tM
+    out["speedup_mixed_vs_fp64"] = tF / tM
+    F.close()
+    M.close()
+    return out
+
+
 def run_b200(args):
     import torch
     import algorithmengineering_altproject_b200 as t3d
@@ -201,9 +280,12 @@ def run_b200(args):
     dev = local
     torch.cuda.set_device(dev)
     cfg = CONFIGS[args.config]
+    mixed = args.precision == "mixed"
+
+    comparison = compare_forms(cfg, dev, args.compare_steps) if (mixed and args.compare_steps > 0) else None
 
     P = t3d.Problem(cfg["nely"], cfg["nelx"], cfg["nelz"], device=dev, mg_max_levels=cfg["max_levels"],
-                    oc_sum_order=t3d.T3D_SUM_FP64)
+                    oc_sum_order=t3d.T3D_SUM_FP64, precision=t3d.T3D_MIXED if mixed else t3d.T3D_FP64)
     P.design_init(cfg["V0"])
     for _ in range(args.warmup):
         P.design_step()
@@ -225,11 +307,11 @@ def run_b200(args):
     clk = clocks.stop()
     dev_time = sum(r["t_total"] for r in recs)
 
-    # roofline of the dominant kernel (K(E)p with fused p.Ap), CUDA events on the library stream
-    mv_ms = P.profile(t3d.T3D_PROFILE_MATVEC, 20)
-    vc_ms = P.profile(t3d.T3D_PROFILE_VCYCLE, 10)
+    # the dominant kernel (K(E)p with the fused p.Ap) and one V-cycle, CUDA events on the library stream
+    mv_ms = P.profile(t3d.T3D_PROFILE_MATVEC32 if mixed else t3d.T3D_PROFILE_MATVEC, args.reps)
+    vc_ms = P.profile(t3d.T3D_PROFILE_VCYCLE32 if mixed else t3d.T3D_PROFILE_VCYCLE, max(1, args.reps // 2))
 
-    # end to end through host buffers
+    # end to end through host buffers: the design field goes host -> device -> host every iteration
     e2e = None
     if not args.no_e2e:
         x = torch.empty(P.ne, dtype=torch.float32, pin_memory=True).numpy()
@@ -239,9 +321,8 @@ def run_b200(args):
         for _ in range(args.steps):
             xo, _ = P.design_step_host(x)
             x[:] = xo
-        e2e_t = time.perf_counter() - t0
         barrier()
-        e2e = e2e_t
+        e2e = time.perf_counter() - t0
 
     times = torch.tensor([dev_time, t_wall, e2e if e2e is not None else 0.0], dtype=torch.float64, device="cuda")
     if world > 1:
@@ -249,34 +330,31 @@ def run_b200(args):
     dev_time, t_wall, e2e = [float(v) for v in times.cpu()]
 
     if rank == 0:
-        w = 8
-        ne, nf = P.ne, P.nf
-        alg_bytes = w * (2 * nf + ne)              # read p, write Ap (free DOFs), read E
-        achieved = alg_bytes / (mv_ms * 1e-3) / 1e9
-        peak, peak_kind = hbm_peak()
+        ne = P.ne
         pcg_its = [r["pcg_iters"] for r in recs]
         line = {
             "metric": METRIC, "value": world * args.steps / dev_time, "unit": "design iter/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * dev_time / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64 (mixed)" if mixed else "f64",
             "data": "synthetic (the reference's built-in cantilever load case; no dataset involved)",
             "config": {"workload": cfg["name"], "V0": cfg["V0"], "mg_max_levels": cfg["max_levels"],
-                       "mg_levels": P.nlev, "coarse_dofs": P.coarse_n, "precision": "fp64 (plain GPU form)",
+                       "mg_levels": P.nlev, "coarse_dofs": P.coarse_n,
+                       "precision": ("mixed: FP32 inner MG-PCG in FP64 defect correction" if mixed
+                                     else "fp64 (plain GPU form)"),
                        "oc_volume_sum": "fp64", "parallelism": "replicas" if world > 1 else "single GPU",
-                       "l2": "inputs larger than L2 (node vectors %.0f MB each)" % (3 * P.nn * 8 / 1e6)},
+                       "l2": "inputs larger than L2 (node vectors %.0f MB each)" % (3 * P.nn * (4 if mixed else 8) / 1e6)},
             "pcg_iterations": pcg_its,
             "per_kernel_ms": {"matvec": mv_ms, "vcycle": vc_ms,
                               "pcg_iteration": 1000.0 * sum(r["t_cg"] for r in recs) / max(1, sum(pcg_its))},
-            "throughput": {"dof_matvecs_per_s": nf / (mv_ms * 1e-3), "vcycles_per_s": 1.0 / (vc_ms * 1e-3)},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic_per_launch(), "peak_source": peak_kind,
-                         "kernel": "k_matvec64 (K(E)p + p.Ap)", "algorithmic_bytes_per_launch": alg_bytes,
-                         "fp64_flops_per_launch": 1152 * ne,
-                         "fp64_tflops": 1152 * ne / (mv_ms * 1e-3) / 1e12},
+            "throughput": {"dof_matvecs_per_s": P.nf / (mv_ms * 1e-3), "vcycles_per_s": 1.0 / (vc_ms * 1e-3)},
+            "roofline": matvec_roofline(P, mixed, mv_ms),
             "clocks": clk,
             "gpu_launches": launches,
             "wall_s_timed": t_wall,
         }
+        if comparison is not None:
+            line["vs_fp64"] = comparison
         if e2e:
             line["e2e"] = {"value": world * args.steps / e2e, "unit": "design iter/s",
                            "h2d_bytes_per_step": 4 * ne, "d2h_bytes_per_step": 4 * ne + 64}
@@ -300,6 +378,8 @@ def main():
     args = parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.kernels_only:
+        return run_kernels_only(args)
     return run_b200(args)
 
 

@@ -36,7 +36,9 @@ enum {
 };
 
 enum { T3D_SUM_REFERENCE = 0, T3D_SUM_FP64 = 1 };   /* OC volume / sharpness summation order */
-enum { T3D_FP64 = 0, T3D_MIXED = 1 };              /* solver precision */
+/* solver precision of the design loop: T3D_FP64 = PCG_free in FP64; T3D_MIXED = FP32 inner MG-PCG (FP64
+ * inner products, alpha/beta, coarsest solve) inside FP64 defect correction on the true residual */
+enum { T3D_FP64 = 0, T3D_MIXED = 1 };
 
 typedef struct t3d_params {
     float E0, Emin, nu, penal;    /* GlobalParams core.hpp:26-33 (Ke always uses nu = 0.3, fea.cpp:345) */
@@ -47,7 +49,7 @@ typedef struct t3d_params {
     float mg_weight;
     float filter_rmin;            /* top3d_cli.cpp:33: sqrt(3) cells */
     int   oc_sum_order;           /* T3D_SUM_REFERENCE (bit-identical bisection) or T3D_SUM_FP64 */
-    int   precision;              /* T3D_FP64 */
+    int   precision;              /* T3D_FP64 or T3D_MIXED (design loop only; t3d_pcg is always FP64) */
     int   device;                 /* CUDA device ordinal */
     int   reserved[7];
 } t3d_params;
@@ -130,6 +132,8 @@ int  t3d_design_step(struct t3d_context* ctx, t3d_iter_record* rec);
 int  t3d_design_step_host(struct t3d_context* ctx, const float* x_in, float* x_out, t3d_iter_record* rec);
 int  t3d_get_density(struct t3d_context* ctx, float* x);
 int  t3d_set_density(struct t3d_context* ctx, const float* x);
+/* the design loop's displacement U restricted to the free DOFs (driver.cpp:128-136 uFreeWarm) */
+int  t3d_get_displacement(struct t3d_context* ctx, double* u_free);
 /* TOP3D_XL_GLOBAL (driver.hpp:4, driver.cpp:23-280) for one simulation: records[nLoop], x_final[num_elements] */
 int  t3d_run_global(struct t3d_context* ctx, float V0, int n_loop, double* c_solid, t3d_iter_record* records,
                     int* n_records, float* x_final);
@@ -140,7 +144,9 @@ int  t3d_synchronize(struct t3d_context* ctx);
  * context's stream, after one untimed launch: T3D_PROFILE_MATVEC = K(E)p with the fused p.Ap,
  * T3D_PROFILE_VCYCLE = one V-cycle z = M r.  Operates on the current device state (E, p, r) and
  * overwrites Ap / z; *ms = mean milliseconds per launch. */
-enum { T3D_PROFILE_MATVEC = 0, T3D_PROFILE_VCYCLE = 1 };
+/* T3D_PROFILE_MATVEC32 / T3D_PROFILE_VCYCLE32: the FP32 forms of the mixed-precision inner solve
+ * (contexts created with precision T3D_MIXED only). */
+enum { T3D_PROFILE_MATVEC = 0, T3D_PROFILE_VCYCLE = 1, T3D_PROFILE_MATVEC32 = 2, T3D_PROFILE_VCYCLE32 = 3 };
 int  t3d_profile(struct t3d_context* ctx, int what, int reps, double* ms);
 
 /* --------------------------------------------------------------- allocation-free compliance
