@@ -23,6 +23,7 @@ HEADER_PATH = os.path.join(os.path.dirname(PKG_DIR), "include", "t3d_b200.h")
 T3D_OK, T3D_ERR_INVALID, T3D_ERR_CUDA, T3D_ERR_OOM, T3D_ERR_NO_DEVICE, T3D_ERR_UNSUPPORTED, T3D_ERR_NUMERIC = range(7)
 T3D_SUM_REFERENCE, T3D_SUM_FP64 = 0, 1
 T3D_FP64, T3D_MIXED = 0, 1
+T3D_MATVEC32_AUTO, T3D_MATVEC32_DENSE = 0, 1
 
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
@@ -41,14 +42,14 @@ class Params(C.Structure):
                 ("cg_tol", C.c_float), ("cg_max_it", C.c_int), ("mg_nondyadic", C.c_int),
                 ("mg_max_levels", C.c_int), ("mg_weight", C.c_float), ("filter_rmin", C.c_float),
                 ("oc_sum_order", C.c_int), ("precision", C.c_int), ("device", C.c_int),
-                ("reserved", C.c_int * 7)]
+                ("matvec32_form", C.c_int), ("reserved", C.c_int * 6)]
 
 
 class Info(C.Structure):
     _fields_ = [("res", C.c_int64 * 3), ("orig", C.c_int64 * 3), ("num_elements", C.c_int64),
                 ("num_nodes", C.c_int64), ("num_free", C.c_int64), ("num_levels", C.c_int64),
                 ("levels", (C.c_int64 * 4) * 8), ("coarse_n", C.c_int64), ("coarse_cholesky_ok", C.c_int64),
-                ("device_bytes", C.c_int64), ("kernel_launches", C.c_int64)]
+                ("device_bytes", C.c_int64), ("kernel_launches", C.c_int64), ("matvec32_modal", C.c_int64)]
 
 
 class IterRecord(C.Structure):
@@ -75,6 +76,7 @@ _SIGS = {
     "t3d_get_free_dofs": (C.c_int, [_CTX, _i32p]),
     "t3d_get_load": (C.c_int, [_CTX, _f64p]),
     "t3d_matvec": (C.c_int, [_CTX, _f64p, _f64p, _f64p]),
+    "t3d_matvec32": (C.c_int, [_CTX, _f64p, _f64p, _f64p]),
     "t3d_mg_setup": (C.c_int, [_CTX, _f64p]),
     "t3d_vcycle": (C.c_int, [_CTX, _f64p, _f64p]),
     "t3d_pcg": (C.c_int, [_CTX, _f64p, _f64p, _f64p, C.c_double, C.c_int, C.POINTER(C.c_int)]),
@@ -224,6 +226,12 @@ class Problem:
     def K_times_u_finest(self, eleE, uFree):
         y = np.zeros(self.nf)
         _check(self._lib.t3d_matvec(self._h, _f64(eleE), _f64(uFree), y))
+        return y
+
+    def K_times_u_finest32(self, eleE, uFree):
+        """the FP32 K(E)u of the mixed-precision inner solve (mixed contexts only), widened to FP64"""
+        y = np.zeros(self.nf)
+        _check(self._lib.t3d_matvec32(self._h, _f64(eleE), _f64(uFree), y))
         return y
 
     def make_diagonal_preconditioner_from_static(self, eleE):

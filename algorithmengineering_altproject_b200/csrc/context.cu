@@ -156,6 +156,10 @@ struct Context {
     // mixed precision (T3D_MIXED): FP32 inner-solve state
     bool mixed = false;
     float* Ke32 = nullptr;
+    ModalKe kh{};               // modal form of Ke for the FP32 K(E)p (valid when `modal`)
+    ModalTiling mt{};
+    bool modal = false;
+    double modal_off = 0.0;     // largest relative off-pattern entry of T^T Ke T
     float* E32 = nullptr;
     float *r32 = nullptr, *d32 = nullptr, *z32 = nullptr, *p32 = nullptr, *Ap32 = nullptr;
     MgLevel32 lv32[8]{};
@@ -310,7 +314,16 @@ static int build_mixed(Context* c) {
     float k32[576];
     for (int i = 0; i < 576; ++i) k32[i] = (float)c->Ke_h[i];
     T3D_CUDA_OK(cudaMemcpyAsync(c->Ke32, k32, sizeof k32, cudaMemcpyHostToDevice, c->st));
+    CHECK(modal_tiling(g, c->dev, &c->mt));
+    c->modal = c->prm.matvec32_form == T3D_MATVEC32_AUTO && modal_ke_from(c->Ke_h, &c->kh, &c->modal_off);
     return sync(c);
+}
+
+// FP32 K(E)p on the FP32 images (E32, x -> y); with dot.partial, x.y goes to S->denom
+static void matvec32(Context* c, const float* x, float* y, RedSlot dot, PcgScalars* S) {
+    c->launches += 1;
+    if (c->modal) launch_matvec32_modal(c->g, c->kh, c->mt, c->E32, c->mask0, x, y, dot, S, c->st);
+    else launch_matvec32(c->g, c->Ke32, c->E32, c->mask0, x, y, dot, S, c->st);
 }
 
 static int create(int nely, int nelx, int nelz, const t3d_params* prm, Context* c) {
@@ -325,6 +338,8 @@ static int create(int nely, int nelx, int nelz, const t3d_params* prm, Context* 
     if (c->prm.device < 0 || c->prm.device >= ndev) return set_error(T3D_ERR_NO_DEVICE, "device index out of range");
     if (c->prm.precision != T3D_FP64 && c->prm.precision != T3D_MIXED)
         return set_error(T3D_ERR_UNSUPPORTED, "precision must be T3D_FP64 or T3D_MIXED");
+    if (c->prm.matvec32_form != T3D_MATVEC32_AUTO && c->prm.matvec32_form != T3D_MATVEC32_DENSE)
+        return set_error(T3D_ERR_UNSUPPORTED, "matvec32_form must be T3D_MATVEC32_AUTO or T3D_MATVEC32_DENSE");
     c->mixed = c->prm.precision == T3D_MIXED;
     c->dev = c->prm.device;
     T3D_CUDA_OK(cudaSetDevice(c->dev));
@@ -618,8 +633,8 @@ static void vcycle32(Context* c, const float* r, float* z, PcgScalars* S, RedSlo
 }
 
 static void pcg32_iteration(Context* c) {
-    c->launches += 3;
-    launch_matvec32(c->g, c->Ke32, c->E32, c->mask0, c->p32, c->Ap32, c->slot[0], c->S32, c->st);
+    c->launches += 2;
+    matvec32(c, c->p32, c->Ap32, c->slot[0], c->S32);
     launch_pcg_update32(c->g, c->d32, c->r32, c->p32, c->Ap32, c->slot[1], c->S32, c->st);
     vcycle32(c, c->r32, c->z32, c->S32, c->slot[2]);
     launch_pcg_direction32(c->g, c->z32, c->p32, c->S32, c->st);
@@ -917,6 +932,7 @@ int t3d_get_info(const t3d_context* ctx, t3d_info* info) {
     info->coarse_cholesky_ok = st;
     info->device_bytes = (int64_t)ctx->bytes;
     info->kernel_launches = ctx->launches;
+    info->matvec32_modal = ctx->modal ? 1 : 0;
     return T3D_OK;
 }
 
@@ -935,6 +951,8 @@ int t3d_set_ke(t3d_context* ctx, const double* ke) {
         float k32[576];
         for (int i = 0; i < 576; ++i) k32[i] = (float)ctx->Ke_h[i];
         T3D_CUDA_OK(cudaMemcpy(ctx->Ke32, k32, sizeof k32, cudaMemcpyHostToDevice));
+        ctx->modal = ctx->prm.matvec32_form == T3D_MATVEC32_AUTO &&
+                     t3d::modal_ke_from(ctx->Ke_h, &ctx->kh, &ctx->modal_off);
     }
     return T3D_OK;
 }
@@ -974,6 +992,22 @@ int t3d_matvec(t3d_context* ctx, const double* E, const double* u, double* y) {
     t3d::launch_matvec64(ctx->g, ctx->Ke, ctx->E, ctx->mask0, ctx->p, ctx->Ap, t3d::RedSlot{nullptr, nullptr},
                          nullptr, ctx->st);
     CHECK(t3d::launch_check("matvec"));
+    return t3d::download_free(ctx, ctx->Ap, y);
+}
+
+int t3d_matvec32(t3d_context* ctx, const double* E, const double* u, double* y) {
+    API_GUARD(ctx);
+    if (!E || !u || !y) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    if (!ctx->mixed) return t3d::set_error(T3D_ERR_INVALID, "FP32 kernels need precision T3D_MIXED");
+    CHECK(t3d::upload_cells_f64(ctx, E, ctx->E));
+    CHECK(t3d::upload_free(ctx, u, ctx->p));
+    t3d::launch_cast(ctx->g.NE, ctx->E, ctx->E32, ctx->st);
+    t3d::launch_cast(3 * ctx->g.NN, ctx->p, ctx->p32, ctx->st);
+    ctx->launches += 2;
+    t3d::matvec32(ctx, ctx->p32, ctx->Ap32, t3d::RedSlot{nullptr, nullptr}, nullptr);
+    t3d::launch_widen(3 * ctx->g.NN, ctx->Ap32, ctx->Ap, ctx->st);
+    ctx->launches += 1;
+    CHECK(t3d::launch_check("matvec32"));
     return t3d::download_free(ctx, ctx->Ap, y);
 }
 
@@ -1218,9 +1252,7 @@ int t3d_profile(t3d_context* ctx, int what, int reps, double* ms) {
         } else if (what == T3D_PROFILE_VCYCLE) {
             t3d::vcycle(ctx, ctx->r, ctx->z, ctx->S, ctx->slot[2]);
         } else if (what == T3D_PROFILE_MATVEC32) {
-            t3d::launch_matvec32(ctx->g, ctx->Ke32, ctx->E32, ctx->mask0, ctx->p32, ctx->Ap32, ctx->slot[0], ctx->S32,
-                                 ctx->st);
-            ctx->launches += 1;
+            t3d::matvec32(ctx, ctx->p32, ctx->Ap32, ctx->slot[0], ctx->S32);
         } else {
             t3d::vcycle32(ctx, ctx->r32, ctx->z32, ctx->S32, ctx->slot[2]);
         }

@@ -27,6 +27,11 @@ __global__ void k_cast(int64_t n, const double* __restrict__ a, float* __restric
 }
 
 // r64 = b - A u64; r32 = (float)r64; d32 = 0; |r64|^2 into *rn2 (FP64)
+__global__ void k_widen(int64_t n, const float* __restrict__ a, double* __restrict__ b) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (double)a[i];
+}
+
 __global__ void __launch_bounds__(RED_THREADS) k_mixed_residual(Grid g, const double* __restrict__ b,
                                                                 const double* __restrict__ Au,
                                                                 float* __restrict__ r32, float* __restrict__ d32,
@@ -361,6 +366,10 @@ void launch_mixed_residual(const Grid& g, const double* b, const double* Au, flo
 void launch_mixed_accumulate(const Grid& g, double* u, const float* d, cudaStream_t s) {
     k_mixed_accumulate<<<RED_BLOCKS, 256, 0, s>>>(3 * g.NN, u, d);
 }
+void launch_widen(int64_t n, const float* a, double* b, cudaStream_t s) {
+    k_widen<<<RED_BLOCKS, 256, 0, s>>>(n, a, b);
+}
+
 void launch_matvec32(const Grid& g, const float* Ke, const float* E, const uint8_t* mask, const float* u, float* y,
                      RedSlot dot, PcgScalars* S, cudaStream_t s) {
     k_matvec32<<<RED_BLOCKS, RED_THREADS, 0, s>>>(g, Ke, E, mask, u, y, dot, S);

@@ -143,6 +143,7 @@ void launch_oc_vec8_stats(int64_t ne, const int32_t* morton_cells, const float* 
 
 // ---- mixed precision (k_mixed.cu)
 void launch_cast(int64_t n, const double* a, float* b, cudaStream_t s);
+void launch_widen(int64_t n, const float* a, double* b, cudaStream_t s);
 void launch_mixed_residual(const Grid& g, const double* b, const double* Au, float* r32, float* d32, RedSlot red,
                            double* rn2, cudaStream_t s);
 void launch_mixed_accumulate(const Grid& g, double* u, const float* d, cudaStream_t s);
@@ -159,5 +160,22 @@ void launch_coarse_solve32(const MgLevel32& L, const double* X, int N, const int
 void launch_pcg_update32(const Grid& g, float* x, float* r, const float* p, const float* Ap, RedSlot red,
                          PcgScalars* S, cudaStream_t s);
 void launch_pcg_direction32(const Grid& g, const float* z, float* p, PcgScalars* S, cudaStream_t s);
+
+// ---- FP32 K(E)p through the modal form of Ke (k_matvec_modal.cu)
+struct ModalKe {         // the 45 nonzeros of T^T Ke T / 64 in the fixed block pattern
+    float v[45];
+};
+struct ModalTiling {     // persistent walk over (x tile, y tile, z slab) work items
+    int tiles_x, tiles_y, slabs, slab, items, grid;
+};
+// Projects Ke (576 doubles, row-major, local DOF 3a+c) onto the modal pattern.  Returns false when Ke
+// has entries off the pattern (relative size above 1e-10), i.e. it is not the stiffness of an
+// axis-aligned cubic isotropic voxel; *off receives the largest relative off-pattern entry.
+bool modal_ke_from(const double* Ke, ModalKe* out, double* off);
+// Tiling and persistent grid size for device `dev` (grid <= RED_BLOCKS).
+int modal_tiling(const Grid& g, int dev, ModalTiling* t);
+void launch_matvec32_modal(const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E,
+                           const uint8_t* mask, const float* u, float* y, RedSlot dot, PcgScalars* S,
+                           cudaStream_t s);
 
 }  // namespace t3d

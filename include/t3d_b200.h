@@ -39,6 +39,10 @@ enum { T3D_SUM_REFERENCE = 0, T3D_SUM_FP64 = 1 };   /* OC volume / sharpness sum
 /* solver precision of the design loop: T3D_FP64 = PCG_free in FP64; T3D_MIXED = FP32 inner MG-PCG (FP64
  * inner products, alpha/beta, coarsest solve) inside FP64 defect correction on the true residual */
 enum { T3D_FP64 = 0, T3D_MIXED = 1 };
+/* FP32 K(E)p of the mixed form: AUTO = the modal (corner-Hadamard, 45-nonzero) form whenever Ke is the
+ * stiffness of an axis-aligned cubic isotropic voxel (always for the built-in Ke), else the dense
+ * 24x24 form; DENSE = always the dense form */
+enum { T3D_MATVEC32_AUTO = 0, T3D_MATVEC32_DENSE = 1 };
 
 typedef struct t3d_params {
     float E0, Emin, nu, penal;    /* GlobalParams core.hpp:26-33 (Ke always uses nu = 0.3, fea.cpp:345) */
@@ -51,7 +55,8 @@ typedef struct t3d_params {
     int   oc_sum_order;           /* T3D_SUM_REFERENCE (bit-identical bisection) or T3D_SUM_FP64 */
     int   precision;              /* T3D_FP64 or T3D_MIXED (design loop only; t3d_pcg is always FP64) */
     int   device;                 /* CUDA device ordinal */
-    int   reserved[7];
+    int   matvec32_form;          /* mixed precision only: T3D_MATVEC32_AUTO or T3D_MATVEC32_DENSE */
+    int   reserved[6];
 } t3d_params;
 
 typedef struct t3d_info {
@@ -66,6 +71,7 @@ typedef struct t3d_info {
     int64_t coarse_cholesky_ok;   /* 1 when the last MG set-up factorised the coarsest matrix */
     int64_t device_bytes;         /* device memory held by the context */
     int64_t kernel_launches;      /* kernels launched by this context so far (graph nodes included) */
+    int64_t matvec32_modal;       /* 1 when the mixed form's FP32 K(E)p uses the modal kernel */
 } t3d_info;
 
 typedef struct t3d_iter_record {  /* one design iteration (driver.cpp:205-216) */
@@ -97,6 +103,9 @@ int  t3d_get_load(struct t3d_context* ctx, double* b_free);               /* res
 /* --------------------------------------------------------------- operators (host buffers) */
 /* K_times_u_finest (fea.hpp:42-45, fea.cpp:763-837) */
 int  t3d_matvec(struct t3d_context* ctx, const double* ele_E, const double* u_free, double* y_free);
+/* K_times_u_finest in the FP32 form used by the mixed-precision inner solve (mixed contexts only):
+ * inputs rounded to FP32, y returned widened to FP64; same layouts as t3d_matvec */
+int  t3d_matvec32(struct t3d_context* ctx, const double* ele_E, const double* u_free, double* y_free);
 /* mg::make_diagonal_preconditioner_from_static (multigrid.hpp:66-68, preconditioner.cpp:38-79) */
 int  t3d_mg_setup(struct t3d_context* ctx, const double* ele_E);
 /* the preconditioner closure z = M^-1 r (preconditioner.cpp:88-265) */
