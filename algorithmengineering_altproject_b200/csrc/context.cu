@@ -290,6 +290,7 @@ static int build_mixed(Context* c) {
     const Grid& g = c->g;
     CHECK(c->alloc(&c->Ke32, 576));
     CHECK(c->alloc(&c->E32, g.NE));
+    T3D_CUDA_OK(cudaMemsetAsync(c->E32, 0, g.NE * sizeof(float), c->st));
     for (float** v : {&c->r32, &c->d32, &c->z32, &c->p32, &c->Ap32}) {
         CHECK(c->alloc(v, 3 * g.NN));
         T3D_CUDA_OK(cudaMemsetAsync(*v, 0, 3 * g.NN * sizeof(float), c->st));
@@ -314,8 +315,9 @@ static int build_mixed(Context* c) {
     float k32[576];
     for (int i = 0; i < 576; ++i) k32[i] = (float)c->Ke_h[i];
     T3D_CUDA_OK(cudaMemcpyAsync(c->Ke32, k32, sizeof k32, cudaMemcpyHostToDevice, c->st));
-    CHECK(modal_tiling(g, c->dev, &c->mt));
     c->modal = c->prm.matvec32_form == T3D_MATVEC32_AUTO && modal_ke_from(c->Ke_h, &c->kh, &c->modal_off);
+    // the tile shape of the modal kernel is chosen by timing each one on this grid (zero vectors)
+    CHECK(modal_autotune(g, c->dev, c->kh, c->E32, c->mask0, c->p32, c->Ap32, c->st, &c->mt));
     return sync(c);
 }
 

@@ -28,6 +28,7 @@
 
 #include "kernels.hpp"
 #include "red.cuh"
+#include "t3d_b200.h"
 
 namespace t3d {
 
@@ -75,34 +76,42 @@ __device__ __forceinline__ void inv2(const Modes2& w, float& v00, float& v10, fl
     v11 = pp + qq;
 }
 
-__device__ __forceinline__ float4 ld_node(const float* __restrict__ u0, const float* __restrict__ u1,
-                                          const float* __restrict__ u2, const Grid& g, int x, int y, int z) {
-    if (x < 0 || y < 0 || z < 0 || x >= g.nnx || y >= g.nny || z >= g.nnz) return make_float4(0.f, 0.f, 0.f, 0.f);
-    const int64_t n = g.node(x, y, z);
-    return make_float4(__ldg(u0 + n), __ldg(u1 + n), __ldg(u2 + n), 0.f);
+__device__ __forceinline__ void cp_async4(unsigned s, const float* gsrc, bool valid) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gsrc), "r"(valid ? 4 : 0)
+                 : "memory");
 }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 }  // namespace
 
-template <int BX, int BY, int MINB>
+// Shared-memory layout of one CTA (dynamic): STAGES ring slots of {node plane footprint, moduli of
+// the element layer below it}, then two corner-exchange buffers.
+template <int BX, int BY, int STAGES>
+struct ModalSmem {
+    static constexpr int PX = BX + 1, PY = BY + 1;
+    float4 plane[STAGES][PY][PX];   // (c0, c1, c2, -) of each footprint node
+    float emod[STAGES][BY][BX];     // E of element column (tx, ty) in the layer below the plane
+    float4 outc[2][3][BY][BX];      // corners (1,0), (0,1), (1,1) of each element column, by plane parity
+    double sh[32];
+};
+
+template <int BX, int BY, int MINB, int STAGES>
 __global__ void __launch_bounds__(BX * BY, MINB)
     k_matvec32_modal(Grid g, ModalKe kh, ModalTiling t, const float* __restrict__ E,
                      const uint8_t* __restrict__ mask, const float* __restrict__ u, float* __restrict__ y,
                      RedSlot dot, PcgScalars* S) {
     constexpr int PX = BX + 1, PY = BY + 1;
-    static_assert(PY <= BX, "the footprint column is loaded by one warp-row of BX threads");
-    __shared__ float4 plane[PY][PX];        // node plane footprint (c0, c1, c2, -)
-    __shared__ float4 outc[4][BY][BX];      // corner (dx + 2 dy) contributions of each element column
-    __shared__ double sh[32];
+    static_assert(PY <= BX, "the footprint column is loaded by one row of BX threads");
+    static_assert(STAGES >= 2, "ring needs two slots at least");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ModalSmem<BX, BY, STAGES>& sm = *reinterpret_cast<ModalSmem<BX, BY, STAGES>*>(smem_raw);
     if (S != nullptr && S->done) return;
     const int tx = threadIdx.x % BX, ty = threadIdx.x / BX;
-    const int64_t NN = g.NN;
-    const float* __restrict__ u0 = u;
-    const float* __restrict__ u1 = u + NN;
-    const float* __restrict__ u2 = u + 2 * NN;
+    const int64_t NN = g.NN, NXY = (int64_t)g.nnx * g.nny, EXY = (int64_t)g.ex * g.ey;
     // besides its own node, thread row 0 loads the footprint's last row, thread row 1 its last column
     const int ex_kind = (ty == 0) ? 1 : ((ty == 1 && tx < PY) ? 2 : 0);
-    const float4 zero4 = make_float4(0.f, 0.f, 0.f, 0.f);
     double part = 0.0;
     for (int w = blockIdx.x; w < t.items; w += gridDim.x) {
         const int itx = w % t.tiles_x;
@@ -114,104 +123,167 @@ __global__ void __launch_bounds__(BX * BY, MINB)
         const int cx = X0 - 1 + tx, cy = Y0 - 1 + ty;           // element column and own node
         const int exx = ex_kind == 1 ? cx : X0 - 1 + BX;
         const int exy = ex_kind == 1 ? Y0 - 1 + BY : Y0 - 1 + tx;
-        const bool owner = tx > 0 && ty > 0 && cx < g.nnx && cy < g.nny;
-        const bool e_in = cx <= g.nx && cy <= g.ny;             // inside the cell array (ghost ring included)
-        float4 own = ld_node(u0, u1, u2, g, cx, cy, Z0 - 1);
-        float4 ext = ex_kind ? ld_node(u0, u1, u2, g, exx, exy, Z0 - 1) : zero4;
-        float4 own_prev = zero4;
+        const bool own_xy = cx >= 0 && cy >= 0 && cx < g.nnx && cy < g.nny;
+        const bool ext_xy = ex_kind != 0 && exx >= 0 && exy >= 0 && exx < g.nnx && exy < g.nny;
+        const bool e_in = cx <= g.nx && cy <= g.ny;             // cell array covers cx, cy in [-1, n]
+        const bool owner = tx > 0 && ty > 0 && own_xy;
+        // plane-0 offsets (32-bit: 3 NN < 2^31); plane q adds q * NXY (nodes) or q * EXY (the layer
+        // below plane q is q-1)
+        const int own_off = own_xy ? cy * g.nnx + cx : 0;
+        const int ext_off = ext_xy ? exy * g.nnx + exx : 0;
+        const int e_off = e_in ? (int)g.cell(cx, cy, -1) : 0;
+        const unsigned own_s = (unsigned)__cvta_generic_to_shared(&sm.plane[0][ty][tx].x);
+        const unsigned ext_s = (unsigned)__cvta_generic_to_shared(
+            ex_kind == 1 ? &sm.plane[0][BY][tx].x : &sm.plane[0][min(tx, PY - 1)][BX].x);
+        const unsigned e_s = (unsigned)__cvta_generic_to_shared(&sm.emod[0][ty][tx]);
+        const int nplanes = Z1 - Z0 + 2;                         // node planes Z0-1 .. Z1
+        auto issue = [&](int k) {                                // plane Z0-1+k into ring slot k % STAGES
+            const int q = Z0 - 1 + k, s = k % STAGES;
+            const bool vz = q >= 0 && q < g.nnz;
+            const int on = q * (int)NXY;
+            const bool vo = own_xy && vz, ve = ext_xy && vz;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                cp_async4(own_s + s * (PY * PX * 16) + 4 * c, u + (vo ? own_off + on + c * (int)NN : 0), vo);
+                if (ex_kind)
+                    cp_async4(ext_s + s * (PY * PX * 16) + 4 * c, u + (ve ? ext_off + on + c * (int)NN : 0), ve);
+            }
+            const bool vm = e_in && q >= 0;
+            cp_async4(e_s + s * (BY * BX * 4), E + (vm ? e_off + q * (int)EXY : 0), vm);
+        };
+        __syncthreads();                                         // the previous item's readers are done
+#pragma unroll
+        for (int k = 0; k < STAGES - 1; ++k) {
+            if (k < nplanes) issue(k);
+            cp_async_commit();
+        }
         Modes2 bot[3], acc[3];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) acc[k] = Modes2{0.f, 0.f, 0.f, 0.f};
-        for (int pz = Z0 - 1; pz <= Z1; ++pz) {
-            plane[ty][tx] = own;
-            if (ex_kind == 1) plane[BY][tx] = ext;
-            else if (ex_kind == 2) plane[tx][BX] = ext;
-            const float4 cur = own;
-            if (pz < Z1) {   // next plane into registers while this one is used
-                own = ld_node(u0, u1, u2, g, cx, cy, pz + 1);
-                if (ex_kind) ext = ld_node(u0, u1, u2, g, exx, exy, pz + 1);
+        for (int k = 0; k < 3; ++k) acc[k] = bot[k] = Modes2{0.f, 0.f, 0.f, 0.f};
+        float4 h1 = make_float4(0.f, 0.f, 0.f, 0.f), h2 = h1;     // own node values of planes pz-1, pz-2
+        float k0 = 0.f, k1 = 0.f, k2 = 0.f;                      // own element's corner (0,0) of plane pz-2
+        int mk_next = 0;                                         // mask byte of plane pz-1
+        const int node_off = owner ? cy * g.nnx + cx : 0;
+        for (int it = 0; it <= nplanes; ++it) {
+            const int pz = Z0 - 1 + it;
+            cp_async_wait<STAGES - 2>();
+            __syncthreads();                 // plane pz and the corners of plane pz-2 are visible
+            if (it + STAGES - 1 < nplanes) issue(it + STAGES - 1);
+            cp_async_commit();
+            if (owner && pz - 2 >= Z0) {     // plane pz-2: own corner + 3 neighbours, fixed order
+                const int pb = (it - 1) & 1;
+                const float4 s1 = sm.outc[pb][0][ty][tx - 1], s2 = sm.outc[pb][1][ty - 1][tx],
+                             s3 = sm.outc[pb][2][ty - 1][tx - 1];
+                float y0 = ((k0 + s1.x) + s2.x) + s3.x;
+                float y1 = ((k1 + s1.y) + s2.y) + s3.y;
+                float y2 = ((k2 + s1.z) + s2.z) + s3.z;
+                if (mk_next & 1) y0 = 0.f;
+                if (mk_next & 2) y1 = 0.f;
+                if (mk_next & 4) y2 = 0.f;
+                const int n = node_off + (pz - 2) * (int)NXY;
+                y[n] = y0;
+                y[(int)NN + n] = y1;
+                y[2 * (int)NN + n] = y2;
+                if (dot.partial) {
+                    part = fma((double)h2.x, (double)y0, part);
+                    part = fma((double)h2.y, (double)y1, part);
+                    part = fma((double)h2.z, (double)y2, part);
+                }
             }
-            __syncthreads();
-            const float4 a = plane[ty][tx], b = plane[ty][tx + 1], c = plane[ty + 1][tx], d = plane[ty + 1][tx + 1];
-            Modes2 top[3];
-            top[0] = fwd2(a.x, b.x, c.x, d.x);
-            top[1] = fwd2(a.y, b.y, c.y, d.y);
-            top[2] = fwd2(a.z, b.z, c.z, d.z);
-            const bool emit = pz - 1 >= Z0;                    // plane pz-1 is owned and now complete
-            if (pz >= Z0) {                                    // element layer cz = pz-1
-                const float Ee = e_in ? __ldg(E + g.cell(cx, cy, pz - 1)) : 0.f;
-                float cm[24];
+            if (owner && pz - 1 >= Z0 && pz - 1 < Z1) mk_next = mask[node_off + (pz - 1) * (int)NXY];
+            if (it < nplanes) {
+                const int s = it % STAGES;
+                const float4 a = sm.plane[s][ty][tx], b = sm.plane[s][ty][tx + 1], c = sm.plane[s][ty + 1][tx],
+                             d = sm.plane[s][ty + 1][tx + 1];
+                Modes2 top[3];
+                top[0] = fwd2(a.x, b.x, c.x, d.x);
+                top[1] = fwd2(a.y, b.y, c.y, d.y);
+                top[2] = fwd2(a.z, b.z, c.z, d.z);
+                if (it >= 1) {               // element layer pz-1 between planes pz-1 (bot) and pz (top)
+                    const float Ee = sm.emod[s][ty][tx];
+                    float cm[24];
 #pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    cm[8 * k + 0] = 0.f;
-                    cm[8 * k + 1] = Ee * (top[k].m10 + bot[k].m10);
-                    cm[8 * k + 2] = Ee * (top[k].m01 + bot[k].m01);
-                    cm[8 * k + 3] = Ee * (top[k].m11 + bot[k].m11);
-                    cm[8 * k + 4] = Ee * (top[k].m00 - bot[k].m00);
-                    cm[8 * k + 5] = Ee * (top[k].m10 - bot[k].m10);
-                    cm[8 * k + 6] = Ee * (top[k].m01 - bot[k].m01);
-                    cm[8 * k + 7] = Ee * (top[k].m11 - bot[k].m11);
-                }
-                float yh[24];
+                    for (int q = 0; q < 3; ++q) {
+                        cm[8 * q + 0] = 0.f;
+                        cm[8 * q + 1] = Ee * (top[q].m10 + bot[q].m10);
+                        cm[8 * q + 2] = Ee * (top[q].m01 + bot[q].m01);
+                        cm[8 * q + 3] = Ee * (top[q].m11 + bot[q].m11);
+                        cm[8 * q + 4] = Ee * (top[q].m00 - bot[q].m00);
+                        cm[8 * q + 5] = Ee * (top[q].m10 - bot[q].m10);
+                        cm[8 * q + 6] = Ee * (top[q].m01 - bot[q].m01);
+                        cm[8 * q + 7] = Ee * (top[q].m11 - bot[q].m11);
+                    }
+                    float yh[24];
 #pragma unroll
-                for (int i = 0; i < 24; ++i) yh[i] = 0.f;
-                {
-                    int e = 0;
-#define T3D_KH_FMA(d, s) yh[d] = fmaf(kh.v[e++], cm[s], yh[d]);
-                    T3D_KH_PATTERN(T3D_KH_FMA)
+                    for (int i = 0; i < 24; ++i) yh[i] = 0.f;
+                    {
+                        int e = 0;
+#define T3D_KH_FMA(dd, ss) yh[dd] = fmaf(kh.v[e++], cm[ss], yh[dd]);
+                        T3D_KH_PATTERN(T3D_KH_FMA)
 #undef T3D_KH_FMA
-                }
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    const float* q = yh + 8 * k;
-                    const Modes2 tb{-q[4], q[1] - q[5], q[2] - q[6], q[3] - q[7]};   // onto plane pz-1
-                    const Modes2 tt{q[4], q[1] + q[5], q[2] + q[6], q[3] + q[7]};    // onto plane pz
-                    const Modes2 fin{acc[k].m00 + tb.m00, acc[k].m10 + tb.m10, acc[k].m01 + tb.m01,
-                                     acc[k].m11 + tb.m11};
-                    acc[k] = tt;
-                    bot[k] = fin;   // reuse as the finished plane pz-1 (bot is replaced by top below)
-                }
-                if (emit) {
+                    }
                     float v[3][4];
 #pragma unroll
-                    for (int k = 0; k < 3; ++k) inv2(bot[k], v[k][0], v[k][1], v[k][2], v[k][3]);
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) outc[q][ty][tx] = make_float4(v[0][q], v[1][q], v[2][q], 0.f);
+                    for (int q = 0; q < 3; ++q) {
+                        const float* r = yh + 8 * q;
+                        const Modes2 fin{acc[q].m00 - r[4], acc[q].m10 + (r[1] - r[5]), acc[q].m01 + (r[2] - r[6]),
+                                         acc[q].m11 + (r[3] - r[7])};                         // plane pz-1 complete
+                        acc[q] = Modes2{r[4], r[1] + r[5], r[2] + r[6], r[3] + r[7]};        // onto plane pz
+                        inv2(fin, v[q][0], v[q][1], v[q][2], v[q][3]);
+                    }
+                    if (it >= 2) {           // plane pz-1 >= Z0 is owned: publish the 3 foreign corners
+                        k0 = v[0][0];
+                        k1 = v[1][0];
+                        k2 = v[2][0];
+                        const int pb = it & 1;
+                        sm.outc[pb][0][ty][tx] = make_float4(v[0][1], v[1][1], v[2][1], 0.f);
+                        sm.outc[pb][1][ty][tx] = make_float4(v[0][2], v[1][2], v[2][2], 0.f);
+                        sm.outc[pb][2][ty][tx] = make_float4(v[0][3], v[1][3], v[2][3], 0.f);
+                    }
                 }
-            }
 #pragma unroll
-            for (int k = 0; k < 3; ++k) bot[k] = top[k];
-            __syncthreads();
-            if (emit && owner) {
-                const float4 s0 = outc[0][ty][tx], s1 = outc[1][ty][tx - 1], s2 = outc[2][ty - 1][tx],
-                             s3 = outc[3][ty - 1][tx - 1];
-                float y0 = ((s0.x + s1.x) + s2.x) + s3.x;
-                float y1 = ((s0.y + s1.y) + s2.y) + s3.y;
-                float y2 = ((s0.z + s1.z) + s2.z) + s3.z;
-                const int64_t n = g.node(cx, cy, pz - 1);
-                const int mk = mask[n];
-                if (mk & 1) y0 = 0.f;
-                if (mk & 2) y1 = 0.f;
-                if (mk & 4) y2 = 0.f;
-                y[n] = y0;
-                y[NN + n] = y1;
-                y[2 * NN + n] = y2;
-                if (dot.partial) {
-                    part = fma((double)own_prev.x, (double)y0, part);
-                    part = fma((double)own_prev.y, (double)y1, part);
-                    part = fma((double)own_prev.z, (double)y2, part);
-                }
+                for (int q = 0; q < 3; ++q) bot[q] = top[q];
+                h2 = h1;
+                h1 = a;
             }
-            own_prev = cur;
         }
+        cp_async_wait<0>();
     }
     if (dot.partial) {
         double tot;
-        if (grid_fold(part, dot, sh, &tot) && threadIdx.x == 0) S->denom = tot;
+        if (grid_fold(part, dot, sm.sh, &tot) && threadIdx.x == 0) S->denom = tot;
     }
 }
 
-constexpr int MODAL_BX = 32, MODAL_BY = 16, MODAL_MINB = 2;
+// Tile shapes the autotuner chooses from: CTA of BX x BY element columns, MINB CTAs per SM, ring depth.
+template <int BX, int BY, int MINB, int ST>
+struct ModalShape {
+    static constexpr int bx = BX, by = BY;
+    static constexpr size_t smem = sizeof(ModalSmem<BX, BY, ST>);
+    static const void* fn() { return reinterpret_cast<const void*>(k_matvec32_modal<BX, BY, MINB, ST>); }
+    static void launch(const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E, const uint8_t* mask,
+                       const float* u, float* y, RedSlot dot, PcgScalars* S, cudaStream_t s) {
+        k_matvec32_modal<BX, BY, MINB, ST><<<t.grid, BX * BY, smem, s>>>(g, kh, t, E, mask, u, y, dot, S);
+    }
+};
+struct ModalVariant {
+    int bx, by;
+    size_t smem;
+    const void* (*fn)();
+    void (*launch)(const Grid&, const ModalKe&, const ModalTiling&, const float*, const uint8_t*, const float*,
+                   float*, RedSlot, PcgScalars*, cudaStream_t);
+};
+template <class V>
+constexpr ModalVariant variant_of() {
+    return ModalVariant{V::bx, V::by, V::smem, &V::fn, &V::launch};
+}
+const ModalVariant MODAL_VARIANTS[] = {
+    variant_of<ModalShape<32, 16, 2, 3>>(),
+    variant_of<ModalShape<32, 8, 3, 3>>(),
+    variant_of<ModalShape<32, 8, 2, 3>>(),
+    variant_of<ModalShape<32, 16, 1, 3>>(),
+};
+constexpr int MODAL_NVARIANTS = sizeof(MODAL_VARIANTS) / sizeof(MODAL_VARIANTS[0]);
 constexpr int MODAL_SLAB_MIN = 8;
 
 // corner a of the reference's local order at grid offset (corner_dx, corner_dy, corner_dz)(a);
@@ -249,16 +321,20 @@ bool modal_ke_from(const double* Ke, ModalKe* out, double* off) {
     return mx > 0.0 && *off <= 1e-10;
 }
 
-int modal_tiling(const Grid& g, int dev, ModalTiling* t) {
+int modal_tiling(const Grid& g, int dev, int variant, ModalTiling* t) {
+    if (variant < 0 || variant >= MODAL_NVARIANTS) return set_error(T3D_ERR_INVALID, "bad modal tile variant");
+    const ModalVariant& v = MODAL_VARIANTS[variant];
     int sms = 0, per_sm = 0;
     cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return set_cuda_error(e, "cudaDeviceGetAttribute", __FILE__, __LINE__);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, k_matvec32_modal<MODAL_BX, MODAL_BY, MODAL_MINB>, MODAL_BX * MODAL_BY, 0);
+    e = cudaFuncSetAttribute(v.fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem);
+    if (e != cudaSuccess) return set_cuda_error(e, "cudaFuncSetAttribute", __FILE__, __LINE__);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn(), v.bx * v.by, v.smem);
     if (e != cudaSuccess) return set_cuda_error(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor", __FILE__, __LINE__);
     const int resident = std::max(1, std::min(sms * std::max(per_sm, 1), RED_BLOCKS));
-    t->tiles_x = (g.nnx + MODAL_BX - 2) / (MODAL_BX - 1);
-    t->tiles_y = (g.nny + MODAL_BY - 2) / (MODAL_BY - 1);
+    t->variant = variant;
+    t->tiles_x = (g.nnx + v.bx - 2) / (v.bx - 1);
+    t->tiles_y = (g.nny + v.by - 2) / (v.by - 1);
     const int tiles = t->tiles_x * t->tiles_y;
     // slabs: enough work items for about 8 waves of the resident CTAs, slabs of at least 8 planes
     int slabs = std::max(1, (8 * resident + tiles - 1) / tiles);
@@ -270,11 +346,46 @@ int modal_tiling(const Grid& g, int dev, ModalTiling* t) {
     return 0;
 }
 
+int modal_autotune(const Grid& g, int dev, const ModalKe& kh, const float* E, const uint8_t* mask, const float* u,
+                   float* y, cudaStream_t s, ModalTiling* best) {
+    cudaEvent_t e0, e1;
+    cudaError_t e = cudaEventCreate(&e0);
+    if (e != cudaSuccess) return set_cuda_error(e, "cudaEventCreate", __FILE__, __LINE__);
+    e = cudaEventCreate(&e1);
+    if (e != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return set_cuda_error(e, "cudaEventCreate", __FILE__, __LINE__);
+    }
+    float best_ms = 0.f;
+    int rc = 0;
+    for (int v = 0; v < MODAL_NVARIANTS && rc == 0; ++v) {
+        ModalTiling t{};
+        if ((rc = modal_tiling(g, dev, v, &t)) != 0) break;
+        const RedSlot none{nullptr, nullptr};
+        MODAL_VARIANTS[v].launch(g, kh, t, E, mask, u, y, none, nullptr, s);   // warm-up
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < 3; ++r) MODAL_VARIANTS[v].launch(g, kh, t, E, mask, u, y, none, nullptr, s);
+        cudaEventRecord(e1, s);
+        if ((e = cudaEventSynchronize(e1)) != cudaSuccess) {
+            rc = set_cuda_error(e, "modal autotune", __FILE__, __LINE__);
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (v == 0 || ms < best_ms) {
+            best_ms = ms;
+            *best = t;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return rc;
+}
+
 void launch_matvec32_modal(const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E,
                            const uint8_t* mask, const float* u, float* y, RedSlot dot, PcgScalars* S,
                            cudaStream_t s) {
-    k_matvec32_modal<MODAL_BX, MODAL_BY, MODAL_MINB>
-        <<<t.grid, MODAL_BX * MODAL_BY, 0, s>>>(g, kh, t, E, mask, u, y, dot, S);
+    MODAL_VARIANTS[t.variant].launch(g, kh, t, E, mask, u, y, dot, S, s);
 }
 
 }  // namespace t3d

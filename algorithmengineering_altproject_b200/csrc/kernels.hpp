@@ -166,14 +166,18 @@ struct ModalKe {         // the 45 nonzeros of T^T Ke T / 64 in the fixed block 
     float v[45];
 };
 struct ModalTiling {     // persistent walk over (x tile, y tile, z slab) work items
-    int tiles_x, tiles_y, slabs, slab, items, grid;
+    int tiles_x, tiles_y, slabs, slab, items, grid, variant;
 };
 // Projects Ke (576 doubles, row-major, local DOF 3a+c) onto the modal pattern.  Returns false when Ke
 // has entries off the pattern (relative size above 1e-10), i.e. it is not the stiffness of an
 // axis-aligned cubic isotropic voxel; *off receives the largest relative off-pattern entry.
 bool modal_ke_from(const double* Ke, ModalKe* out, double* off);
-// Tiling and persistent grid size for device `dev` (grid <= RED_BLOCKS).
-int modal_tiling(const Grid& g, int dev, ModalTiling* t);
+// Tiling and persistent grid size of tile shape `variant` on device `dev` (grid <= RED_BLOCKS).
+int modal_tiling(const Grid& g, int dev, int variant, ModalTiling* t);
+// Times every tile shape on the given buffers (3 launches each, stream-ordered, CUDA events) and returns
+// the fastest one's tiling.  y is overwritten.
+int modal_autotune(const Grid& g, int dev, const ModalKe& kh, const float* E, const uint8_t* mask, const float* u,
+                   float* y, cudaStream_t s, ModalTiling* best);
 void launch_matvec32_modal(const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E,
                            const uint8_t* mask, const float* u, float* y, RedSlot dot, PcgScalars* S,
                            cudaStream_t s);
