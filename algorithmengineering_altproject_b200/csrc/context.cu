@@ -537,7 +537,7 @@ static int mg_setup(Context* c) {
         launch_coarse_inverse(c->Lrow, c->Nc, c->chol_status, c->Xc, c->st);
     }
     if (c->mixed) {
-        for (int l = 0; l < c->nlev; ++l) launch_cast(3 * c->lv[l].nn, c->lv[l].diag, c->lv32[l].diag, c->st);
+        for (int l = 0; l < c->nlev; ++l) launch_recip_diag32(3 * c->lv[l].nn, c->lv[l].diag, c->lv32[l].diag, c->st);
         c->launches += c->nlev;
     }
     c->mg_ready = true;

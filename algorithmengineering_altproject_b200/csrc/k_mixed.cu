@@ -27,6 +27,12 @@ __global__ void k_cast(int64_t n, const double* __restrict__ a, float* __restric
 }
 
 // r64 = b - A u64; r32 = (float)r64; d32 = 0; |r64|^2 into *rn2 (FP64)
+// FP32 image of a level diagonal as the reciprocal 1 / max(1e-30, D) used by the FP32 smoother
+__global__ void k_recip_diag32(int64_t n, const double* __restrict__ d, float* __restrict__ rd) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        rd[i] = (float)(1.0 / (1.0e-30 < d[i] ? d[i] : 1.0e-30));
+}
+
 __global__ void k_widen(int64_t n, const float* __restrict__ a, double* __restrict__ b) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         b[i] = (double)a[i];
@@ -215,21 +221,24 @@ __global__ void k_restrict_z32(MgLevel32 Lc, MgLevel32 Lf, const float* __restri
     rc[2 * Lc.nn + n] = (m & 4) ? 0.0f : v2 * iw;
 }
 
+// Trilinear prolongation at fine node (fx,fy,fz) from the coarse cell fx >> sh (span 1 << sh), clamped to the
+// last coarse cell (transfers.cpp:396-408).
 __device__ __forceinline__ void prolong_node32(const MgLevel32& Lc, const float* __restrict__ xc, int fx, int fy,
-                                               int fz, float P[3]) {
-    const int s = Lc.span;
+                                               int fz, int sh, float P[3]) {
+    const int s = 1 << sh;
     const int cnx = Lc.nx + 1, cny = Lc.ny + 1;
-    int cx = fx / s, cy = fy / s, cz = fz / s;
-    int rx = fx % s, ry = fy % s, rz = fz % s;
+    int cx = fx >> sh, cy = fy >> sh, cz = fz >> sh;
+    int rx = fx & (s - 1), ry = fy & (s - 1), rz = fz & (s - 1);
     if (cx >= Lc.nx) { cx = Lc.nx - 1; rx = s; }
     if (cy >= Lc.ny) { cy = Lc.ny - 1; ry = s; }
     if (cz >= Lc.nz) { cz = Lc.nz - 1; rz = s; }
-    const float inv = 1.0f / s;
+    const float inv = 1.0f / (float)s;   // exact: s is a power of two
     const float wx1 = rx * inv, wx0 = 1.0f - wx1;
     const float wy1 = ry * inv, wy0 = 1.0f - wy1;
     const float wz1 = rz * inv, wz0 = 1.0f - wz1;
     const int b = (cz * cny + cy) * cnx + cx;
     const int pz = cnx * cny;
+#pragma unroll
     for (int c = 0; c < 3; ++c) {
         const float* X = xc + c * Lc.nn;
         const float lo = fmaf(wy1, fmaf(wx1, X[b + cnx + 1], wx0 * X[b + cnx]), wy0 * fmaf(wx1, X[b + 1], wx0 * X[b]));
@@ -248,10 +257,10 @@ __global__ void k_prolong_smooth32(MgLevel32 Lc, MgLevel32 Lf, const float* __re
     const int fnx = Lf.nx + 1, fny = Lf.ny + 1;
     const int fx = n % fnx, fy = (n / fnx) % fny, fz = n / (fnx * fny);
     float P[3];
-    prolong_node32(Lc, xc, fx, fy, fz, P);
+    prolong_node32(Lc, xc, fx, fy, fz, __ffs(Lc.span) - 1, P);
     const int m = Lf.mask[n];
     for (int c = 0; c < 3; ++c) {
-        const float t = w * rf[c * Lf.nn + n] / fmaxf(1.0e-30f, Lf.diag[c * Lf.nn + n]);
+        const float t = (w * rf[c * Lf.nn + n]) * Lf.diag[c * Lf.nn + n];
         xf[c * Lf.nn + n] = ((m >> c) & 1) ? 0.0f : (t + P[c]) + t;
     }
 }
@@ -265,18 +274,48 @@ __global__ void __launch_bounds__(RED_THREADS) k_prolong_smooth0_32(MgLevel32 Lc
     if (S->done) return;
     const int NN = (int)Lf.nn;
     const int fnx = Lf.nx + 1, fny = Lf.ny + 1;
+    // items of 4 x 32 consecutive nodes of one row (row = fz * fny + fy); each lane takes 4 nodes 32 apart
+    // and issues all their loads before using any of them
+    constexpr int U = 4;
+    const int chunks = (fnx + 32 * U - 1) / (32 * U);
+    const int items = chunks * fny * (Lf.nz + 1);
+    const int lane = threadIdx.x & 31;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    const int sh2 = __ffs(Lc.span) - 1;
     double part = 0.0;
-    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < NN; n += gridDim.x * blockDim.x) {
-        const int fx = n % fnx, fy = (n / fnx) % fny, fz = n / (fnx * fny);
-        float P[3];
-        prolong_node32(Lc, xc, fx, fy, fz, P);
-        const int m = Lf.mask[n];
-        for (int c = 0; c < 3; ++c) {
-            const float rv = r[c * (int64_t)NN + n];
-            const float t = w * rv / fmaxf(1.0e-30f, Lf.diag[c * (int64_t)NN + n]);
-            const float zv = ((m >> c) & 1) ? 0.0f : (t + P[c]) + t;
-            z[c * (int64_t)NN + n] = zv;
-            part = fma((double)rv, (double)zv, part);
+    for (int it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < items; it += nw) {
+        const int row = it / chunks;
+        const int x0 = (it - row * chunks) * (32 * U) + lane;
+        const int fz = row / fny, fy = row - fz * fny;
+        const int nb = row * fnx;
+        float rv[U][3], dv[U][3];
+        int mv[U];
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+            const int fx = x0 + 32 * k;
+            const bool in = fx < fnx;
+            const int n = nb + (in ? fx : 0);
+            mv[k] = in ? (int)Lf.mask[n] : 7;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                rv[k][c] = in ? r[c * NN + n] : 0.0f;
+                dv[k][c] = in ? Lf.diag[c * NN + n] : 0.0f;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < U; ++k) {
+            const int fx = x0 + 32 * k;
+            if (fx >= fnx) break;
+            const int n = nb + fx;
+            float P[3];
+            prolong_node32(Lc, xc, fx, fy, fz, sh2, P);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const float t = (w * rv[k][c]) * dv[k][c];
+                const float zv = ((mv[k] >> c) & 1) ? 0.0f : (t + P[c]) + t;
+                z[c * NN + n] = zv;
+                part = fma((double)rv[k][c], (double)zv, part);
+            }
         }
     }
     double tot;
@@ -302,7 +341,7 @@ __global__ void __launch_bounds__(128) k_coarse_solve32(MgLevel32 L, const doubl
         for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x) {
             const int m = L.mask[n];
             for (int c = 0; c < 3; ++c)
-                L.x[c * nn + n] = ((m >> c) & 1) ? 0.0f : L.r[c * nn + n] / fmaxf(1.0e-30f, L.diag[c * nn + n]);
+                L.x[c * nn + n] = ((m >> c) & 1) ? 0.0f : L.r[c * nn + n] * L.diag[c * nn + n];
         }
         return;
     }
@@ -366,6 +405,10 @@ void launch_mixed_residual(const Grid& g, const double* b, const double* Au, flo
 void launch_mixed_accumulate(const Grid& g, double* u, const float* d, cudaStream_t s) {
     k_mixed_accumulate<<<RED_BLOCKS, 256, 0, s>>>(3 * g.NN, u, d);
 }
+void launch_recip_diag32(int64_t n, const double* d, float* rd, cudaStream_t s) {
+    k_recip_diag32<<<RED_BLOCKS, 256, 0, s>>>(n, d, rd);
+}
+
 void launch_widen(int64_t n, const float* a, double* b, cudaStream_t s) {
     k_widen<<<RED_BLOCKS, 256, 0, s>>>(n, a, b);
 }

@@ -27,7 +27,7 @@ struct MgLevel32 {       // FP32 copy of a level's vectors for the mixed-precisi
     int64_t nn;
     float* r;
     float* x;
-    float* diag;
+    float* diag;          // reciprocal diagonal 1 / max(1e-30, D) in FP32
     const uint8_t* mask;  // shared with the FP64 level
 };
 
@@ -144,6 +144,7 @@ void launch_oc_vec8_stats(int64_t ne, const int32_t* morton_cells, const float* 
 // ---- mixed precision (k_mixed.cu)
 void launch_cast(int64_t n, const double* a, float* b, cudaStream_t s);
 void launch_widen(int64_t n, const float* a, double* b, cudaStream_t s);
+void launch_recip_diag32(int64_t n, const double* d, float* rd, cudaStream_t s);
 void launch_mixed_residual(const Grid& g, const double* b, const double* Au, float* r32, float* d32, RedSlot red,
                            double* rn2, cudaStream_t s);
 void launch_mixed_accumulate(const Grid& g, double* u, const float* d, cudaStream_t s);
