@@ -167,6 +167,7 @@ struct Context {
     float* ra2_32[8]{};
     PcgScalars* S32 = nullptr;
     cudaGraphExec_t pcg32_graph = nullptr;
+    int64_t pcg32_graph_launches = 0;
     int last_outer = 0;
     // lazily built maps between the reference's layouts and the grid
     int32_t* morton = nullptr;          // [ne] cell index of the k-th element in Morton order
@@ -623,7 +624,9 @@ static int pcg_solve(Context* c, double tol, int maxit, int* iters) {
 // ------------------------------------------------------------------ mixed-precision solve
 static void vcycle32(Context* c, const float* r, float* z, PcgScalars* S, RedSlot dot) {
     const int L = c->nlev;
-    c->launches += 4 * (L - 1) + 1;
+    // per transition: restriction (x, y, z passes; x-y fused for span 2) and prolongation
+    for (int l = 0; l + 1 < L; ++l) c->launches += c->lv32[l + 1].span == 2 ? 3 : 4;
+    c->launches += 1;
     for (int l = 0; l + 1 < L; ++l)
         launch_restrict32(c->lv32[l + 1], c->lv32[l], l == 0 ? r : c->lv32[l].r, c->lv32[l + 1].r, c->ra1_32[l],
                           c->ra2_32[l], S, c->st);
@@ -649,6 +652,7 @@ static int ensure_pcg32_graph(Context* c) {
     T3D_CUDA_OK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < PCG_CHUNK; ++k) pcg32_iteration(c);
     T3D_CUDA_OK(cudaStreamEndCapture(c->st, &graph));
+    c->pcg32_graph_launches = (c->launches - l0) / PCG_CHUNK;   // kernels per iteration in the graph
     c->launches = l0;
     cudaError_t e = cudaGraphInstantiate(&c->pcg32_graph, graph, 0);
     cudaGraphDestroy(graph);
@@ -696,7 +700,7 @@ static int mixed_solve(Context* c, double tol, int maxit, int* iters) {
             const int n = std::min(PCG_CHUNK, budget - queued);
             if (c->use_graph && n == PCG_CHUNK) {
                 T3D_CUDA_OK(cudaGraphLaunch(c->pcg32_graph, c->st));
-                c->launches += (int64_t)PCG_CHUNK * (3 + 4 * (c->nlev - 1) + 1);
+                c->launches += (int64_t)PCG_CHUNK * c->pcg32_graph_launches;
             } else {
                 for (int k = 0; k < n; ++k) pcg32_iteration(c);
                 CHECK(launch_check("pcg32 iteration"));

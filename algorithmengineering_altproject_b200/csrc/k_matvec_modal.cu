@@ -164,6 +164,7 @@ __global__ void __launch_bounds__(BX * BY, MINB)
         float k0 = 0.f, k1 = 0.f, k2 = 0.f;                      // own element's corner (0,0) of plane pz-2
         int mk_next = 0;                                         // mask byte of plane pz-1
         const int node_off = owner ? cy * g.nnx + cx : 0;
+#pragma unroll 2
         for (int it = 0; it <= nplanes; ++it) {
             const int pz = Z0 - 1 + it;
             cp_async_wait<STAGES - 2>();
@@ -184,11 +185,8 @@ __global__ void __launch_bounds__(BX * BY, MINB)
                 y[n] = y0;
                 y[(int)NN + n] = y1;
                 y[2 * (int)NN + n] = y2;
-                if (dot.partial) {
-                    part = fma((double)h2.x, (double)y0, part);
-                    part = fma((double)h2.y, (double)y1, part);
-                    part = fma((double)h2.z, (double)y2, part);
-                }
+                if (dot.partial)   // the node's 3 FP32 products summed in FP32, accumulated in FP64
+                    part += (double)fmaf(h2.z, y2, fmaf(h2.y, y1, h2.x * y0));
             }
             if (owner && pz - 1 >= Z0 && pz - 1 < Z1) mk_next = mask[node_off + (pz - 1) * (int)NXY];
             if (it < nplanes) {

@@ -187,6 +187,47 @@ __global__ void k_restrict_y32(MgLevel32 Lc, MgLevel32 Lf, const float* __restri
     a2[2 * total + t] = v2;
 }
 
+// x and y window sums of one fine z-plane in one pass (the x-then-y passes of k_restrict_x32 and
+// k_restrict_y32 fused): a2[fz][cy][cx] = sum_iy w(iy) sum_ix w(ix) r[fz][fy][fx], unnormalised.
+template <int SP>
+__global__ void __launch_bounds__(256) k_restrict_xy32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ rf,
+                                                       float* __restrict__ a2, const PcgScalars* S) {
+    if (S->done) return;
+    constexpr int WS = 2 * SP - 1;
+    const int cnx = Lc.nx + 1, cny = Lc.ny + 1, fnx = Lf.nx + 1, fny = Lf.ny + 1, fnz = Lf.nz + 1;
+    const int total = fnz * cny * cnx;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    const int cx = t % cnx;
+    const int rest = t / cnx;
+    const int cy = rest % cny, fz = rest / cny;
+    const int fNN = (int)Lf.nn;
+    float v0 = 0.0f, v1 = 0.0f, v2 = 0.0f;
+#pragma unroll
+    for (int iy = 0; iy < WS; ++iy) {
+        const int fy = cy * SP + iy - (SP - 1);
+        if (fy < 0 || fy >= fny) continue;
+        const float* __restrict__ src = rf + (fz * fny + fy) * fnx;
+        float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
+#pragma unroll
+        for (int ix = 0; ix < WS; ++ix) {
+            const int fx = cx * SP + ix - (SP - 1);
+            if (fx < 0 || fx >= fnx) continue;
+            const float w = hatf(ix, SP);
+            s0 = fmaf(w, src[fx], s0);
+            s1 = fmaf(w, src[fNN + fx], s1);
+            s2 = fmaf(w, src[2 * fNN + fx], s2);
+        }
+        const float w = hatf(iy, SP);
+        v0 = fmaf(w, s0, v0);
+        v1 = fmaf(w, s1, v1);
+        v2 = fmaf(w, s2, v2);
+    }
+    a2[t] = v0;
+    a2[total + t] = v1;
+    a2[2 * total + t] = v2;
+}
+
 __global__ void k_restrict_z32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ a2, float* __restrict__ rc,
                                const PcgScalars* S) {
     if (S->done) return;
@@ -421,8 +462,13 @@ void launch_restrict32(const MgLevel32& Lc, const MgLevel32& Lf, const float* rf
                        const PcgScalars* S, cudaStream_t s) {
     const int64_t n1 = (int64_t)(Lf.nz + 1) * (Lf.ny + 1) * (Lc.nx + 1);
     const int64_t n2 = (int64_t)(Lf.nz + 1) * (Lc.ny + 1) * (Lc.nx + 1);
-    k_restrict_x32<<<blocks_for(n1, 256), 256, 0, s>>>(Lc, Lf, rf, a1, S);
-    k_restrict_y32<<<blocks_for(n2, 256), 256, 0, s>>>(Lc, Lf, a1, a2, S);
+    // span 2: one fused x-y pass is faster; span 4 (the finest transition): the separable passes are
+    if (Lc.span == 2) {
+        k_restrict_xy32<2><<<blocks_for(n2, 256), 256, 0, s>>>(Lc, Lf, rf, a2, S);
+    } else {
+        k_restrict_x32<<<blocks_for(n1, 256), 256, 0, s>>>(Lc, Lf, rf, a1, S);
+        k_restrict_y32<<<blocks_for(n2, 256), 256, 0, s>>>(Lc, Lf, a1, a2, S);
+    }
     k_restrict_z32<<<blocks_for(Lc.nn, 128), 128, 0, s>>>(Lc, Lf, a2, rc, S);
 }
 void launch_prolong_smooth32(const MgLevel32& Lc, const MgLevel32& Lf, const float* xc, const float* rf, float* xf,
