@@ -45,6 +45,26 @@ class Params(C.Structure):
                 ("matvec32_form", C.c_int), ("reserved", C.c_int * 6)]
 
 
+T3D_LOAD_TIP_LINE, T3D_LOAD_TOP_TRACTION, T3D_LOAD_TORSION = 0, 1, 2
+T3D_MAX_VOIDS = 4
+
+
+class ProblemSpec(C.Structure):
+    """t3d_problem: load case and passive-void ellipsoids (centre ex,ey,ez and radii rx,ry,rz in element
+    units of the reference's element coordinates)."""
+    _fields_ = [("load_case", C.c_int), ("num_voids", C.c_int), ("voids", (C.c_double * 6) * T3D_MAX_VOIDS)]
+
+    @classmethod
+    def make(cls, load_case=T3D_LOAD_TIP_LINE, voids=()):
+        p = cls()
+        p.load_case = load_case
+        p.num_voids = len(voids)
+        for k, v in enumerate(voids):
+            for d in range(6):
+                p.voids[k][d] = float(v[d])
+        return p
+
+
 class Info(C.Structure):
     _fields_ = [("res", C.c_int64 * 3), ("orig", C.c_int64 * 3), ("num_elements", C.c_int64),
                 ("num_nodes", C.c_int64), ("num_free", C.c_int64), ("num_levels", C.c_int64),
@@ -67,6 +87,8 @@ _CTX = C.c_void_p
 _SIGS = {
     "t3d_params_default": (C.c_int, [C.POINTER(Params)]),
     "t3d_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(Params), C.POINTER(_CTX)]),
+    "t3d_create_problem": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(Params), C.POINTER(ProblemSpec),
+                                     C.POINTER(_CTX)]),
     "t3d_destroy": (C.c_int, [_CTX]),
     "t3d_get_info": (C.c_int, [_CTX, C.POINTER(Info)]),
     "t3d_last_error": (C.c_char_p, []),
@@ -155,11 +177,16 @@ class Problem:
     filter.cpp:9).  Methods keep the reference's names and array layouts.
     """
 
-    def __init__(self, nely, nelx, nelz, **params):
+    def __init__(self, nely, nelx, nelz, problem=None, **params):
+        """`problem`: optional ProblemSpec (load case, passive voids); None = the reference cantilever."""
         self._lib = library()
         self.params = default_params(**params)
         h = _CTX()
-        _check(self._lib.t3d_create(nely, nelx, nelz, C.byref(self.params), C.byref(h)))
+        if problem is None:
+            _check(self._lib.t3d_create(nely, nelx, nelz, C.byref(self.params), C.byref(h)))
+        else:
+            _check(self._lib.t3d_create_problem(nely, nelx, nelz, C.byref(self.params), C.byref(problem),
+                                                C.byref(h)))
         self._h = h
         info = Info()
         _check(self._lib.t3d_get_info(self._h, C.byref(info)))

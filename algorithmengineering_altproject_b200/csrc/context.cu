@@ -125,6 +125,8 @@ struct Context {
     t3d_params prm{};
     Grid g{};
     Cuboid cub{};
+    VoidSet voids{};            // passive-void ellipsoids (absent voxels)
+    int load_case = T3D_LOAD_TIP_LINE;
     int dev = 0;
     cudaStream_t st = nullptr;
     int nlev = 0;
@@ -329,8 +331,49 @@ static void matvec32(Context* c, const float* x, float* y, RedSlot dot, PcgScala
     else launch_matvec32(c->g, c->Ke32, c->E32, c->mask0, x, y, dot, S, c->st);
 }
 
-static int create(int nely, int nelx, int nelz, const t3d_params* prm, Context* c) {
+// Load vector b of the context's load case on its free DOFs (fixed DOFs are skipped).
+//   T3D_LOAD_TIP_LINE: the reference cantilever, F_z = -1/count on nodes ix = nelx, iz <= max(1, nz/6),
+//     every iy of the padded grid (fea.cpp:388-403);
+//   T3D_LOAD_TOP_TRACTION: total -1 in z spread evenly over the nodes of the top face iz = nelz;
+//   T3D_LOAD_TORSION: +1 in y spread over the line ix = nelx, iz = nelz and -1 in y over ix = nelx,
+//     iz = 0 (a couple about the x axis at the free end).
+static int setup_load(Context* c) {
+    const Grid& g = c->g;
+    const Cuboid& q = c->cub;
+    T3D_CUDA_OK(cudaMemsetAsync(c->b, 0, 3 * g.NN * sizeof(double), c->st));
+    const int y0 = g.ny - q.nely, y1 = g.ny;    // node rows of the solid region (grid y)
+    if (c->load_case == T3D_LOAD_TIP_LINE) {
+        const int ix_load = std::min(q.nelx, g.nnx - 1);
+        const int iz_max = std::max(1, g.nz / 6);
+        const int count = (iz_max + 1) * g.nny;
+        launch_setup_load(g, ix_load, iz_max, -1.0 / (double)count, c->mask0, c->b, c->st);
+    } else if (c->load_case == T3D_LOAD_TOP_TRACTION) {
+        const double f = -1.0 / ((double)(q.nelx + 1) * (q.nely + 1));
+        launch_setup_box_load(g, 0, q.nelx, y0, y1, q.nelz, q.nelz, 2, f, c->mask0, c->b, c->st);
+    } else {
+        const double f = 1.0 / (double)(q.nely + 1);
+        launch_setup_box_load(g, q.nelx, q.nelx, y0, y1, q.nelz, q.nelz, 1, f, c->mask0, c->b, c->st);
+        launch_setup_box_load(g, q.nelx, q.nelx, y0, y1, 0, 0, 1, -f, c->mask0, c->b, c->st);
+    }
+    return launch_check("load set-up");
+}
+
+static int create(int nely, int nelx, int nelz, const t3d_params* prm, const t3d_problem* pb, Context* c) {
     if (nely <= 0 || nelx <= 0 || nelz <= 0) return set_error(T3D_ERR_INVALID, "element counts must be positive");
+    if (pb) {
+        if (pb->load_case < T3D_LOAD_TIP_LINE || pb->load_case > T3D_LOAD_TORSION)
+            return set_error(T3D_ERR_INVALID, "unknown load case");
+        if (pb->num_voids < 0 || pb->num_voids > T3D_MAX_VOIDS)
+            return set_error(T3D_ERR_INVALID, "num_voids must be in [0, T3D_MAX_VOIDS]");
+        c->load_case = pb->load_case;
+        c->voids.n = pb->num_voids;
+        for (int k = 0; k < pb->num_voids; ++k)
+            for (int d = 0; d < 3; ++d) {
+                if (!(pb->voids[k][3 + d] > 0.0)) return set_error(T3D_ERR_INVALID, "void radii must be positive");
+                c->voids.c[k][d] = pb->voids[k][d];
+                c->voids.r[k][d] = pb->voids[k][3 + d];
+            }
+    }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -359,6 +402,14 @@ static int create(int nely, int nelx, int nelz, const t3d_params* prm, Context* 
     c->g = make_grid(nx, ny, nz);
     c->cub = Cuboid{nelx, nely, nelz};
     c->ne = (int64_t)nelx * nely * nelz;
+    if (c->voids.n > 0) {   // solid elements = cuboid minus the void ellipsoids (same test as k_setup_cells)
+        int64_t ne = 0;
+        for (int ez = 0; ez < nelz; ++ez)
+            for (int ey = 0; ey < nely; ++ey)
+                for (int ex = 0; ex < nelx; ++ex) ne += in_void(c->voids, ex, ey, ez) ? 0 : 1;
+        if (ne == 0) return set_error(T3D_ERR_INVALID, "the voids remove every element");
+        c->ne = ne;
+    }
     const Grid& g = c->g;
 
     CHECK(c->alloc(&c->Ke, 576));
@@ -411,15 +462,10 @@ static int create(int nely, int nelx, int nelz, const t3d_params* prm, Context* 
     T3D_CUDA_OK(cudaMemsetAsync(c->scal, 0, 8 * sizeof(double), c->st));
 
     // model: solid cells, fixed DOFs, load (fea.cpp:181-447)
-    launch_setup_cells(g, c->cub, c->solid, c->st);
+    launch_setup_cells(g, c->cub, c->voids, c->solid, c->st);
     launch_setup_mask0(g, c->solid, c->mask0, c->st);
-    {
-        const int ix_load = std::min(nelx, g.nnx - 1);
-        const int iz_max = std::max(1, nz / 6);
-        const int count = (iz_max + 1) * g.nny;
-        launch_setup_load(g, ix_load, iz_max, -1.0 / (double)count, c->mask0, c->b, c->st);
-    }
     CHECK(launch_check("model set-up"));
+    CHECK(setup_load(c));
     CHECK(build_levels(c));
     if (c->mixed) CHECK(build_mixed(c));
     launch_filter_diag(g, c->solid, c->kf, c->fdiag, c->st);
@@ -434,7 +480,7 @@ static void morton_walk(const Context* c, int x0, int y0, int z0, int h, std::ve
     const Cuboid& q = c->cub;
     if (x0 >= q.nelx || y0 >= q.nely || z0 >= q.nelz) return;
     if (h == 1) {
-        out.push_back((int32_t)c->g.cell(x0, c->g.ny - 1 - y0, z0));
+        if (!in_void(c->voids, x0, y0, z0)) out.push_back((int32_t)c->g.cell(x0, c->g.ny - 1 - y0, z0));
         return;
     }
     const int m = h / 2;
@@ -893,12 +939,27 @@ int t3d_params_default(t3d_params* p) {
 
 const char* t3d_last_error(void) { return t3d::g_err.c_str(); }
 
+int t3d_create_problem(int nely, int nelx, int nelz, const t3d_params* p, const t3d_problem* problem,
+                       t3d_context** out) {
+    if (!out || !problem) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    *out = nullptr;
+    t3d_context* c = new (std::nothrow) t3d_context();
+    if (!c) return t3d::set_error(T3D_ERR_OOM, "host allocation failed");
+    int rc = t3d::create(nely, nelx, nelz, p, problem, c);
+    if (rc != T3D_OK) {
+        delete c;
+        return rc;
+    }
+    *out = c;
+    return T3D_OK;
+}
+
 int t3d_create(int nely, int nelx, int nelz, const t3d_params* p, t3d_context** out) {
     if (!out) return t3d::set_error(T3D_ERR_INVALID, "null output pointer");
     *out = nullptr;
     t3d_context* c = new (std::nothrow) t3d_context();
     if (!c) return t3d::set_error(T3D_ERR_OOM, "host allocation failed");
-    int rc = t3d::create(nely, nelx, nelz, p, c);
+    int rc = t3d::create(nely, nelx, nelz, p, nullptr, c);
     if (rc != T3D_OK) {
         delete c;
         return rc;
@@ -922,10 +983,14 @@ int t3d_get_info(const t3d_context* ctx, t3d_info* info) {
     info->orig[0] = ctx->cub.nelx; info->orig[1] = ctx->cub.nely; info->orig[2] = ctx->cub.nelz;
     info->num_elements = ctx->ne;
     info->num_nodes = ctx->g.NN;
-    // free DOFs of the cantilever: nodes used by a solid element and not on the x=0 face
-    {
+    // free DOFs: nodes used by a solid element and not on the x=0 face
+    if (ctx->voids.n == 0) {
         const int64_t ux = ctx->cub.nelx + 1, uy = ctx->cub.nely + 1, uz = ctx->cub.nelz + 1;
         info->num_free = 3 * (ux - 1) * uy * uz;
+    } else {
+        t3d_context* mc = const_cast<t3d_context*>(ctx);   // the free-DOF list is a lazily built cache
+        CHECK(t3d::ensure_free(mc));
+        info->num_free = (int64_t)mc->free_h.size();
     }
     info->num_levels = ctx->nlev;
     for (int l = 0; l < ctx->nlev; ++l) {
@@ -1048,14 +1113,8 @@ int t3d_pcg(t3d_context* ctx, const double* E, const double* b, double* x, doubl
     CHECK(t3d::pcg_solve(ctx, tol, max_it, &its));
     if (iters) *iters = its;
     CHECK(t3d::download_free(ctx, ctx->u, x));
-    // restore the cantilever load for later design iterations
-    T3D_CUDA_OK(cudaMemsetAsync(ctx->b, 0, 3 * ctx->g.NN * sizeof(double), ctx->st));
-    {
-        const int ix_load = std::min(ctx->cub.nelx, ctx->g.nnx - 1);
-        const int iz_max = std::max(1, ctx->g.nz / 6);
-        t3d::launch_setup_load(ctx->g, ix_load, iz_max, -1.0 / (double)((iz_max + 1) * ctx->g.nny), ctx->mask0,
-                               ctx->b, ctx->st);
-    }
+    // restore the context's load for later design iterations
+    CHECK(t3d::setup_load(ctx));
     return t3d::sync(ctx);
 }
 

@@ -15,7 +15,7 @@ __device__ __forceinline__ void node_ijk(const Grid& g, int n, int& ix, int& iy,
 }
 
 // ------------------------------------------------------------------ set-up (fea.cpp:181-447)
-__global__ void k_setup_cells(Grid g, Cuboid c, uint8_t* solid) {
+__global__ void k_setup_cells(Grid g, Cuboid c, VoidSet v, uint8_t* solid) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g.NE) return;
     const int gx = (int)(i % g.ex);
@@ -24,7 +24,7 @@ __global__ void k_setup_cells(Grid g, Cuboid c, uint8_t* solid) {
     const int cx = gx - 1, cy = gy - 1, cz = gz - 1;
     uint8_t s = 0;
     if (cx >= 0 && cx < g.nx && cy >= 0 && cy < g.ny && cz >= 0 && cz < g.nz)
-        s = (cx < c.nelx && cy >= g.ny - c.nely && cz < c.nelz) ? 1 : 0;
+        s = (cx < c.nelx && cy >= g.ny - c.nely && cz < c.nelz && !in_void(v, cx, g.ny - 1 - cy, cz)) ? 1 : 0;
     solid[i] = s;
 }
 
@@ -49,6 +49,16 @@ __global__ void k_setup_load(Grid g, int ix_load, int iz_max, double fz, const u
     const int iy = i % g.nny, iz = i / g.nny;
     const int64_t n = g.node(ix_load, iy, iz);
     if (!(mask[n] & 4)) bz[n] = fz;
+}
+
+// force f on component comp of every free node in a box of nodes (load cases beyond the reference's)
+__global__ void k_setup_box_load(Grid g, int x0, int x1, int y0, int y1, int z0, int z1, int comp, double f,
+                                 const uint8_t* __restrict__ mask, double* __restrict__ b) {
+    const int nx = x1 - x0 + 1, ny = y1 - y0 + 1, nz = z1 - z0 + 1;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nx * ny * nz) return;
+    const int64_t n = g.node(x0 + i % nx, y0 + (i / nx) % ny, z0 + i / (nx * ny));
+    if (!((mask[n] >> comp) & 1)) b[comp * g.NN + n] += f;
 }
 
 // ------------------------------------------------------------------ K(E) u  (fea.cpp:692-837)
@@ -306,8 +316,13 @@ inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t
 
 }  // namespace
 
-void launch_setup_cells(const Grid& g, Cuboid c, uint8_t* solid, cudaStream_t s) {
-    k_setup_cells<<<blocks_for(g.NE, 256), 256, 0, s>>>(g, c, solid);
+void launch_setup_cells(const Grid& g, Cuboid c, const VoidSet& v, uint8_t* solid, cudaStream_t s) {
+    k_setup_cells<<<blocks_for(g.NE, 256), 256, 0, s>>>(g, c, v, solid);
+}
+void launch_setup_box_load(const Grid& g, int x0, int x1, int y0, int y1, int z0, int z1, int comp, double f,
+                           const uint8_t* mask, double* b, cudaStream_t s) {
+    const int n = (x1 - x0 + 1) * (y1 - y0 + 1) * (z1 - z0 + 1);
+    k_setup_box_load<<<blocks_for(n, 256), 256, 0, s>>>(g, x0, x1, y0, y1, z0, z1, comp, f, mask, b);
 }
 void launch_setup_mask0(const Grid& g, const uint8_t* solid, uint8_t* mask, cudaStream_t s) {
     k_setup_mask0<<<blocks_for(g.NN, 256), 256, 0, s>>>(g, solid, mask);

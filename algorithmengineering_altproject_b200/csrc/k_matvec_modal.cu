@@ -25,6 +25,9 @@
 // share their halo planes through L2.
 #include <algorithm>
 #include <cmath>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "kernels.hpp"
 #include "red.cuh"
@@ -344,8 +347,20 @@ int modal_tiling(const Grid& g, int dev, int variant, ModalTiling* t) {
     return 0;
 }
 
+// The choice is cached per (device, grid) for the life of the process, so that every context of one grid
+// size uses the same tile shape: results then do not depend on which contexts ran before or beside it
+// (the shape fixes the block order of the FP64 p.Ap partial sums).
 int modal_autotune(const Grid& g, int dev, const ModalKe& kh, const float* E, const uint8_t* mask, const float* u,
                    float* y, cudaStream_t s, ModalTiling* best) {
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int, int>, ModalTiling> cache;
+    const auto key = std::make_tuple(dev, g.nx, g.ny, g.nz);
+    std::lock_guard<std::mutex> lock(mu);
+    const auto hit = cache.find(key);
+    if (hit != cache.end()) {
+        *best = hit->second;
+        return modal_tiling(g, dev, best->variant, best);   // sets the shared-memory attribute on this device
+    }
     cudaEvent_t e0, e1;
     cudaError_t e = cudaEventCreate(&e0);
     if (e != cudaSuccess) return set_cuda_error(e, "cudaEventCreate", __FILE__, __LINE__);
@@ -377,6 +392,7 @@ int modal_autotune(const Grid& g, int dev, const ModalKe& kh, const float* E, co
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    if (rc == 0) cache[key] = *best;
     return rc;
 }
 

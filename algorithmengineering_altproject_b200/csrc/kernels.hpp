@@ -10,6 +10,24 @@ struct Cuboid {          // solid region of the padded grid (fea.cpp:204-215)
     int nelx, nely, nelz;
 };
 
+// Passive-void ellipsoids removed from the cuboid (absent voxels, like the padding of fea.cpp:204-215):
+// element (ex, ey, ez) in the reference's element coordinates is void when its centre lies inside.
+constexpr int MAX_VOIDS = 4;
+struct VoidSet {
+    int n;
+    double c[MAX_VOIDS][3];   // centres (element units)
+    double r[MAX_VOIDS][3];   // radii (element units, > 0)
+};
+__host__ __device__ inline bool in_void(const VoidSet& v, int ex, int ey, int ez) {
+    for (int k = 0; k < v.n; ++k) {
+        const double dx = (ex + 0.5 - v.c[k][0]) / v.r[k][0];
+        const double dy = (ey + 0.5 - v.c[k][1]) / v.r[k][1];
+        const double dz = (ez + 0.5 - v.c[k][2]) / v.r[k][2];
+        if (dx * dx + dy * dy + dz * dz <= 1.0) return true;
+    }
+    return false;
+}
+
 int set_cuda_error(cudaError_t e, const char* what, const char* file, int line);
 int set_error(int code, const std::string& msg);
 
@@ -32,10 +50,13 @@ struct MgLevel32 {       // FP32 copy of a level's vectors for the mixed-precisi
 };
 
 // ---- model set-up (fea.cpp:181-447)
-void launch_setup_cells(const Grid& g, Cuboid c, uint8_t* solid, cudaStream_t s);
+void launch_setup_cells(const Grid& g, Cuboid c, const VoidSet& v, uint8_t* solid, cudaStream_t s);
 void launch_setup_mask0(const Grid& g, const uint8_t* solid, uint8_t* mask, cudaStream_t s);
 void launch_setup_load(const Grid& g, int ix_load, int iz_max, double fz, const uint8_t* mask, double* b,
                        cudaStream_t s);
+// force f (component comp) on every free DOF of the node box [x0,x1]x[y0,y1]x[z0,z1] (grid coordinates)
+void launch_setup_box_load(const Grid& g, int x0, int x1, int y0, int y1, int z0, int z1, int comp, double f,
+                           const uint8_t* mask, double* b, cudaStream_t s);
 
 // ---- FEA operators
 // Ke: device pointer to the 576 stiffness coefficients

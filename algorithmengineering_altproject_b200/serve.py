@@ -1,0 +1,265 @@
+"""Continuous-batching design server on one GPU.
+
+Requests (grid dims, volume fraction, load case, passive voids, OC iteration count) are admitted in
+arrival order as soon as a slot and the HBM budget allow: each admitted request gets its own device
+context (model, MG hierarchy, density, warm-start displacement and filter state stay resident for all
+its OC iterations) and its own CUDA stream, and runs on a worker thread, so the kernels of all
+admitted requests overlap on the device while later arrivals wait.  The projected footprint of a
+request is bytes-per-node (learned from the contexts created so far, per precision) times its padded
+node count, with a margin; a request that alone exceeds the budget is rejected.
+
+The reference has no batching or serving (its driver runs one cuboid design per process,
+driver.cpp:23-280); this module is the request loop around the same design iteration.
+
+    python -m algorithmengineering_altproject_b200.serve --rate 2 --requests 24 --iters 10
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import threading
+import time
+from concurrent.futures import Future
+
+import numpy as np
+
+from . import (T3D_FP64, T3D_MIXED, T3D_SUM_FP64, Problem, ProblemSpec, T3DError)
+
+# bytes per padded grid node of a context, before the first context of a precision is measured
+DEFAULT_BYTES_PER_NODE = {T3D_FP64: 900.0, T3D_MIXED: 1100.0}
+MARGIN = 1.15
+
+
+class DesignRequest:
+    def __init__(self, nely, nelx, nelz, V0, load_case=0, voids=(), iters=40, rid=None, keep_density=False):
+        self.nely, self.nelx, self.nelz = int(nely), int(nelx), int(nelz)
+        self.V0 = float(V0)
+        self.load_case = int(load_case)
+        self.voids = [tuple(float(x) for x in v) for v in voids]
+        self.iters = int(iters)
+        self.rid = rid
+        self.keep_density = keep_density
+        self.arrival = None
+
+    def padded_nodes(self):
+        # dims of multiples of 8 are never padded (the reference's rule pads to multiples of 2^L)
+        return (self.nelx + 1) * (self.nely + 1) * (self.nelz + 1)
+
+    def spec(self):
+        return ProblemSpec.make(self.load_case, self.voids)
+
+    def as_dict(self):
+        return {"rid": self.rid, "dims": [self.nely, self.nelx, self.nelz], "V0": self.V0,
+                "load_case": self.load_case, "voids": len(self.voids), "iters": self.iters}
+
+
+class DesignResult:
+    def __init__(self, req):
+        self.request = req
+        self.c_solid = None
+        self.objectives = []
+        self.pcg_iters = []
+        self.density = None
+        self.error = None
+        self.admitted = None
+        self.finished = None
+
+    @property
+    def latency(self):
+        return self.finished - self.request.arrival
+
+
+class DesignServer:
+    """Admits DesignRequests against an HBM budget and runs them concurrently on one GPU."""
+
+    def __init__(self, device=0, hbm_budget=160e9, max_active=8, precision=T3D_MIXED, **params):
+        self.device = device
+        self.budget = float(hbm_budget)
+        self.max_active = int(max_active)
+        self.precision = precision
+        self.params = dict(params)
+        self._cv = threading.Condition()
+        self._queue = []            # (request, future) in arrival order
+        self._active = 0
+        self._reserved = 0.0
+        self._bpn = dict(DEFAULT_BYTES_PER_NODE)
+        self._closed = False
+        self._threads = []
+        self._dispatcher = threading.Thread(target=self._dispatch, daemon=True)
+        self._dispatcher.start()
+
+    # ---- public API
+    def submit(self, req: DesignRequest) -> Future:
+        fut = Future()
+        req.arrival = time.perf_counter() if req.arrival is None else req.arrival
+        if self.projected_bytes(req) > self.budget:
+            res = DesignResult(req)
+            res.error = "projected footprint %.3g B exceeds the HBM budget" % self.projected_bytes(req)
+            res.finished = time.perf_counter()
+            fut.set_result(res)
+            return fut
+        with self._cv:
+            self._queue.append((req, fut))
+            self._cv.notify_all()
+        return fut
+
+    def projected_bytes(self, req):
+        return MARGIN * self._bpn[self.precision] * req.padded_nodes()
+
+    def close(self):
+        with self._cv:
+            self._closed = True
+            self._cv.notify_all()
+        self._dispatcher.join()
+        for t in self._threads:
+            t.join()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    # ---- internals
+    def _dispatch(self):
+        while True:
+            with self._cv:
+                while True:
+                    if self._queue:
+                        req, fut = self._queue[0]
+                        need = self.projected_bytes(req)
+                        if self._active < self.max_active and self._reserved + need <= self.budget:
+                            self._queue.pop(0)
+                            self._active += 1
+                            self._reserved += need
+                            break
+                    elif self._closed:
+                        return
+                    self._cv.wait()
+            t = threading.Thread(target=self._run, args=(req, fut, need), daemon=True)
+            self._threads.append(t)
+            t.start()
+
+    def _run(self, req, fut, need):
+        res = DesignResult(req)
+        res.admitted = time.perf_counter()
+        try:
+            self._execute(req, res)
+        except T3DError as e:
+            res.error = str(e)
+        finally:
+            res.finished = time.perf_counter()
+            with self._cv:
+                self._active -= 1
+                self._reserved -= need
+                self._cv.notify_all()
+            fut.set_result(res)
+
+    def _execute(self, req, res):
+        """Runs one request to completion on its own context (and stream)."""
+        P = Problem(req.nely, req.nelx, req.nelz, problem=req.spec(), device=self.device,
+                    precision=self.precision, oc_sum_order=T3D_SUM_FP64, **self.params)
+        try:
+            with self._cv:   # learn the footprint per node from the real allocation
+                self._bpn[self.precision] = max(self._bpn[self.precision], P.device_bytes / P.nn)
+            res.c_solid = P.design_init(req.V0)
+            for _ in range(req.iters):
+                r = P.design_step()
+                res.objectives.append(r["obj"])
+                res.pcg_iters.append(r["pcg_iters"])
+            if req.keep_density:
+                res.density = P.density()
+        finally:
+            P.close()
+
+
+# ---------------------------------------------------------------- workload generators
+def _round8(v):
+    return max(8, int(round(v / 8.0)) * 8)
+
+
+def draw_instance(rng, nelx=None, iters=40):
+    """One instance drawn as in the batched workload: nelx a multiple of 8 in [32, 192]; nely, nelz =
+    nelx/2 scaled by U(0.5, 1.0), multiples of 8; V0 ~ U(0.06, 0.30); load case uniform over the three;
+    0-3 void ellipsoids with radii 10-25 % of the shortest side at uniform centres."""
+    if nelx is None:
+        nelx = int(rng.integers(4, 25)) * 8
+    nely = _round8(nelx / 2 * rng.uniform(0.5, 1.0))
+    nelz = _round8(nelx / 2 * rng.uniform(0.5, 1.0))
+    short = min(nelx, nely, nelz)
+    voids = []
+    for _ in range(int(rng.integers(0, 4))):
+        r = [short * rng.uniform(0.10, 0.25) for _ in range(3)]
+        c = [rng.uniform(0, nelx), rng.uniform(0, nely), rng.uniform(0, nelz)]
+        voids.append(tuple(c + r))
+    return DesignRequest(nely, nelx, nelz, rng.uniform(0.06, 0.30), int(rng.integers(0, 3)), voids, iters)
+
+
+def draw_served(rng, iters=40, median=0.5e6, lo=30e3, hi=16e6):
+    """A served request: element count lognormal (median 0.5M, clipped to [30k, 16M]); shape, V0, load
+    case and voids as draw_instance."""
+    ne = float(np.clip(rng.lognormal(math.log(median), 1.0), lo, hi))
+    ay, az = rng.uniform(0.5, 1.0), rng.uniform(0.5, 1.0)
+    nelx = _round8((ne / (0.25 * ay * az)) ** (1.0 / 3.0))
+    req = draw_instance(rng, nelx=nelx, iters=iters)
+    return req
+
+
+def percentile(v, q):
+    return float(np.percentile(np.asarray(v), q)) if len(v) else None
+
+
+def run_poisson(server, rng, rate, n, iters, median=0.5e6, hi=16e6):
+    """Submits n served requests with Poisson arrivals at `rate` per second; returns the results."""
+    futs = []
+    t0 = time.perf_counter()
+    t_next = t0
+    for k in range(n):
+        req = draw_served(rng, iters=iters, median=median, hi=hi)
+        req.rid = k
+        now = time.perf_counter()
+        if t_next > now:
+            time.sleep(t_next - now)
+        req.arrival = time.perf_counter()
+        futs.append(server.submit(req))
+        t_next += rng.exponential(1.0 / rate)
+    results = [f.result() for f in futs]
+    return results, time.perf_counter() - t0
+
+
+def summary(results, wall):
+    ok = [r for r in results if r.error is None]
+    lat = [r.latency for r in ok]
+    return {"requests": len(results), "completed": len(ok), "errors": [r.error for r in results if r.error],
+            "designs_per_s": len(ok) / wall if wall > 0 else None, "wall_s": wall,
+            "latency_s": {"p50": percentile(lat, 50), "p95": percentile(lat, 95), "p99": percentile(lat, 99)}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--rate", type=float, default=2.0)
+    ap.add_argument("--requests", type=int, default=24)
+    ap.add_argument("--iters", type=int, default=10)
+    ap.add_argument("--max-active", type=int, default=8)
+    ap.add_argument("--budget-gb", type=float, default=160.0)
+    ap.add_argument("--median", type=float, default=0.5e6)
+    ap.add_argument("--max-elements", type=float, default=16e6)
+    ap.add_argument("--seed", type=int, default=20251203)
+    ap.add_argument("--sequential-fp64", action="store_true", help="also run the same requests one at a time in FP64")
+    a = ap.parse_args()
+    rng = np.random.default_rng(a.seed)
+    with DesignServer(hbm_budget=a.budget_gb * 1e9, max_active=a.max_active, precision=T3D_MIXED) as srv:
+        res, wall = run_poisson(srv, rng, a.rate, a.requests, a.iters, a.median, a.max_elements)
+    out = {"mode": "continuous batching, mixed precision", "rate_per_s": a.rate, "iters": a.iters,
+           "max_active": a.max_active, "budget_gb": a.budget_gb, **summary(res, wall)}
+    if a.sequential_fp64:
+        rng = np.random.default_rng(a.seed)
+        with DesignServer(hbm_budget=a.budget_gb * 1e9, max_active=1, precision=T3D_FP64) as srv:
+            res2, wall2 = run_poisson(srv, rng, a.rate, a.requests, a.iters, a.median, a.max_elements)
+        out["sequential_fp64"] = summary(res2, wall2)
+    print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

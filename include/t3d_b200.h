@@ -59,6 +59,22 @@ typedef struct t3d_params {
     int   reserved[6];
 } t3d_params;
 
+/* Problem spec beyond the reference's built-in cantilever (the reference hard-codes one load case and a
+ * full cuboid, fea.cpp:181-447; the MATLAB original reads loads and passive regions from files,
+ * TOP3D_XL.m:1319-1362,1536-1612).  Fixations stay the reference's: the x = 0 face and every node
+ * touched by no solid element (fea.cpp:374-417). */
+enum { T3D_LOAD_TIP_LINE = 0, T3D_LOAD_TOP_TRACTION = 1, T3D_LOAD_TORSION = 2 };
+#define T3D_MAX_VOIDS 4
+typedef struct t3d_problem {
+    int    load_case;             /* T3D_LOAD_*: TIP_LINE = the reference's -Z line load at x = nelx;
+                                     TOP_TRACTION = total -1 in z over the top-face nodes (z = nelz);
+                                     TORSION = +1 / -1 in y over the lines x = nelx, z = nelz / z = 0 */
+    int    num_voids;             /* passive-void ellipsoids, 0..T3D_MAX_VOIDS */
+    double voids[T3D_MAX_VOIDS][6]; /* centre (ex, ey, ez) and radii (rx, ry, rz) in element units of the
+                                     reference's element coordinates; an element whose centre
+                                     (ex+0.5, ey+0.5, ez+0.5) lies inside is absent from the model */
+} t3d_problem;
+
 typedef struct t3d_info {
     int64_t res[3];               /* padded element counts resX,resY,resZ (padding.hpp:42-53) */
     int64_t orig[3];              /* original nelx, nely, nelz */
@@ -89,6 +105,10 @@ int  t3d_params_default(t3d_params* p);
 /* CreateVoxelFEAmodel_Cuboid + ApplyBoundaryConditions + mg::build_static_once + SetupPDEFilter
  * (fea.cpp:181-447, preconditioner.cpp:19-34, filter.cpp:9-75) for the built-in cantilever. */
 int  t3d_create(int nely, int nelx, int nelz, const t3d_params* p, struct t3d_context** out);
+/* t3d_create for a problem spec: load case and passive voids.  Element arrays cover only the solid
+ * (non-void) elements, in the reference's Morton order of those elements */
+int  t3d_create_problem(int nely, int nelx, int nelz, const t3d_params* p, const t3d_problem* problem,
+                        struct t3d_context** out);
 int  t3d_destroy(struct t3d_context* ctx);
 int  t3d_get_info(const struct t3d_context* ctx, t3d_info* info);
 const char* t3d_last_error(void);

@@ -1,0 +1,66 @@
+"""Admission logic of the design server, on the CPU: requests are admitted in arrival order while a
+slot and the HBM budget allow, never more at once than either limit, and a request that alone exceeds
+the budget is rejected.  The device work is replaced by a timed sleep (the GPU path is covered by
+tests/test_gpu_serve.py)."""
+import threading
+import time
+
+import algorithmengineering_altproject_b200.serve as serve
+
+
+class FakeServer(serve.DesignServer):
+    def __init__(self, *a, **kw):
+        self.log = []
+        self.peak_active = 0
+        self.peak_bytes = 0.0
+        self._lk = threading.Lock()
+        super().__init__(*a, **kw)
+
+    def _execute(self, req, res):
+        with self._lk:
+            self.log.append(req.rid)
+            self.peak_active = max(self.peak_active, self._active)
+            self.peak_bytes = max(self.peak_bytes, self._reserved)
+        time.sleep(0.05)
+        res.objectives = [float(req.rid)]
+
+
+def test_admission_respects_slots_budget_and_order():
+    reqs = [serve.DesignRequest(8, 16, 8, 0.1, rid=k, iters=1) for k in range(12)]
+    one = FakeServer(hbm_budget=1e18).projected_bytes(reqs[0])
+    srv = FakeServer(hbm_budget=3.5 * one, max_active=8)   # the budget, not the slots, limits to 3
+    futs = [srv.submit(r) for r in reqs]
+    res = [f.result() for f in futs]
+    srv.close()
+    assert [r.objectives[0] for r in res] == list(range(12))
+    assert srv.log == list(range(12))            # admitted in arrival order
+    assert srv.peak_active <= 3 and srv.peak_bytes <= 3.5 * one
+    assert all(r.latency >= 0.05 for r in res)
+
+
+def test_slots_limit_and_oversized_rejection():
+    srv = FakeServer(hbm_budget=1e18, max_active=2)
+    futs = [srv.submit(serve.DesignRequest(8, 16, 8, 0.1, rid=k, iters=1)) for k in range(6)]
+    [f.result() for f in futs]
+    assert srv.peak_active <= 2
+    srv.close()
+    small = FakeServer(hbm_budget=1e6, max_active=2)
+    r = small.submit(serve.DesignRequest(64, 128, 64, 0.1, rid=0)).result()
+    small.close()
+    assert r.error and "budget" in r.error
+
+
+def test_workload_generators_follow_the_batched_distributions():
+    import numpy as np
+    rng = np.random.default_rng(20251203)
+    for _ in range(200):
+        q = serve.draw_instance(rng)
+        assert q.nelx % 8 == 0 and q.nely % 8 == 0 and q.nelz % 8 == 0
+        assert 32 <= q.nelx <= 192 and 0.06 <= q.V0 <= 0.30 and q.load_case in (0, 1, 2)
+        assert len(q.voids) <= 3
+        short = min(q.nelx, q.nely, q.nelz)
+        assert all(0.10 * short <= v[3 + d] <= 0.25 * short for v in q.voids for d in range(3))
+    for _ in range(200):
+        q = serve.draw_served(rng)
+        ne = q.nelx * q.nely * q.nelz
+        assert 8 * 8 * 8 <= ne <= 2.2 * 16e6
