@@ -101,6 +101,7 @@ _SIGS = {
     "t3d_matvec32": (C.c_int, [_CTX, _f64p, _f64p, _f64p]),
     "t3d_mg_setup": (C.c_int, [_CTX, _f64p]),
     "t3d_vcycle": (C.c_int, [_CTX, _f64p, _f64p]),
+    "t3d_vcycle32": (C.c_int, [_CTX, _f64p, _f64p]),
     "t3d_pcg": (C.c_int, [_CTX, _f64p, _f64p, _f64p, C.c_double, C.c_int, C.POINTER(C.c_int)]),
     "t3d_compliance": (C.c_int, [_CTX, _f64p, _f64p, _f64p, C.POINTER(C.c_double)]),
     "t3d_mg_get_diag": (C.c_int, [_CTX, C.c_int, _f64p]),
@@ -267,6 +268,12 @@ class Problem:
     def vcycle(self, rFree):
         z = np.zeros(self.nf)
         _check(self._lib.t3d_vcycle(self._h, _f64(rFree), z))
+        return z
+
+    def vcycle32(self, rFree):
+        """the FP32 V-cycle of the mixed-precision inner solve (mixed contexts only), widened to FP64"""
+        z = np.zeros(self.nf)
+        _check(self._lib.t3d_vcycle32(self._h, _f64(rFree), z))
         return z
 
     def PCG_free(self, eleE, bFree, xFree, tol=None, maxIt=800):

@@ -1101,6 +1101,22 @@ int t3d_vcycle(t3d_context* ctx, const double* r, double* z) {
     return t3d::download_free(ctx, ctx->z, z);
 }
 
+int t3d_vcycle32(t3d_context* ctx, const double* r, double* z) {
+    API_GUARD(ctx);
+    if (!r || !z) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    if (!ctx->mixed) return t3d::set_error(T3D_ERR_INVALID, "FP32 kernels need precision T3D_MIXED");
+    if (!ctx->mg_ready) return t3d::set_error(T3D_ERR_INVALID, "t3d_mg_setup not called");
+    CHECK(t3d::upload_free(ctx, r, ctx->r));
+    t3d::launch_cast(3 * ctx->g.NN, ctx->r, ctx->r32, ctx->st);
+    T3D_CUDA_OK(cudaMemsetAsync(ctx->S32, 0, sizeof(t3d::PcgScalars), ctx->st));
+    ctx->launches += 1;
+    t3d::vcycle32(ctx, ctx->r32, ctx->z32, ctx->S32, ctx->slot[2]);
+    t3d::launch_widen(3 * ctx->g.NN, ctx->z32, ctx->z, ctx->st);
+    ctx->launches += 1;
+    CHECK(t3d::launch_check("vcycle32"));
+    return t3d::download_free(ctx, ctx->z, z);
+}
+
 int t3d_pcg(t3d_context* ctx, const double* E, const double* b, double* x, double tol, int max_it, int* iters) {
     API_GUARD(ctx);
     if (!E || !b || !x || max_it < 0) return t3d::set_error(T3D_ERR_INVALID, "bad argument");

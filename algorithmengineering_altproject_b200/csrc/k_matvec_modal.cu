@@ -279,10 +279,11 @@ constexpr ModalVariant variant_of() {
     return ModalVariant{V::bx, V::by, V::smem, &V::fn, &V::launch};
 }
 const ModalVariant MODAL_VARIANTS[] = {
-    variant_of<ModalShape<32, 16, 2, 3>>(),
-    variant_of<ModalShape<32, 8, 3, 3>>(),
+    variant_of<ModalShape<32, 8, 2, 4>>(),
     variant_of<ModalShape<32, 8, 2, 3>>(),
-    variant_of<ModalShape<32, 16, 1, 3>>(),
+    variant_of<ModalShape<32, 8, 3, 3>>(),
+    variant_of<ModalShape<32, 16, 2, 3>>(),
+    variant_of<ModalShape<32, 16, 1, 4>>(),
 };
 constexpr int MODAL_NVARIANTS = sizeof(MODAL_VARIANTS) / sizeof(MODAL_VARIANTS[0]);
 constexpr int MODAL_SLAB_MIN = 8;

@@ -306,6 +306,11 @@ __global__ void k_prolong_smooth32(MgLevel32 Lc, MgLevel32 Lf, const float* __re
     }
 }
 
+// Finest-level prolongation + smoothing + r.z.  Each lane takes a run of SP consecutive fine nodes of one
+// row that share one coarse cell in x (fine x = SP * j + k): the 8 coarse corners are gathered once and
+// interpolated in y and z once per run; each node then only interpolates in x.  The last node of a row
+// (fine x = nx, clamped to the last coarse cell with weight 1) is its own run.
+template <int SP>
 __global__ void __launch_bounds__(RED_THREADS) k_prolong_smooth0_32(MgLevel32 Lc, MgLevel32 Lf,
                                                                     const float* __restrict__ xc,
                                                                     const float* __restrict__ r,
@@ -315,47 +320,52 @@ __global__ void __launch_bounds__(RED_THREADS) k_prolong_smooth0_32(MgLevel32 Lc
     if (S->done) return;
     const int NN = (int)Lf.nn;
     const int fnx = Lf.nx + 1, fny = Lf.ny + 1;
-    // items of 4 x 32 consecutive nodes of one row (row = fz * fny + fy); each lane takes 4 nodes 32 apart
-    // and issues all their loads before using any of them
-    constexpr int U = 4;
-    const int chunks = (fnx + 32 * U - 1) / (32 * U);
+    const int cnx = Lc.nx + 1, cny = Lc.ny + 1, cnn = (int)Lc.nn;
+    const int runs = Lf.nx / SP + 1;                 // runs per row (the last one is the single node x = nx)
+    const int chunks = (runs + 31) >> 5;
     const int items = chunks * fny * (Lf.nz + 1);
     const int lane = threadIdx.x & 31;
     const int nw = (gridDim.x * blockDim.x) >> 5;
-    const int sh2 = __ffs(Lc.span) - 1;
+    constexpr float inv = 1.0f / (float)SP;          // exact: SP is a power of two
     double part = 0.0;
     for (int it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < items; it += nw) {
         const int row = it / chunks;
-        const int x0 = (it - row * chunks) * (32 * U) + lane;
+        const int j = (it - row * chunks) * 32 + lane;
+        if (j >= runs) continue;
         const int fz = row / fny, fy = row - fz * fny;
-        const int nb = row * fnx;
-        float rv[U][3], dv[U][3];
-        int mv[U];
+        int cx = j, cy = fy / SP, cz = fz / SP;
+        int ry = fy - cy * SP, rz = fz - cz * SP;
+        const bool last = cx >= Lc.nx;               // fine x = nx: weight 1 on the last coarse node
+        if (last) cx = Lc.nx - 1;
+        if (cy >= Lc.ny) { cy = Lc.ny - 1; ry = SP; }
+        if (cz >= Lc.nz) { cz = Lc.nz - 1; rz = SP; }
+        const float wy1 = ry * inv, wy0 = 1.0f - wy1, wz1 = rz * inv, wz0 = 1.0f - wz1;
+        const int b = (cz * cny + cy) * cnx + cx, pz = cnx * cny;
+        float L[3], R[3];
 #pragma unroll
-        for (int k = 0; k < U; ++k) {
-            const int fx = x0 + 32 * k;
-            const bool in = fx < fnx;
-            const int n = nb + (in ? fx : 0);
-            mv[k] = in ? (int)Lf.mask[n] : 7;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                rv[k][c] = in ? r[c * NN + n] : 0.0f;
-                dv[k][c] = in ? Lf.diag[c * NN + n] : 0.0f;
-            }
+        for (int c = 0; c < 3; ++c) {
+            const float* X = xc + c * cnn;
+            const float x00 = X[b], x10 = X[b + 1], x01 = X[b + cnx], x11 = X[b + cnx + 1];
+            const float y00 = X[b + pz], y10 = X[b + pz + 1], y01 = X[b + pz + cnx], y11 = X[b + pz + cnx + 1];
+            L[c] = fmaf(wz1, fmaf(wy1, y01, wy0 * y00), wz0 * fmaf(wy1, x01, wy0 * x00));
+            R[c] = fmaf(wz1, fmaf(wy1, y11, wy0 * y10), wz0 * fmaf(wy1, x11, wy0 * x10));
         }
+        const int nb = row * fnx + SP * j;
+        const int nk = last ? 1 : SP;
 #pragma unroll
-        for (int k = 0; k < U; ++k) {
-            const int fx = x0 + 32 * k;
-            if (fx >= fnx) break;
-            const int n = nb + fx;
-            float P[3];
-            prolong_node32(Lc, xc, fx, fy, fz, sh2, P);
+        for (int k = 0; k < SP; ++k) {
+            if (k >= nk) break;
+            const int n = nb + k;
+            const float wx1 = last ? 1.0f : k * inv, wx0 = 1.0f - wx1;
+            const int m = Lf.mask[n];
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                const float t = (w * rv[k][c]) * dv[k][c];
-                const float zv = ((mv[k] >> c) & 1) ? 0.0f : (t + P[c]) + t;
+                const float rv = r[c * NN + n];
+                const float t = (w * rv) * Lf.diag[c * NN + n];
+                const float P = fmaf(wx1, R[c], wx0 * L[c]);
+                const float zv = ((m >> c) & 1) ? 0.0f : (t + P) + t;
                 z[c * NN + n] = zv;
-                part = fma((double)rv[k][c], (double)zv, part);
+                part = fma((double)rv, (double)zv, part);
             }
         }
     }
@@ -477,7 +487,8 @@ void launch_prolong_smooth32(const MgLevel32& Lc, const MgLevel32& Lf, const flo
 }
 void launch_prolong_smooth0_32(const MgLevel32& Lc, const MgLevel32& Lf, const float* xc, const float* r, float* z,
                                float w, RedSlot dot, PcgScalars* S, cudaStream_t s) {
-    k_prolong_smooth0_32<<<RED_BLOCKS, RED_THREADS, 0, s>>>(Lc, Lf, xc, r, z, w, dot, S);
+    if (Lc.span == 4) k_prolong_smooth0_32<4><<<RED_BLOCKS, RED_THREADS, 0, s>>>(Lc, Lf, xc, r, z, w, dot, S);
+    else k_prolong_smooth0_32<2><<<RED_BLOCKS, RED_THREADS, 0, s>>>(Lc, Lf, xc, r, z, w, dot, S);
 }
 void launch_coarse_solve32(const MgLevel32& L, const double* X, int N, const int* status, const PcgScalars* S,
                            cudaStream_t s) {

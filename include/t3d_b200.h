@@ -130,6 +130,9 @@ int  t3d_matvec32(struct t3d_context* ctx, const double* ele_E, const double* u_
 int  t3d_mg_setup(struct t3d_context* ctx, const double* ele_E);
 /* the preconditioner closure z = M^-1 r (preconditioner.cpp:88-265) */
 int  t3d_vcycle(struct t3d_context* ctx, const double* r_free, double* z_free);
+/* the preconditioner in the FP32 form of the mixed-precision inner solve (mixed contexts, after
+ * t3d_mg_setup): r rounded to FP32, z returned widened to FP64 */
+int  t3d_vcycle32(struct t3d_context* ctx, const double* r_free, double* z_free);
 /* PCG_free (solver.hpp:24-27, solver.cpp:87-217) with the preconditioner of t3d_mg_setup;
  * x_free is the warm start on entry and the solution on return */
 int  t3d_pcg(struct t3d_context* ctx, const double* ele_E, const double* b_free, double* x_free, double tol,

@@ -4,7 +4,8 @@ Two FP32 forms exist: the modal (corner-Hadamard) kernel, used whenever Ke is th
 axis-aligned cubic isotropic voxel, and the dense 24x24 gather kernel.  Both compute the reference's
 K_times_u_finest (fea.cpp:763-837) with FP32 inputs, so each must agree with the FP64 product to
 FP32 accuracy: ||y32 - y64|| <= 2e-6 ||y64|| on random moduli and displacements.  The grids cover a
-padded one (30x60x30 -> 64x32x32 elements) and ones that do not divide the kernel's 31x15 node tiles.
+padded one (30x60x30 -> 64x32x32 elements) and ones that do not divide the kernel's node tiles.
+The FP32 V-cycle of the same inner solve is checked against the FP64 V-cycle the same way (1e-5).
 """
 import numpy as np
 import pytest
@@ -66,4 +67,20 @@ def test_modal_matvec_p_dot_ap_is_deterministic():
     a = P.K_times_u_finest32(E, u)
     b = P.K_times_u_finest32(E, u)
     np.testing.assert_array_equal(a, b)
+    P.close()
+
+
+@pytest.mark.parametrize("dims", [(6, 12, 6), (30, 60, 30), (17, 40, 23)])
+def test_fp32_vcycle_matches_fp64(dims):
+    # the FP32 V-cycle (transfers, smoother, FP64 coarsest solve on the FP32 residual) against the FP64 one on
+    # the same FP32-rounded residual: ||z32 - z64|| <= 1e-5 ||z64||
+    import algorithmengineering_altproject_b200 as t3d
+    P = t3d.Problem(*dims, precision=t3d.T3D_MIXED)
+    rng = np.random.default_rng(9)
+    E = rng.uniform(1e-3, 1.0, P.ne)
+    P.make_diagonal_preconditioner_from_static(E)
+    r = rng.standard_normal(P.nf).astype(np.float32).astype(np.float64)
+    z64 = P.vcycle(r)
+    z32 = P.vcycle32(r)
+    assert np.linalg.norm(z32 - z64) <= 1e-5 * np.linalg.norm(z64), np.linalg.norm(z32 - z64) / np.linalg.norm(z64)
     P.close()
