@@ -415,9 +415,27 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_update32(Grid g, float* __r
     if (S->done) return;
     const double den = S->denom;
     const float alpha = (float)(S->rz / (1.0e-30 < den ? den : 1.0e-30));
-    const int64_t n3 = 3 * g.NN;
+    // the three component planes are contiguous: one flat vector of 3 NN floats, 16-byte accesses
+    // (cudaMalloc bases are 256-byte aligned) and a scalar tail
+    const int n3 = (int)(3 * g.NN), n4 = n3 >> 2;
+    const int stride = gridDim.x * blockDim.x;
+    float4* __restrict__ x4 = reinterpret_cast<float4*>(x);
+    float4* __restrict__ r4 = reinterpret_cast<float4*>(r);
+    const float4* __restrict__ p4 = reinterpret_cast<const float4*>(p);
+    const float4* __restrict__ a4 = reinterpret_cast<const float4*>(Ap);
     double part = 0.0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (int64_t)gridDim.x * blockDim.x) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
+        const float4 pv = p4[i], av = a4[i];
+        float4 xv = x4[i], rv = r4[i];
+        xv.x = fmaf(alpha, pv.x, xv.x); xv.y = fmaf(alpha, pv.y, xv.y);
+        xv.z = fmaf(alpha, pv.z, xv.z); xv.w = fmaf(alpha, pv.w, xv.w);
+        rv.x = fmaf(-alpha, av.x, rv.x); rv.y = fmaf(-alpha, av.y, rv.y);
+        rv.z = fmaf(-alpha, av.z, rv.z); rv.w = fmaf(-alpha, av.w, rv.w);
+        x4[i] = xv;
+        r4[i] = rv;
+        part += (double)fmaf(rv.w, rv.w, fmaf(rv.z, rv.z, fmaf(rv.y, rv.y, rv.x * rv.x)));
+    }
+    for (int i = 4 * n4 + blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += stride) {
         x[i] = fmaf(alpha, p[i], x[i]);
         const float rv = fmaf(-alpha, Ap[i], r[i]);
         r[i] = rv;
@@ -437,9 +455,18 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_update32(Grid g, float* __r
 __global__ void k_pcg_direction32(Grid g, const float* __restrict__ z, float* __restrict__ p, PcgScalars* S) {
     if (S->done) return;
     const float beta = (float)S->beta;
-    const int64_t n3 = 3 * g.NN;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (int64_t)gridDim.x * blockDim.x)
-        p[i] = fmaf(beta, p[i], z[i]);
+    const int n3 = (int)(3 * g.NN), n4 = n3 >> 2;
+    const int stride = gridDim.x * blockDim.x;
+    float4* __restrict__ p4 = reinterpret_cast<float4*>(p);
+    const float4* __restrict__ z4 = reinterpret_cast<const float4*>(z);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
+        const float4 zv = z4[i];
+        float4 pv = p4[i];
+        pv.x = fmaf(beta, pv.x, zv.x); pv.y = fmaf(beta, pv.y, zv.y);
+        pv.z = fmaf(beta, pv.z, zv.z); pv.w = fmaf(beta, pv.w, zv.w);
+        p4[i] = pv;
+    }
+    for (int i = 4 * n4 + blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += stride) p[i] = fmaf(beta, p[i], z[i]);
 }
 
 inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
