@@ -670,8 +670,8 @@ static int pcg_solve(Context* c, double tol, int maxit, int* iters) {
 // ------------------------------------------------------------------ mixed-precision solve
 static void vcycle32(Context* c, const float* r, float* z, PcgScalars* S, RedSlot dot) {
     const int L = c->nlev;
-    // per transition: restriction (x, y, z passes; x-y fused for span 2) and prolongation
-    for (int l = 0; l + 1 < L; ++l) c->launches += c->lv32[l + 1].span == 2 ? 3 : 4;
+    // per transition: restriction (x + y-z passes for span 4, one x-y-z pass for span 2) and prolongation
+    for (int l = 0; l + 1 < L; ++l) c->launches += c->lv32[l + 1].span == 2 ? 2 : 3;
     c->launches += 1;
     for (int l = 0; l + 1 < L; ++l)
         launch_restrict32(c->lv32[l + 1], c->lv32[l], l == 0 ? r : c->lv32[l].r, c->lv32[l + 1].r, c->ra1_32[l],

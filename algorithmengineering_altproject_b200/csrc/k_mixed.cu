@@ -161,101 +161,103 @@ __global__ void k_restrict_x32(MgLevel32 Lc, MgLevel32 Lf, const float* __restri
     a1[2 * total + t] = v2;
 }
 
-__global__ void k_restrict_y32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ a1, float* __restrict__ a2,
-                               const PcgScalars* S) {
-    if (S->done) return;
-    const int cnx = Lc.nx + 1, cny = Lc.ny + 1, fny = Lf.ny + 1, fnz = Lf.nz + 1;
-    const int64_t total = (int64_t)fnz * cny * cnx, total1 = (int64_t)fnz * fny * cnx;
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= total) return;
-    const int cx = (int)(t % cnx);
-    const int cy = (int)((t / cnx) % cny);
-    const int fz = (int)(t / ((int64_t)cnx * cny));
-    const int s = Lc.span, ws = 2 * s - 1;
-    float v0 = 0.0f, v1 = 0.0f, v2 = 0.0f;
-    for (int iy = 0; iy < ws; ++iy) {
-        const int fy = cy * s + iy - (s - 1);
-        if (fy < 0 || fy >= fny) continue;
-        const float w = hatf(iy, s);
-        const int64_t i = ((int64_t)fz * fny + fy) * cnx + cx;
-        v0 = fmaf(w, a1[i], v0);
-        v1 = fmaf(w, a1[total1 + i], v1);
-        v2 = fmaf(w, a1[2 * total1 + i], v2);
+// Sum of the in-range hat weights of the window of coarse index c (span SP) over n fine points.
+template <int SP>
+__device__ __forceinline__ float hat_sum(int c, int n) {
+    float sw = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 2 * SP - 1; ++i) {
+        const int f = c * SP + i - (SP - 1);
+        if (f >= 0 && f < n) sw += hatf(i, SP);
     }
-    a2[t] = v0;
-    a2[total + t] = v1;
-    a2[2 * total + t] = v2;
+    return sw;
 }
 
-// x and y window sums of one fine z-plane in one pass (the x-then-y passes of k_restrict_x32 and
-// k_restrict_y32 fused): a2[fz][cy][cx] = sum_iy w(iy) sum_ix w(ix) r[fz][fy][fx], unnormalised.
+// y and z window sums of the x-pass result a1[fz][fy][cx] in one pass, normalised by the summed in-range
+// weights and masked (the k_restrict_y32 + k_restrict_z32 pair fused; one thread per coarse node).
 template <int SP>
-__global__ void __launch_bounds__(256) k_restrict_xy32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ rf,
-                                                       float* __restrict__ a2, const PcgScalars* S) {
+__global__ void __launch_bounds__(256) k_restrict_yz32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ a1,
+                                                       float* __restrict__ rc, const PcgScalars* S) {
     if (S->done) return;
     constexpr int WS = 2 * SP - 1;
-    const int cnx = Lc.nx + 1, cny = Lc.ny + 1, fnx = Lf.nx + 1, fny = Lf.ny + 1, fnz = Lf.nz + 1;
-    const int total = fnz * cny * cnx;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= total) return;
-    const int cx = t % cnx;
-    const int rest = t / cnx;
-    const int cy = rest % cny, fz = rest / cny;
-    const int fNN = (int)Lf.nn;
-    float v0 = 0.0f, v1 = 0.0f, v2 = 0.0f;
-#pragma unroll
-    for (int iy = 0; iy < WS; ++iy) {
-        const int fy = cy * SP + iy - (SP - 1);
-        if (fy < 0 || fy >= fny) continue;
-        const float* __restrict__ src = rf + (fz * fny + fy) * fnx;
-        float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
-#pragma unroll
-        for (int ix = 0; ix < WS; ++ix) {
-            const int fx = cx * SP + ix - (SP - 1);
-            if (fx < 0 || fx >= fnx) continue;
-            const float w = hatf(ix, SP);
-            s0 = fmaf(w, src[fx], s0);
-            s1 = fmaf(w, src[fNN + fx], s1);
-            s2 = fmaf(w, src[2 * fNN + fx], s2);
-        }
-        const float w = hatf(iy, SP);
-        v0 = fmaf(w, s0, v0);
-        v1 = fmaf(w, s1, v1);
-        v2 = fmaf(w, s2, v2);
-    }
-    a2[t] = v0;
-    a2[total + t] = v1;
-    a2[2 * total + t] = v2;
-}
-
-__global__ void k_restrict_z32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ a2, float* __restrict__ rc,
-                               const PcgScalars* S) {
-    if (S->done) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= Lc.nn) return;
     const int cnx = Lc.nx + 1, cny = Lc.ny + 1;
     const int fnx = Lf.nx + 1, fny = Lf.ny + 1, fnz = Lf.nz + 1;
     const int cx = n % cnx, cy = (n / cnx) % cny, cz = n / (cnx * cny);
-    const int s = Lc.span, ws = 2 * s - 1;
-    const int64_t total2 = (int64_t)fnz * cny * cnx;
-    float swx = 0.0f, swy = 0.0f, swz = 0.0f;
-    for (int i = 0; i < ws; ++i) {
-        const int fx = cx * s + i - (s - 1), fy = cy * s + i - (s - 1);
-        if (fx >= 0 && fx < fnx) swx += hatf(i, s);
-        if (fy >= 0 && fy < fny) swy += hatf(i, s);
-    }
+    const int total1 = fnz * fny * cnx;
     float v0 = 0.0f, v1 = 0.0f, v2 = 0.0f;
-    for (int iz = 0; iz < ws; ++iz) {
-        const int fz = cz * s + iz - (s - 1);
+#pragma unroll
+    for (int iz = 0; iz < WS; ++iz) {
+        const int fz = cz * SP + iz - (SP - 1);
         if (fz < 0 || fz >= fnz) continue;
-        const float w = hatf(iz, s);
-        swz += w;
-        const int64_t i = ((int64_t)fz * cny + cy) * cnx + cx;
-        v0 = fmaf(w, a2[i], v0);
-        v1 = fmaf(w, a2[total2 + i], v1);
-        v2 = fmaf(w, a2[2 * total2 + i], v2);
+        float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
+#pragma unroll
+        for (int iy = 0; iy < WS; ++iy) {
+            const int fy = cy * SP + iy - (SP - 1);
+            if (fy < 0 || fy >= fny) continue;
+            const float w = hatf(iy, SP);
+            const int i = (fz * fny + fy) * cnx + cx;
+            s0 = fmaf(w, a1[i], s0);
+            s1 = fmaf(w, a1[total1 + i], s1);
+            s2 = fmaf(w, a1[2 * total1 + i], s2);
+        }
+        const float w = hatf(iz, SP);
+        v0 = fmaf(w, s0, v0);
+        v1 = fmaf(w, s1, v1);
+        v2 = fmaf(w, s2, v2);
     }
-    const float iw = 1.0f / (swz * swy * swx);
+    const float iw = 1.0f / (hat_sum<SP>(cz, fnz) * hat_sum<SP>(cy, fny) * hat_sum<SP>(cx, fnx));
+    const int m = Lc.mask[n];
+    rc[n] = (m & 1) ? 0.0f : v0 * iw;
+    rc[Lc.nn + n] = (m & 2) ? 0.0f : v1 * iw;
+    rc[2 * Lc.nn + n] = (m & 4) ? 0.0f : v2 * iw;
+}
+
+// The whole 3D window of the fine residual in one pass (levels small enough to sit in L2).
+template <int SP>
+__global__ void __launch_bounds__(256) k_restrict_xyz32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ rf,
+                                                        float* __restrict__ rc, const PcgScalars* S) {
+    if (S->done) return;
+    constexpr int WS = 2 * SP - 1;
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= Lc.nn) return;
+    const int cnx = Lc.nx + 1, cny = Lc.ny + 1;
+    const int fnx = Lf.nx + 1, fny = Lf.ny + 1, fnz = Lf.nz + 1;
+    const int cx = n % cnx, cy = (n / cnx) % cny, cz = n / (cnx * cny);
+    const int fNN = (int)Lf.nn;
+    float v0 = 0.0f, v1 = 0.0f, v2 = 0.0f;
+#pragma unroll
+    for (int iz = 0; iz < WS; ++iz) {
+        const int fz = cz * SP + iz - (SP - 1);
+        if (fz < 0 || fz >= fnz) continue;
+        float t0 = 0.0f, t1 = 0.0f, t2 = 0.0f;
+#pragma unroll
+        for (int iy = 0; iy < WS; ++iy) {
+            const int fy = cy * SP + iy - (SP - 1);
+            if (fy < 0 || fy >= fny) continue;
+            const float* __restrict__ src = rf + (fz * fny + fy) * fnx;
+            float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
+#pragma unroll
+            for (int ix = 0; ix < WS; ++ix) {
+                const int fx = cx * SP + ix - (SP - 1);
+                if (fx < 0 || fx >= fnx) continue;
+                const float w = hatf(ix, SP);
+                s0 = fmaf(w, src[fx], s0);
+                s1 = fmaf(w, src[fNN + fx], s1);
+                s2 = fmaf(w, src[2 * fNN + fx], s2);
+            }
+            const float w = hatf(iy, SP);
+            t0 = fmaf(w, s0, t0);
+            t1 = fmaf(w, s1, t1);
+            t2 = fmaf(w, s2, t2);
+        }
+        const float w = hatf(iz, SP);
+        v0 = fmaf(w, t0, v0);
+        v1 = fmaf(w, t1, v1);
+        v2 = fmaf(w, t2, v2);
+    }
+    const float iw = 1.0f / (hat_sum<SP>(cz, fnz) * hat_sum<SP>(cy, fny) * hat_sum<SP>(cx, fnx));
     const int m = Lc.mask[n];
     rc[n] = (m & 1) ? 0.0f : v0 * iw;
     rc[Lc.nn + n] = (m & 2) ? 0.0f : v1 * iw;
@@ -495,18 +497,18 @@ void launch_matvec32(const Grid& g, const float* Ke, const float* E, const uint8
                      RedSlot dot, PcgScalars* S, cudaStream_t s) {
     k_matvec32<<<RED_BLOCKS, RED_THREADS, 0, s>>>(g, Ke, E, mask, u, y, dot, S);
 }
+// x pass then a fused y-z pass on the finest transition (span 4); one fused x-y-z pass on the
+// coarser ones (span 2), whose fine residual sits in L2.
 void launch_restrict32(const MgLevel32& Lc, const MgLevel32& Lf, const float* rf, float* rc, float* a1, float* a2,
                        const PcgScalars* S, cudaStream_t s) {
+    (void)a2;
     const int64_t n1 = (int64_t)(Lf.nz + 1) * (Lf.ny + 1) * (Lc.nx + 1);
-    const int64_t n2 = (int64_t)(Lf.nz + 1) * (Lc.ny + 1) * (Lc.nx + 1);
-    // span 2: one fused x-y pass is faster; span 4 (the finest transition): the separable passes are
-    if (Lc.span == 2) {
-        k_restrict_xy32<2><<<blocks_for(n2, 256), 256, 0, s>>>(Lc, Lf, rf, a2, S);
-    } else {
+    if (Lc.span == 4) {
         k_restrict_x32<<<blocks_for(n1, 256), 256, 0, s>>>(Lc, Lf, rf, a1, S);
-        k_restrict_y32<<<blocks_for(n2, 256), 256, 0, s>>>(Lc, Lf, a1, a2, S);
+        k_restrict_yz32<4><<<blocks_for(Lc.nn, 256), 256, 0, s>>>(Lc, Lf, a1, rc, S);
+    } else {
+        k_restrict_xyz32<2><<<blocks_for(Lc.nn, 256), 256, 0, s>>>(Lc, Lf, rf, rc, S);
     }
-    k_restrict_z32<<<blocks_for(Lc.nn, 128), 128, 0, s>>>(Lc, Lf, a2, rc, S);
 }
 void launch_prolong_smooth32(const MgLevel32& Lc, const MgLevel32& Lf, const float* xc, const float* rf, float* xf,
                              float w, const PcgScalars* S, cudaStream_t s) {
