@@ -688,7 +688,7 @@ static void pcg32_iteration(Context* c) {
     matvec32(c, c->p32, c->Ap32, c->slot[0], c->S32);
     launch_pcg_update32(c->g, c->d32, c->r32, c->p32, c->Ap32, c->slot[1], c->S32, c->st);
     vcycle32(c, c->r32, c->z32, c->S32, c->slot[2]);
-    launch_pcg_direction32(c->g, c->z32, c->p32, c->S32, c->st);
+    launch_pcg_direction32(c->g, c->z32, c->p32, c->d32, c->S32, c->st);
 }
 
 static int ensure_pcg32_graph(Context* c) {

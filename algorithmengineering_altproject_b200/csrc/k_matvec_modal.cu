@@ -110,6 +110,7 @@ __global__ void __launch_bounds__(BX * BY, MINB)
     static_assert(STAGES >= 2, "ring needs two slots at least");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ModalSmem<BX, BY, STAGES>& sm = *reinterpret_cast<ModalSmem<BX, BY, STAGES>*>(smem_raw);
+    if (S != nullptr && blockIdx.x == 0 && threadIdx.x == 0) S->xit = S->it;   // last alpha is in x
     if (S != nullptr && S->done) return;
     const int tx = threadIdx.x % BX, ty = threadIdx.x / BX;
     const int64_t NN = g.NN, NXY = (int64_t)g.nnx * g.nny, EXY = (int64_t)g.ex * g.ey;

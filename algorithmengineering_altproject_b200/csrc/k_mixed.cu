@@ -71,6 +71,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_matvec32(Grid g, const float* _
                                                           RedSlot dot, PcgScalars* S) {
     __shared__ __align__(16) float Ke[576];
     __shared__ double sh[32];
+    if (S != nullptr && blockIdx.x == 0 && threadIdx.x == 0) S->xit = S->it;   // last alpha is in x
     if (S != nullptr && S->done) return;
     for (int i = threadIdx.x; i < 576; i += blockDim.x) Ke[i] = Keg[i];
     __syncthreads();
@@ -409,36 +410,32 @@ __global__ void __launch_bounds__(128) k_coarse_solve32(MgLevel32 L, const doubl
 }
 
 // ---------------------------------------------------------------- PCG vector steps in FP32
-__global__ void __launch_bounds__(RED_THREADS) k_pcg_update32(Grid g, float* __restrict__ x, float* __restrict__ r,
-                                                              const float* __restrict__ p,
+// r -= alpha Ap and |r|^2 (alpha = r.z / p.Ap of this iteration, stored for the direction kernel, which
+// applies x += alpha p while it reads p anyway)
+__global__ void __launch_bounds__(RED_THREADS) k_pcg_update32(Grid g, float* __restrict__ r,
                                                               const float* __restrict__ Ap, RedSlot red,
                                                               PcgScalars* S) {
     __shared__ double sh[32];
     if (S->done) return;
     const double den = S->denom;
     const float alpha = (float)(S->rz / (1.0e-30 < den ? den : 1.0e-30));
+    if (blockIdx.x == 0 && threadIdx.x == 0) S->alpha = alpha;
     // the three component planes are contiguous: one flat vector of 3 NN floats, 16-byte accesses
     // (cudaMalloc bases are 256-byte aligned) and a scalar tail
     const int n3 = (int)(3 * g.NN), n4 = n3 >> 2;
     const int stride = gridDim.x * blockDim.x;
-    float4* __restrict__ x4 = reinterpret_cast<float4*>(x);
     float4* __restrict__ r4 = reinterpret_cast<float4*>(r);
-    const float4* __restrict__ p4 = reinterpret_cast<const float4*>(p);
     const float4* __restrict__ a4 = reinterpret_cast<const float4*>(Ap);
     double part = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
-        const float4 pv = p4[i], av = a4[i];
-        float4 xv = x4[i], rv = r4[i];
-        xv.x = fmaf(alpha, pv.x, xv.x); xv.y = fmaf(alpha, pv.y, xv.y);
-        xv.z = fmaf(alpha, pv.z, xv.z); xv.w = fmaf(alpha, pv.w, xv.w);
+        const float4 av = a4[i];
+        float4 rv = r4[i];
         rv.x = fmaf(-alpha, av.x, rv.x); rv.y = fmaf(-alpha, av.y, rv.y);
         rv.z = fmaf(-alpha, av.z, rv.z); rv.w = fmaf(-alpha, av.w, rv.w);
-        x4[i] = xv;
         r4[i] = rv;
         part += (double)fmaf(rv.w, rv.w, fmaf(rv.z, rv.z, fmaf(rv.y, rv.y, rv.x * rv.x)));
     }
     for (int i = 4 * n4 + blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += stride) {
-        x[i] = fmaf(alpha, p[i], x[i]);
         const float rv = fmaf(-alpha, Ap[i], r[i]);
         r[i] = rv;
         part = fma((double)rv, (double)rv, part);
@@ -454,21 +451,35 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_update32(Grid g, float* __r
     }
 }
 
-__global__ void k_pcg_direction32(Grid g, const float* __restrict__ z, float* __restrict__ p, PcgScalars* S) {
-    if (S->done) return;
-    const float beta = (float)S->beta;
+// x += alpha p_old and, unless the update just converged, p = z + beta p_old.  Once converged, the
+// step is applied by the first launch only (xit == it afterwards).
+__global__ void k_pcg_direction32(Grid g, const float* __restrict__ z, float* __restrict__ p,
+                                  float* __restrict__ x, PcgScalars* S) {
+    if (S->xit == S->it) return;
+    const bool move = !S->done;
+    const float beta = (float)S->beta, alpha = S->alpha;
     const int n3 = (int)(3 * g.NN), n4 = n3 >> 2;
     const int stride = gridDim.x * blockDim.x;
     float4* __restrict__ p4 = reinterpret_cast<float4*>(p);
+    float4* __restrict__ x4 = reinterpret_cast<float4*>(x);
     const float4* __restrict__ z4 = reinterpret_cast<const float4*>(z);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
-        const float4 zv = z4[i];
-        float4 pv = p4[i];
-        pv.x = fmaf(beta, pv.x, zv.x); pv.y = fmaf(beta, pv.y, zv.y);
-        pv.z = fmaf(beta, pv.z, zv.z); pv.w = fmaf(beta, pv.w, zv.w);
-        p4[i] = pv;
+        float4 pv = p4[i], xv = x4[i];
+        xv.x = fmaf(alpha, pv.x, xv.x); xv.y = fmaf(alpha, pv.y, xv.y);
+        xv.z = fmaf(alpha, pv.z, xv.z); xv.w = fmaf(alpha, pv.w, xv.w);
+        x4[i] = xv;
+        if (move) {
+            const float4 zv = z4[i];
+            pv.x = fmaf(beta, pv.x, zv.x); pv.y = fmaf(beta, pv.y, zv.y);
+            pv.z = fmaf(beta, pv.z, zv.z); pv.w = fmaf(beta, pv.w, zv.w);
+            p4[i] = pv;
+        }
     }
-    for (int i = 4 * n4 + blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += stride) p[i] = fmaf(beta, p[i], z[i]);
+    for (int i = 4 * n4 + blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += stride) {
+        const float pv = p[i];
+        x[i] = fmaf(alpha, pv, x[i]);
+        if (move) p[i] = fmaf(beta, pv, z[i]);
+    }
 }
 
 inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
@@ -527,10 +538,12 @@ void launch_coarse_solve32(const MgLevel32& L, const double* X, int N, const int
 }
 void launch_pcg_update32(const Grid& g, float* x, float* r, const float* p, const float* Ap, RedSlot red,
                          PcgScalars* S, cudaStream_t s) {
-    k_pcg_update32<<<RED_BLOCKS, RED_THREADS, 0, s>>>(g, x, r, p, Ap, red, S);
+    (void)x;
+    (void)p;
+    k_pcg_update32<<<RED_BLOCKS, RED_THREADS, 0, s>>>(g, r, Ap, red, S);
 }
-void launch_pcg_direction32(const Grid& g, const float* z, float* p, PcgScalars* S, cudaStream_t s) {
-    k_pcg_direction32<<<RED_BLOCKS, RED_THREADS, 0, s>>>(g, z, p, S);
+void launch_pcg_direction32(const Grid& g, const float* z, float* p, float* x, PcgScalars* S, cudaStream_t s) {
+    k_pcg_direction32<<<RED_BLOCKS, RED_THREADS, 0, s>>>(g, z, p, x, S);
 }
 
 }  // namespace t3d

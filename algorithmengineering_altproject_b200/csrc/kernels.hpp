@@ -181,7 +181,8 @@ void launch_coarse_solve32(const MgLevel32& L, const double* X, int N, const int
                            cudaStream_t s);
 void launch_pcg_update32(const Grid& g, float* x, float* r, const float* p, const float* Ap, RedSlot red,
                          PcgScalars* S, cudaStream_t s);
-void launch_pcg_direction32(const Grid& g, const float* z, float* p, PcgScalars* S, cudaStream_t s);
+// p = z + beta p and the deferred x += alpha p of the same iteration (see PcgScalars::xit)
+void launch_pcg_direction32(const Grid& g, const float* z, float* p, float* x, PcgScalars* S, cudaStream_t s);
 
 // ---- FP32 K(E)p through the modal form of Ke (k_matvec_modal.cu)
 struct ModalKe {         // the 45 nonzeros of T^T Ke T / 64 in the fixed block pattern

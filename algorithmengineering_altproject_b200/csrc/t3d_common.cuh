@@ -73,6 +73,10 @@ struct PcgScalars {
     int done;         // 1 once |r| < stop
     int result;       // PCG_free return value (solver.cpp:184,216)
     int first;        // 1 while the initial r.z is being formed
+    // FP32 inner solve only: the direction kernel applies x += alpha p_old; xit = the iteration whose
+    // alpha is already in x (set by the next K(E)p launch), so a converged step is applied exactly once
+    int xit;
+    float alpha;      // alpha of iteration `it`, stored by the update kernel
 };
 
 // Reduction scratch: RED_BLOCKS partials + arrival counter per reduction slot.
