@@ -124,6 +124,7 @@ _SIGS = {
     "t3d_run_global": (C.c_int, [_CTX, C.c_float, C.c_int, C.POINTER(C.c_double), C.POINTER(IterRecord),
                                  C.POINTER(C.c_int), _f32p]),
     "t3d_synchronize": (C.c_int, [_CTX]),
+    "t3d_export_stl": (C.c_int, [_CTX, C.c_void_p, C.c_float, C.c_char_p, C.POINTER(C.c_int64)]),
     "t3d_profile": (C.c_int, [_CTX, C.c_int, C.c_int, C.POINTER(C.c_double)]),
     "t3d_compliance_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, _f64p, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_void_p]),
@@ -269,6 +270,15 @@ class Problem:
         z = np.zeros(self.nf)
         _check(self._lib.t3d_vcycle(self._h, _f64(rFree), z))
         return z
+
+    def export_stl(self, path, iso=0.3, xPhys=None):
+        """export_surface_stl (io.cpp:80-87): binary STL of the current design (or of xPhys, reference element
+        order) at threshold iso; returns the triangle count"""
+        n = C.c_int64(0)
+        xp = None if xPhys is None else _f32(xPhys)
+        _check(self._lib.t3d_export_stl(self._h, None if xp is None else xp.ctypes.data_as(C.c_void_p),
+                                        C.c_float(iso), str(path).encode(), C.byref(n)))
+        return int(n.value)
 
     def vcycle32(self, rFree):
         """the FP32 V-cycle of the mixed-precision inner solve (mixed contexts only), widened to FP64"""

@@ -1350,4 +1350,52 @@ int t3d_profile(t3d_context* ctx, int what, int reps, double* ms) {
     return T3D_OK;
 }
 
+int t3d_export_stl(t3d_context* ctx, const float* xphys, float iso, const char* path, int64_t* ntri) {
+    API_GUARD(ctx);
+    if (!path) return t3d::set_error(T3D_ERR_INVALID, "null path");
+    const t3d::Grid& g = ctx->g;
+    const float* dens = ctx->x;
+    if (xphys) {   // densities given in the reference's element order: staged into xnew (cells)
+        CHECK(t3d::upload_cells_f32(ctx, xphys, ctx->xnew));
+        dens = ctx->xnew;
+    }
+    const int nb = t3d::stl_chunks(g);
+    unsigned* bsum = nullptr;
+    uint16_t* body = nullptr;
+    unsigned faces = 0;
+    int rc = T3D_OK;
+    cudaError_t e = cudaMalloc(&bsum, (size_t)(nb + 1) * sizeof(unsigned));
+    if (e != cudaSuccess) return t3d::set_cuda_error(e, "cudaMalloc", __FILE__, __LINE__);
+    t3d::launch_stl_count(g, dens, iso, bsum, ctx->st);
+    e = cudaMemcpyAsync(&faces, bsum + nb, sizeof faces, cudaMemcpyDeviceToHost, ctx->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
+    const int64_t n_tri = 2 * (int64_t)faces;
+    std::vector<char> host;
+    if (e == cudaSuccess && n_tri > 0) {
+        e = cudaMalloc(&body, (size_t)n_tri * 50);
+        if (e == cudaSuccess) {
+            t3d::launch_stl_write(g, dens, iso, bsum, body, ctx->st);
+            host.resize((size_t)n_tri * 50);
+            e = cudaMemcpyAsync(host.data(), body, host.size(), cudaMemcpyDeviceToHost, ctx->st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);
+        }
+    }
+    if (e != cudaSuccess) rc = t3d::set_cuda_error(e, "stl export", __FILE__, __LINE__);
+    cudaFree(bsum);
+    if (body) cudaFree(body);
+    if (rc != T3D_OK) return rc;
+    // export_stl.hpp:14-33: 80-byte header, triangle count, records
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return t3d::set_error(T3D_ERR_INVALID, std::string("cannot open ") + path);
+    char header[80] = {0};
+    std::strncpy(header, "Generated by TOP3D_XL", 79);
+    const uint32_t n32 = (uint32_t)n_tri;
+    bool ok = std::fwrite(header, 1, 80, f) == 80 && std::fwrite(&n32, 4, 1, f) == 1 &&
+              (host.empty() || std::fwrite(host.data(), 1, host.size(), f) == host.size());
+    ok = (std::fclose(f) == 0) && ok;
+    if (!ok) return t3d::set_error(T3D_ERR_INVALID, std::string("write failed: ") + path);
+    if (ntri) *ntri = n_tri;
+    return T3D_OK;
+}
+
 }  // extern "C"

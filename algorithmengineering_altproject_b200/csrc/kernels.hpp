@@ -205,4 +205,13 @@ void launch_matvec32_modal(const Grid& g, const ModalKe& kh, const ModalTiling& 
                            const uint8_t* mask, const float* u, float* y, RedSlot dot, PcgScalars* S,
                            cudaStream_t s);
 
+// ---- surface export (k_stl.cu, io.cpp:80-87)
+int stl_chunks(const Grid& g);
+// per-chunk face counts scanned in place: bsum[i] = faces before chunk i, bsum[chunks] = total faces
+// (bsum holds stl_chunks(g) + 1 entries)
+void launch_stl_count(const Grid& g, const float* density_cells, float iso, unsigned* bsum, cudaStream_t s);
+// the STL records (50 bytes per triangle, 2 triangles per face) at their final offsets
+void launch_stl_write(const Grid& g, const float* density_cells, float iso, const unsigned* boff, uint16_t* body,
+                      cudaStream_t s);
+
 }  // namespace t3d

@@ -200,6 +200,12 @@ int  t3d_profile(struct t3d_context* ctx, int what, int reps, double* ms);
 int  t3d_compliance_noalloc(int nely, int nelx, int nelz, const double* ke576, const double* d_E, const double* d_u,
                             double* d_ce, double* d_C, void* stream);
 
+/* export_surface_stl (io.cpp:80-87): binary STL of the boundary faces of the voxels with density >= iso
+ * (the reference exports at iso 0.3, driver.cpp:274), byte-identical to the reference's file.  xphys:
+ * densities in the reference's element order, or NULL for the context's current design density.
+ * *ntri receives the triangle count. */
+int  t3d_export_stl(struct t3d_context* ctx, const float* xphys, float iso, const char* path, int64_t* ntri);
+
 #ifdef __cplusplus
 }
 #endif

@@ -198,6 +198,8 @@ class Oracle(_Common):
             L.orc_vol_sum.restype = C.c_float
             L.orc_sharpness.argtypes = [C.c_void_p, _f32p, C.c_int]
             L.orc_sharpness.restype = C.c_float
+            L.orc_export_stl.argtypes = [C.c_void_p, _f32p, C.c_char_p, C.c_float]
+            L.orc_export_stl.restype = C.c_int64
             L.orc_design_loop.argtypes = [C.c_void_p, C.c_float, C.c_int, C.c_float, C.POINTER(C.c_double),
                                           C.POINTER(OrcIterRecord), _f32p]
             L.orc_design_loop.restype = C.c_int
@@ -272,6 +274,13 @@ class Oracle(_Common):
         self.lib().orc_dc_scale(self.h, np.ascontiguousarray(dcf, np.float32), np.ascontiguousarray(x, np.float32), dc)
         return dc
 
+    def export_stl(self, xphys, path, iso=0.3):
+        """restated export_surface_stl (io.cpp:80-87); returns the triangle count"""
+        n = self.lib().orc_export_stl(self.h, np.ascontiguousarray(xphys, np.float32), path.encode(), C.c_float(iso))
+        if n < 0:
+            raise OSError("cannot write %s" % path)
+        return int(n)
+
     def vol_sum(self, x):
         return float(self.lib().orc_vol_sum(self.h, np.ascontiguousarray(x, np.float32), len(x)))
 
@@ -327,6 +336,7 @@ class Reference(_Common):
             L.ref_sample_iteration.argtypes = [C.c_void_p, C.c_float, C.c_int, C.c_int, _f64p]
             L.ref_sample_iteration.restype = C.c_int
             L.ref_run_global.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, C.c_float, C.c_char_p]
+            L.ref_export_stl.argtypes = [C.c_void_p, _f32p, C.c_char_p, C.c_float]
             cls._lib = L
         return cls._lib
 
@@ -338,6 +348,10 @@ class Reference(_Common):
     def run_global(cls, nely, nelx, nelz, V0, nloop, capdir, rmin=float(np.sqrt(np.float32(3.0)))):
         cls.lib().ref_run_global(nely, nelx, nelz, C.c_float(V0), nloop, C.c_float(rmin),
                                  capdir.encode() if capdir else b"")
+
+    def export_stl(self, xphys, path, iso=0.3):
+        """the reference's export_surface_stl (io.cpp:80-87) of densities in Morton order"""
+        self.lib().ref_export_stl(self.h, np.ascontiguousarray(xphys, np.float32), path.encode(), C.c_float(iso))
 
     def __init__(self, nely, nelx, nelz, emin=None, max_levels=5):
         L = self.lib()

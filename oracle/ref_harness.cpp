@@ -427,4 +427,12 @@ int ref_sample_iteration(void* h, float V0, int pcg_max, int rebuild_mg, double*
     return it;
 }
 
+// The reference's own surface export (io.cpp:80-87) of densities in Morton order, written to `path`.
+int ref_export_stl(void* h, const float* xphys, const char* path, float iso) {
+    RefCtx* c = static_cast<RefCtx*>(h);
+    std::vector<float> x(xphys, xphys + c->pb.mesh.numElements);
+    real_stl(c->pb, x, std::string(path), iso);
+    return 0;
+}
+
 }  // extern "C"

@@ -1482,3 +1482,62 @@ void orc_mg_diag(const orc_problem* P, int level, double* out) {
 void orc_mg_mask(const orc_problem* P, int level, uint8_t* out) {
     memcpy(out, P->lv[level].mask, (size_t)(3 * P->lv[level].nn));
 }
+
+/* ------------------------------------------------------------------ surface export (test infrastructure)
+ * io.cpp:80-87 scatters xPhys onto vol[ny*nx*ez + ny*ex + y] (y is the flipped row, fea.cpp:222);
+ * voxel_surface.hpp:44-92 visits z, then x, then y, and per voxel the faces -X, +X, -Y, +Y, -Z, +Z of an
+ * inside voxel (value >= iso) whose neighbour is outside or absent; each face is 4 vertices (x, y, z)
+ * and 2 triangles (0,1,2), (0,2,3) (voxel_surface.hpp:17-43); export_stl.hpp:14-33 writes an 80-byte
+ * header, the triangle count and 50-byte records (zero normal, 3 vertices, zero attribute). */
+static void stl_face(FILE* f, int axis, float y0, float x0, float z0) {
+    float v[4][3];
+    for (int i = 0; i < 4; ++i) { v[i][0] = x0; v[i][1] = y0; v[i][2] = z0; }
+    if (axis == 0) {        /* plane x = const: vary y, z */
+        v[1][1] += 1.0f; v[2][1] += 1.0f; v[2][2] += 1.0f; v[3][2] += 1.0f;
+    } else if (axis == 1) { /* plane y = const: vary x, z */
+        v[1][0] += 1.0f; v[2][0] += 1.0f; v[2][2] += 1.0f; v[3][2] += 1.0f;
+    } else {                /* plane z = const: vary x, y */
+        v[1][0] += 1.0f; v[2][0] += 1.0f; v[2][1] += 1.0f; v[3][1] += 1.0f;
+    }
+    static const int tri[2][3] = {{0, 1, 2}, {0, 2, 3}};
+    const float n[3] = {0.0f, 0.0f, 0.0f};
+    const uint16_t attr = 0;
+    for (int t = 0; t < 2; ++t) {
+        fwrite(n, 4, 3, f);
+        for (int k = 0; k < 3; ++k) fwrite(v[tri[t][k]], 4, 3, f);
+        fwrite(&attr, 2, 1, f);
+    }
+}
+
+int64_t orc_export_stl(const orc_problem* P, const float* xphys, const char* path, float iso) {
+    const int ny = P->ny, nx = P->nx, nz = P->nz;
+    const int64_t nv = (int64_t)ny * nx * nz;
+    float* vol = xcalloc((size_t)nv, sizeof(float));
+    for (int64_t e = 0; e < P->ne; ++e) vol[P->ele_full[e]] = xphys[e];
+    FILE* f = fopen(path, "wb");
+    if (!f) { free(vol); return -1; }
+    char header[80];
+    memset(header, 0, sizeof header);
+    strncpy(header, "Generated by TOP3D_XL", 79);
+    fwrite(header, 1, 80, f);
+    uint32_t ntri = 0;
+    fwrite(&ntri, 4, 1, f);   /* patched below */
+#define AT(y, x, z) (vol[(int64_t)(y) + (int64_t)ny * (x) + (int64_t)ny * nx * (z)] >= iso)
+    for (int z = 0; z < nz; ++z)
+        for (int x = 0; x < nx; ++x)
+            for (int y = 0; y < ny; ++y) {
+                if (!AT(y, x, z)) continue;
+                if (x == 0 || !AT(y, x - 1, z)) { stl_face(f, 0, (float)y, (float)x, (float)z); ntri += 2; }
+                if (x == nx - 1 || !AT(y, x + 1, z)) { stl_face(f, 0, (float)y, (float)(x + 1), (float)z); ntri += 2; }
+                if (y == 0 || !AT(y - 1, x, z)) { stl_face(f, 1, (float)y, (float)x, (float)z); ntri += 2; }
+                if (y == ny - 1 || !AT(y + 1, x, z)) { stl_face(f, 1, (float)(y + 1), (float)x, (float)z); ntri += 2; }
+                if (z == 0 || !AT(y, x, z - 1)) { stl_face(f, 2, (float)y, (float)x, (float)z); ntri += 2; }
+                if (z == nz - 1 || !AT(y, x, z + 1)) { stl_face(f, 2, (float)y, (float)x, (float)(z + 1)); ntri += 2; }
+            }
+#undef AT
+    fseek(f, 80, SEEK_SET);
+    fwrite(&ntri, 4, 1, f);
+    fclose(f);
+    free(vol);
+    return (int64_t)ntri;
+}

@@ -97,6 +97,11 @@ float orc_sharpness(const orc_problem* P, const float* x, int n);
 int orc_design_loop(orc_problem* P, float V0, int nLoop, float rMin, double* Csolid,
                     orc_iter_record* recs, float* xfinal);
 
+/* export_surface_stl (io.cpp:80-87): element densities (Morton order) scattered onto the padded
+ * [ny][nx][nz] volume, boundary faces at threshold iso (voxel_surface.hpp:12-93), binary STL
+ * (export_stl.hpp:14-33).  Returns the triangle count, or -1 when the file cannot be written. */
+int64_t orc_export_stl(const orc_problem* P, const float* xphys, const char* path, float iso);
+
 #ifdef __cplusplus
 }
 #endif
