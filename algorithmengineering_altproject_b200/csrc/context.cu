@@ -384,6 +384,8 @@ static int create(int nely, int nelx, int nelz, const t3d_params* prm, const t3d
     if (c->prm.device < 0 || c->prm.device >= ndev) return set_error(T3D_ERR_NO_DEVICE, "device index out of range");
     if (c->prm.precision != T3D_FP64 && c->prm.precision != T3D_MIXED)
         return set_error(T3D_ERR_UNSUPPORTED, "precision must be T3D_FP64 or T3D_MIXED");
+    if (c->prm.mg_coarse_assembly != T3D_COARSE_REFERENCE && c->prm.mg_coarse_assembly != T3D_COARSE_FULL)
+        return set_error(T3D_ERR_UNSUPPORTED, "mg_coarse_assembly must be T3D_COARSE_REFERENCE or T3D_COARSE_FULL");
     if (c->prm.matvec32_form != T3D_MATVEC32_AUTO && c->prm.matvec32_form != T3D_MATVEC32_DENSE)
         return set_error(T3D_ERR_UNSUPPORTED, "matvec32_form must be T3D_MATVEC32_AUTO or T3D_MATVEC32_DENSE");
     c->mixed = c->prm.precision == T3D_MIXED;
@@ -578,7 +580,12 @@ static int mg_setup(Context* c) {
     for (int l = 0; l + 1 < c->nlev; ++l) launch_diag_coarsen(c->lv[l + 1], c->lv[l], c->st);
     if (c->Nc) {
         const MgLevel& Lc = c->lv[c->nlev - 1];
-        launch_coarse_element_matrices(c->g, Lc, c->mask0, c->E, c->Ke, (double)c->prm.Emin, c->Kce, c->st);
+        // the reference samples s^3 fine elements per coarse element with s the coarsest level's own span
+        // (coarsest.cpp:138-323; a corner sub-block of the grid when there are more than 2 levels); the full
+        // Galerkin form samples all of them (s = product of the spans)
+        int span = Lc.span;
+        if (c->prm.mg_coarse_assembly == T3D_COARSE_FULL) span = c->g.nx / Lc.nx;
+        launch_coarse_element_matrices(c->g, Lc, span, c->mask0, c->E, c->Ke, (double)c->prm.Emin, c->Kce, c->st);
         launch_coarse_assemble(Lc, c->Kce, c->Kc, c->st);
         launch_cholesky(c->Kc, c->LT, c->Lrow, c->Nc, c->chol_status, c->st);
         launch_coarse_inverse(c->Lrow, c->Nc, c->chol_status, c->Xc, c->st);

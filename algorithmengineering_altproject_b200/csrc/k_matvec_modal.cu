@@ -299,7 +299,8 @@ bool modal_ke_from(const double* Ke, ModalKe* out, double* off) {
             T8[a][m] = (double)((m & 1 ? s[0] : 1) * (m & 2 ? s[1] : 1) * (m & 4 ? s[2] : 1));
     }
     // Kh[(c,m)][(e,n)] = sum_{a,b} T8[a][m] Ke[3a+c][3b+e] T8[b][n] / 64, index comp*8 + mode
-    static double Kh[24][24];
+    // (local: contexts may be created concurrently from several host threads)
+    double Kh[24][24];
     double mx = 0.0;
     for (int c = 0; c < 3; ++c)
         for (int m = 0; m < 8; ++m)

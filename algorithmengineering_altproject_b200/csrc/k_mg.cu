@@ -308,7 +308,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_prolong_smooth0(MgLevel Lc, MgL
 // One CTA (576 threads, thread = entry (i,j)) per coarse element.  The s^3 finest-grid sub-elements
 // at the corner-sampled positions contribute T'(Kf T); Kf = Ke with modulus max(Emin,E) of the
 // y-mirrored cell, with fixed DOFs' rows/cols replaced by identity when the sub-element touches any.
-__global__ void __launch_bounds__(576) k_coarse_element(Grid g0, MgLevel Lc, const uint8_t* __restrict__ mask0,
+__global__ void __launch_bounds__(576) k_coarse_element(Grid g0, MgLevel Lc, int s, const uint8_t* __restrict__ mask0,
                                                         const double* __restrict__ E, const double* __restrict__ Keg,
                                                         double emin, double* __restrict__ Kce) {
     __shared__ double T[576], Kf[576], M[576];
@@ -316,7 +316,6 @@ __global__ void __launch_bounds__(576) k_coarse_element(Grid g0, MgLevel Lc, con
     const int cel = blockIdx.x;   // (cez*nxc + cex)*nyc + cey
     const int nyc = Lc.ny, nxc = Lc.nx;
     const int cey = cel % nyc, cex = (cel / nyc) % nxc, cez = cel / (nyc * nxc);
-    const int s = Lc.span;
     const int i = threadIdx.x / 24, j = threadIdx.x % 24;
     double acc_e = 0.0;
     for (int iz = 0; iz < s; ++iz)
@@ -508,10 +507,10 @@ void launch_prolong_smooth0(const MgLevel& Lc, const MgLevel& Lf, const double* 
                             double weight, RedSlot dot, PcgScalars* S, cudaStream_t s) {
     k_prolong_smooth0<<<RED_BLOCKS, RED_THREADS, 0, s>>>(Lc, Lf, xc, r, z, weight, dot, S);
 }
-void launch_coarse_element_matrices(const Grid& g0, const MgLevel& Lc, const uint8_t* mask0, const double* E,
+void launch_coarse_element_matrices(const Grid& g0, const MgLevel& Lc, int span, const uint8_t* mask0, const double* E,
                                     const double* Ke, double emin, double* Kce, cudaStream_t s) {
     const int ncel = Lc.nx * Lc.ny * Lc.nz;
-    k_coarse_element<<<ncel, 576, 0, s>>>(g0, Lc, mask0, E, Ke, emin, Kce);
+    k_coarse_element<<<ncel, 576, 0, s>>>(g0, Lc, span, mask0, E, Ke, emin, Kce);
 }
 void launch_coarse_assemble(const MgLevel& Lc, const double* Kce, double* Kc, cudaStream_t s) {
     const int64_t N = 3 * Lc.nn;

@@ -418,7 +418,18 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_update32(Grid g, float* __r
     __shared__ double sh[32];
     if (S->done) return;
     const double den = S->denom;
-    const float alpha = (float)(S->rz / (1.0e-30 < den ? den : 1.0e-30));
+    // breakdown of the FP32 recurrence (p.Ap <= 0 or r.z <= 0, e.g. an indefinite preconditioner): stop this
+    // inner solve before the step; the FP64 outer loop restarts from the true residual.  Every block reads the
+    // same scalars, so they all take the same branch.
+    if (!(den > 0.0) || !(S->rz > 0.0)) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            S->alpha = 0.0f;
+            S->done = 1;
+            S->result = S->it;
+        }
+        return;
+    }
+    const float alpha = (float)(S->rz / den);
     if (blockIdx.x == 0 && threadIdx.x == 0) S->alpha = alpha;
     // the three component planes are contiguous: one flat vector of 3 NN floats, 16-byte accesses
     // (cudaMalloc bases are 256-byte aligned) and a scalar tail

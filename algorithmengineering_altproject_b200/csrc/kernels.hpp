@@ -85,7 +85,9 @@ void launch_prolong_smooth(const MgLevel& Lc, const MgLevel& Lf, const double* x
 void launch_prolong_smooth0(const MgLevel& Lc, const MgLevel& Lf, const double* xc, const double* r, double* z,
                             double weight, RedSlot dot, PcgScalars* S, cudaStream_t s);
 // coarsest dense Galerkin matrix, Cholesky factor and triangular solves (coarsest.cpp, preconditioner.cpp:47-78)
-void launch_coarse_element_matrices(const Grid& g0, const MgLevel& Lc, const uint8_t* mask0, const double* E,
+// span: fine elements per coarse element edge that are sampled (the coarsest level's own span in the
+// reference's assembly; the product of all spans for the full Galerkin operator)
+void launch_coarse_element_matrices(const Grid& g0, const MgLevel& Lc, int span, const uint8_t* mask0, const double* E,
                                     const double* Ke, double emin, double* Kce, cudaStream_t s);
 void launch_coarse_assemble(const MgLevel& Lc, const double* Kce, double* Kc, cudaStream_t s);
 void launch_cholesky(const double* A, double* LT, double* Lrow, int N, int* status, cudaStream_t s);

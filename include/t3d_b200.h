@@ -43,6 +43,11 @@ enum { T3D_FP64 = 0, T3D_MIXED = 1 };
  * stiffness of an axis-aligned cubic isotropic voxel (always for the built-in Ke), else the dense
  * 24x24 form; DENSE = always the dense form */
 enum { T3D_MATVEC32_AUTO = 0, T3D_MATVEC32_DENSE = 1 };
+/* dense coarsest operator: REFERENCE = the reference's assembly (coarsest.cpp:138-323), which samples the
+ * s^3 fine elements of each coarse element with s the coarsest level's own span, i.e. only a corner
+ * sub-block of the grid when there are more than two levels (on some grids PCG then stalls);
+ * FULL = the Galerkin operator of the whole grid (s = product of all spans) */
+enum { T3D_COARSE_REFERENCE = 0, T3D_COARSE_FULL = 1 };
 
 typedef struct t3d_params {
     float E0, Emin, nu, penal;    /* GlobalParams core.hpp:26-33 (Ke always uses nu = 0.3, fea.cpp:345) */
@@ -56,7 +61,8 @@ typedef struct t3d_params {
     int   precision;              /* T3D_FP64 or T3D_MIXED (design loop only; t3d_pcg is always FP64) */
     int   device;                 /* CUDA device ordinal */
     int   matvec32_form;          /* mixed precision only: T3D_MATVEC32_AUTO or T3D_MATVEC32_DENSE */
-    int   reserved[6];
+    int   mg_coarse_assembly;     /* T3D_COARSE_REFERENCE (default) or T3D_COARSE_FULL */
+    int   reserved[5];
 } t3d_params;
 
 /* Problem spec beyond the reference's built-in cantilever (the reference hard-codes one load case and a

@@ -31,7 +31,7 @@ class OrcParams(C.Structure):
     _fields_ = [("E0", C.c_float), ("Emin", C.c_float), ("nu", C.c_float), ("penal", C.c_float),
                 ("cg_tol", C.c_float), ("cg_max_it", C.c_int), ("mg_nondyadic", C.c_int),
                 ("mg_max_levels", C.c_int), ("mg_weight", C.c_float), ("pow_mode", C.c_int),
-                ("vol_mode", C.c_int), ("approx_mode", C.c_int), ("red_mode", C.c_int)]
+                ("vol_mode", C.c_int), ("approx_mode", C.c_int), ("red_mode", C.c_int), ("coarse_full", C.c_int)]
 
 
 class OrcIterRecord(C.Structure):
@@ -207,7 +207,7 @@ class Oracle(_Common):
         return cls._lib
 
     def __init__(self, nely, nelx, nelz, emin=None, max_levels=5, pow_mode=0, vol_mode=0, approx_mode=0, red_mode=0,
-                 penal=None):
+                 penal=None, coarse_full=0):
         L = self.lib()
         p = OrcParams()
         L.orc_params_default(C.byref(p))
@@ -220,6 +220,7 @@ class Oracle(_Common):
         p.vol_mode = vol_mode
         p.approx_mode = approx_mode
         p.red_mode = red_mode
+        p.coarse_full = coarse_full
         self.params = p
         self.h = C.c_void_p(L.orc_create(nely, nelx, nelz, C.byref(p)))
         self._info = L.orc_info

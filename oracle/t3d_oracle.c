@@ -82,6 +82,7 @@ void orc_params_default(orc_params* p) {
     p->cg_tol = 1.0e-3f; p->cg_max_it = 800;
     p->mg_nondyadic = 1; p->mg_max_levels = 5; p->mg_weight = 0.6f;
     p->pow_mode = 0; p->vol_mode = 0; p->approx_mode = 0; p->red_mode = 0;
+    p->coarse_full = 0;
 }
 
 /* ------------------------------------------------------------------ padding
@@ -601,7 +602,7 @@ static int assemble_coarse(orc_problem* P, const double* E, double* Kc) {
     const int N = (int)(3 * Lc->nn);
     if (P->nlev == 1 || N > 1000) return 0;
     memset(Kc, 0, (size_t)N * N * sizeof(double));
-    const int s = Lc->span;
+    const int s = P->p.coarse_full ? P->nx / Lc->nx : Lc->span;
     /* full-grid moduli: padding elements read 0 (EleMod_CompactToFull_Finest) */
     double* Efull = xcalloc((size_t)P->nx * P->ny * P->nz, sizeof(double));
     for (int e = 0; e < P->ne; ++e) Efull[P->ele_full[e]] = E[e];

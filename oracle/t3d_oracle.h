@@ -45,6 +45,8 @@ typedef struct orc_params {
                                        1 = the CUDA path's canonical deterministic order (grid-stride over
                                            nodes/cells with 1184 x 256 threads, warp and block butterflies),
                                            so that the two can be compared bit for bit */
+    int   coarse_full;              /* 0 = the reference's coarsest assembly (s = coarsest level's own span);
+                                       1 = full Galerkin operator of the grid (s = product of the spans) */
 } orc_params;
 
 typedef struct orc_iter_record {    /* one line of driver.cpp:205-211 */

@@ -77,3 +77,46 @@ def test_mixed_design_loop_is_deterministic():
     np.testing.assert_array_equal(M.density(), M2.density())
     for P in (F, M, M2):
         P.close()
+
+
+@pytest.mark.parametrize("dims", [(30, 60, 30), (24, 88, 40)])
+def test_full_galerkin_coarsest_matches_oracle(dims):
+    # T3D_COARSE_FULL samples every fine element of each coarsest element (span = product of the level spans)
+    # instead of the reference's corner sub-block; bit-identical to the oracle's restatement of the same assembly
+    import algorithmengineering_altproject_b200 as t3d
+    from oracle.bindings import Oracle
+    P = t3d.Problem(*dims, mg_coarse_assembly=t3d.T3D_COARSE_FULL)
+    O = Oracle(*dims, red_mode=1, coarse_full=1)
+    rng = np.random.default_rng(6)
+    E = rng.uniform(1e-3, 1.0, P.ne)
+    assert np.array_equal(P.coarse_matrix(E), O.coarse_matrix(E))
+    P.close()
+
+
+def test_full_galerkin_coarsest_repairs_a_stalling_grid():
+    # 24x88x40 (levels 88x24x40 / 22x6x10 / 11x3x5): with the reference's assembly PCG on the solid domain is
+    # still at half the initial residual after 800 iterations; with the full Galerkin operator it gets within
+    # 1e-2 of the tolerance (oracle: 0.505 vs 0.00146)
+    import algorithmengineering_altproject_b200 as t3d
+    res = {}
+    for mode in (t3d.T3D_COARSE_REFERENCE, t3d.T3D_COARSE_FULL):
+        P = t3d.Problem(24, 88, 40, mg_coarse_assembly=mode)
+        b = P.bfree()
+        E1 = np.ones(P.ne)
+        P.make_diagonal_preconditioner_from_static(E1)
+        x, its = P.PCG_free(E1, b, np.zeros(P.nf), tol=1e-3, maxIt=800)
+        res[mode] = np.linalg.norm(b - P.K_times_u_finest(E1, x)) / np.linalg.norm(b)
+        P.close()
+    assert res[t3d.T3D_COARSE_FULL] < 1e-2 < 0.1 < res[t3d.T3D_COARSE_REFERENCE], res
+
+
+def test_fp32_breakdown_stops_the_inner_solve_without_nan():
+    # 16x72x24 with the reference's coarsest assembly: the preconditioner is not positive definite and the
+    # FP32 recurrence breaks down; the inner solve stops at the breakdown and the FP64 outer loop restarts,
+    # so the design iteration stays finite
+    import algorithmengineering_altproject_b200 as t3d
+    M = t3d.Problem(16, 72, 24, precision=t3d.T3D_MIXED, oc_sum_order=t3d.T3D_SUM_FP64)
+    cs = M.design_init(0.2)
+    r = M.design_step()
+    assert np.isfinite(cs) and np.isfinite(r["obj"])
+    M.close()

@@ -16,6 +16,9 @@ class FakeServer(serve.DesignServer):
         self._lk = threading.Lock()
         super().__init__(*a, **kw)
 
+    def _warm_up(self):
+        self._warm = True
+
     def _execute(self, req, res):
         with self._lk:
             self.log.append(req.rid)
