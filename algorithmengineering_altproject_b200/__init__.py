@@ -70,7 +70,8 @@ class Info(C.Structure):
     _fields_ = [("res", C.c_int64 * 3), ("orig", C.c_int64 * 3), ("num_elements", C.c_int64),
                 ("num_nodes", C.c_int64), ("num_free", C.c_int64), ("num_levels", C.c_int64),
                 ("levels", (C.c_int64 * 4) * 8), ("coarse_n", C.c_int64), ("coarse_cholesky_ok", C.c_int64),
-                ("device_bytes", C.c_int64), ("kernel_launches", C.c_int64), ("matvec32_modal", C.c_int64)]
+                ("device_bytes", C.c_int64), ("kernel_launches", C.c_int64), ("matvec32_modal", C.c_int64),
+                ("matvec32_tile", C.c_int64 * 4)]
 
 
 class IterRecord(C.Structure):

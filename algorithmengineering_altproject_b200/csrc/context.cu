@@ -1011,6 +1011,11 @@ int t3d_get_info(const t3d_context* ctx, t3d_info* info) {
     info->device_bytes = (int64_t)ctx->bytes;
     info->kernel_launches = ctx->launches;
     info->matvec32_modal = ctx->modal ? 1 : 0;
+    if (ctx->mixed) {
+        int d[4];
+        t3d::modal_variant_desc(ctx->mt.variant, d);
+        for (int k = 0; k < 4; ++k) info->matvec32_tile[k] = d[k];
+    }
     return T3D_OK;
 }
 

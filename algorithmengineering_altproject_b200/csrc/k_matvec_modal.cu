@@ -79,6 +79,26 @@ __device__ __forceinline__ void inv2(const Modes2& w, float& v00, float& v10, fl
     v11 = pp + qq;
 }
 
+// The same two stages on components 0 and 1 at once (packed FP32x2 arithmetic, .x = component 0,
+// .y = component 1); a - b is fma(b, -1, a), which is exact.
+struct Modes2x2 {
+    float2 m00, m10, m01, m11;
+};
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ Modes2x2 fwd2x2(float2 u00, float2 u10, float2 u01, float2 u11) {
+    const float2 s0 = add2(u00, u10), d0 = sub2(u10, u00), s1 = add2(u01, u11), d1 = sub2(u11, u01);
+    return Modes2x2{add2(s0, s1), add2(d0, d1), sub2(s1, s0), sub2(d1, d0)};
+}
+__device__ __forceinline__ void inv2x2(const Modes2x2& w, float2& v00, float2& v10, float2& v01, float2& v11) {
+    const float2 p = sub2(w.m00, w.m01), q = sub2(w.m10, w.m11), pp = add2(w.m00, w.m01), qq = add2(w.m10, w.m11);
+    v00 = sub2(p, q);
+    v10 = add2(p, q);
+    v01 = sub2(pp, qq);
+    v11 = add2(pp, qq);
+}
+
 __device__ __forceinline__ void cp_async4(unsigned s, const float* gsrc, bool valid) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gsrc), "r"(valid ? 4 : 0)
                  : "memory");
@@ -100,7 +120,7 @@ struct ModalSmem {
     double sh[32];
 };
 
-template <int BX, int BY, int MINB, int STAGES>
+template <int BX, int BY, int MINB, int STAGES, int PACK>
 __global__ void __launch_bounds__(BX * BY, MINB)
     k_matvec32_modal(Grid g, ModalKe kh, ModalTiling t, const float* __restrict__ E,
                      const uint8_t* __restrict__ mask, const float* __restrict__ u, float* __restrict__ y,
@@ -164,6 +184,8 @@ __global__ void __launch_bounds__(BX * BY, MINB)
         Modes2 bot[3], acc[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) acc[k] = bot[k] = Modes2{0.f, 0.f, 0.f, 0.f};
+        const float2 z2 = make_float2(0.f, 0.f);
+        Modes2x2 bot01{z2, z2, z2, z2}, acc01{z2, z2, z2, z2};   // PACK: components 0 and 1 (bot/acc[2] = comp 2)
         float4 h1 = make_float4(0.f, 0.f, 0.f, 0.f), h2 = h1;     // own node values of planes pz-1, pz-2
         float k0 = 0.f, k1 = 0.f, k2 = 0.f;                      // own element's corner (0,0) of plane pz-2
         int mk_next = 0;                                         // mask byte of plane pz-1
@@ -193,7 +215,7 @@ __global__ void __launch_bounds__(BX * BY, MINB)
                     part += (double)fmaf(h2.z, y2, fmaf(h2.y, y1, h2.x * y0));
             }
             if (owner && pz - 1 >= Z0 && pz - 1 < Z1) mk_next = mask[node_off + (pz - 1) * (int)NXY];
-            if (it < nplanes) {
+            if (!PACK && it < nplanes) {
                 const int s = it % STAGES;
                 const float4 a = sm.plane[s][ty][tx], b = sm.plane[s][ty][tx + 1], c = sm.plane[s][ty + 1][tx],
                              d = sm.plane[s][ty + 1][tx + 1];
@@ -248,6 +270,77 @@ __global__ void __launch_bounds__(BX * BY, MINB)
                 h2 = h1;
                 h1 = a;
             }
+            if (PACK && it < nplanes) {      // same layer arithmetic, components 0 and 1 packed
+                const int s = it % STAGES;
+                const float4 a = sm.plane[s][ty][tx], b = sm.plane[s][ty][tx + 1], c = sm.plane[s][ty + 1][tx],
+                             d = sm.plane[s][ty + 1][tx + 1];
+                const Modes2x2 top01 = fwd2x2(make_float2(a.x, a.y), make_float2(b.x, b.y), make_float2(c.x, c.y),
+                                              make_float2(d.x, d.y));
+                const Modes2 top2 = fwd2(a.z, b.z, c.z, d.z);
+                if (it >= 1) {
+                    const float Ee = sm.emod[s][ty][tx];
+                    const float2 E2 = make_float2(Ee, Ee);
+                    float2 cm01[8];
+                    cm01[0] = z2;
+                    cm01[1] = mul2(E2, add2(top01.m10, bot01.m10));
+                    cm01[2] = mul2(E2, add2(top01.m01, bot01.m01));
+                    cm01[3] = mul2(E2, add2(top01.m11, bot01.m11));
+                    cm01[4] = mul2(E2, sub2(top01.m00, bot01.m00));
+                    cm01[5] = mul2(E2, sub2(top01.m10, bot01.m10));
+                    cm01[6] = mul2(E2, sub2(top01.m01, bot01.m01));
+                    cm01[7] = mul2(E2, sub2(top01.m11, bot01.m11));
+                    float cm[24];
+#pragma unroll
+                    for (int m = 0; m < 8; ++m) {
+                        cm[m] = cm01[m].x;
+                        cm[8 + m] = cm01[m].y;
+                    }
+                    cm[16] = 0.f;
+                    cm[17] = Ee * (top2.m10 + bot[2].m10);
+                    cm[18] = Ee * (top2.m01 + bot[2].m01);
+                    cm[19] = Ee * (top2.m11 + bot[2].m11);
+                    cm[20] = Ee * (top2.m00 - bot[2].m00);
+                    cm[21] = Ee * (top2.m10 - bot[2].m10);
+                    cm[22] = Ee * (top2.m01 - bot[2].m01);
+                    cm[23] = Ee * (top2.m11 - bot[2].m11);
+                    float yh[24];
+#pragma unroll
+                    for (int i = 0; i < 24; ++i) yh[i] = 0.f;
+                    {
+                        int e = 0;
+#define T3D_KH_FMA(dd, ss) yh[dd] = fmaf(kh.v[e++], cm[ss], yh[dd]);
+                        T3D_KH_PATTERN(T3D_KH_FMA)
+#undef T3D_KH_FMA
+                    }
+                    float2 q01[8];
+#pragma unroll
+                    for (int m = 0; m < 8; ++m) q01[m] = make_float2(yh[m], yh[8 + m]);
+                    const Modes2x2 fin01{sub2(acc01.m00, q01[4]), add2(acc01.m10, sub2(q01[1], q01[5])),
+                                         add2(acc01.m01, sub2(q01[2], q01[6])), add2(acc01.m11, sub2(q01[3], q01[7]))};
+                    acc01 = Modes2x2{q01[4], add2(q01[1], q01[5]), add2(q01[2], q01[6]), add2(q01[3], q01[7])};
+                    const float* r = yh + 16;
+                    const Modes2 fin2{acc[2].m00 - r[4], acc[2].m10 + (r[1] - r[5]), acc[2].m01 + (r[2] - r[6]),
+                                      acc[2].m11 + (r[3] - r[7])};
+                    acc[2] = Modes2{r[4], r[1] + r[5], r[2] + r[6], r[3] + r[7]};
+                    float2 w00, w10, w01, w11;
+                    inv2x2(fin01, w00, w10, w01, w11);
+                    float v200, v210, v201, v211;
+                    inv2(fin2, v200, v210, v201, v211);
+                    if (it >= 2) {
+                        k0 = w00.x;
+                        k1 = w00.y;
+                        k2 = v200;
+                        const int pb = it & 1;
+                        sm.outc[pb][0][ty][tx] = make_float4(w10.x, w10.y, v210, 0.f);
+                        sm.outc[pb][1][ty][tx] = make_float4(w01.x, w01.y, v201, 0.f);
+                        sm.outc[pb][2][ty][tx] = make_float4(w11.x, w11.y, v211, 0.f);
+                    }
+                }
+                bot01 = top01;
+                bot[2] = top2;
+                h2 = h1;
+                h1 = a;
+            }
         }
         cp_async_wait<0>();
     }
@@ -258,18 +351,18 @@ __global__ void __launch_bounds__(BX * BY, MINB)
 }
 
 // Tile shapes the autotuner chooses from: CTA of BX x BY element columns, MINB CTAs per SM, ring depth.
-template <int BX, int BY, int MINB, int ST>
+template <int BX, int BY, int MINB, int ST, int PACK = 0>
 struct ModalShape {
-    static constexpr int bx = BX, by = BY;
+    static constexpr int bx = BX, by = BY, stages = ST, packed = PACK;
     static constexpr size_t smem = sizeof(ModalSmem<BX, BY, ST>);
-    static const void* fn() { return reinterpret_cast<const void*>(k_matvec32_modal<BX, BY, MINB, ST>); }
+    static const void* fn() { return reinterpret_cast<const void*>(k_matvec32_modal<BX, BY, MINB, ST, PACK>); }
     static void launch(const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E, const uint8_t* mask,
                        const float* u, float* y, RedSlot dot, PcgScalars* S, cudaStream_t s) {
-        k_matvec32_modal<BX, BY, MINB, ST><<<t.grid, BX * BY, smem, s>>>(g, kh, t, E, mask, u, y, dot, S);
+        k_matvec32_modal<BX, BY, MINB, ST, PACK><<<t.grid, BX * BY, smem, s>>>(g, kh, t, E, mask, u, y, dot, S);
     }
 };
 struct ModalVariant {
-    int bx, by;
+    int bx, by, stages, packed;
     size_t smem;
     const void* (*fn)();
     void (*launch)(const Grid&, const ModalKe&, const ModalTiling&, const float*, const uint8_t*, const float*,
@@ -277,9 +370,10 @@ struct ModalVariant {
 };
 template <class V>
 constexpr ModalVariant variant_of() {
-    return ModalVariant{V::bx, V::by, V::smem, &V::fn, &V::launch};
+    return ModalVariant{V::bx, V::by, V::stages, V::packed, V::smem, &V::fn, &V::launch};
 }
 const ModalVariant MODAL_VARIANTS[] = {
+    variant_of<ModalShape<32, 8, 2, 4, 1>>(),
     variant_of<ModalShape<32, 8, 2, 4>>(),
     variant_of<ModalShape<32, 8, 2, 3>>(),
     variant_of<ModalShape<32, 8, 3, 3>>(),
@@ -323,6 +417,14 @@ bool modal_ke_from(const double* Ke, ModalKe* out, double* off) {
             if (!in[i][j]) worst = std::fmax(worst, std::fabs(Kh[i][j]));
     *off = mx > 0.0 ? worst / mx : 1.0;
     return mx > 0.0 && *off <= 1e-10;
+}
+
+void modal_variant_desc(int variant, int out[4]) {
+    const ModalVariant& v = MODAL_VARIANTS[variant < 0 || variant >= MODAL_NVARIANTS ? 0 : variant];
+    out[0] = v.bx;
+    out[1] = v.by;
+    out[2] = v.stages;
+    out[3] = v.packed;
 }
 
 int modal_tiling(const Grid& g, int dev, int variant, ModalTiling* t) {

@@ -197,6 +197,8 @@ struct ModalTiling {     // persistent walk over (x tile, y tile, z slab) work i
 // has entries off the pattern (relative size above 1e-10), i.e. it is not the stiffness of an
 // axis-aligned cubic isotropic voxel; *off receives the largest relative off-pattern entry.
 bool modal_ke_from(const double* Ke, ModalKe* out, double* off);
+// (threads in x, threads in y, ring slots, packed FP32x2) of tile shape `variant`
+void modal_variant_desc(int variant, int out[4]);
 // Tiling and persistent grid size of tile shape `variant` on device `dev` (grid <= RED_BLOCKS).
 int modal_tiling(const Grid& g, int dev, int variant, ModalTiling* t);
 // Times every tile shape on the given buffers (3 launches each, stream-ordered, CUDA events) and returns

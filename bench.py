@@ -231,6 +231,7 @@ def run_kernels_only(args):
     mv = P.profile(t3d.T3D_PROFILE_MATVEC32 if mixed else t3d.T3D_PROFILE_MATVEC, args.reps)
     vc = P.profile(t3d.T3D_PROFILE_VCYCLE32 if mixed else t3d.T3D_PROFILE_VCYCLE, args.reps)
     print(json.dumps({"config": cfg["name"], "precision": args.precision, "matvec_ms": mv, "vcycle_ms": vc,
+                      "matvec32_tile": list(P.info().matvec32_tile) if mixed else None,
                       "roofline": matvec_roofline(P, mixed, mv)}), flush=True)
     P.close()
     return 0
@@ -349,6 +350,7 @@ def run_b200(args):
                               "pcg_iteration": 1000.0 * sum(r["t_cg"] for r in recs) / max(1, sum(pcg_its))},
             "throughput": {"dof_matvecs_per_s": P.nf / (mv_ms * 1e-3), "vcycles_per_s": 1.0 / (vc_ms * 1e-3)},
             "roofline": matvec_roofline(P, mixed, mv_ms),
+            "matvec32_tile": list(P.info().matvec32_tile) if mixed else None,
             "clocks": clk,
             "gpu_launches": launches,
             "wall_s_timed": t_wall,

@@ -94,6 +94,8 @@ typedef struct t3d_info {
     int64_t device_bytes;         /* device memory held by the context */
     int64_t kernel_launches;      /* kernels launched by this context so far (graph nodes included) */
     int64_t matvec32_modal;       /* 1 when the mixed form's FP32 K(E)p uses the modal kernel */
+    int64_t matvec32_tile[4];     /* tile shape the modal kernel's autotuner chose: threads in x, threads in y,
+                                     plane-ring slots, packed FP32x2 arithmetic (0/1) */
 } t3d_info;
 
 typedef struct t3d_iter_record {  /* one design iteration (driver.cpp:205-216) */
