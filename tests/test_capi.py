@@ -55,3 +55,33 @@ def test_no_device_is_an_error_not_a_fallback():
     with pytest.raises(t3d.T3DError) as e:
         t3d.Problem(6, 12, 6)
     assert e.value.code == t3d.T3D_ERR_NO_DEVICE
+
+
+@pytest.mark.parametrize("dims", [(0, 12, 6), (6, 0, 6), (6, 12, -1)])
+def test_empty_grids_are_rejected_before_any_device_work(dims):
+    with pytest.raises(t3d.T3DError) as e:
+        t3d.Problem(*dims)
+    assert e.value.code == t3d.T3D_ERR_INVALID
+
+
+@pytest.mark.parametrize("spec,msg", [
+    (dict(load_case=3), "load case"),
+    (dict(load_case=-1), "load case"),
+    (dict(voids=[(1, 1, 1, 0.0, 1, 1)]), "radii"),
+    (dict(voids=[(1, 1, 1, 1, 1, 1)] * 4, extra=True), "num_voids"),
+])
+def test_bad_problem_specs_are_rejected(spec, msg):
+    extra = spec.pop("extra", False)
+    p = t3d.ProblemSpec.make(**spec)
+    if extra:
+        p.num_voids = t3d.T3D_MAX_VOIDS + 1
+    with pytest.raises(t3d.T3DError) as e:
+        t3d.Problem(6, 12, 6, problem=p)
+    assert e.value.code == t3d.T3D_ERR_INVALID and msg in str(e.value)
+
+
+def test_null_arguments_are_errors():
+    lib = t3d.library()
+    assert lib.t3d_create(6, 12, 6, None, None) == t3d.T3D_ERR_INVALID
+    assert lib.t3d_get_info(None, None) == t3d.T3D_ERR_INVALID
+    assert lib.t3d_destroy(None) == t3d.T3D_OK

@@ -111,3 +111,13 @@ def test_design_loop_runs_on_each_case(load_case):
     (c64, o64), (c32, o32) = out[t3d.T3D_FP64], out[t3d.T3D_MIXED]
     assert abs(c32 - c64) <= 1e-8 * c64
     assert abs(o32[0] - o64[0]) <= 1e-8 * o64[0]
+
+
+def test_degenerate_and_oversized_problems_are_errors():
+    import algorithmengineering_altproject_b200 as t3d
+    with pytest.raises(t3d.T3DError) as e:   # a void that swallows the whole cuboid
+        t3d.Problem(6, 12, 6, problem=t3d.ProblemSpec.make(0, [(6.0, 3.0, 3.0, 50.0, 50.0, 50.0)]))
+    assert e.value.code == t3d.T3D_ERR_INVALID and "every element" in str(e.value)
+    with pytest.raises(t3d.T3DError) as e:   # 3 x nodes beyond 32-bit DOF indices: refused before any allocation
+        t3d.Problem(896, 1024, 896)
+    assert e.value.code == t3d.T3D_ERR_UNSUPPORTED
