@@ -201,6 +201,21 @@ def run_reference_arm(args):
     return 0
 
 
+# ---------------------------------------------------------------- replicas (one independent design per GPU)
+def max_over_ranks(values, world, device):
+    """Each rank's timings -> the maximum over all ranks (the job's time is its slowest replica)."""
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
+def job_throughput(world, steps, seconds):
+    """Whole-job design iterations/s: every replica runs `steps` iterations in at most `seconds`."""
+    return world * steps / seconds
+
+
 # ---------------------------------------------------------------- B200 arm
 def matvec_roofline(P, mixed, mv_ms):
     """roofline of K(E)p (+ p.Ap): algorithmic bytes = w*(2 n_free + n_elements), w = 4 (FP32) or 8."""
@@ -325,16 +340,14 @@ def run_b200(args):
         barrier()
         e2e = time.perf_counter() - t0
 
-    times = torch.tensor([dev_time, t_wall, e2e if e2e is not None else 0.0], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(times, op=torch.distributed.ReduceOp.MAX)
-    dev_time, t_wall, e2e = [float(v) for v in times.cpu()]
+    dev_time, t_wall, e2e = max_over_ranks([dev_time, t_wall, e2e if e2e is not None else 0.0], world, "cuda")
 
     if rank == 0:
         ne = P.ne
         pcg_its = [r["pcg_iters"] for r in recs]
         line = {
-            "metric": METRIC, "value": world * args.steps / dev_time, "unit": "design iter/s", "n_gpus": world,
+            "metric": METRIC, "value": job_throughput(world, args.steps, dev_time), "unit": "design iter/s",
+            "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * dev_time / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32+f64 (mixed)" if mixed else "f64",
@@ -358,7 +371,7 @@ def run_b200(args):
         if comparison is not None:
             line["vs_fp64"] = comparison
         if e2e:
-            line["e2e"] = {"value": world * args.steps / e2e, "unit": "design iter/s",
+            line["e2e"] = {"value": job_throughput(world, args.steps, e2e), "unit": "design iter/s",
                            "h2d_bytes_per_step": 4 * ne, "d2h_bytes_per_step": 4 * ne + 64}
         if not args.no_cpu_baseline and world == 1:
             try:
