@@ -25,6 +25,7 @@ T3D_SUM_REFERENCE, T3D_SUM_FP64 = 0, 1
 T3D_FP64, T3D_MIXED = 0, 1
 T3D_MATVEC32_AUTO, T3D_MATVEC32_DENSE = 0, 1
 T3D_COARSE_REFERENCE, T3D_COARSE_FULL = 0, 1
+T3D_MATVEC64_AUTO, T3D_MATVEC64_NODES = 0, 1
 
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
@@ -43,7 +44,8 @@ class Params(C.Structure):
                 ("cg_tol", C.c_float), ("cg_max_it", C.c_int), ("mg_nondyadic", C.c_int),
                 ("mg_max_levels", C.c_int), ("mg_weight", C.c_float), ("filter_rmin", C.c_float),
                 ("oc_sum_order", C.c_int), ("precision", C.c_int), ("device", C.c_int),
-                ("matvec32_form", C.c_int), ("mg_coarse_assembly", C.c_int), ("reserved", C.c_int * 5)]
+                ("matvec32_form", C.c_int), ("mg_coarse_assembly", C.c_int), ("matvec64_form", C.c_int),
+                ("reserved", C.c_int * 4)]
 
 
 T3D_LOAD_TIP_LINE, T3D_LOAD_TOP_TRACTION, T3D_LOAD_TORSION = 0, 1, 2

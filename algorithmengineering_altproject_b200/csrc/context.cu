@@ -148,6 +148,8 @@ struct Context {
     FilterScalars* FS = nullptr;
     OcState* OC = nullptr;
     double* scal = nullptr;     // [0] C, [1] Csolid, [2] objective
+    bool mv64_stream = false;   // FP64 K(E)u by the element-streaming kernel (else node-centric)
+    Stream64Tiling st64{};
     RedSlot slot[4]{};
     double *Kce = nullptr, *Kc = nullptr, *LT = nullptr, *Lrow = nullptr, *Xc = nullptr;
     double* ra1[8]{};           // separable-restriction pass buffers per level transition
@@ -388,6 +390,8 @@ static int create(int nely, int nelx, int nelz, const t3d_params* prm, const t3d
         return set_error(T3D_ERR_UNSUPPORTED, "mg_coarse_assembly must be T3D_COARSE_REFERENCE or T3D_COARSE_FULL");
     if (c->prm.matvec32_form != T3D_MATVEC32_AUTO && c->prm.matvec32_form != T3D_MATVEC32_DENSE)
         return set_error(T3D_ERR_UNSUPPORTED, "matvec32_form must be T3D_MATVEC32_AUTO or T3D_MATVEC32_DENSE");
+    if (c->prm.matvec64_form != T3D_MATVEC64_AUTO && c->prm.matvec64_form != T3D_MATVEC64_NODES)
+        return set_error(T3D_ERR_UNSUPPORTED, "matvec64_form must be T3D_MATVEC64_AUTO or T3D_MATVEC64_NODES");
     c->mixed = c->prm.precision == T3D_MIXED;
     c->dev = c->prm.device;
     T3D_CUDA_OK(cudaSetDevice(c->dev));
@@ -413,6 +417,8 @@ static int create(int nely, int nelx, int nelz, const t3d_params* prm, const t3d
         c->ne = ne;
     }
     const Grid& g = c->g;
+    c->mv64_stream = c->prm.matvec64_form == T3D_MATVEC64_AUTO;
+    if (c->mv64_stream) CHECK(stream64_tiling(g, c->dev, &c->st64));
 
     CHECK(c->alloc(&c->Ke, 576));
     CHECK(c->alloc(&c->kf, 72));
@@ -598,6 +604,19 @@ static int mg_setup(Context* c) {
     return launch_check("mg set-up");
 }
 
+// FP64 y = K(E) u on c->E (bit-identical in both forms); with dot.partial, u.y goes to S->denom unless
+// S->done.  Returns the number of kernels launched.
+static int matvec64(Context* c, const double* u, double* y, RedSlot dot, PcgScalars* S) {
+    if (!c->mv64_stream) {
+        launch_matvec64(c->g, c->Ke, c->E, c->mask0, u, y, dot, S, c->st);
+        return 1;
+    }
+    launch_matvec64_stream(c->g, c->st64, c->Ke_h, c->E, c->mask0, u, y, S, c->st);
+    if (!dot.partial) return 1;
+    launch_dot_pcg(c->g, u, y, dot, S, c->st);
+    return 2;
+}
+
 // z = M r for grid vectors; with S, r.z goes to S (rz / beta)
 static void vcycle(Context* c, const double* r, double* z, PcgScalars* S, RedSlot dot) {
     const int L = c->nlev;
@@ -614,8 +633,7 @@ static void vcycle(Context* c, const double* r, double* z, PcgScalars* S, RedSlo
 
 // ------------------------------------------------------------------ PCG (solver.cpp:87-217)
 static void pcg_iteration(Context* c) {
-    c->launches += 3;
-    launch_matvec64(c->g, c->Ke, c->E, c->mask0, c->p, c->Ap, c->slot[0], c->S, c->st);
+    c->launches += 2 + matvec64(c, c->p, c->Ap, c->slot[0], c->S);
     launch_pcg_update(c->g, c->u, c->r, c->p, c->Ap, c->slot[1], c->S, c->st);
     vcycle(c, c->r, c->z, c->S, c->slot[2]);
     launch_pcg_direction(c->g, c->z, c->p, c->S, c->st);
@@ -641,9 +659,8 @@ static int ensure_pcg_graph(Context* c) {
 static int pcg_solve(Context* c, double tol, int maxit, int* iters) {
     if (!c->mg_ready) return set_error(T3D_ERR_INVALID, "multigrid preconditioner not set up");
     CHECK(ensure_pcg_graph(c));
-    launch_matvec64(c->g, c->Ke, c->E, c->mask0, c->u, c->Ap, RedSlot{nullptr, nullptr}, nullptr, c->st);
+    c->launches += 1 + matvec64(c, c->u, c->Ap, RedSlot{nullptr, nullptr}, nullptr);
     launch_pcg_init(c->g, c->b, c->Ap, c->r, c->slot[1], c->S, tol, c->st);
-    c->launches += 2;
     vcycle(c, c->r, c->z, c->S, c->slot[2]);
     launch_pcg_start(c->g, c->z, c->p, c->st);
     CHECK(launch_check("pcg start"));
@@ -653,7 +670,7 @@ static int pcg_solve(Context* c, double tol, int maxit, int* iters) {
         const int n = std::min(PCG_CHUNK, maxit - queued);
         if (c->use_graph && n == PCG_CHUNK) {
             T3D_CUDA_OK(cudaGraphLaunch(c->pcg_graph, c->st));
-            c->launches += (int64_t)PCG_CHUNK * (3 + 4 * (c->nlev - 1) + 1);
+            c->launches += (int64_t)PCG_CHUNK * ((c->mv64_stream ? 4 : 3) + 4 * (c->nlev - 1) + 1);
         } else {
             for (int k = 0; k < n; ++k) pcg_iteration(c);
             CHECK(launch_check("pcg iteration"));
@@ -731,9 +748,8 @@ static int mixed_solve(Context* c, double tol, int maxit, int* iters) {
     int budget = maxit, used = 0, outer = 0;
     bool converged = false;
     for (; outer < 64; ++outer) {
-        launch_matvec64(c->g, c->Ke, c->E, c->mask0, c->u, c->Ap, RedSlot{nullptr, nullptr}, nullptr, c->st);
+        c->launches += 1 + matvec64(c, c->u, c->Ap, RedSlot{nullptr, nullptr}, nullptr);
         launch_mixed_residual(g, c->b, c->Ap, c->r32, c->d32, c->slot[3], c->scal + 6, c->st);
-        c->launches += 2;
         CHECK(launch_check("mixed residual"));
         T3D_CUDA_OK(cudaMemcpyAsync(c->scal_h + 6, c->scal + 6, sizeof(double), cudaMemcpyDeviceToHost, c->st));
         CHECK(sync(c));
@@ -1037,6 +1053,11 @@ int t3d_set_ke(t3d_context* ctx, const double* ke) {
         ctx->modal = ctx->prm.matvec32_form == T3D_MATVEC32_AUTO &&
                      t3d::modal_ke_from(ctx->Ke_h, &ctx->kh, &ctx->modal_off);
     }
+    // the captured PCG iterations hold Ke (FP64 streaming form) and the modal coefficients by value
+    if (ctx->pcg_graph) cudaGraphExecDestroy(ctx->pcg_graph);
+    if (ctx->pcg32_graph) cudaGraphExecDestroy(ctx->pcg32_graph);
+    ctx->pcg_graph = nullptr;
+    ctx->pcg32_graph = nullptr;
     return T3D_OK;
 }
 
@@ -1072,8 +1093,7 @@ int t3d_matvec(t3d_context* ctx, const double* E, const double* u, double* y) {
     if (!E || !u || !y) return t3d::set_error(T3D_ERR_INVALID, "null argument");
     CHECK(t3d::upload_cells_f64(ctx, E, ctx->E));
     CHECK(t3d::upload_free(ctx, u, ctx->p));
-    t3d::launch_matvec64(ctx->g, ctx->Ke, ctx->E, ctx->mask0, ctx->p, ctx->Ap, t3d::RedSlot{nullptr, nullptr},
-                         nullptr, ctx->st);
+    ctx->launches += t3d::matvec64(ctx, ctx->p, ctx->Ap, t3d::RedSlot{nullptr, nullptr}, nullptr);
     CHECK(t3d::launch_check("matvec"));
     return t3d::download_free(ctx, ctx->Ap, y);
 }
@@ -1340,8 +1360,7 @@ int t3d_profile(t3d_context* ctx, int what, int reps, double* ms) {
     }
     auto once = [&]() {
         if (what == T3D_PROFILE_MATVEC) {
-            t3d::launch_matvec64(ctx->g, ctx->Ke, ctx->E, ctx->mask0, ctx->p, ctx->Ap, ctx->slot[0], ctx->S, ctx->st);
-            ctx->launches += 1;
+            ctx->launches += t3d::matvec64(ctx, ctx->p, ctx->Ap, ctx->slot[0], ctx->S);
         } else if (what == T3D_PROFILE_VCYCLE) {
             t3d::vcycle(ctx, ctx->r, ctx->z, ctx->S, ctx->slot[2]);
         } else if (what == T3D_PROFILE_MATVEC32) {

@@ -62,6 +62,20 @@ void launch_setup_box_load(const Grid& g, int x0, int x1, int y0, int y1, int z0
 // Ke: device pointer to the 576 stiffness coefficients
 void launch_matvec64(const Grid& g, const double* Ke, const double* E, const uint8_t* mask, const double* u,
                      double* y, RedSlot dot, PcgScalars* S, cudaStream_t s);
+// Element-streaming form of the same product (bit-identical; no fused dot).  The tiling is fixed per
+// grid and device: stream64_tiling also sets the kernel's shared-memory attribute on the current device.
+struct Stream64Tiling {   // persistent walk over (x tile, y tile, z slab) work items
+    int tiles_x, tiles_y, slabs, slab, items, grid;
+};
+struct Ke64 {             // Ke by value (576 doubles, row-major): a kernel parameter, read from the constant bank
+    double v[576];
+};
+int stream64_tiling(const Grid& g, int dev, Stream64Tiling* t);
+// Ke_host: the context's host copy of Ke; it is copied into the launch (and into a graph that captures it)
+void launch_matvec64_stream(const Grid& g, const Stream64Tiling& t, const double* Ke_host, const double* E,
+                            const uint8_t* mask, const double* u, double* y, const PcgScalars* S, cudaStream_t s);
+// S->denom = p.Ap (3 components) in the canonical reduction order, unless S->done
+void launch_dot_pcg(const Grid& g, const double* p, const double* Ap, RedSlot red, PcgScalars* S, cudaStream_t s);
 void launch_compliance64(const Grid& g, const double* Ke, const double* E, const double* u, double* ce,
                          RedSlot red, double* C, cudaStream_t s);
 void launch_simp(const Grid& g, const uint8_t* solid, const float* x, float E0, float Emin, float penal, double* E,

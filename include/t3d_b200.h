@@ -48,6 +48,9 @@ enum { T3D_MATVEC32_AUTO = 0, T3D_MATVEC32_DENSE = 1 };
  * sub-block of the grid when there are more than two levels (on some grids PCG then stalls);
  * FULL = the Galerkin operator of the whole grid (s = product of all spans) */
 enum { T3D_COARSE_REFERENCE = 0, T3D_COARSE_FULL = 1 };
+/* FP64 K(E)u (t3d_matvec, FP64 PCG, the mixed form's outer residual): AUTO = element-streaming kernel,
+ * NODES = node-centric gather kernel.  Both are bit-identical to the reference's product. */
+enum { T3D_MATVEC64_AUTO = 0, T3D_MATVEC64_NODES = 1 };
 
 typedef struct t3d_params {
     float E0, Emin, nu, penal;    /* GlobalParams core.hpp:26-33 (Ke always uses nu = 0.3, fea.cpp:345) */
@@ -62,7 +65,8 @@ typedef struct t3d_params {
     int   device;                 /* CUDA device ordinal */
     int   matvec32_form;          /* mixed precision only: T3D_MATVEC32_AUTO or T3D_MATVEC32_DENSE */
     int   mg_coarse_assembly;     /* T3D_COARSE_REFERENCE (default) or T3D_COARSE_FULL */
-    int   reserved[5];
+    int   matvec64_form;          /* T3D_MATVEC64_AUTO (default) or T3D_MATVEC64_NODES */
+    int   reserved[4];
 } t3d_params;
 
 /* Problem spec beyond the reference's built-in cantilever (the reference hard-codes one load case and a
