@@ -40,6 +40,7 @@ def nvcc() -> str:
 def _compile(src: str) -> str:
     obj = os.path.join(OBJ, os.path.basename(src).replace(".cu", ".o"))
     deps = [src] + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.hpp")) + \
+        glob.glob(os.path.join(CSRC, "*.inc")) + \
         glob.glob(os.path.join(INCLUDE, "*.h"))
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps):
         return obj

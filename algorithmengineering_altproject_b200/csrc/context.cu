@@ -3,6 +3,7 @@
 // the kernels of the design iteration on one stream, captures the PCG iteration in CUDA graphs and
 // implements the C-ABI declared in include/t3d_b200.h.
 #include "t3d_b200.h"
+#include "hex8.hpp"
 #include "kernels.hpp"
 
 #include <algorithm>
@@ -33,52 +34,7 @@ int set_cuda_error(cudaError_t e, const char* what, const char* file, int line) 
 }
 
 // ------------------------------------------------------------------ host-side model constants
-// Unit-modulus hex8 stiffness (fea.cpp:117-179): 2x2x2 Gauss, Voigt [xx,yy,zz,yz,xz,xy],
-// local DOF 3a+c with the natural-coordinate node order (-,-,-),(+,-,-),(+,+,-),(-,+,-), then +z.
-static void hex8_stiffness(double nu, double h, double* Ke) {
-    const double lam = nu / ((1.0 + nu) * (1.0 - 2.0 * nu));
-    const double mu = 1.0 / (2.0 * (1.0 + nu));
-    double D[6][6] = {{0}};
-    for (int i = 0; i < 3; ++i) {
-        for (int j = 0; j < 3; ++j) D[i][j] = lam;
-        D[i][i] = lam + 2.0 * mu;
-        D[3 + i][3 + i] = mu;
-    }
-    static const double sg[8] = {-1, 1, 1, -1, -1, 1, 1, -1};
-    static const double tg[8] = {-1, -1, 1, 1, -1, -1, 1, 1};
-    static const double pg[8] = {-1, -1, -1, -1, 1, 1, 1, 1};
-    const double gq = 1.0 / std::sqrt(3.0);
-    const double detJ = (h * h * h) / 8.0, sc = 2.0 / h;
-    std::memset(Ke, 0, 576 * sizeof(double));
-    for (int a = 0; a < 2; ++a)
-        for (int b = 0; b < 2; ++b)
-            for (int c = 0; c < 2; ++c) {
-                const double s = a ? gq : -gq, t = b ? gq : -gq, q = c ? gq : -gq;
-                double B[6][24] = {{0}};
-                for (int n = 0; n < 8; ++n) {
-                    const double dx = 0.125 * sg[n] * (1 + tg[n] * t) * (1 + pg[n] * q) * sc;
-                    const double dy = 0.125 * tg[n] * (1 + sg[n] * s) * (1 + pg[n] * q) * sc;
-                    const double dz = 0.125 * pg[n] * (1 + sg[n] * s) * (1 + tg[n] * t) * sc;
-                    B[0][3 * n] = dx; B[1][3 * n + 1] = dy; B[2][3 * n + 2] = dz;
-                    B[3][3 * n + 1] = dz; B[3][3 * n + 2] = dy;
-                    B[4][3 * n] = dz; B[4][3 * n + 2] = dx;
-                    B[5][3 * n] = dy; B[5][3 * n + 1] = dx;
-                }
-                double DB[6][24];
-                for (int i = 0; i < 6; ++i)
-                    for (int j = 0; j < 24; ++j) {
-                        double acc = 0.0;
-                        for (int k = 0; k < 6; ++k) acc += D[i][k] * B[k][j];
-                        DB[i][j] = acc;
-                    }
-                for (int i = 0; i < 24; ++i)
-                    for (int j = 0; j < 24; ++j) {
-                        double acc = 0.0;
-                        for (int k = 0; k < 6; ++k) acc += B[k][i] * DB[k][j];
-                        Ke[i * 24 + j] += acc * detJ;
-                    }
-            }
-}
+// (the hex8 element stiffness is in hex8.hpp)
 
 // PDE-filter 8x8 kernel r^2 KEF0 + KEF1 (filter.cpp:11-54) followed by its 8 row sums (:56-62)
 static void filter_kernel(float rmin, double* kf) {
@@ -150,6 +106,8 @@ struct Context {
     double* scal = nullptr;     // [0] C, [1] Csolid, [2] objective
     bool mv64_stream = false;   // FP64 K(E)u by the element-streaming kernel (else node-centric)
     Stream64Tiling st64{};
+    bool ke_pat = false;        // Ke has the built-in coefficient pattern: its magnitudes are in Kd
+    double* Kd = nullptr;       // [KE_MAX_DISTINCT]
     RedSlot slot[4]{};
     double *Kce = nullptr, *Kc = nullptr, *LT = nullptr, *Lrow = nullptr, *Xc = nullptr;
     double* ra1[8]{};           // separable-restriction pass buffers per level transition
@@ -224,6 +182,8 @@ struct Context {
         if (st) cudaStreamDestroy(st);
     }
 };
+
+static int update_ke_pattern(Context* c);
 
 #define CHECK(call)                       \
     do {                                  \
@@ -421,6 +381,7 @@ static int create(int nely, int nelx, int nelz, const t3d_params* prm, const t3d
     if (c->mv64_stream) CHECK(stream64_tiling(g, c->dev, &c->st64));
 
     CHECK(c->alloc(&c->Ke, 576));
+    CHECK(c->alloc(&c->Kd, KE_MAX_DISTINCT));
     CHECK(c->alloc(&c->kf, 72));
     CHECK(c->alloc(&c->solid, g.NE));
     CHECK(c->alloc(&c->mask0, g.NN));
@@ -453,6 +414,7 @@ static int create(int nely, int nelx, int nelz, const t3d_params* prm, const t3d
     // element stiffness (fea.cpp:345 passes nu = 0.3 literally) and filter kernel
     hex8_stiffness(0.3, 1.0, c->Ke_h);
     T3D_CUDA_OK(cudaMemcpyAsync(c->Ke, c->Ke_h, sizeof c->Ke_h, cudaMemcpyHostToDevice, c->st));
+    CHECK(update_ke_pattern(c));
     double kf[72];
     filter_kernel(c->prm.filter_rmin, kf);
     T3D_CUDA_OK(cudaMemcpyAsync(c->kf, kf, sizeof kf, cudaMemcpyHostToDevice, c->st));
@@ -604,6 +566,15 @@ static int mg_setup(Context* c) {
     return launch_check("mg set-up");
 }
 
+// Selects the FP64 streaming kernel's coefficient form for c->Ke_h (ordered on c->st)
+static int update_ke_pattern(Context* c) {
+    static_assert(sizeof(c->Ke_h) == 576 * sizeof(double), "Ke_h");
+    double D[KE_MAX_DISTINCT] = {0};
+    c->ke_pat = ke_pattern_magnitudes(c->Ke_h, D);
+    if (c->ke_pat) T3D_CUDA_OK(cudaMemcpyAsync(c->Kd, D, sizeof D, cudaMemcpyHostToDevice, c->st));
+    return T3D_OK;
+}
+
 // FP64 y = K(E) u on c->E (bit-identical in both forms); with dot.partial, u.y goes to S->denom unless
 // S->done.  Returns the number of kernels launched.
 static int matvec64(Context* c, const double* u, double* y, RedSlot dot, PcgScalars* S) {
@@ -611,7 +582,7 @@ static int matvec64(Context* c, const double* u, double* y, RedSlot dot, PcgScal
         launch_matvec64(c->g, c->Ke, c->E, c->mask0, u, y, dot, S, c->st);
         return 1;
     }
-    launch_matvec64_stream(c->g, c->st64, c->Ke_h, c->E, c->mask0, u, y, S, c->st);
+    launch_matvec64_stream(c->g, c->st64, c->Ke_h, c->ke_pat ? c->Kd : nullptr, c->E, c->mask0, u, y, S, c->st);
     if (!dot.partial) return 1;
     launch_dot_pcg(c->g, u, y, dot, S, c->st);
     return 2;
@@ -1027,6 +998,7 @@ int t3d_get_info(const t3d_context* ctx, t3d_info* info) {
     info->device_bytes = (int64_t)ctx->bytes;
     info->kernel_launches = ctx->launches;
     info->matvec32_modal = ctx->modal ? 1 : 0;
+    info->matvec64_kernel = !ctx->mv64_stream ? 0 : ctx->ke_pat ? 2 : 1;
     if (ctx->mixed) {
         int d[4];
         t3d::modal_variant_desc(ctx->mt.variant, d);
@@ -1046,6 +1018,8 @@ int t3d_set_ke(t3d_context* ctx, const double* ke) {
     if (!ke) return t3d::set_error(T3D_ERR_INVALID, "null Ke");
     std::memcpy(ctx->Ke_h, ke, sizeof ctx->Ke_h);
     T3D_CUDA_OK(cudaMemcpy(ctx->Ke, ctx->Ke_h, sizeof ctx->Ke_h, cudaMemcpyHostToDevice));
+    CHECK(t3d::update_ke_pattern(ctx));
+    T3D_CUDA_OK(cudaStreamSynchronize(ctx->st));
     if (ctx->Ke32) {
         float k32[576];
         for (int i = 0; i < 576; ++i) k32[i] = (float)ctx->Ke_h[i];

@@ -13,12 +13,18 @@
 // the chains' results for the bottom and top corners go to shared memory; each owned node folds its 4
 // same-layer elements in colour order and carries the other layer's part to the next plane (a partial
 // sum when that layer comes first in the node's colour order, the 4 raw triples otherwise).
-// Ke is a kernel parameter: with the chains fully unrolled every coefficient is a constant-bank operand
-// of its DFMA (a broadcast shared-memory load of FP64 coefficients would cost more issue and L1
-// bandwidth than the DFMAs it feeds).  p.Ap is not fused: the caller folds it in the canonical order.
+// Coefficients: a DFMA whose coefficient is a constant-bank operand issues at about half the rate of
+// one with register operands only, and a shared-memory broadcast of FP64 coefficients costs more than
+// the DFMAs it feeds.  The built-in Ke has only KE_ND distinct magnitudes (ke_pattern.inc), so for it
+// (PAT) they sit in registers and each coefficient is +-D[ke_idx(i)] (negation is an exact operand
+// modifier); the 24 rows of a column run in ke_row_order so that consecutive DFMAs share a coefficient
+// register.  Any other Ke (t3d_set_ke) is passed by value and read from the constant bank.
+// p.Ap is not fused: the caller folds it in the canonical order.
 #include <algorithm>
+#include <cmath>
 
 #include "kernels.hpp"
+#include "ke_pattern.inc"
 #include "red.cuh"
 #include "t3d_b200.h"
 
@@ -33,6 +39,8 @@ __device__ __forceinline__ void cp_async8(unsigned s, const double* gsrc, bool v
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
+
+static_assert(KE_ND <= KE_MAX_DISTINCT, "distinct-magnitude buffer too small");
 
 constexpr int S64_BX = 32;
 constexpr int S64_BY = 8;
@@ -78,7 +86,9 @@ __device__ __forceinline__ void load_emod(const Grid& g, const double* __restric
     cp_async8(smem_addr(dst + threadIdx.x), ok ? E + g.cell(cx, cy, cz) : E, ok);
 }
 
+template <bool PAT>
 __global__ void __launch_bounds__(S64::NT, 2) k_matvec64_stream(Grid g, Stream64Tiling t, const Ke64 ke,
+                                                                const double* __restrict__ Kd,
                                                                 const double* __restrict__ E,
                                                                 const uint8_t* __restrict__ mask,
                                                                 const double* __restrict__ u,
@@ -89,6 +99,9 @@ __global__ void __launch_bounds__(S64::NT, 2) k_matvec64_stream(Grid g, Stream64
     double* Fb = sm + S64::FB;
     const int tx = threadIdx.x % BX, ty = threadIdx.x / BX;
     const int64_t NN = g.NN;
+    double D[PAT ? KE_ND : 1];   // PAT: the distinct magnitudes of Ke, loaded once into registers
+#pragma unroll
+    for (int d = 0; d < (PAT ? KE_ND : 1); ++d) D[d] = PAT ? __ldg(Kd + d) : 0.0;
 
     for (int w = blockIdx.x; w < t.items; w += gridDim.x) {
         const int tix = w % t.tiles_x, rest = w / t.tiles_x;
@@ -111,10 +124,30 @@ __global__ void __launch_bounds__(S64::NT, 2) k_matvec64_stream(Grid g, Stream64
                 load_emod(g, E, X0, Y0, cz + 1, sm + S64::EMOD + ((k + 1) % 3) * NT);
             }
             cp_commit();
-            // ---- element (tx, ty) of layer cz: the 24 FMA chains of Ke u_e, in two halves of 12 rows
+            // ---- element (tx, ty) of layer cz: the 24 FMA chains f_row = fma(Ke[row][j], u_e[j], f_row), j = 0..23
             double* Ft = sm + S64::FT + (k & 1) * 12 * NT;
             const double Ee = sm[S64::EMOD + (k % 3) * NT + threadIdx.x];
-            if (!(Ee <= 1.0e-16)) {     // the owners skip exactly the elements skipped here
+            if (PAT && !(Ee <= 1.0e-16)) {   // the owners skip exactly the elements skipped here
+                const double* Pb = sm + S64::PLANE + (k % 3) * S64::PLANE_SZ;
+                const double* Pt = sm + S64::PLANE + ((k + 1) % 3) * S64::PLANE_SZ;
+                double f[24];
+#pragma unroll
+                for (int q = 0; q < 24; ++q) f[q] = 0.0;
+#pragma unroll
+                for (int j = 0; j < 24; ++j) {
+                    const int a = j / 3, c = j % 3;
+                    const double uj = (a < 4 ? Pb : Pt)[c * AREA + (ty + corner_dy(a)) * PX + tx + corner_dx(a)];
+#pragma unroll
+                    for (int r = 0; r < 24; ++r) {
+                        const int q = ke_row_order(24 * j + r), i = 24 * q + j;
+                        f[q] = fma(ke_neg(i) ? -D[ke_idx(i)] : D[ke_idx(i)], uj, f[q]);
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 12; ++q) Fb[q * NT + threadIdx.x] = f[q];
+#pragma unroll
+                for (int q = 0; q < 12; ++q) Ft[q * NT + threadIdx.x] = f[12 + q];
+            } else if (!PAT && !(Ee <= 1.0e-16)) {   // any Ke: two halves of 12 rows, coefficients from the constant bank
                 const double* Pb = sm + S64::PLANE + (k % 3) * S64::PLANE_SZ;
                 const double* Pt = sm + S64::PLANE + ((k + 1) % 3) * S64::PLANE_SZ;
                 double ue[24];
@@ -192,14 +225,25 @@ __global__ void __launch_bounds__(RED_THREADS) k_dot_pcg(Grid g, const double* _
 
 }  // namespace
 
+bool ke_pattern_magnitudes(const double* Ke, double* D) {
+    for (int d = 0; d < KE_ND; ++d) D[d] = std::fabs(Ke[ke_first(d)]);
+    for (int i = 0; i < 576; ++i)
+        if (Ke[i] != (ke_neg(i) ? -D[ke_idx(i)] : D[ke_idx(i)])) return false;
+    return true;
+}
+
 int stream64_tiling(const Grid& g, int dev, Stream64Tiling* t) {
-    cudaError_t e = cudaFuncSetAttribute(k_matvec64_stream, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)S64::BYTES);
-    if (e != cudaSuccess) return set_cuda_error(e, "cudaFuncSetAttribute", __FILE__, __LINE__);
-    int per_sm = 0, sms = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_matvec64_stream, S64::NT, S64::BYTES);
-    if (e != cudaSuccess) return set_cuda_error(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor", __FILE__, __LINE__);
-    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int per_sm = 1 << 30, sms = 0;
+    for (auto fn : {k_matvec64_stream<true>, k_matvec64_stream<false>}) {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S64::BYTES);
+        if (e != cudaSuccess) return set_cuda_error(e, "cudaFuncSetAttribute", __FILE__, __LINE__);
+        int n = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, S64::NT, S64::BYTES);
+        if (e != cudaSuccess)
+            return set_cuda_error(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor", __FILE__, __LINE__);
+        per_sm = std::min(per_sm, n);
+    }
+    cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return set_cuda_error(e, "cudaDeviceGetAttribute", __FILE__, __LINE__);
     if (per_sm < 1) return set_error(T3D_ERR_CUDA, "FP64 streaming K(E)u does not fit on an SM");
     const int resident = per_sm * sms;
@@ -216,11 +260,17 @@ int stream64_tiling(const Grid& g, int dev, Stream64Tiling* t) {
     return T3D_OK;
 }
 
-void launch_matvec64_stream(const Grid& g, const Stream64Tiling& t, const double* Ke_host, const double* E,
-                            const uint8_t* mask, const double* u, double* y, const PcgScalars* S, cudaStream_t s) {
+void launch_matvec64_stream(const Grid& g, const Stream64Tiling& t, const double* Ke_host, const double* Kd,
+                            const double* E, const uint8_t* mask, const double* u, double* y, const PcgScalars* S,
+                            cudaStream_t s) {
+    if (Kd) {   // the by-value Ke is not read in this form
+        static const Ke64 unused{};
+        k_matvec64_stream<true><<<t.grid, S64::NT, S64::BYTES, s>>>(g, t, unused, Kd, E, mask, u, y, S);
+        return;
+    }
     Ke64 ke;
     for (int i = 0; i < 576; ++i) ke.v[i] = Ke_host[i];
-    k_matvec64_stream<<<t.grid, S64::NT, S64::BYTES, s>>>(g, t, ke, E, mask, u, y, S);
+    k_matvec64_stream<false><<<t.grid, S64::NT, S64::BYTES, s>>>(g, t, ke, nullptr, E, mask, u, y, S);
 }
 
 void launch_dot_pcg(const Grid& g, const double* p, const double* Ap, RedSlot red, PcgScalars* S, cudaStream_t s) {

@@ -70,10 +70,16 @@ struct Stream64Tiling {   // persistent walk over (x tile, y tile, z slab) work 
 struct Ke64 {             // Ke by value (576 doubles, row-major): a kernel parameter, read from the constant bank
     double v[576];
 };
+constexpr int KE_MAX_DISTINCT = 32;   // room for the distinct-magnitude list of the built-in Ke
+// true when Ke has the coefficient pattern of the built-in hex8 Ke; D[0..KE_MAX_DISTINCT) receives its
+// distinct magnitudes (the streaming kernel's register-operand form)
+bool ke_pattern_magnitudes(const double* Ke, double* D);
 int stream64_tiling(const Grid& g, int dev, Stream64Tiling* t);
-// Ke_host: the context's host copy of Ke; it is copied into the launch (and into a graph that captures it)
-void launch_matvec64_stream(const Grid& g, const Stream64Tiling& t, const double* Ke_host, const double* E,
-                            const uint8_t* mask, const double* u, double* y, const PcgScalars* S, cudaStream_t s);
+// Kd: device copy of the magnitudes when Ke has the built-in pattern, else nullptr; then Ke_host (the
+// context's host copy of Ke) is copied into the launch (and into a graph that captures it)
+void launch_matvec64_stream(const Grid& g, const Stream64Tiling& t, const double* Ke_host, const double* Kd,
+                            const double* E, const uint8_t* mask, const double* u, double* y, const PcgScalars* S,
+                            cudaStream_t s);
 // S->denom = p.Ap (3 components) in the canonical reduction order, unless S->done
 void launch_dot_pcg(const Grid& g, const double* p, const double* Ap, RedSlot red, PcgScalars* S, cudaStream_t s);
 void launch_compliance64(const Grid& g, const double* Ke, const double* E, const double* u, double* ce,

@@ -100,6 +100,8 @@ typedef struct t3d_info {
     int64_t matvec32_modal;       /* 1 when the mixed form's FP32 K(E)p uses the modal kernel */
     int64_t matvec32_tile[4];     /* tile shape the modal kernel's autotuner chose: threads in x, threads in y,
                                      plane-ring slots, packed FP32x2 arithmetic (0/1) */
+    int64_t matvec64_kernel;      /* FP64 K(E)u kernel: 0 node-centric, 1 streaming with Ke from the constant bank,
+                                     2 streaming with the built-in Ke's magnitudes in registers */
 } t3d_info;
 
 typedef struct t3d_iter_record {  /* one design iteration (driver.cpp:205-216) */

@@ -95,3 +95,27 @@ def test_set_ke_reaches_captured_pcg_iterations(precision):
     assert ca == cb and abs(ca - 0.5 * c1) <= 1e-3 * c1, (c1, ca, cb)
     A.close()
     B.close()
+
+
+def test_kernel_forms_follow_ke():
+    # the built-in Ke runs the register-operand form (2); any other Ke the constant-bank form (1); both
+    # agree bit for bit with the node-centric kernel (0)
+    import algorithmengineering_altproject_b200 as t3d
+    S, N = pair((10, 20, 10))
+    assert S.info().matvec64_kernel == 2 and N.info().matvec64_kernel == 0
+    rng = np.random.default_rng(13)
+    E = rng.uniform(1e-3, 1.0, S.ne)
+    u = rng.standard_normal(S.nf)
+    Ke = S.ke()
+    A = rng.standard_normal((24, 24)) * 1e-3
+    K2 = Ke + (A + A.T)
+    for P in (S, N):
+        P.set_ke(K2)
+    assert S.info().matvec64_kernel == 1
+    np.testing.assert_array_equal(bits(S.K_times_u_finest(E, u)), bits(N.K_times_u_finest(E, u)))
+    for P in (S, N):
+        P.set_ke(Ke)
+    assert S.info().matvec64_kernel == 2
+    np.testing.assert_array_equal(bits(S.K_times_u_finest(E, u)), bits(N.K_times_u_finest(E, u)))
+    S.close()
+    N.close()
