@@ -226,7 +226,8 @@ def matvec_roofline(P, mixed, mv_ms):
     flops = 1152 * P.ne
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic_per_launch("matvec32" if mixed else "matvec64"), "peak_source": peak_kind,
-            "kernel": ("k_matvec32 (FP32 K(E)p + FP64 p.Ap)" if mixed
+            "kernel": (("k_matvec32_modal" if P.info().matvec32_modal else "k_matvec32") +
+                       " (FP32 K(E)p + FP64 p.Ap)" if mixed
                        else "k_matvec64_stream + k_dot_pcg (FP64 K(E)p, then p.Ap)"),
             "algorithmic_bytes_per_launch": alg_bytes, "flops_per_launch": flops,
             "tflops": flops / (mv_ms * 1e-3) / 1e12, "ms": mv_ms}
