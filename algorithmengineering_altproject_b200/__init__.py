@@ -93,6 +93,8 @@ _SIGS = {
     "t3d_create": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(Params), C.POINTER(_CTX)]),
     "t3d_create_problem": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(Params), C.POINTER(ProblemSpec),
                                      C.POINTER(_CTX)]),
+    "t3d_topvoxel_info": (C.c_int, [C.c_char_p, C.POINTER(C.c_int64)]),
+    "t3d_create_from_topvoxel": (C.c_int, [C.c_char_p, C.POINTER(Params), C.POINTER(_CTX)]),
     "t3d_destroy": (C.c_int, [_CTX]),
     "t3d_get_info": (C.c_int, [_CTX, C.POINTER(Info)]),
     "t3d_last_error": (C.c_char_p, []),
@@ -159,6 +161,14 @@ def _check(rc):
         raise T3DError(rc, library().t3d_last_error().decode())
 
 
+def topvoxel_info(path):
+    """Parses a TopVoxel file (no GPU needed) and returns its sizes."""
+    v = (C.c_int64 * 8)()
+    _check(library().t3d_topvoxel_info(os.fsencode(path), v))
+    keys = ("nelx", "nely", "nelz", "solid", "passive", "fixed_nodes", "loaded_nodes", "additional_load_cases")
+    return dict(zip(keys, (int(x) for x in v)))
+
+
 def default_params(**kw):
     p = Params()
     _check(library().t3d_params_default(C.byref(p)))
@@ -193,6 +203,22 @@ class Problem:
         else:
             _check(self._lib.t3d_create_problem(nely, nelx, nelz, C.byref(self.params), C.byref(problem),
                                                 C.byref(h)))
+        self._attach(h)
+
+    @classmethod
+    def from_topvoxel(cls, path, **params):
+        """An external design domain from a TopVoxel file (the MATLAB original's CreateVoxelFEAmodel,
+        TOP3D_XL.m:458-586): its solid voxels, passive elements, fixations and loads replace the built-in
+        cantilever.  Element arrays cover the solid voxels in Morton order."""
+        self = cls.__new__(cls)
+        self._lib = library()
+        self.params = default_params(**params)
+        h = _CTX()
+        _check(self._lib.t3d_create_from_topvoxel(os.fsencode(path), C.byref(self.params), C.byref(h)))
+        self._attach(h)
+        return self
+
+    def _attach(self, h):
         self._h = h
         info = Info()
         _check(self._lib.t3d_get_info(self._h, C.byref(info)))

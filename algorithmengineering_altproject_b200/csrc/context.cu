@@ -5,6 +5,7 @@
 #include "t3d_b200.h"
 #include "hex8.hpp"
 #include "kernels.hpp"
+#include "topvoxel.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -106,6 +107,7 @@ struct Context {
     double* scal = nullptr;     // [0] C, [1] Csolid, [2] objective
     bool mv64_stream = false;   // FP64 K(E)u by the element-streaming kernel (else node-centric)
     Stream64Tiling st64{};
+    std::shared_ptr<const VoxelModel> vox;   // external (TopVoxel) model, else the built-in cuboid
     bool ke_pat = false;        // Ke has the built-in coefficient pattern: its magnitudes are in Kd
     double* Kd = nullptr;       // [KE_MAX_DISTINCT]
     RedSlot slot[4]{};
@@ -320,6 +322,55 @@ static int setup_load(Context* c) {
     return launch_check("load set-up");
 }
 
+// External model (TopVoxel, TOP3D_XL.m:458-586): solid cells from the voxel list (passive elements as
+// solid = 2), fixations and loads from the node lists.  The reference's x = 0 fixation does not apply;
+// nodes touched by no solid element stay fixed, as for every model.  File coordinates (x, y, z) are the
+// reference's element / node coordinates: cell (x, ny-1-y, z), grid node (x, ny-y, z).
+static int setup_voxel_model(Context* c) {
+    const Grid& g = c->g;
+    const VoxelModel& v = *c->vox;
+    std::vector<uint8_t> cells((size_t)g.NE, 0);
+    for (int z = 0; z < v.nelz; ++z)
+        for (int x = 0; x < v.nelx; ++x)
+            for (int y = 0; y < v.nely; ++y) {
+                const uint8_t s = v.voxel[(size_t)y + (size_t)v.nely * ((size_t)x + (size_t)v.nelx * z)];
+                if (s) cells[(size_t)g.cell(x, g.ny - 1 - y, z)] = s;
+            }
+    auto grid_node = [&](int64_t m) {
+        const int64_t py = v.nely + 1, px = v.nelx + 1;
+        const int y = (int)(m % py), x = (int)((m / py) % px), z = (int)(m / (py * px));
+        return (int32_t)g.node(x, g.ny - y, z);
+    };
+    const int nf = (int)v.fix_node.size(), nl = (int)v.load_node.size();
+    std::vector<int32_t> nodes((size_t)nf + nl);
+    for (int i = 0; i < nf; ++i) nodes[i] = grid_node(v.fix_node[i]);
+    for (int i = 0; i < nl; ++i) nodes[nf + i] = grid_node(v.load_node[i]);
+    int32_t* d_nodes = nullptr;
+    uint8_t* d_bits = nullptr;
+    double* d_f = nullptr;
+    cudaError_t e = cudaMalloc(&d_nodes, (nodes.size() + 1) * sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&d_bits, (size_t)nf + 1);
+    if (e == cudaSuccess) e = cudaMalloc(&d_f, (3 * (size_t)nl + 1) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(c->solid, cells.data(), cells.size(), cudaMemcpyHostToDevice, c->st);
+    if (e == cudaSuccess && !nodes.empty())
+        e = cudaMemcpyAsync(d_nodes, nodes.data(), nodes.size() * sizeof(int32_t), cudaMemcpyHostToDevice, c->st);
+    if (e == cudaSuccess && nf) e = cudaMemcpyAsync(d_bits, v.fix_bits.data(), nf, cudaMemcpyHostToDevice, c->st);
+    if (e == cudaSuccess && nl)
+        e = cudaMemcpyAsync(d_f, v.load_f.data(), 3 * (size_t)nl * sizeof(double), cudaMemcpyHostToDevice, c->st);
+    if (e == cudaSuccess) {
+        launch_setup_mask0(g, c->solid, 0, c->mask0, c->st);
+        launch_setup_fix_list(nf, d_nodes, d_bits, c->mask0, c->st);
+        launch_setup_load_list(g, nl, d_nodes + nf, d_f, c->mask0, c->b, c->st);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);   // the host vectors and temporaries end here
+    cudaFree(d_nodes);
+    cudaFree(d_bits);
+    cudaFree(d_f);
+    if (e != cudaSuccess) return set_cuda_error(e, "external model set-up", __FILE__, __LINE__);
+    return T3D_OK;
+}
+
 static int create(int nely, int nelx, int nelz, const t3d_params* prm, const t3d_problem* pb, Context* c) {
     if (nely <= 0 || nelx <= 0 || nelz <= 0) return set_error(T3D_ERR_INVALID, "element counts must be positive");
     if (pb) {
@@ -376,6 +427,7 @@ static int create(int nely, int nelx, int nelz, const t3d_params* prm, const t3d
         if (ne == 0) return set_error(T3D_ERR_INVALID, "the voids remove every element");
         c->ne = ne;
     }
+    if (c->vox) c->ne = c->vox->num_solid;
     const Grid& g = c->g;
     c->mv64_stream = c->prm.matvec64_form == T3D_MATVEC64_AUTO;
     if (c->mv64_stream) CHECK(stream64_tiling(g, c->dev, &c->st64));
@@ -432,10 +484,14 @@ static int create(int nely, int nelx, int nelz, const t3d_params* prm, const t3d
     T3D_CUDA_OK(cudaMemsetAsync(c->scal, 0, 8 * sizeof(double), c->st));
 
     // model: solid cells, fixed DOFs, load (fea.cpp:181-447)
-    launch_setup_cells(g, c->cub, c->voids, c->solid, c->st);
-    launch_setup_mask0(g, c->solid, c->mask0, c->st);
-    CHECK(launch_check("model set-up"));
-    CHECK(setup_load(c));
+    if (c->vox) {
+        CHECK(setup_voxel_model(c));
+    } else {
+        launch_setup_cells(g, c->cub, c->voids, c->solid, c->st);
+        launch_setup_mask0(g, c->solid, 1, c->mask0, c->st);
+        CHECK(launch_check("model set-up"));
+        CHECK(setup_load(c));
+    }
     CHECK(build_levels(c));
     if (c->mixed) CHECK(build_mixed(c));
     launch_filter_diag(g, c->solid, c->kf, c->fdiag, c->st);
@@ -450,7 +506,9 @@ static void morton_walk(const Context* c, int x0, int y0, int z0, int h, std::ve
     const Cuboid& q = c->cub;
     if (x0 >= q.nelx || y0 >= q.nely || z0 >= q.nelz) return;
     if (h == 1) {
-        if (!in_void(c->voids, x0, y0, z0)) out.push_back((int32_t)c->g.cell(x0, c->g.ny - 1 - y0, z0));
+        const bool solid = c->vox ? c->vox->voxel[(size_t)y0 + (size_t)q.nely * ((size_t)x0 + (size_t)q.nelx * z0)] != 0
+                                  : !in_void(c->voids, x0, y0, z0);
+        if (solid) out.push_back((int32_t)c->g.cell(x0, c->g.ny - 1 - y0, z0));
         return;
     }
     const int m = h / 2;
@@ -948,6 +1006,41 @@ int t3d_create_problem(int nely, int nelx, int nelz, const t3d_params* p, const 
     return T3D_OK;
 }
 
+int t3d_topvoxel_info(const char* path, int64_t* info) {
+    if (!path || !info) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    t3d::VoxelModel m;
+    std::string err;
+    if (!t3d::parse_topvoxel(path, &m, &err)) return t3d::set_error(T3D_ERR_INVALID, err);
+    const int64_t v[8] = {m.nelx, m.nely, m.nelz, m.num_solid, m.num_passive, (int64_t)m.fix_node.size(),
+                          (int64_t)m.load_node.size(), m.num_additional_loads};
+    std::memcpy(info, v, sizeof v);
+    return T3D_OK;
+}
+
+int t3d_create_from_topvoxel(const char* path, const t3d_params* p, t3d_context** out) {
+    if (!out || !path) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    *out = nullptr;
+    auto m = std::make_shared<t3d::VoxelModel>();
+    std::string err;
+    if (!t3d::parse_topvoxel(path, m.get(), &err)) return t3d::set_error(T3D_ERR_INVALID, err);
+    if (m->fix_node.empty())
+        return t3d::set_error(T3D_ERR_INVALID, "TopVoxel file fixes no DOF: the stiffness would be singular");
+    if (m->load_node.empty()) return t3d::set_error(T3D_ERR_INVALID, "TopVoxel file has no loads");
+    if (m->num_additional_loads > 0)
+        return t3d::set_error(T3D_ERR_UNSUPPORTED, "TopVoxel file has additional load cases; the design loop "
+                                                   "optimises a single load case");
+    t3d_context* c = new (std::nothrow) t3d_context();
+    if (!c) return t3d::set_error(T3D_ERR_OOM, "host allocation failed");
+    c->vox = m;
+    int rc = t3d::create(m->nely, m->nelx, m->nelz, p, nullptr, c);
+    if (rc != T3D_OK) {
+        delete c;
+        return rc;
+    }
+    *out = c;
+    return T3D_OK;
+}
+
 int t3d_create(int nely, int nelx, int nelz, const t3d_params* p, t3d_context** out) {
     if (!out) return t3d::set_error(T3D_ERR_INVALID, "null output pointer");
     *out = nullptr;
@@ -977,8 +1070,8 @@ int t3d_get_info(const t3d_context* ctx, t3d_info* info) {
     info->orig[0] = ctx->cub.nelx; info->orig[1] = ctx->cub.nely; info->orig[2] = ctx->cub.nelz;
     info->num_elements = ctx->ne;
     info->num_nodes = ctx->g.NN;
-    // free DOFs: nodes used by a solid element and not on the x=0 face
-    if (ctx->voids.n == 0) {
+    // free DOFs: nodes used by a solid element and not on the x=0 face (the built-in cuboid), else counted
+    if (ctx->voids.n == 0 && !ctx->vox) {
         const int64_t ux = ctx->cub.nelx + 1, uy = ctx->cub.nely + 1, uz = ctx->cub.nelz + 1;
         info->num_free = 3 * (ux - 1) * uy * uz;
     } else {

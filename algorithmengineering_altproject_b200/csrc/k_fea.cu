@@ -28,8 +28,9 @@ __global__ void k_setup_cells(Grid g, Cuboid c, VoidSet v, uint8_t* solid) {
     solid[i] = s;
 }
 
-// fixed = x=0 face (fea.cpp:374-385) or node touched by no solid element (fea.cpp:406-417)
-__global__ void k_setup_mask0(Grid g, const uint8_t* __restrict__ solid, uint8_t* __restrict__ mask) {
+// fixed = x=0 face (fea.cpp:374-385; fix_x0 = 0 for external models, whose fixations come from a list)
+// or node touched by no solid element (fea.cpp:406-417)
+__global__ void k_setup_mask0(Grid g, const uint8_t* __restrict__ solid, int fix_x0, uint8_t* __restrict__ mask) {
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= g.NN) return;
     int ix, iy, iz;
@@ -38,7 +39,24 @@ __global__ void k_setup_mask0(Grid g, const uint8_t* __restrict__ solid, uint8_t
     for (int dz = -1; dz <= 0; ++dz)
         for (int dy = -1; dy <= 0; ++dy)
             for (int dx = -1; dx <= 0; ++dx) used |= solid[g.cell(ix + dx, iy + dy, iz + dz)];
-    mask[n] = (ix == 0 || !used) ? 7 : 0;
+    mask[n] = ((fix_x0 && ix == 0) || !used) ? 7 : 0;
+}
+
+// listed fixations of an external model (TOP3D_XL.m:529-534): OR the DOF bits into distinct nodes
+__global__ void k_setup_fix_list(int n, const int32_t* __restrict__ node, const uint8_t* __restrict__ bits,
+                                 uint8_t* __restrict__ mask) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) mask[node[i]] |= bits[i];
+}
+
+// listed loads of an external model (TOP3D_XL.m:536-545) on distinct nodes, dropped on fixed DOFs
+__global__ void k_setup_load_list(Grid g, int n, const int32_t* __restrict__ node, const double* __restrict__ f,
+                                  const uint8_t* __restrict__ mask, double* __restrict__ b) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t m = node[i];
+    for (int c = 0; c < 3; ++c)
+        if (!((mask[m] >> c) & 1)) b[c * g.NN + m] = f[3 * i + c];
 }
 
 // -Z load slab on ix = ix_load, iz <= iz_max, all iy (fea.cpp:388-403), dropped on fixed DOFs
@@ -324,8 +342,15 @@ void launch_setup_box_load(const Grid& g, int x0, int x1, int y0, int y1, int z0
     const int n = (x1 - x0 + 1) * (y1 - y0 + 1) * (z1 - z0 + 1);
     k_setup_box_load<<<blocks_for(n, 256), 256, 0, s>>>(g, x0, x1, y0, y1, z0, z1, comp, f, mask, b);
 }
-void launch_setup_mask0(const Grid& g, const uint8_t* solid, uint8_t* mask, cudaStream_t s) {
-    k_setup_mask0<<<blocks_for(g.NN, 256), 256, 0, s>>>(g, solid, mask);
+void launch_setup_mask0(const Grid& g, const uint8_t* solid, int fix_x0, uint8_t* mask, cudaStream_t s) {
+    k_setup_mask0<<<blocks_for(g.NN, 256), 256, 0, s>>>(g, solid, fix_x0, mask);
+}
+void launch_setup_fix_list(int n, const int32_t* node, const uint8_t* bits, uint8_t* mask, cudaStream_t s) {
+    if (n > 0) k_setup_fix_list<<<blocks_for(n, 256), 256, 0, s>>>(n, node, bits, mask);
+}
+void launch_setup_load_list(const Grid& g, int n, const int32_t* node, const double* f, const uint8_t* mask, double* b,
+                            cudaStream_t s) {
+    if (n > 0) k_setup_load_list<<<blocks_for(n, 256), 256, 0, s>>>(g, n, node, f, mask, b);
 }
 void launch_setup_load(const Grid& g, int ix_load, int iz_max, double fz, const uint8_t* mask, double* b,
                        cudaStream_t s) {

@@ -65,8 +65,10 @@ __global__ void __launch_bounds__(RED_THREADS) k_oc_pass(Grid g, const uint8_t* 
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < ncell; k += gridDim.x * blockDim.x) {
         const int cx = k % g.nx, cy = (k / g.nx) % g.ny, cz = k / (g.nx * g.ny);
         const int64_t ci = g.cell(cx, cy, cz);
-        if (!solid[ci]) continue;
-        const float xn = oc_candidate(x[ci], dc[ci], rl);
+        const uint8_t sc = solid[ci];
+        if (!sc) continue;
+        // passive solid elements of an external model (solid = 2) stay at 1 (TOP3D_XL.m:152,166)
+        const float xn = sc == 2 ? 1.0f : oc_candidate(x[ci], dc[ci], rl);
         xnew[ci] = xn;
         part = part + (double)xn;
     }

@@ -51,7 +51,12 @@ struct MgLevel32 {       // FP32 copy of a level's vectors for the mixed-precisi
 
 // ---- model set-up (fea.cpp:181-447)
 void launch_setup_cells(const Grid& g, Cuboid c, const VoidSet& v, uint8_t* solid, cudaStream_t s);
-void launch_setup_mask0(const Grid& g, const uint8_t* solid, uint8_t* mask, cudaStream_t s);
+// fix_x0: the reference's x = 0 face fixation (0 for external models with listed fixations)
+void launch_setup_mask0(const Grid& g, const uint8_t* solid, int fix_x0, uint8_t* mask, cudaStream_t s);
+// listed fixations / loads on distinct grid nodes (external models); loads are dropped on fixed DOFs
+void launch_setup_fix_list(int n, const int32_t* node, const uint8_t* bits, uint8_t* mask, cudaStream_t s);
+void launch_setup_load_list(const Grid& g, int n, const int32_t* node, const double* f, const uint8_t* mask, double* b,
+                            cudaStream_t s);
 void launch_setup_load(const Grid& g, int ix_load, int iz_max, double fz, const uint8_t* mask, double* b,
                        cudaStream_t s);
 // force f (component comp) on every free DOF of the node box [x0,x1]x[y0,y1]x[z0,z1] (grid coordinates)

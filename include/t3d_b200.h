@@ -123,6 +123,15 @@ int  t3d_create(int nely, int nelx, int nelz, const t3d_params* p, struct t3d_co
  * (non-void) elements, in the reference's Morton order of those elements */
 int  t3d_create_problem(int nely, int nelx, int nelz, const t3d_params* p, const t3d_problem* problem,
                         struct t3d_context** out);
+/* External design domains in the MATLAB original's TopVoxel format, version 1.0 (CreateVoxelFEAmodel,
+ * TOP3D_XL.m:458-586): solid voxels, passive elements (kept at density 1 by the OC update,
+ * TOP3D_XL.m:152,166), per-node DOF fixations and per-node loads; the reference's built-in x = 0
+ * fixation and tip load are not applied.  Element arrays cover the solid voxels in the reference's Morton
+ * order.  Files with additional load cases are refused (T3D_ERR_UNSUPPORTED): the design loop optimises
+ * one load case.  t3d_topvoxel_info parses only (no device needed): info[8] = nelx, nely, nelz, solid
+ * voxels, passive elements, fixed nodes, loaded nodes, additional load cases. */
+int  t3d_topvoxel_info(const char* path, int64_t* info8);
+int  t3d_create_from_topvoxel(const char* path, const t3d_params* p, struct t3d_context** out);
 int  t3d_destroy(struct t3d_context* ctx);
 int  t3d_get_info(const struct t3d_context* ctx, t3d_info* info);
 const char* t3d_last_error(void);

@@ -1,0 +1,71 @@
+"""TopVoxel reader (the MATLAB original's CreateVoxelFEAmodel, TOP3D_XL.m:458-586), parse only, on CPU.
+
+Files are written with `algorithmengineering_altproject_b200.topvoxel`; `t3d_topvoxel_info` parses them
+without a device.  Checked: the sizes it reports (solid voxels, passive elements, fixed and loaded nodes
+after dropping all-zero fixation rows and duplicate nodes, as MATLAB's unique() does), the optional
+density column, and that every malformed file is an error with a message, never a crash.
+"""
+import pytest
+
+import algorithmengineering_altproject_b200 as t3d
+from algorithmengineering_altproject_b200.topvoxel import cantilever_topvoxel, write_topvoxel
+
+
+def test_cantilever_file_sizes(tmp_path):
+    p = str(tmp_path / "cantilever.TopVoxel")
+    cantilever_topvoxel(p, 6, 12, 6, (16, 8, 8))
+    info = t3d.topvoxel_info(p)
+    assert info == {"nelx": 12, "nely": 6, "nelz": 6, "solid": 432, "passive": 0, "fixed_nodes": 49,
+                    "loaded_nodes": 14, "additional_load_cases": 0}
+
+
+def test_duplicates_zero_rows_passive_and_extra_cases(tmp_path):
+    p = str(tmp_path / "l.TopVoxel")
+    solid = [(x, y, z) for z in range(3) for x in range(4) for y in range(2) if not (x >= 2 and z >= 1)]
+    fix = [(0, 0, 0, 1, 1, 1), (0, 0, 0, 0, 0, 1), (0, 1, 0, 0, 0, 0), (0, 2, 1, 1, 0, 0)]
+    loads = [(4, 0, 0, 0.0, 0.0, -1.0), (4, 0, 0, 5.0, 5.0, 5.0), (4, 2, 0, 0.0, 0.0, -1.0)]
+    write_topvoxel(p, 4, 2, 3, solid, passive=[(0, 0, 0), (1, 1, 2)], fixations=fix, loads=loads,
+                   extra_load_cases=[[(4, 1, 1, 1.0, 0.0, 0.0)]])
+    info = t3d.topvoxel_info(p)
+    assert info["solid"] == len(solid) and info["passive"] == 2
+    assert info["fixed_nodes"] == 2            # duplicate keeps its first row; the all-zero row fixes nothing
+    assert info["loaded_nodes"] == 2
+    assert info["additional_load_cases"] == 1
+
+
+def test_density_column_is_read(tmp_path):
+    p = tmp_path / "d.TopVoxel"
+    p.write_text("# TopVoxel design domain\nVersion: 1.0\nResolution: 2 2 2\nDensity values: 1\n"
+                 "Solid voxels: 2\n1 0.5\n8 1e-3\nPassive elements: 0\nFixations: 1\n1 1 1 1\n"
+                 "Loads: 1\n27 0 0 -1\nAdditional loads: 0\n")
+    assert t3d.topvoxel_info(str(p))["solid"] == 2
+
+
+GOOD = ("# TopVoxel design domain\nVersion: 1.0\nResolution: 2 2 2\nDensity values: 0\nSolid voxels: 2\n1\n8\n"
+        "Passive elements: 1\n8\nFixations: 1\n1 1 1 1\nLoads: 1\n27 0 0 -1\nAdditional loads: 0\n")
+
+
+@pytest.mark.parametrize("bad, fragment", [
+    (GOOD.replace("Version: 1.0", "Version: 2.0"), "version"),
+    (GOOD.replace("Resolution:", "Res:"), "Resolution:"),
+    (GOOD.replace("Resolution: 2 2 2", "Resolution: 2 0 2"), "resolution"),
+    (GOOD.replace("Solid voxels: 2\n1\n8", "Solid voxels: 2\n1\n9"), "voxel index"),
+    (GOOD.replace("Passive elements: 1\n8", "Passive elements: 1\n2"), "not a solid voxel"),
+    (GOOD.replace("Passive elements", "Active elements"), "Passive"),
+    (GOOD.replace("Fixations: 1\n1 1 1 1", "Fixations: 1\n28 1 1 1"), "node index"),
+    (GOOD.replace("27 0 0 -1", "27 0 x -1"), "bad number"),
+    (GOOD.replace("Loads: 1", "Loads: -1"), "negative"),
+    (GOOD[: GOOD.index("Loads:")], "end of file"),
+])
+def test_malformed_files_are_errors(tmp_path, bad, fragment):
+    p = tmp_path / "bad.TopVoxel"
+    p.write_text(bad)
+    with pytest.raises(t3d.T3DError) as e:
+        t3d.topvoxel_info(str(p))
+    assert e.value.code == t3d.T3D_ERR_INVALID and fragment in str(e.value), str(e.value)
+
+
+def test_missing_file_is_an_error(tmp_path):
+    with pytest.raises(t3d.T3DError) as e:
+        t3d.topvoxel_info(str(tmp_path / "absent.TopVoxel"))
+    assert e.value.code == t3d.T3D_ERR_INVALID and "cannot open" in str(e.value)
