@@ -108,6 +108,9 @@ struct Context {
     bool mv64_stream = false;   // FP64 K(E)u by the element-streaming kernel (else node-centric)
     Stream64Tiling st64{};
     std::shared_ptr<const VoxelModel> vox;   // external (TopVoxel) model, else the built-in cuboid
+    // several load cases (external models): per-case loads and warm starts, weighted element compliance
+    int ncases = 1;
+    double *b_cases = nullptr, *u_cases = nullptr, *ce_acc = nullptr, *one = nullptr;
     bool ke_pat = false;        // Ke has the built-in coefficient pattern: its magnitudes are in Kd
     double* Kd = nullptr;       // [KE_MAX_DISTINCT]
     RedSlot slot[4]{};
@@ -341,27 +344,43 @@ static int setup_voxel_model(Context* c) {
         const int y = (int)(m % py), x = (int)((m / py) % px), z = (int)(m / (py * px));
         return (int32_t)g.node(x, g.ny - y, z);
     };
-    const int nf = (int)v.fix_node.size(), nl = (int)v.load_node.size();
-    std::vector<int32_t> nodes((size_t)nf + nl);
-    for (int i = 0; i < nf; ++i) nodes[i] = grid_node(v.fix_node[i]);
-    for (int i = 0; i < nl; ++i) nodes[nf + i] = grid_node(v.load_node[i]);
+    // fixation nodes, then the loaded nodes of case 0, 1, ... ; forces of all cases in the same order
+    const int nf = (int)v.fix_node.size();
+    std::vector<int32_t> nodes;
+    std::vector<double> forces;
+    std::vector<int> case_off{nf}, case_n;
+    for (int i = 0; i < nf; ++i) nodes.push_back(grid_node(v.fix_node[i]));
+    for (int k = 0; k < c->ncases; ++k) {
+        const std::vector<int64_t>& ln = k ? v.case_node[k - 1] : v.load_node;
+        const std::vector<double>& lf = k ? v.case_f[k - 1] : v.load_f;
+        for (int64_t m : ln) nodes.push_back(grid_node(m));
+        forces.insert(forces.end(), lf.begin(), lf.end());
+        case_n.push_back((int)ln.size());
+        case_off.push_back(case_off.back() + (int)ln.size());
+    }
     int32_t* d_nodes = nullptr;
     uint8_t* d_bits = nullptr;
     double* d_f = nullptr;
     cudaError_t e = cudaMalloc(&d_nodes, (nodes.size() + 1) * sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMalloc(&d_bits, (size_t)nf + 1);
-    if (e == cudaSuccess) e = cudaMalloc(&d_f, (3 * (size_t)nl + 1) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_f, (forces.size() + 1) * sizeof(double));
     if (e == cudaSuccess) e = cudaMemcpyAsync(c->solid, cells.data(), cells.size(), cudaMemcpyHostToDevice, c->st);
     if (e == cudaSuccess && !nodes.empty())
         e = cudaMemcpyAsync(d_nodes, nodes.data(), nodes.size() * sizeof(int32_t), cudaMemcpyHostToDevice, c->st);
     if (e == cudaSuccess && nf) e = cudaMemcpyAsync(d_bits, v.fix_bits.data(), nf, cudaMemcpyHostToDevice, c->st);
-    if (e == cudaSuccess && nl)
-        e = cudaMemcpyAsync(d_f, v.load_f.data(), 3 * (size_t)nl * sizeof(double), cudaMemcpyHostToDevice, c->st);
+    if (e == cudaSuccess && !forces.empty())
+        e = cudaMemcpyAsync(d_f, forces.data(), forces.size() * sizeof(double), cudaMemcpyHostToDevice, c->st);
     if (e == cudaSuccess) {
         launch_setup_mask0(g, c->solid, 0, c->mask0, c->st);
         launch_setup_fix_list(nf, d_nodes, d_bits, c->mask0, c->st);
-        launch_setup_load_list(g, nl, d_nodes + nf, d_f, c->mask0, c->b, c->st);
-        e = cudaGetLastError();
+        const int64_t n3 = 3 * g.NN;
+        for (int k = 0; k < c->ncases; ++k) {   // case 0 into b, and every case into its slot of b_cases
+            double* bk = c->ncases > 1 ? c->b_cases + k * n3 : c->b;
+            launch_setup_load_list(g, case_n[k], d_nodes + case_off[k], d_f + 3 * (size_t)(case_off[k] - nf),
+                                   c->mask0, bk, c->st);
+        }
+        if (c->ncases > 1) e = cudaMemcpyAsync(c->b, c->b_cases, n3 * sizeof(double), cudaMemcpyDeviceToDevice, c->st);
+        if (e == cudaSuccess) e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);   // the host vectors and temporaries end here
     cudaFree(d_nodes);
@@ -447,6 +466,17 @@ static int create(int nely, int nelx, int nelz, const t3d_params* prm, const t3d
     for (double** v : {&c->b, &c->u, &c->r, &c->z, &c->p, &c->Ap}) CHECK(c->alloc(v, 3 * g.NN));
     for (double** v : {&c->frhs, &c->fx, &c->fr, &c->fz, &c->fp, &c->fAp, &c->flastx, &c->flastrhs, &c->fdiag})
         CHECK(c->alloc(v, g.NN));
+    if (c->vox && c->vox->num_additional_loads > 0) {
+        c->ncases = 1 + c->vox->num_additional_loads;
+        CHECK(c->alloc(&c->b_cases, (size_t)c->ncases * 3 * g.NN));
+        CHECK(c->alloc(&c->u_cases, (size_t)c->ncases * 3 * g.NN));
+        CHECK(c->alloc(&c->ce_acc, g.NE));
+        CHECK(c->alloc(&c->one, 1));
+        const double one = 1.0;
+        T3D_CUDA_OK(cudaMemcpy(c->one, &one, sizeof one, cudaMemcpyHostToDevice));
+        T3D_CUDA_OK(cudaMemsetAsync(c->b_cases, 0, (size_t)c->ncases * 3 * g.NN * sizeof(double), c->st));
+        T3D_CUDA_OK(cudaMemsetAsync(c->u_cases, 0, (size_t)c->ncases * 3 * g.NN * sizeof(double), c->st));
+    }
     CHECK(c->alloc(&c->S, 1));
     CHECK(c->alloc(&c->FS, 1));
     CHECK(c->alloc(&c->OC, 1));
@@ -893,6 +923,41 @@ static int fill_cells(Context* c, float v) {
     return upload_cells_f32(c, h.data(), c->x);
 }
 
+// Solves every load case on c->E and leaves the element compliance in c->ce and its E-weighted sum in
+// *C.  Several cases (external models): each is solved from its own previous displacement, and
+// ce = sum_k ce_k / K (TOP3D_XL.m:105,125,605-621); c->b and c->u are left holding case 0.
+static int solve_all(Context* c, double tol, int maxit, int* iters, double* C) {
+    const Grid& g = c->g;
+    if (c->ncases == 1) {
+        CHECK(solve(c, tol, maxit, iters));
+        launch_compliance64(g, c->Ke, c->E, c->u, c->ce, c->slot[0], C, c->st);
+        c->launches += 1;
+        return T3D_OK;
+    }
+    const int64_t n3 = 3 * g.NN;
+    const size_t bytes = n3 * sizeof(double);
+    const double w = 1.0 / c->ncases;
+    int total = 0;
+    for (int k = 0; k < c->ncases; ++k) {
+        T3D_CUDA_OK(cudaMemcpyAsync(c->b, c->b_cases + k * n3, bytes, cudaMemcpyDeviceToDevice, c->st));
+        T3D_CUDA_OK(cudaMemcpyAsync(c->u, c->u_cases + k * n3, bytes, cudaMemcpyDeviceToDevice, c->st));
+        int its = 0;
+        CHECK(solve(c, tol, maxit, &its));
+        total += its;
+        T3D_CUDA_OK(cudaMemcpyAsync(c->u_cases + k * n3, c->u, bytes, cudaMemcpyDeviceToDevice, c->st));
+        launch_compliance64(g, c->Ke, c->E, c->u, c->ce, c->slot[0], c->scal + 3, c->st);
+        launch_cells_axpy(g.NE, k == 0, w, c->ce, c->ce_acc, c->st);
+        c->launches += 2;
+    }
+    T3D_CUDA_OK(cudaMemcpyAsync(c->ce, c->ce_acc, g.NE * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+    launch_objective(g, c->E, c->ce, c->one, c->slot[0], C, c->st);   // sum E ce
+    T3D_CUDA_OK(cudaMemcpyAsync(c->b, c->b_cases, bytes, cudaMemcpyDeviceToDevice, c->st));
+    T3D_CUDA_OK(cudaMemcpyAsync(c->u, c->u_cases, bytes, cudaMemcpyDeviceToDevice, c->st));
+    c->launches += 1;
+    *iters = total;
+    return launch_check("load cases");
+}
+
 static int design_init(Context* c, float V0, double* Csolid) {
     CHECK(ensure_morton(c));
     c->V0 = V0;
@@ -903,12 +968,13 @@ static int design_init(Context* c, float V0, double* Csolid) {
         CHECK(upload_cells_f64(c, e.data(), c->E));
     }
     T3D_CUDA_OK(cudaMemsetAsync(c->u, 0, 3 * c->g.NN * sizeof(double), c->st));
+    if (c->ncases > 1)
+        T3D_CUDA_OK(cudaMemsetAsync(c->u_cases, 0, (size_t)c->ncases * 3 * c->g.NN * sizeof(double), c->st));
     T3D_CUDA_OK(cudaMemsetAsync(c->flastx, 0, c->g.NN * sizeof(double), c->st));
     T3D_CUDA_OK(cudaMemsetAsync(c->flastrhs, 0, c->g.NN * sizeof(double), c->st));
     CHECK(mg_setup(c));
     int its = 0;
-    CHECK(solve(c, (double)c->prm.cg_tol, c->prm.cg_max_it, &its));
-    launch_compliance64(c->g, c->Ke, c->E, c->u, c->ce, c->slot[0], c->scal + 1, c->st);
+    CHECK(solve_all(c, (double)c->prm.cg_tol, c->prm.cg_max_it, &its, c->scal + 1));
     CHECK(launch_check("solid compliance"));
     T3D_CUDA_OK(cudaMemcpyAsync(c->scal_h, c->scal, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
     CHECK(sync(c));
@@ -925,12 +991,11 @@ static int design_step(Context* c, t3d_iter_record* rec) {
     cudaEvent_t e0 = c->ev[2], e1 = c->ev[3], e2 = c->ev[4], e3 = c->ev[5], e4 = c->ev[6];
     T3D_CUDA_OK(cudaEventRecord(e0, c->st));
     launch_simp(g, c->solid, c->x, P.E0, P.Emin, P.penal, c->E, c->st);
-    c->launches += 5;   // simp, compliance, objective, sensitivities, dc scale
+    c->launches += 4;   // simp, objective, sensitivities, dc scale
     if (c->loop == 1 || c->loop % 5 == 0) CHECK(mg_setup(c));
     int its = 0;
-    CHECK(solve(c, (double)P.cg_tol, P.cg_max_it, &its));
+    CHECK(solve_all(c, (double)P.cg_tol, P.cg_max_it, &its, c->scal + 0));
     T3D_CUDA_OK(cudaEventRecord(e1, c->st));
-    launch_compliance64(g, c->Ke, c->E, c->u, c->ce, c->slot[0], c->scal + 0, c->st);
     launch_objective(g, c->E, c->ce, c->scal + 1, c->slot[1], c->scal + 2, c->st);
     launch_sens(g, c->solid, c->x, c->ce, c->scal + 1, P.E0, P.Emin, P.penal, c->dc, c->xdc, c->st);
     CHECK(launch_check("sensitivities"));
@@ -1026,9 +1091,6 @@ int t3d_create_from_topvoxel(const char* path, const t3d_params* p, t3d_context*
     if (m->fix_node.empty())
         return t3d::set_error(T3D_ERR_INVALID, "TopVoxel file fixes no DOF: the stiffness would be singular");
     if (m->load_node.empty()) return t3d::set_error(T3D_ERR_INVALID, "TopVoxel file has no loads");
-    if (m->num_additional_loads > 0)
-        return t3d::set_error(T3D_ERR_UNSUPPORTED, "TopVoxel file has additional load cases; the design loop "
-                                                   "optimises a single load case");
     t3d_context* c = new (std::nothrow) t3d_context();
     if (!c) return t3d::set_error(T3D_ERR_OOM, "host allocation failed");
     c->vox = m;

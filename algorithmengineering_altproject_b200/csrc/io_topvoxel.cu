@@ -183,14 +183,25 @@ bool parse_topvoxel(const char* path, VoxelModel* out, std::string* err) {
     if (!read_node_rows(rd, nload, nn, "loads", &load, false)) return done(false);
     if (!rd.skip(2, "additional-loads words") || !rd.integer(&nadd, "additional load case count")) return done(false);
     if (nadd < 0) return done(rd.fail("negative additional load case count"));
+    if (nadd > 64) return done(rd.fail("more than 64 additional load cases"));
     m.num_additional_loads = (int)nadd;
-    for (int64_t a = 0; a < nadd; ++a) {   // read for validation; not used by the single-load design loop
+    m.case_node.resize((size_t)nadd);
+    m.case_f.resize((size_t)nadd);
+    std::vector<bool> seen((size_t)nadd, false);
+    for (int64_t a = 0; a < nadd; ++a) {   // "Loads: n idx": case idx (2..K+1) of the loadingCond_ cell array
         int64_t n, idx;
         std::map<int64_t, std::array<double, 3>> extra;
         if (!rd.expect("Loads:") || !rd.integer(&n, "load count") || !rd.integer(&idx, "load case index"))
             return done(false);
         if (n < 0) return done(rd.fail("negative load count"));
+        if (idx < 2 || idx > nadd + 1 || seen[(size_t)(idx - 2)])
+            return done(rd.fail("load case indices must be 2..K+1, each once"));
+        seen[(size_t)(idx - 2)] = true;
         if (!read_node_rows(rd, n, nn, "additional loads", &extra, false)) return done(false);
+        for (const auto& kv : extra) {
+            m.case_node[(size_t)(idx - 2)].push_back(kv.first);
+            for (int c = 0; c < 3; ++c) m.case_f[(size_t)(idx - 2)].push_back(kv.second[c]);
+        }
     }
     for (const auto& kv : fix) {
         const uint8_t bits = (uint8_t)((kv.second[0] ? 1 : 0) | (kv.second[1] ? 2 : 0) | (kv.second[2] ? 4 : 0));

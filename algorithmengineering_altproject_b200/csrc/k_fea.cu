@@ -49,6 +49,14 @@ __global__ void k_setup_fix_list(int n, const int32_t* __restrict__ node, const 
     if (i < n) mask[node[i]] |= bits[i];
 }
 
+// weighted element compliance of several load cases (TOP3D_XL.m:621): acc = w ce (first case), acc + w ce
+__global__ void k_cells_axpy(int64_t n, int first, double w, const double* __restrict__ ce, double* __restrict__ acc) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double t = w * ce[i];
+    acc[i] = first ? t : acc[i] + t;
+}
+
 // listed loads of an external model (TOP3D_XL.m:536-545) on distinct nodes, dropped on fixed DOFs
 __global__ void k_setup_load_list(Grid g, int n, const int32_t* __restrict__ node, const double* __restrict__ f,
                                   const uint8_t* __restrict__ mask, double* __restrict__ b) {
@@ -344,6 +352,9 @@ void launch_setup_box_load(const Grid& g, int x0, int x1, int y0, int y1, int z0
 }
 void launch_setup_mask0(const Grid& g, const uint8_t* solid, int fix_x0, uint8_t* mask, cudaStream_t s) {
     k_setup_mask0<<<blocks_for(g.NN, 256), 256, 0, s>>>(g, solid, fix_x0, mask);
+}
+void launch_cells_axpy(int64_t n, int first, double w, const double* ce, double* acc, cudaStream_t s) {
+    k_cells_axpy<<<blocks_for(n, 256), 256, 0, s>>>(n, first, w, ce, acc);
 }
 void launch_setup_fix_list(int n, const int32_t* node, const uint8_t* bits, uint8_t* mask, cudaStream_t s) {
     if (n > 0) k_setup_fix_list<<<blocks_for(n, 256), 256, 0, s>>>(n, node, bits, mask);

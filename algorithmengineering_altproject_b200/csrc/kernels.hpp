@@ -54,6 +54,8 @@ void launch_setup_cells(const Grid& g, Cuboid c, const VoidSet& v, uint8_t* soli
 // fix_x0: the reference's x = 0 face fixation (0 for external models with listed fixations)
 void launch_setup_mask0(const Grid& g, const uint8_t* solid, int fix_x0, uint8_t* mask, cudaStream_t s);
 // listed fixations / loads on distinct grid nodes (external models); loads are dropped on fixed DOFs
+// acc = w ce (first) or acc + w ce over n cells: the weighted compliance of several load cases
+void launch_cells_axpy(int64_t n, int first, double w, const double* ce, double* acc, cudaStream_t s);
 void launch_setup_fix_list(int n, const int32_t* node, const uint8_t* bits, uint8_t* mask, cudaStream_t s);
 void launch_setup_load_list(const Grid& g, int n, const int32_t* node, const double* f, const uint8_t* mask, double* b,
                             cudaStream_t s);

@@ -19,7 +19,10 @@ struct VoxelModel {
     std::vector<int64_t> load_node;    // loaded nodes, ascending
     std::vector<double> load_f;        // 3 per loaded node
     int64_t num_solid = 0, num_passive = 0;
-    int num_additional_loads = 0;      // load cases after the first (the design loop optimises one)
+    int num_additional_loads = 0;      // load cases after the first
+    // load cases 2.. (file indices 2..K+1, in that order): loaded nodes ascending, 3 forces per node
+    std::vector<std::vector<int64_t>> case_node;
+    std::vector<std::vector<double>> case_f;
     bool has_densities = false;        // per-voxel densities were listed (read and not used)
 };
 

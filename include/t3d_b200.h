@@ -127,9 +127,10 @@ int  t3d_create_problem(int nely, int nelx, int nelz, const t3d_params* p, const
  * TOP3D_XL.m:458-586): solid voxels, passive elements (kept at density 1 by the OC update,
  * TOP3D_XL.m:152,166), per-node DOF fixations and per-node loads; the reference's built-in x = 0
  * fixation and tip load are not applied.  Element arrays cover the solid voxels in the reference's Morton
- * order.  Files with additional load cases are refused (T3D_ERR_UNSUPPORTED): the design loop optimises
- * one load case.  t3d_topvoxel_info parses only (no device needed): info[8] = nelx, nely, nelz, solid
- * voxels, passive elements, fixed nodes, loaded nodes, additional load cases. */
+ * order.  Further load cases are solved one after the other in each design iteration and the element
+ * compliance is their mean (TOP3D_XL.m:605-621); the load and displacement the context exposes are
+ * case 1's.  t3d_topvoxel_info parses only (no device needed): info[8] = nelx, nely, nelz, solid
+ * voxels, passive elements, fixed nodes, loaded nodes (case 1), additional load cases. */
 int  t3d_topvoxel_info(const char* path, int64_t* info8);
 int  t3d_create_from_topvoxel(const char* path, const t3d_params* p, struct t3d_context** out);
 int  t3d_destroy(struct t3d_context* ctx);

@@ -7,7 +7,11 @@
   DOFs and load match a numpy restatement of the file's meaning (file node (x, y, z) is reference node
   (x, y, z); the operator is checked against the element-by-element assembly of the problem-spec tests),
   passive elements stay at density 1 after every OC update (TOP3D_XL.m:152,166) and count in the volume.
-* Files the design loop cannot run are refused: extra load cases, no fixation, no load.
+* Several load cases (TOP3D_XL.m:105,125,605-621): each solved from its own previous displacement, the
+  element compliance averaged.  Two identical cases must reproduce the single-case design bit for bit
+  (weights 1/2 are exact) with twice the PCG iterations; two different cases give the mean of the
+  single-case solid compliances.
+* Files the design loop cannot run are refused: no fixation, no load.
 """
 import numpy as np
 import pytest
@@ -113,7 +117,6 @@ def test_unrunnable_files_are_refused(tmp_path):
     from algorithmengineering_altproject_b200.topvoxel import write_topvoxel
     solid, passive, fix, loads = l_domain(8, 4, 4)
     cases = {
-        "extra": (dict(fixations=fix, loads=loads, extra_load_cases=[loads]), t3d.T3D_ERR_UNSUPPORTED, "load case"),
         "nofix": (dict(fixations=[], loads=loads), t3d.T3D_ERR_INVALID, "singular"),
         "noload": (dict(fixations=fix, loads=[]), t3d.T3D_ERR_INVALID, "no loads"),
     }
@@ -123,3 +126,38 @@ def test_unrunnable_files_are_refused(tmp_path):
         with pytest.raises(t3d.T3DError) as e:
             t3d.Problem.from_topvoxel(path)
         assert e.value.code == code and fragment in str(e.value), (name, str(e.value))
+
+
+def test_identical_load_cases_reproduce_the_single_case(tmp_path):
+    import algorithmengineering_altproject_b200 as t3d
+    from algorithmengineering_altproject_b200.topvoxel import write_topvoxel
+    solid, passive, fix, loads = l_domain(12, 6, 8)
+    one, two = str(tmp_path / "one.TopVoxel"), str(tmp_path / "two.TopVoxel")
+    write_topvoxel(one, 12, 6, 8, solid, passive=passive, fixations=fix, loads=loads)
+    write_topvoxel(two, 12, 6, 8, solid, passive=passive, fixations=fix, loads=loads, extra_load_cases=[loads])
+    assert t3d.topvoxel_info(two)["additional_load_cases"] == 1
+    kw = dict(oc_sum_order=t3d.T3D_SUM_FP64)
+    A, B = t3d.Problem.from_topvoxel(one, **kw), t3d.Problem.from_topvoxel(two, **kw)
+    assert A.design_init(0.3) == B.design_init(0.3)
+    for _ in range(2):
+        ra, rb = A.design_step(), B.design_step()
+        assert ra["obj"] == rb["obj"] and rb["pcg_iters"] == 2 * ra["pcg_iters"], (ra, rb)
+    np.testing.assert_array_equal(A.density(), B.density())
+    np.testing.assert_array_equal(bits(A.bfree()), bits(B.bfree()))   # the context's load is case 1
+    A.close()
+    B.close()
+
+
+def test_two_load_cases_average_the_compliance(tmp_path):
+    import algorithmengineering_altproject_b200 as t3d
+    from algorithmengineering_altproject_b200.topvoxel import write_topvoxel
+    nelx, nely, nelz = 12, 6, 8
+    solid, passive, fix, loads = l_domain(nelx, nely, nelz)
+    side = [(nelx, y, 2, 0.0, 1.0 / (nely + 1), 0.0) for y in range(nely + 1)]   # a lateral case
+    paths = [str(tmp_path / n) for n in ("a.TopVoxel", "b.TopVoxel", "ab.TopVoxel")]
+    write_topvoxel(paths[0], nelx, nely, nelz, solid, fixations=fix, loads=loads)
+    write_topvoxel(paths[1], nelx, nely, nelz, solid, fixations=fix, loads=side)
+    write_topvoxel(paths[2], nelx, nely, nelz, solid, fixations=fix, loads=loads, extra_load_cases=[side])
+    kw = dict(cg_tol=1e-10, cg_max_it=5000)
+    cs = [t3d.Problem.from_topvoxel(p, **kw).design_init(0.3) for p in paths]
+    assert abs(cs[2] - 0.5 * (cs[0] + cs[1])) <= 1e-12 * cs[2], cs

@@ -3,7 +3,8 @@
 Files are written with `algorithmengineering_altproject_b200.topvoxel`; `t3d_topvoxel_info` parses them
 without a device.  Checked: the sizes it reports (solid voxels, passive elements, fixed and loaded nodes
 after dropping all-zero fixation rows and duplicate nodes, as MATLAB's unique() does), the optional
-density column, and that every malformed file is an error with a message, never a crash.
+density column, further load cases ("Loads: n idx" blocks, idx = 2..K+1), and that every malformed
+file is an error with a message, never a crash.
 """
 import pytest
 
@@ -56,6 +57,7 @@ GOOD = ("# TopVoxel design domain\nVersion: 1.0\nResolution: 2 2 2\nDensity valu
     (GOOD.replace("27 0 0 -1", "27 0 x -1"), "bad number"),
     (GOOD.replace("Loads: 1", "Loads: -1"), "negative"),
     (GOOD[: GOOD.index("Loads:")], "end of file"),
+    (GOOD.replace("Additional loads: 0", "Additional loads: 1\nLoads: 1 3\n27 0 0 -1"), "load case indices"),
 ])
 def test_malformed_files_are_errors(tmp_path, bad, fragment):
     p = tmp_path / "bad.TopVoxel"
