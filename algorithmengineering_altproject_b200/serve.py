@@ -1,7 +1,8 @@
 """Continuous-batching design server on one GPU.
 
-Requests (grid dims, volume fraction, load case, passive voids, OC iteration count) are admitted in
-arrival order as soon as a slot and the HBM budget allow: each admitted request gets its own device
+Requests (grid dims, volume fraction, load case, passive voids, OC iteration count; or a TopVoxel design
+domain, `DesignRequest.from_topvoxel`) are admitted in arrival order as soon as a slot and the HBM budget
+allow: each admitted request gets its own device
 context (model, MG hierarchy, density, warm-start displacement and filter state stay resident for all
 its OC iterations) and its own CUDA stream, and runs on a worker thread, so the kernels of all
 admitted requests overlap on the device while later arrivals wait.  The projected footprint of a
@@ -29,7 +30,8 @@ import numpy as np
 # request threads start at once, and their first launches should not race the module loader.
 os.environ.setdefault("CUDA_MODULE_LOADING", "EAGER")
 
-from . import (T3D_COARSE_FULL, T3D_FP64, T3D_MIXED, T3D_SUM_FP64, Problem, ProblemSpec, T3DError)  # noqa: E402
+from . import (T3D_COARSE_FULL, T3D_FP64, T3D_MIXED, T3D_SUM_FP64, Problem, ProblemSpec, T3DError,  # noqa: E402
+               topvoxel_info)
 
 # bytes per padded grid node of a context, before the first context of a precision is measured
 DEFAULT_BYTES_PER_NODE = {T3D_FP64: 900.0, T3D_MIXED: 1100.0}
@@ -46,6 +48,17 @@ class DesignRequest:
         self.rid = rid
         self.keep_density = keep_density
         self.arrival = None
+        self.topvoxel = None        # path of a TopVoxel design domain (replaces dims, load case and voids)
+        self.load_cases = 1
+
+    @classmethod
+    def from_topvoxel(cls, path, V0, iters=40, rid=None, keep_density=False):
+        """A request for an external design domain (TopVoxel file); its size is read without a device."""
+        info = topvoxel_info(path)
+        req = cls(info["nely"], info["nelx"], info["nelz"], V0, iters=iters, rid=rid, keep_density=keep_density)
+        req.topvoxel = str(path)
+        req.load_cases = 1 + info["additional_load_cases"]
+        return req
 
     def padded_nodes(self):
         # dims of multiples of 8 are never padded (the reference's rule pads to multiples of 2^L)
@@ -55,8 +68,11 @@ class DesignRequest:
         return ProblemSpec.make(self.load_case, self.voids)
 
     def as_dict(self):
-        return {"rid": self.rid, "dims": [self.nely, self.nelx, self.nelz], "V0": self.V0,
-                "load_case": self.load_case, "voids": len(self.voids), "iters": self.iters}
+        d = {"rid": self.rid, "dims": [self.nely, self.nelx, self.nelz], "V0": self.V0,
+             "load_case": self.load_case, "voids": len(self.voids), "iters": self.iters}
+        if self.topvoxel:
+            d.update(topvoxel=self.topvoxel, load_cases=self.load_cases)
+        return d
 
 
 class DesignResult:
@@ -115,7 +131,9 @@ class DesignServer:
         return fut
 
     def projected_bytes(self, req):
-        return MARGIN * self._bpn[self.precision] * req.padded_nodes()
+        # several load cases keep a load and a displacement (3 doubles each) per node per case
+        extra = 48.0 * req.load_cases if req.load_cases > 1 else 0.0
+        return MARGIN * (self._bpn[self.precision] + extra) * req.padded_nodes()
 
     def close(self):
         with self._cv:
@@ -170,6 +188,8 @@ class DesignServer:
             self._execute(req, res)
         except T3DError as e:
             res.error = str(e)
+        except Exception as e:   # any other failure is reported on the request, never lost in the worker
+            res.error = "%s: %s" % (type(e).__name__, e)
         finally:
             res.finished = time.perf_counter()
             with self._cv:
@@ -180,12 +200,16 @@ class DesignServer:
 
     def _execute(self, req, res):
         """Runs one request to completion on its own context (and stream)."""
+        kw = dict(device=self.device, precision=self.precision, oc_sum_order=T3D_SUM_FP64, **self.params)
         with self._create_lock:
-            P = Problem(req.nely, req.nelx, req.nelz, problem=req.spec(), device=self.device,
-                        precision=self.precision, oc_sum_order=T3D_SUM_FP64, **self.params)
+            if getattr(req, "topvoxel", None):
+                P = Problem.from_topvoxel(req.topvoxel, **kw)
+            else:
+                P = Problem(req.nely, req.nelx, req.nelz, problem=req.spec(), **kw)
         try:
-            with self._cv:   # learn the footprint per node from the real allocation
-                self._bpn[self.precision] = max(self._bpn[self.precision], P.device_bytes / P.nn)
+            with self._cv:   # learn the footprint per node from the real allocation (single-case problems)
+                if getattr(req, "load_cases", 1) == 1:
+                    self._bpn[self.precision] = max(self._bpn[self.precision], P.device_bytes / P.nn)
             res.c_solid = P.design_init(req.V0)
             for _ in range(req.iters):
                 r = P.design_step()

@@ -33,3 +33,30 @@ def test_results_alone_equal_results_in_the_mix():
         assert a.c_solid == m.c_solid
         assert a.objectives == m.objectives and a.pcg_iters == m.pcg_iters
         np.testing.assert_array_equal(a.density, m.density)
+
+
+def test_topvoxel_requests_in_the_mix(tmp_path):
+    # an external domain with two load cases served next to built-in requests: same results alone and mixed
+    from algorithmengineering_altproject_b200.serve import DesignRequest, DesignServer
+    from algorithmengineering_altproject_b200.topvoxel import write_topvoxel
+    solid = [(x, y, z) for z in range(8) for x in range(16) for y in range(8) if not (x >= 8 and z >= 4)]
+    fix = [(0, y, z, 1, 1, 1) for z in range(9) for y in range(9)]
+    down = [(16, y, 0, 0.0, 0.0, -1.0 / 9) for y in range(9)]
+    side = [(16, y, 2, 0.0, 1.0 / 9, 0.0) for y in range(9)]
+    path = str(tmp_path / "l.TopVoxel")
+    write_topvoxel(path, 16, 8, 8, solid, passive=[(15, y, 0) for y in range(8)], fixations=fix, loads=down,
+                   extra_load_cases=[side])
+
+    def reqs():
+        return [DesignRequest.from_topvoxel(path, 0.3, iters=3, rid="tv", keep_density=True)] + _requests()[:2]
+
+    with DesignServer(max_active=1) as srv:
+        alone = [srv.submit(r).result() for r in reqs()]
+    with DesignServer(max_active=3) as srv:
+        futs = [srv.submit(r) for r in reqs()]
+        mixed = [f.result() for f in futs]
+    for a, m in zip(alone, mixed):
+        assert a.error is None and m.error is None, (a.error, m.error)
+        assert a.c_solid == m.c_solid and a.objectives == m.objectives and a.pcg_iters == m.pcg_iters
+        np.testing.assert_array_equal(a.density, m.density)
+    assert len(alone[0].objectives) == 3 and all(np.isfinite(alone[0].objectives))

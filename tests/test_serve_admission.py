@@ -67,3 +67,33 @@ def test_workload_generators_follow_the_batched_distributions():
         q = serve.draw_served(rng)
         ne = q.nelx * q.nely * q.nelz
         assert 8 * 8 * 8 <= ne <= 2.2 * 16e6
+
+
+def test_topvoxel_requests_are_sized_from_the_file(tmp_path):
+    from algorithmengineering_altproject_b200.topvoxel import write_topvoxel
+    solid = [(x, y, z) for z in range(6) for x in range(10) for y in range(4)]
+    fix = [(0, y, z, 1, 1, 1) for z in range(7) for y in range(5)]
+    loads = [(10, y, 0, 0.0, 0.0, -0.2) for y in range(5)]
+    one, two = str(tmp_path / "one.TopVoxel"), str(tmp_path / "two.TopVoxel")
+    write_topvoxel(one, 10, 4, 6, solid, fixations=fix, loads=loads)
+    write_topvoxel(two, 10, 4, 6, solid, fixations=fix, loads=loads, extra_load_cases=[loads])
+    a = serve.DesignRequest.from_topvoxel(one, 0.3, rid=0)
+    b = serve.DesignRequest.from_topvoxel(two, 0.3, rid=1)
+    assert (a.nely, a.nelx, a.nelz, a.load_cases, b.load_cases) == (4, 10, 6, 1, 2)
+    assert a.as_dict()["topvoxel"] == one and b.as_dict()["load_cases"] == 2
+    srv = FakeServer(hbm_budget=1e18)
+    assert srv.projected_bytes(b) > srv.projected_bytes(a) == srv.projected_bytes(serve.DesignRequest(4, 10, 6, 0.3))
+    futs = [srv.submit(r) for r in (a, b)]
+    [f.result() for f in futs]
+    srv.close()
+    assert srv.log == [0, 1]
+
+
+def test_unexpected_failures_are_reported_on_the_request():
+    class Failing(FakeServer):
+        def _execute(self, req, res):
+            raise ValueError("boom %s" % req.rid)
+    srv = Failing(hbm_budget=1e18)
+    r = srv.submit(serve.DesignRequest(8, 16, 8, 0.1, rid=7)).result()
+    srv.close()
+    assert r.error == "ValueError: boom 7"
