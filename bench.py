@@ -233,6 +233,27 @@ def matvec_roofline(P, mixed, mv_ms):
             "tflops": flops / (mv_ms * 1e-3) / 1e12, "ms": mv_ms}
 
 
+def throughput_fractions(P, mixed, mv_ms, vc_ms, it_ms):
+    """DOF-matvecs/s, V-cycles/s and PCG iterations/s with the HBM-roofline fraction of each, from the
+    algorithmic bytes per unit: V-cycle w*4*(n + sum of the coarse levels' 3*nodes) (down: read r; up: read
+    r and D, write z), PCG iteration w*(15n + N_e) (K(E)p 2n + N_e, update 6n, V-cycle 4n, p-update 3n);
+    n = free DOFs, w = bytes per value of the inner solve."""
+    w = 4 if mixed else 8
+    peak, _ = hbm_peak()
+    coarse = sum(3 * (nx + 1) * (ny + 1) * (nz + 1) for nx, ny, nz, _ in P.levels[1:])
+    vc_bytes = w * 4 * (P.nf + coarse)
+    it_bytes = w * (15 * P.nf + P.ne)
+    out = {"dof_matvecs_per_s": P.nf / (mv_ms * 1e-3), "vcycles_per_s": 1.0 / (vc_ms * 1e-3),
+           "vcycle_bytes": vc_bytes, "vcycle_gbs": vc_bytes / (vc_ms * 1e-3) / 1e9,
+           "pcg_iteration_bytes": it_bytes}
+    out["vcycle_frac"] = out["vcycle_gbs"] / peak
+    if it_ms and it_ms > 0:
+        out["pcg_iterations_per_s"] = 1.0 / (it_ms * 1e-3)
+        out["pcg_iteration_gbs"] = it_bytes / (it_ms * 1e-3) / 1e9
+        out["pcg_iteration_frac"] = out["pcg_iteration_gbs"] / peak
+    return out
+
+
 def run_kernels_only(args):
     """K(E)p and one V-cycle timed alone with CUDA events on a design-like state (E = SIMP of V0)."""
     import algorithmengineering_altproject_b200 as t3d
@@ -347,6 +368,7 @@ def run_b200(args):
     if rank == 0:
         ne = P.ne
         pcg_its = [r["pcg_iters"] for r in recs]
+        it_ms = 1000.0 * sum(r["t_cg"] for r in recs) / max(1, sum(pcg_its))
         line = {
             "metric": METRIC, "value": job_throughput(world, args.steps, dev_time), "unit": "design iter/s",
             "n_gpus": world,
@@ -361,9 +383,8 @@ def run_b200(args):
                        "oc_volume_sum": "fp64", "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (node vectors %.0f MB each)" % (3 * P.nn * (4 if mixed else 8) / 1e6)},
             "pcg_iterations": pcg_its,
-            "per_kernel_ms": {"matvec": mv_ms, "vcycle": vc_ms,
-                              "pcg_iteration": 1000.0 * sum(r["t_cg"] for r in recs) / max(1, sum(pcg_its))},
-            "throughput": {"dof_matvecs_per_s": P.nf / (mv_ms * 1e-3), "vcycles_per_s": 1.0 / (vc_ms * 1e-3)},
+            "per_kernel_ms": {"matvec": mv_ms, "vcycle": vc_ms, "pcg_iteration": it_ms},
+            "throughput": throughput_fractions(P, mixed, mv_ms, vc_ms, it_ms),
             "roofline": matvec_roofline(P, mixed, mv_ms),
             "matvec32_tile": list(P.info().matvec32_tile) if mixed else None,
             "clocks": clk,
