@@ -19,6 +19,7 @@
 #include <fstream>
 #include <iterator>
 #include <map>
+#include <new>
 
 #include "topvoxel.hpp"
 
@@ -117,7 +118,7 @@ bool read_node_rows(Reader& rd, int64_t n, int64_t nn, const char* what, std::ma
 
 }  // namespace
 
-bool parse_topvoxel(const char* path, VoxelModel* out, std::string* err) {
+static bool parse_topvoxel_impl(const char* path, VoxelModel* out, std::string* err) {
     std::ifstream f(path, std::ios::binary);
     if (!f) {
         *err = std::string("cannot open ") + path;
@@ -137,8 +138,9 @@ bool parse_topvoxel(const char* path, VoxelModel* out, std::string* err) {
     if (!rd.expect("Resolution:") || !rd.integer(&nx, "resolution") || !rd.integer(&ny, "resolution") ||
         !rd.integer(&nz, "resolution"))
         return done(false);
+    // the grid of a context holds fewer than 2^31 / 3 nodes, so larger domains could not run anyway
     if (nx < 1 || ny < 1 || nz < 1 || nx > (1 << 20) || ny > (1 << 20) || nz > (1 << 20) ||
-        nx * ny * nz > (int64_t)1 << 33)
+        nx * ny * nz > (int64_t)1 << 30)
         return done(rd.fail("resolution out of range"));
     m.nelx = (int)nx;
     m.nely = (int)ny;
@@ -214,6 +216,15 @@ bool parse_topvoxel(const char* path, VoxelModel* out, std::string* err) {
         for (int c = 0; c < 3; ++c) m.load_f.push_back(kv.second[c]);
     }
     return done(true);
+}
+
+bool parse_topvoxel(const char* path, VoxelModel* out, std::string* err) {
+    try {
+        return parse_topvoxel_impl(path, out, err);
+    } catch (const std::bad_alloc&) {   // no exception crosses the C-ABI
+        *err = std::string("TopVoxel ") + path + ": out of host memory";
+        return false;
+    }
 }
 
 }  // namespace t3d

@@ -50,6 +50,7 @@ GOOD = ("# TopVoxel design domain\nVersion: 1.0\nResolution: 2 2 2\nDensity valu
     (GOOD.replace("Version: 1.0", "Version: 2.0"), "version"),
     (GOOD.replace("Resolution:", "Res:"), "Resolution:"),
     (GOOD.replace("Resolution: 2 2 2", "Resolution: 2 0 2"), "resolution"),
+    (GOOD.replace("Resolution: 2 2 2", "Resolution: 1048576 1048576 8"), "resolution"),
     (GOOD.replace("Solid voxels: 2\n1\n8", "Solid voxels: 2\n1\n9"), "voxel index"),
     (GOOD.replace("Passive elements: 1\n8", "Passive elements: 1\n2"), "not a solid voxel"),
     (GOOD.replace("Passive elements", "Active elements"), "Passive"),
