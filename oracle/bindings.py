@@ -150,6 +150,36 @@ class _Common:
         self._fss(self.h, np.ascontiguousarray(lastx, np.float64), np.ascontiguousarray(lastrhs, np.float64))
 
 
+def voxel_model_from_rows(nelx, nely, nelz, solid, passive=(), fixations=(), load_cases=((),)):
+    """The arrays of an external model for `Oracle(..., voxel_model=...)` from 0-based rows: solid and passive
+    voxels (x, y, z), fixations (x, y, z, fx, fy, fz) with 0/1 flags, load cases of (x, y, z, Fx, Fy, Fz).
+    As in the MATLAB reader (TOP3D_XL.m:529-545): duplicate nodes keep their first row, nodes ascending;
+    all-zero fixation rows fix nothing."""
+    vox = np.zeros(nelx * nely * nelz, dtype=np.uint8)
+    for x, y, z in solid:
+        vox[y + nely * (x + nelx * z)] = 1
+    for x, y, z in passive:
+        vox[y + nely * (x + nelx * z)] = 2
+    node = lambda x, y, z: y + (nely + 1) * (x + (nelx + 1) * z)
+    fix = {}
+    for x, y, z, fx, fy, fz in fixations:
+        fix.setdefault(node(x, y, z), (1 if fx else 0) | (2 if fy else 0) | (4 if fz else 0))
+    fix = {k: v for k, v in fix.items() if v}
+    nodes, forces, counts = [], [], []
+    for case in load_cases:
+        rows = {}
+        for x, y, z, fx, fy, fz in case:
+            rows.setdefault(node(x, y, z), (fx, fy, fz))
+        keys = sorted(rows)
+        nodes += keys
+        forces += [v for k in keys for v in rows[k]]
+        counts.append(len(keys))
+    keys = sorted(fix)
+    return {"voxel": vox, "fix_node": np.array(keys, dtype=np.int64), "fix_bits": np.array([fix[k] for k in keys],
+            dtype=np.uint8), "case_n": np.array(counts, dtype=np.int32), "load_node": np.array(nodes, dtype=np.int64),
+            "load_f": np.array(forces, dtype=np.float64)}
+
+
 class Oracle(_Common):
     """The C restatement (oracle/t3d_oracle.c)."""
 
@@ -160,6 +190,9 @@ class Oracle(_Common):
         if cls._lib is None:
             L = C.CDLL(build_oracle())
             L.orc_create.restype = C.c_void_p
+            L.orc_create_voxel.restype = C.c_void_p
+            L.orc_create_voxel.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(OrcParams), C.c_void_p, C.c_int,
+                                           C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
             L.orc_create.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(OrcParams)]
             L.orc_destroy.argtypes = [C.c_void_p]
             L.orc_params_default.argtypes = [C.POINTER(OrcParams)]
@@ -207,7 +240,8 @@ class Oracle(_Common):
         return cls._lib
 
     def __init__(self, nely, nelx, nelz, emin=None, max_levels=5, pow_mode=0, vol_mode=0, approx_mode=0, red_mode=0,
-                 penal=None, coarse_full=0):
+                 penal=None, coarse_full=0, voxel_model=None):
+        """voxel_model: an external (TopVoxel) model from `voxel_model_from_rows`, else the cantilever."""
         L = self.lib()
         p = OrcParams()
         L.orc_params_default(C.byref(p))
@@ -222,7 +256,14 @@ class Oracle(_Common):
         p.red_mode = red_mode
         p.coarse_full = coarse_full
         self.params = p
-        self.h = C.c_void_p(L.orc_create(nely, nelx, nelz, C.byref(p)))
+        if voxel_model is None:
+            self.h = C.c_void_p(L.orc_create(nely, nelx, nelz, C.byref(p)))
+        else:
+            self._vm = vm = voxel_model        # the C side keeps pointers into these arrays
+            ptr = lambda a: a.ctypes.data_as(C.c_void_p)
+            self.h = C.c_void_p(L.orc_create_voxel(nely, nelx, nelz, C.byref(p), ptr(vm["voxel"]), len(vm["fix_node"]),
+                                                   ptr(vm["fix_node"]), ptr(vm["fix_bits"]), len(vm["case_n"]),
+                                                   ptr(vm["case_n"]), ptr(vm["load_node"]), ptr(vm["load_f"])))
         self._info = L.orc_info
         self._emb, self._fd, self._bf, self._ke = L.orc_ele_map_back, L.orc_free_dofs, L.orc_bfree, L.orc_ke
         self._mv, self._mgb, self._vc, self._pcg, self._cc = (L.orc_matvec, L.orc_mg_build, L.orc_vcycle,

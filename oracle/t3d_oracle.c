@@ -48,6 +48,17 @@ struct orc_problem {
     int32_t* free_dofs;            /* [nf] */
     int32_t* dof2free;             /* [ndof] */
     double* F;                     /* [ndof] interleaved 3n+c */
+    /* external model (TopVoxel, TOP3D_XL.m:458-586); NULL voxel = the built-in cuboid */
+    const uint8_t* voxel;          /* [nelx*nely*nelz], k = y + nely*(x + nelx*z): 0 void, 1 solid, 2 passive */
+    int nfix;                      /* fixations: file nodes m = y + (nely+1)*(x + (nelx+1)*z), DOF bits */
+    const int64_t* fix_node;
+    const uint8_t* fix_bits;
+    int ncases;                    /* load cases; loads concatenated: case k has case_n[k] nodes */
+    const int* case_n;
+    const int64_t* load_node;
+    const double* load_f;          /* 3 per loaded node */
+    double* Fcases;                /* [ncases*ndof] when ncases > 1 */
+    uint8_t* passive;              /* [ne] 1 = passive element (kept at 1 by the OC update) */
     double Ke[576];
     int nlev;
     orc_level lv[8];
@@ -176,22 +187,28 @@ static int64_t node_id(const orc_problem* P, int ix, int iy, int iz) {
     return (int64_t)P->nnx * P->nny * iz + (int64_t)P->nnx * iy + ix;
 }
 
+static int voxel_of(const orc_problem* P, int ex, int ey, int ez) {   /* 1 for the built-in cuboid */
+    return P->voxel ? P->voxel[(int64_t)ey + (int64_t)P->nely * (ex + (int64_t)P->nelx * ez)] : 1;
+}
+
 static void build_mesh(orc_problem* P) {
     const int nx = P->nx, ny = P->ny;
-    P->ne = P->nelx * P->nely * P->nelz;
-    keyed* k = xcalloc((size_t)P->ne, sizeof(keyed));
+    keyed* k = xcalloc((size_t)P->nelx * P->nely * P->nelz, sizeof(keyed));
     int n = 0;
-    /* solid region: ex < nelx, ey < nely, ez < nelz (fea.cpp:204-215) */
+    /* solid region: ex < nelx, ey < nely, ez < nelz (fea.cpp:204-215), or the external model's voxels */
     for (int ez = 0; ez < P->nelz; ++ez)
         for (int ex = 0; ex < P->nelx; ++ex)
             for (int ey = 0; ey < P->nely; ++ey) {
+                if (!voxel_of(P, ex, ey, ez)) continue;
                 k[n].key = (spread_bits3((uint32_t)ex) << 2) | (spread_bits3((uint32_t)ey) << 1) |
                            spread_bits3((uint32_t)ez);
                 k[n].full = ny * nx * ez + ny * ex + (ny - 1 - ey);
                 ++n;
             }
     qsort(k, (size_t)n, sizeof(keyed), cmp_keyed);   /* keys are unique */
+    P->ne = n;
     P->ele_full = xcalloc((size_t)n, sizeof(int32_t));
+    P->passive = xcalloc((size_t)n, 1);
     P->enod = xcalloc((size_t)n * 8, sizeof(int32_t));
     uint8_t* color = xcalloc((size_t)n, 1);
     for (int e = 0; e < n; ++e) {
@@ -202,6 +219,7 @@ static void build_mesh(orc_problem* P) {
         for (int a = 0; a < 8; ++a)
             P->enod[8 * e + a] = (int32_t)node_id(P, ex + CORNER[a][0], ny - ey - 1 + CORNER[a][1], ez + CORNER[a][2]);
         color[e] = (uint8_t)((ex & 1) | ((ey & 1) << 1) | ((ez & 1) << 2));   /* fea.cpp:300 */
+        P->passive[e] = voxel_of(P, ex, ey, ez) == 2;
     }
     /* colour buckets in Morton order (fea.cpp:318-326) */
     P->bucket = xcalloc((size_t)n, sizeof(int32_t));
@@ -223,12 +241,32 @@ static void build_bcs(orc_problem* P) {
     P->isfree = xcalloc((size_t)P->ndof, 1);
     P->F = xcalloc((size_t)P->ndof, sizeof(double));
     memset(P->isfree, 1, (size_t)P->ndof);
-    for (int iz = 0; iz < P->nnz; ++iz)
-        for (int iy = 0; iy < P->nny; ++iy) {
-            const int64_t nd = node_id(P, 0, iy, iz);
-            P->isfree[3 * nd] = P->isfree[3 * nd + 1] = P->isfree[3 * nd + 2] = 0;
+    if (P->voxel) {   /* external model: listed fixations and loads; file node (x, y, z) = grid node (x, ny-y, z) */
+        const int64_t py = P->nely + 1, px = P->nelx + 1;
+#define GRID_NODE(m) node_id(P, (int)(((m) / py) % px), P->ny - (int)((m) % py), (int)((m) / (py * px)))
+        for (int i = 0; i < P->nfix; ++i) {
+            const int64_t nd = GRID_NODE(P->fix_node[i]);
+            for (int c = 0; c < 3; ++c)
+                if ((P->fix_bits[i] >> c) & 1) P->isfree[3 * nd + c] = 0;
         }
-    {
+        if (P->ncases > 1) P->Fcases = xcalloc((size_t)P->ncases * P->ndof, sizeof(double));
+        int off = 0;
+        for (int k = 0; k < P->ncases; ++k) {
+            double* Fk = P->ncases > 1 ? P->Fcases + (int64_t)k * P->ndof : P->F;
+            for (int i = off; i < off + P->case_n[k]; ++i) {
+                const int64_t nd = GRID_NODE(P->load_node[i]);
+                for (int c = 0; c < 3; ++c) Fk[3 * nd + c] = P->load_f[3 * i + c];
+            }
+            off += P->case_n[k];
+        }
+        if (P->ncases > 1) memcpy(P->F, P->Fcases, (size_t)P->ndof * sizeof(double));
+#undef GRID_NODE
+    } else {
+        for (int iz = 0; iz < P->nnz; ++iz)
+            for (int iy = 0; iy < P->nny; ++iy) {
+                const int64_t nd = node_id(P, 0, iy, iz);
+                P->isfree[3 * nd] = P->isfree[3 * nd + 1] = P->isfree[3 * nd + 2] = 0;
+            }
         const int ixl = P->nelx < P->nnx - 1 ? P->nelx : P->nnx - 1;
         const int izmax = (P->nz / 6) > 1 ? (P->nz / 6) : 1;
         const int count = (izmax + 1) * P->nny;
@@ -1353,6 +1391,7 @@ int orc_oc(const orc_problem* P, const float* x, const float* dc, float V0, floa
             xe = xe < lo ? lo : (hi < xe ? hi : xe);
             xe = xe < 0.0f ? 0.0f : (1.0f < xe ? 1.0f : xe);
             xnew[e] = 1.0e-3f < xe ? xe : 1.0e-3f;
+            if (P->passive[e]) xnew[e] = 1.0f;   /* passive elements stay solid (TOP3D_XL.m:152,166) */
         }
         float vol;
         if (P->p.vol_mode == 2) vol = orc_vol_sum(P, xnew, n) / (float)n;
@@ -1389,14 +1428,39 @@ int orc_design_loop(orc_problem* P, float V0, int nLoop, float rMin, double* Cso
     float* dcf = xcalloc((size_t)ne, sizeof(float));
     double* E = xcalloc((size_t)ne, sizeof(double));
     double* ce = xcalloc((size_t)ne, sizeof(double));
-    double* b = xcalloc((size_t)nf, sizeof(double));
-    double* u = xcalloc((size_t)nf, sizeof(double));
+    /* load cases (external models, TOP3D_XL.m:105,125,605-621): each solved from its own previous
+     * displacement; ce = sum_k ce_k / K accumulated as acc = w ce_0, then acc + w ce_k; C = sum E ce */
+    const int K = P->ncases > 1 ? P->ncases : 1;
+    const double w = 1.0 / K;
+    double* b = xcalloc((size_t)nf * K, sizeof(double));
+    double* u = xcalloc((size_t)nf * K, sizeof(double));
+    double* cek = K > 1 ? xcalloc((size_t)ne, sizeof(double)) : NULL;
     for (int e = 0; e < ne; ++e) { x[e] = V0; E[e] = (double)P->p.E0; }
-    orc_bfree(P, b);
+    for (int k = 0; k < K; ++k) {
+        const double* Fk = K > 1 ? P->Fcases + (int64_t)k * P->ndof : P->F;
+        for (int64_t i = 0; i < nf; ++i) b[k * nf + i] = Fk[P->free_dofs[i]];
+    }
     const double tol = (double)P->p.cg_tol;
+#define SOLVE_CASES(ITS, CTOTAL)                                                                   \
+    do {                                                                                           \
+        if (K == 1) {                                                                              \
+            ITS = orc_pcg(P, E, b, u, tol, P->p.cg_max_it);                                        \
+            CTOTAL = orc_compliance(P, E, u, ce);                                                  \
+        } else {                                                                                   \
+            ITS = 0;                                                                               \
+            for (int k = 0; k < K; ++k) {                                                          \
+                ITS += orc_pcg(P, E, b + k * nf, u + k * nf, tol, P->p.cg_max_it);                 \
+                orc_compliance(P, E, u + k * nf, cek);                                             \
+                for (int e = 0; e < ne; ++e) ce[e] = k == 0 ? w * cek[e] : ce[e] + w * cek[e];     \
+            }                                                                                      \
+            CTOTAL = orc_objective(P, E, ce, 1.0);                                                 \
+        }                                                                                          \
+    } while (0)
     orc_mg_build(P, E);
-    orc_pcg(P, E, b, u, tol, P->p.cg_max_it);
-    const double Csolid = orc_compliance(P, E, u, ce);
+    int its0 = 0;
+    double Csolid = 0.0;
+    SOLVE_CASES(its0, Csolid);
+    (void)its0;
     if (Csolid_out) *Csolid_out = Csolid;
     int loop = 0;
     float change = 1.0f, sharp = 1.0f;
@@ -1404,8 +1468,10 @@ int orc_design_loop(orc_problem* P, float V0, int nLoop, float rMin, double* Cso
         ++loop;
         orc_simp(P, x, E);
         if (loop == 1 || loop % 5 == 0) orc_mg_build(P, E);
-        const int its = orc_pcg(P, E, b, u, tol, P->p.cg_max_it);
-        orc_compliance(P, E, u, ce);
+        int its = 0;
+        double Cdummy = 0.0;
+        SOLVE_CASES(its, Cdummy);
+        (void)Cdummy;
         const double Cdisp = orc_objective(P, E, ce, Csolid);
         orc_sens(P, x, ce, Csolid, dc);
         for (int e = 0; e < ne; ++e) xdc[e] = x[e] * dc[e];
@@ -1421,15 +1487,36 @@ int orc_design_loop(orc_problem* P, float V0, int nLoop, float rMin, double* Cso
         R->cons = vf - V0; R->change = change; R->lmid = lm; R->bisections = passes;
     }
     if (xfinal) memcpy(xfinal, x, (size_t)ne * sizeof(float));
-    free(x); free(xnew); free(dc); free(xdc); free(dcf); free(E); free(ce); free(b); free(u);
+#undef SOLVE_CASES
+    free(x); free(xnew); free(dc); free(xdc); free(dcf); free(E); free(ce); free(b); free(u); free(cek);
     return loop;
 }
 
 /* ------------------------------------------------------------------ lifecycle, accessors */
+static orc_problem* create_common(orc_problem* P, int nely, int nelx, int nelz);
+
 orc_problem* orc_create(int nely, int nelx, int nelz, const orc_params* prm) {
     orc_problem* P = xcalloc(1, sizeof(orc_problem));
     if (prm) P->p = *prm;
     else orc_params_default(&P->p);
+    return create_common(P, nely, nelx, nelz);
+}
+
+/* An external model (TopVoxel, TOP3D_XL.m:458-586) in the file's index spaces; the arrays must outlive
+ * the problem.  Fixations and loads are on distinct nodes (the file reader keeps the first row). */
+orc_problem* orc_create_voxel(int nely, int nelx, int nelz, const orc_params* prm, const uint8_t* voxel, int nfix,
+                              const int64_t* fix_node, const uint8_t* fix_bits, int ncases, const int* case_n,
+                              const int64_t* load_node, const double* load_f) {
+    orc_problem* P = xcalloc(1, sizeof(orc_problem));
+    if (prm) P->p = *prm;
+    else orc_params_default(&P->p);
+    P->voxel = voxel;
+    P->nfix = nfix; P->fix_node = fix_node; P->fix_bits = fix_bits;
+    P->ncases = ncases; P->case_n = case_n; P->load_node = load_node; P->load_f = load_f;
+    return create_common(P, nely, nelx, nelz);
+}
+
+static orc_problem* create_common(orc_problem* P, int nely, int nelx, int nelz) {
     P->nelx = nelx; P->nely = nely; P->nelz = nelz;
     const int L = pad_levels((uint64_t)nelx * nely * nelz);
     P->nx = pad_dim(nelx, L); P->ny = pad_dim(nely, L); P->nz = pad_dim(nelz, L);
@@ -1451,7 +1538,7 @@ orc_problem* orc_create(int nely, int nelx, int nelz, const orc_params* prm) {
 void orc_destroy(orc_problem* P) {
     if (!P) return;
     free(P->ele_full); free(P->enod); free(P->bucket); free(P->isfree); free(P->free_dofs);
-    free(P->dof2free); free(P->F);
+    free(P->dof2free); free(P->F); free(P->Fcases); free(P->passive);
     for (int l = 0; l < P->nlev; ++l) { free(P->lv[l].mask); free(P->lv[l].diag); free(P->lv[l].r); free(P->lv[l].x); }
     free(P->Lc); free(P->Xc); free(P->tmpf); free(P->r); free(P->z); free(P->pp); free(P->Ap);
     free(P->fdiag); free(P->flastx); free(P->flastrhs); free(P->frhs); free(P->fx); free(P->fr); free(P->fz);

@@ -62,6 +62,12 @@ typedef struct orc_problem orc_problem;
 
 void orc_params_default(orc_params* p);
 orc_problem* orc_create(int nely, int nelx, int nelz, const orc_params* p);
+/* external model (TopVoxel): voxel[k], k = y + nely*(x + nelx*z), 0 void / 1 solid / 2 passive; fixations
+ * and loads on file nodes m = y + (nely+1)*(x + (nelx+1)*z); load cases concatenated, case k has case_n[k]
+ * nodes (3 forces each).  The arrays must outlive the problem. */
+orc_problem* orc_create_voxel(int nely, int nelx, int nelz, const orc_params* prm, const uint8_t* voxel, int nfix,
+                              const int64_t* fix_node, const uint8_t* fix_bits, int ncases, const int* case_n,
+                              const int64_t* load_node, const double* load_f);
 void orc_destroy(orc_problem* P);
 
 /* info: resX,resY,resZ, numElements, numNodes, nFree, nLevels, then per level (resX,resY,resZ,span) */

@@ -11,6 +11,9 @@
   element compliance averaged.  Two identical cases must reproduce the single-case design bit for bit
   (weights 1/2 are exact) with twice the PCG iterations; two different cases give the mean of the
   single-case solid compliances.
+* The whole design loop on an external domain with passive elements and two load cases matches the
+  oracle's restatement (oracle/t3d_oracle.c, external-model path) bit for bit: solid compliance, every
+  iteration's objective, PCG count and change, and the final densities.
 * Files the design loop cannot run are refused: no fixation, no load.
 """
 import numpy as np
@@ -161,3 +164,28 @@ def test_two_load_cases_average_the_compliance(tmp_path):
     kw = dict(cg_tol=1e-10, cg_max_it=5000)
     cs = [t3d.Problem.from_topvoxel(p, **kw).design_init(0.3) for p in paths]
     assert abs(cs[2] - 0.5 * (cs[0] + cs[1])) <= 1e-12 * cs[2], cs
+
+
+@pytest.mark.parametrize("two_cases", [False, True])
+def test_external_design_loop_matches_the_oracle(tmp_path, two_cases):
+    import algorithmengineering_altproject_b200 as t3d
+    from algorithmengineering_altproject_b200.topvoxel import write_topvoxel
+    from oracle.bindings import Oracle, voxel_model_from_rows
+    nelx, nely, nelz = 12, 6, 8
+    solid, passive, fix, loads = l_domain(nelx, nely, nelz)
+    side = [(nelx, y, 2, 0.0, 1.0 / (nely + 1), 0.0) for y in range(nely + 1)]
+    cases = [loads, side] if two_cases else [loads]
+    path = str(tmp_path / "l.TopVoxel")
+    write_topvoxel(path, nelx, nely, nelz, solid, passive=passive, fixations=fix, loads=loads,
+                   extra_load_cases=cases[1:])
+    P = t3d.Problem.from_topvoxel(path)
+    csg, recg, xg = P.run_global(0.3, 3)
+    P.close()
+    vm = voxel_model_from_rows(nelx, nely, nelz, solid, passive=passive, fixations=fix, load_cases=cases)
+    O = Oracle(nely, nelx, nelz, voxel_model=vm, red_mode=1, pow_mode=0, vol_mode=0, approx_mode=0)
+    cso, reco, xo = O.design_loop(0.3, 3)
+    assert csg == cso, (csg, cso)
+    assert len(recg) == len(reco)
+    for a, b in zip(recg, reco):
+        assert a["obj"] == b["obj"] and a["pcg_iters"] == b["pcg_iters"] and a["change"] == b["change"], (a, b)
+    np.testing.assert_array_equal(xg, xo)

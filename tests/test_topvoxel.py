@@ -72,3 +72,28 @@ def test_missing_file_is_an_error(tmp_path):
     with pytest.raises(t3d.T3DError) as e:
         t3d.topvoxel_info(str(tmp_path / "absent.TopVoxel"))
     assert e.value.code == t3d.T3D_ERR_INVALID and "cannot open" in str(e.value)
+
+
+def test_oracle_voxel_model_reproduces_the_builtin_cantilever():
+    # the oracle's external-model path (test infrastructure for the GPU TopVoxel tests) against its own
+    # built-in cantilever: same element order, free DOFs, load and a bit-identical design loop
+    import numpy as np
+    from oracle.bindings import Oracle, voxel_model_from_rows
+    nely, nelx, nelz = 6, 12, 6
+    kw = dict(red_mode=1, pow_mode=0, vol_mode=0, approx_mode=0)
+    A = Oracle(nely, nelx, nelz, **kw)
+    nx, ny, nz = A.res
+    iz_max = max(1, nz // 6)
+    count = (iz_max + 1) * (ny + 1)
+    solid = [(x, y, z) for z in range(nelz) for x in range(nelx) for y in range(nely)]
+    fix = [(0, y, z, 1, 1, 1) for z in range(nelz + 1) for y in range(nely + 1)]
+    loads = [(nelx, y, z, 0.0, 0.0, -1.0 / count) for z in range(min(iz_max, nelz) + 1) for y in range(nely + 1)]
+    B = Oracle(nely, nelx, nelz, voxel_model=voxel_model_from_rows(nelx, nely, nelz, solid, fixations=fix,
+                                                                   load_cases=[loads]), **kw)
+    np.testing.assert_array_equal(A.ele_map_back(), B.ele_map_back())
+    np.testing.assert_array_equal(A.free_dofs(), B.free_dofs())
+    np.testing.assert_array_equal(A.bfree(), B.bfree())
+    ca, ra, xa = A.design_loop(0.12, 2)
+    cb, rb, xb = B.design_loop(0.12, 2)
+    assert ca == cb and [r["obj"] for r in ra] == [r["obj"] for r in rb]
+    np.testing.assert_array_equal(xa, xb)
