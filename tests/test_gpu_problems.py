@@ -121,3 +121,48 @@ def test_degenerate_and_oversized_problems_are_errors():
     with pytest.raises(t3d.T3DError) as e:   # 3 x nodes beyond 32-bit DOF indices: refused before any allocation
         t3d.Problem(896, 1024, 896)
     assert e.value.code == t3d.T3D_ERR_UNSUPPORTED
+
+
+def spec_as_voxel_model(P, nely, nelx, nelz, load_case, voids):
+    """The problem spec as the oracle's external model: cuboid minus the voids, the x = 0 face fixed, and the
+    load case's forces on the reference's nodes (file coordinates: element / node (x, y, z) of the reference,
+    y = the reference's row index)."""
+    from oracle.bindings import voxel_model_from_rows
+    nx, ny, nz = P.res
+    solid = [(x, y, z) for z in range(nelz) for x in range(nelx) for y in range(nely)
+             if all(((x + 0.5 - cx) / rx) ** 2 + ((y + 0.5 - cy) / ry) ** 2 + ((z + 0.5 - cz) / rz) ** 2 > 1.0
+                    for cx, cy, cz, rx, ry, rz in voids)]
+    fix = [(0, y, z, 1, 1, 1) for z in range(nelz + 1) for y in range(nely + 1)]
+    if load_case == 0:     # tip line: -1/count over the padded grid's rows, z <= max(1, nz // 6)
+        iz_max = max(1, nz // 6)
+        count = (iz_max + 1) * (ny + 1)
+        loads = [(nelx, y, z, 0.0, 0.0, -1.0 / count) for z in range(min(iz_max, nelz) + 1) for y in range(nely + 1)]
+    elif load_case == 1:   # top traction on the z = nelz face
+        f = -1.0 / ((nelx + 1) * (nely + 1))
+        loads = [(x, y, nelz, 0.0, 0.0, f) for x in range(nelx + 1) for y in range(nely + 1)]
+    else:                  # torsion couple at x = nelx: +f on the top edge, -f on the bottom edge
+        f = 1.0 / (nely + 1)
+        loads = [(nelx, y, nelz, 0.0, f, 0.0) for y in range(nely + 1)] + \
+                [(nelx, y, 0, 0.0, -f, 0.0) for y in range(nely + 1)]
+    return voxel_model_from_rows(nelx, nely, nelz, solid, fixations=fix, load_cases=[loads])
+
+
+@pytest.mark.parametrize("load_case", [0, 1, 2])
+def test_problem_spec_design_loop_matches_the_oracle(load_case):
+    # the problem-spec path (load cases, voids) against the oracle's external-model restatement, bit for bit
+    import algorithmengineering_altproject_b200 as t3d
+    from oracle.bindings import Oracle
+    dims = (6, 12, 6)
+    P = t3d.Problem(*dims, problem=t3d.ProblemSpec.make(load_case, VOIDS))
+    vm = spec_as_voxel_model(P, *dims, load_case, VOIDS)
+    O = Oracle(*dims, voxel_model=vm, red_mode=1, pow_mode=0, vol_mode=0, approx_mode=0)
+    np.testing.assert_array_equal(P.ele_map_back(), O.ele_map_back())
+    np.testing.assert_array_equal(P.free_dofs(), O.free_dofs())
+    np.testing.assert_array_equal(P.bfree(), O.bfree())
+    csg, recg, xg = P.run_global(0.2, 3)
+    P.close()
+    cso, reco, xo = O.design_loop(0.2, 3)
+    assert csg == cso
+    for a, b in zip(recg, reco):
+        assert a["obj"] == b["obj"] and a["pcg_iters"] == b["pcg_iters"] and a["change"] == b["change"], (a, b)
+    np.testing.assert_array_equal(xg, xo)
