@@ -26,6 +26,7 @@ T3D_FP64, T3D_MIXED = 0, 1
 T3D_MATVEC32_AUTO, T3D_MATVEC32_DENSE = 0, 1
 T3D_COARSE_REFERENCE, T3D_COARSE_FULL = 0, 1
 T3D_MATVEC64_AUTO, T3D_MATVEC64_NODES = 0, 1
+T3D_VCYCLE_ADAPTED, T3D_VCYCLE_STANDARD = 0, 1
 
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
@@ -45,7 +46,8 @@ class Params(C.Structure):
                 ("mg_max_levels", C.c_int), ("mg_weight", C.c_float), ("filter_rmin", C.c_float),
                 ("oc_sum_order", C.c_int), ("precision", C.c_int), ("device", C.c_int),
                 ("matvec32_form", C.c_int), ("mg_coarse_assembly", C.c_int), ("matvec64_form", C.c_int),
-                ("reserved", C.c_int * 4)]
+                ("mg_vcycle", C.c_int), ("mg_standard_weight", C.c_float),
+                ("mg_rebuild_period", C.c_int), ("reserved", C.c_int * 1)]
 
 
 T3D_LOAD_TIP_LINE, T3D_LOAD_TOP_TRACTION, T3D_LOAD_TORSION = 0, 1, 2

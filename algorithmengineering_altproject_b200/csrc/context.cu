@@ -111,6 +111,13 @@ struct Context {
     // several load cases (external models): per-case loads and warm starts, weighted element compliance
     int ncases = 1;
     double *b_cases = nullptr, *u_cases = nullptr, *ce_acc = nullptr, *one = nullptr;
+    // 'Standard' V-cycle option: Galerkin element matrices per level (l >= 1), child-position products of
+    // Ke for level 1, and one scratch vector per level
+    bool standard = false;
+    double* E_mg = nullptr;     // the moduli the hierarchy was built from (the cycle's level-0 operator)
+    double* Kel[8]{};
+    double* Gpos = nullptr;
+    double* vtmp[8]{};
     bool ke_pat = false;        // Ke has the built-in coefficient pattern: its magnitudes are in Kd
     double* Kd = nullptr;       // [KE_MAX_DISTINCT]
     RedSlot slot[4]{};
@@ -190,6 +197,15 @@ struct Context {
 
 static int update_ke_pattern(Context* c);
 
+// W^T Ke W for the child positions of the first coarsening (the 'Standard' V-cycle's level-1 Galerkin)
+static int upload_gpos(Context* c) {
+    const int s1 = c->lv[1].span;
+    std::vector<double> G((size_t)s1 * s1 * s1 * 576);
+    galerkin_positions(s1, c->Ke_h, G.data());
+    T3D_CUDA_OK(cudaMemcpy(c->Gpos, G.data(), G.size() * sizeof(double), cudaMemcpyHostToDevice));
+    return T3D_OK;
+}
+
 #define CHECK(call)                       \
     do {                                  \
         int rc_ = (call);                 \
@@ -253,6 +269,18 @@ static int build_levels(Context* c) {
     CHECK(c->alloc(&c->chol_status, 1));
     T3D_CUDA_OK(cudaMemsetAsync(c->chol_status, 0, sizeof(int), c->st));
     for (int l = 0; l + 1 < c->nlev; ++l) launch_mask_restrict(c->lv[l + 1], c->lv[l], c->st);
+    c->standard = c->prm.mg_vcycle == T3D_VCYCLE_STANDARD;
+    if (c->standard) {
+        for (int l = 1; l < c->nlev; ++l) {
+            const MgLevel& L = c->lv[l];
+            CHECK(c->alloc(&c->Kel[l], (size_t)L.nx * L.ny * L.nz * 576));
+            CHECK(c->alloc(&c->vtmp[l], 3 * L.nn));
+        }
+        const int s1 = c->lv[1].span;
+        CHECK(c->alloc(&c->E_mg, c->g.NE));
+        CHECK(c->alloc(&c->Gpos, (size_t)s1 * s1 * s1 * 576));
+        CHECK(upload_gpos(c));
+    }
     return launch_check("mask restriction");
 }
 
@@ -422,6 +450,16 @@ static int create(int nely, int nelx, int nelz, const t3d_params* prm, const t3d
         return set_error(T3D_ERR_UNSUPPORTED, "matvec32_form must be T3D_MATVEC32_AUTO or T3D_MATVEC32_DENSE");
     if (c->prm.matvec64_form != T3D_MATVEC64_AUTO && c->prm.matvec64_form != T3D_MATVEC64_NODES)
         return set_error(T3D_ERR_UNSUPPORTED, "matvec64_form must be T3D_MATVEC64_AUTO or T3D_MATVEC64_NODES");
+    if (c->prm.mg_vcycle != T3D_VCYCLE_ADAPTED && c->prm.mg_vcycle != T3D_VCYCLE_STANDARD)
+        return set_error(T3D_ERR_UNSUPPORTED, "mg_vcycle must be T3D_VCYCLE_ADAPTED or T3D_VCYCLE_STANDARD");
+    if (c->prm.mg_vcycle == T3D_VCYCLE_STANDARD && c->prm.precision != T3D_FP64)
+        return set_error(T3D_ERR_UNSUPPORTED, "the Standard V-cycle is built for precision T3D_FP64 only");
+    // fields that were reserved (zero) in earlier versions of t3d_params: 0 selects the default
+    if (c->prm.mg_rebuild_period == 0) c->prm.mg_rebuild_period = 5;
+    if (c->prm.mg_standard_weight == 0.0f) c->prm.mg_standard_weight = 0.35f;
+    if (c->prm.mg_rebuild_period < 1) return set_error(T3D_ERR_INVALID, "mg_rebuild_period must be >= 1");
+    if (c->prm.mg_vcycle == T3D_VCYCLE_STANDARD && !(c->prm.mg_standard_weight > 0.0f))
+        return set_error(T3D_ERR_INVALID, "mg_standard_weight must be positive");
     c->mixed = c->prm.precision == T3D_MIXED;
     c->dev = c->prm.device;
     T3D_CUDA_OK(cudaSetDevice(c->dev));
@@ -633,6 +671,24 @@ static int download_cells_f32(Context* c, const float* cells, float* h) {
 static int mg_setup(Context* c) {
     c->launches += 1 + (c->nlev - 1) + (c->Nc ? 4 : 0);
     launch_diag0(c->g, c->Ke, c->E, c->mask0, c->lv[0].diag, c->st);
+    if (c->standard) {   // Galerkin element matrices and their diagonals on every coarse level
+        // the cycle's level-0 operator is K(E) of these moduli, so that a hierarchy kept between rebuilds
+        // (loop 1 and every 5th, driver.cpp:132) stays one symmetric positive definite preconditioner
+        T3D_CUDA_OK(cudaMemcpyAsync(c->E_mg, c->E, c->g.NE * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
+        launch_galerkin_fine(c->g, c->lv[1], c->E, c->mask0, c->Gpos, c->Ke, c->Kel[1], c->st);
+        for (int l = 2; l < c->nlev; ++l) launch_galerkin_coarse(c->lv[l - 1], c->lv[l], c->Kel[l - 1], c->Kel[l], c->st);
+        for (int l = 1; l < c->nlev; ++l) launch_level_diag(c->lv[l], c->Kel[l], c->st);
+        c->launches += 2 * (c->nlev - 1);
+        if (c->Nc) {
+            const MgLevel& Lc = c->lv[c->nlev - 1];
+            launch_to_coarse_layout(Lc, c->Kel[c->nlev - 1], c->Kce, c->st);
+            launch_coarse_assemble(Lc, c->Kce, c->Kc, c->st);
+            launch_cholesky(c->Kc, c->LT, c->Lrow, c->Nc, c->chol_status, c->st);
+            launch_coarse_inverse(c->Lrow, c->Nc, c->chol_status, c->Xc, c->st);
+        }
+        c->mg_ready = true;
+        return launch_check("mg set-up");
+    }
     for (int l = 0; l + 1 < c->nlev; ++l) launch_diag_coarsen(c->lv[l + 1], c->lv[l], c->st);
     if (c->Nc) {
         const MgLevel& Lc = c->lv[c->nlev - 1];
@@ -676,8 +732,54 @@ static int matvec64(Context* c, const double* u, double* y, RedSlot dot, PcgScal
     return 2;
 }
 
+// y = K_l x on level l (level 0: K(E) of the moduli the hierarchy was built from)
+static void level_matvec(Context* c, int l, const double* x, double* y, const PcgScalars* S) {
+    if (l == 0)
+        launch_matvec64_stream(c->g, c->st64, c->Ke_h, c->ke_pat ? c->Kd : nullptr, c->E_mg, c->mask0, x, y, S,
+                               c->st);
+    else
+        launch_level_matvec(c->lv[l], c->Kel[l], x, y, S, c->st);
+}
+
+// kernels of one V-cycle
+static int vcycle_launches(const Context* c) {
+    const int L = c->nlev;
+    return c->standard ? 9 * (L - 1) + 2 : 4 * (L - 1) + 1;
+}
+
+// The 'Standard' cycle (see k_mg_standard.cu); level 0 uses Ap as scratch (free between the PCG update
+// and the next K(E)p)
+static void vcycle_standard(Context* c, const double* r, double* z, PcgScalars* S, RedSlot dot) {
+    const int L = c->nlev;
+    const double w = (double)c->prm.mg_standard_weight;
+    c->launches += vcycle_launches(c);
+    for (int l = 0; l + 1 < L; ++l) {
+        const double* rl = l == 0 ? r : c->lv[l].r;
+        double* xl = l == 0 ? z : c->lv[l].x;
+        double* t = l == 0 ? c->Ap : c->vtmp[l];
+        launch_jacobi_init(c->lv[l], rl, xl, w, S, c->st);
+        level_matvec(c, l, xl, t, S);
+        launch_residual(c->lv[l], rl, t, S, c->st);
+        launch_restrict(c->lv[l + 1], c->lv[l], t, c->lv[l + 1].r, c->ra1[l], c->ra2[l], S, c->st, false);
+    }
+    launch_coarse_solve(c->lv[L - 1], c->Xc, c->Nc, c->chol_status, S, c->st);
+    for (int l = L - 2; l >= 0; --l) {
+        const double* rl = l == 0 ? r : c->lv[l].r;
+        double* xl = l == 0 ? z : c->lv[l].x;
+        double* t = l == 0 ? c->Ap : c->vtmp[l];
+        launch_prolong_add(c->lv[l + 1], c->lv[l], c->lv[l + 1].x, xl, S, c->st);
+        level_matvec(c, l, xl, t, S);
+        launch_jacobi_correct(c->lv[l], rl, t, xl, w, S, c->st);
+    }
+    if (S) launch_dot_rz(c->g.NN, r, z, dot, S, c->st);
+}
+
 // z = M r for grid vectors; with S, r.z goes to S (rz / beta)
 static void vcycle(Context* c, const double* r, double* z, PcgScalars* S, RedSlot dot) {
+    if (c->standard) {
+        vcycle_standard(c, r, z, S, dot);
+        return;
+    }
     const int L = c->nlev;
     c->launches += 4 * (L - 1) + 1;
     for (int l = 0; l + 1 < L; ++l)
@@ -729,7 +831,7 @@ static int pcg_solve(Context* c, double tol, int maxit, int* iters) {
         const int n = std::min(PCG_CHUNK, maxit - queued);
         if (c->use_graph && n == PCG_CHUNK) {
             T3D_CUDA_OK(cudaGraphLaunch(c->pcg_graph, c->st));
-            c->launches += (int64_t)PCG_CHUNK * ((c->mv64_stream ? 4 : 3) + 4 * (c->nlev - 1) + 1);
+            c->launches += (int64_t)PCG_CHUNK * ((c->mv64_stream ? 4 : 3) + vcycle_launches(c));
         } else {
             for (int k = 0; k < n; ++k) pcg_iteration(c);
             CHECK(launch_check("pcg iteration"));
@@ -992,7 +1094,7 @@ static int design_step(Context* c, t3d_iter_record* rec) {
     T3D_CUDA_OK(cudaEventRecord(e0, c->st));
     launch_simp(g, c->solid, c->x, P.E0, P.Emin, P.penal, c->E, c->st);
     c->launches += 4;   // simp, objective, sensitivities, dc scale
-    if (c->loop == 1 || c->loop % 5 == 0) CHECK(mg_setup(c));
+    if (c->loop == 1 || c->loop % c->prm.mg_rebuild_period == 0) CHECK(mg_setup(c));
     int its = 0;
     CHECK(solve_all(c, (double)P.cg_tol, P.cg_max_it, &its, c->scal + 0));
     T3D_CUDA_OK(cudaEventRecord(e1, c->st));
@@ -1047,6 +1149,8 @@ int t3d_params_default(t3d_params* p) {
     p->E0 = 1.0f; p->Emin = 1.0e-6f; p->nu = 0.3f; p->penal = 3.0f;     // core.hpp:28-31
     p->cg_tol = 1.0e-3f; p->cg_max_it = 800;                             // core.hpp:35-36
     p->mg_nondyadic = 1; p->mg_max_levels = 5; p->mg_weight = 0.6f;      // driver.cpp:54
+    p->mg_standard_weight = 0.35f;
+    p->mg_rebuild_period = 5;                                            // driver.cpp:132
     p->filter_rmin = std::sqrt(3.0f);                                    // top3d_cli.cpp:33
     p->oc_sum_order = T3D_SUM_REFERENCE;
     p->precision = T3D_FP64;
@@ -1174,6 +1278,7 @@ int t3d_set_ke(t3d_context* ctx, const double* ke) {
     std::memcpy(ctx->Ke_h, ke, sizeof ctx->Ke_h);
     T3D_CUDA_OK(cudaMemcpy(ctx->Ke, ctx->Ke_h, sizeof ctx->Ke_h, cudaMemcpyHostToDevice));
     CHECK(t3d::update_ke_pattern(ctx));
+    if (ctx->standard) CHECK(t3d::upload_gpos(ctx));   // the Standard V-cycle's level-1 Galerkin products
     T3D_CUDA_OK(cudaStreamSynchronize(ctx->st));
     if (ctx->Ke32) {
         float k32[576];

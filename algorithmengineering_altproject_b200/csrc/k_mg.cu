@@ -167,8 +167,10 @@ __global__ void k_restrict_y(MgLevel Lc, MgLevel Lf, const double* __restrict__ 
     a2[2 * total + t] = v2;
 }
 
+// normalize = 0: the plain hat-weighted sum, i.e. the transpose of the trilinear prolongation (the
+// 'Standard' V-cycle option)
 __global__ void k_restrict_z(MgLevel Lc, MgLevel Lf, const double* __restrict__ a2, double* __restrict__ rc,
-                             const PcgScalars* S) {
+                             const PcgScalars* S, int normalize) {
     if (S != nullptr && S->done) return;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= Lc.nn) return;
@@ -196,7 +198,11 @@ __global__ void k_restrict_z(MgLevel Lc, MgLevel Lf, const double* __restrict__ 
     }
     const double wsum = swz * swy * swx;
     double o0 = 0.0, o1 = 0.0, o2 = 0.0;
-    if (wsum > 1e-12) {
+    if (!normalize) {
+        o0 = v0;
+        o1 = v1;
+        o2 = v2;
+    } else if (wsum > 1e-12) {
         const double iw = 1.0 / wsum;
         o0 = v0 * iw;
         o1 = v1 * iw;
@@ -489,12 +495,12 @@ void launch_diag_coarsen(const MgLevel& Lc, const MgLevel& Lf, cudaStream_t s) {
     k_diag_coarsen<<<blocks_for(Lc.nn, 128), 128, 0, s>>>(Lc, Lf);
 }
 void launch_restrict(const MgLevel& Lc, const MgLevel& Lf, const double* rf, double* rc, double* a1, double* a2,
-                     const PcgScalars* S, cudaStream_t s) {
+                     const PcgScalars* S, cudaStream_t s, bool normalize) {
     const int64_t n1 = (int64_t)(Lf.nz + 1) * (Lf.ny + 1) * (Lc.nx + 1);
     const int64_t n2 = (int64_t)(Lf.nz + 1) * (Lc.ny + 1) * (Lc.nx + 1);
     k_restrict_x<<<blocks_for(n1, 256), 256, 0, s>>>(Lc, Lf, rf, a1, S);
     k_restrict_y<<<blocks_for(n2, 256), 256, 0, s>>>(Lc, Lf, a1, a2, S);
-    k_restrict_z<<<blocks_for(Lc.nn, 128), 128, 0, s>>>(Lc, Lf, a2, rc, S);
+    k_restrict_z<<<blocks_for(Lc.nn, 128), 128, 0, s>>>(Lc, Lf, a2, rc, S, normalize ? 1 : 0);
 }
 void launch_coarse_jacobi(const MgLevel& L, const PcgScalars* S, cudaStream_t s) {
     k_coarse_jacobi<<<blocks_for(L.nn, 128), 128, 0, s>>>(L, S);

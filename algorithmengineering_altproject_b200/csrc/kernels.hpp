@@ -104,8 +104,9 @@ void launch_diag0(const Grid& g, const double* Ke, const double* E, const uint8_
 void launch_mask_restrict(const MgLevel& Lc, const MgLevel& Lf, cudaStream_t s);
 void launch_diag_coarsen(const MgLevel& Lc, const MgLevel& Lf, cudaStream_t s);
 // separable restriction; a1, a2: pass buffers of 3*(fnz*fny*cnx) and 3*(fnz*cny*cnx) doubles
+// normalize = false: the transpose of the trilinear prolongation (no division by the weight sum)
 void launch_restrict(const MgLevel& Lc, const MgLevel& Lf, const double* rf, double* rc, double* a1, double* a2,
-                     const PcgScalars* S, cudaStream_t s);
+                     const PcgScalars* S, cudaStream_t s, bool normalize = true);
 void launch_coarse_jacobi(const MgLevel& L, const PcgScalars* S, cudaStream_t s);
 void launch_prolong_smooth(const MgLevel& Lc, const MgLevel& Lf, const double* xc, const double* rf, double* xf,
                            double weight, const PcgScalars* S, cudaStream_t s);
@@ -123,6 +124,25 @@ void launch_cholesky(const double* A, double* LT, double* Lrow, int N, int* stat
 void launch_coarse_inverse(const double* Lrow, int N, const int* status, double* X, cudaStream_t s);
 void launch_coarse_solve(const MgLevel& L, const double* X, int N, const int* status, const PcgScalars* S,
                          cudaStream_t s);
+
+// ---- 'Standard' V-cycle option (TOP3D_XL.m:772-807): Galerkin element matrices per level, smoothing with
+// the true residual; FP64
+// G[pos][576] = W_pos^T Ke W_pos for the s^3 child positions of a span-s coarse element (host)
+void galerkin_positions(int s, const double* Ke, double* G);
+void launch_galerkin_fine(const Grid& g, const MgLevel& L1, const double* E, const uint8_t* mask0, const double* Gpos,
+                          const double* Ke, double* Kel, cudaStream_t s);
+void launch_galerkin_coarse(const MgLevel& Lf, const MgLevel& Lc, const double* Kf, double* Kc, cudaStream_t s);
+void launch_level_diag(const MgLevel& L, const double* Kel, cudaStream_t s);
+void launch_level_matvec(const MgLevel& L, const double* Kel, const double* x, double* y, const PcgScalars* S,
+                         cudaStream_t s);
+void launch_jacobi_init(const MgLevel& L, const double* r, double* x, double w, const PcgScalars* S, cudaStream_t s);
+void launch_residual(const MgLevel& L, const double* r, double* kx, const PcgScalars* S, cudaStream_t s);
+void launch_jacobi_correct(const MgLevel& L, const double* r, const double* kx, double* x, double w,
+                           const PcgScalars* S, cudaStream_t s);
+void launch_prolong_add(const MgLevel& Lc, const MgLevel& Lf, const double* xc, double* xf, const PcgScalars* S,
+                        cudaStream_t s);
+void launch_dot_rz(int64_t NN, const double* r, const double* z, RedSlot red, PcgScalars* S, cudaStream_t s);
+void launch_to_coarse_layout(const MgLevel& L, const double* Kel, double* Kce, cudaStream_t s);
 
 // ---- PCG vector steps (solver.cpp:87-217)
 void launch_pcg_init(const Grid& g, const double* b, const double* Ax, double* r, RedSlot red, PcgScalars* S,

@@ -51,6 +51,11 @@ enum { T3D_COARSE_REFERENCE = 0, T3D_COARSE_FULL = 1 };
 /* FP64 K(E)u (t3d_matvec, FP64 PCG, the mixed form's outer residual): AUTO = element-streaming kernel,
  * NODES = node-centric gather kernel.  Both are bit-identical to the reference's product. */
 enum { T3D_MATVEC64_AUTO = 0, T3D_MATVEC64_NODES = 1 };
+/* V-cycle: ADAPTED = the reference's (preconditioner.cpp:88-265: no residual smoothing, restricted
+ * diagonals); STANDARD = smoothing with the true residual on every level, Galerkin coarse operators and
+ * the transposed prolongation as restriction (the MATLAB original's 'Standard', TOP3D_XL.m:772-807);
+ * FP64 precision only */
+enum { T3D_VCYCLE_ADAPTED = 0, T3D_VCYCLE_STANDARD = 1 };
 
 typedef struct t3d_params {
     float E0, Emin, nu, penal;    /* GlobalParams core.hpp:26-33 (Ke always uses nu = 0.3, fea.cpp:345) */
@@ -66,7 +71,13 @@ typedef struct t3d_params {
     int   matvec32_form;          /* mixed precision only: T3D_MATVEC32_AUTO or T3D_MATVEC32_DENSE */
     int   mg_coarse_assembly;     /* T3D_COARSE_REFERENCE (default) or T3D_COARSE_FULL */
     int   matvec64_form;          /* T3D_MATVEC64_AUTO (default) or T3D_MATVEC64_NODES */
-    int   reserved[4];
+    int   mg_vcycle;              /* T3D_VCYCLE_ADAPTED (default) or T3D_VCYCLE_STANDARD */
+    float mg_standard_weight;     /* Jacobi weight of the Standard V-cycle (0 = the default 0.35): below 2 / 5.36, where
+                                     5.36 bounds lambda_max(D^-1 K) for the hex8 Ke and any moduli (Gershgorin),
+                                     so its residual smoother converges; the reference's 0.6 does not */
+    int   mg_rebuild_period;      /* design iterations between MG rebuilds: 5 = the reference's loop 1 and every
+                                     5th (driver.cpp:132); 1 = every iteration; 0 = the default (5) */
+    int   reserved[1];
 } t3d_params;
 
 /* Problem spec beyond the reference's built-in cantilever (the reference hard-codes one load case and a
