@@ -435,25 +435,31 @@ __global__ void __launch_bounds__(1024) k_cholesky(const double* __restrict__ A,
 // Coarsest inverse for the canonical coarsest solve: column j of X = L'^-1 L^-1 e_j computed by
 // thread j with the reference's substitution order (coarsest.cpp:92-122); column j is stored
 // contiguously (X[j*N + i]).  Runs at each MG set-up after a successful factorisation.
+// Column j of the coarsest inverse by forward and backward substitution with the factor's rows, each
+// sum in increasing k (the oracle's order).  A block of INV_COLS threads owns INV_COLS columns, whose
+// working vectors sit in shared memory as [i][lane] (no bank conflicts; factor rows are broadcast loads).
+constexpr int INV_COLS = 16;
 __global__ void k_coarse_inverse(const double* __restrict__ Lrow, int N, const int* __restrict__ status,
                                  double* __restrict__ X) {
+    extern __shared__ double xs[];   // [N][INV_COLS]
     if (*status != 1) return;
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= N) return;
-    double* x = X + (int64_t)j * N;
-    for (int i = 0; i < N; ++i) x[i] = (i == j) ? 1.0 : 0.0;
+    const int lane = threadIdx.x;
+    const int j = blockIdx.x * INV_COLS + lane;
+    for (int i = 0; i < N; ++i) xs[i * INV_COLS + lane] = (i == j) ? 1.0 : 0.0;
     for (int i = 0; i < N; ++i) {
-        double s = x[i];
+        double sum = xs[i * INV_COLS + lane];
         const double* Li = Lrow + (int64_t)i * N;
-        for (int k = 0; k < i; ++k) s = s - Li[k] * x[k];
-        x[i] = s / Li[i];
+        for (int k = 0; k < i; ++k) sum = sum - Li[k] * xs[k * INV_COLS + lane];
+        xs[i * INV_COLS + lane] = sum / Li[i];
     }
     for (int i = N - 1; i >= 0; --i) {
         const double* Li = Lrow + (int64_t)i * N;
-        x[i] = x[i] / Li[i];
-        const double xi = x[i];
-        for (int k = 0; k < i; ++k) x[k] = x[k] - Li[k] * xi;
+        const double xi = xs[i * INV_COLS + lane] / Li[i];
+        xs[i * INV_COLS + lane] = xi;
+        for (int k = 0; k < i; ++k) xs[k * INV_COLS + lane] = xs[k * INV_COLS + lane] - Li[k] * xi;
     }
+    if (j < N)
+        for (int i = 0; i < N; ++i) X[(int64_t)j * N + i] = xs[i * INV_COLS + lane];
 }
 
 // Coarsest solve x_i = sum_j X[i][j] r_j (sequential in j) when the factorisation succeeded, else
@@ -526,7 +532,9 @@ void launch_cholesky(const double* A, double* LT, double* Lrow, int N, int* stat
     k_cholesky<<<1, 1024, 0, s>>>(A, LT, Lrow, N, status);
 }
 void launch_coarse_inverse(const double* Lrow, int N, const int* status, double* X, cudaStream_t s) {
-    k_coarse_inverse<<<blocks_for(N, 32), 32, 0, s>>>(Lrow, N, status, X);
+    const size_t smem = (size_t)N * INV_COLS * sizeof(double);   // N <= 1000: at most 128 KB
+    cudaFuncSetAttribute(k_coarse_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_coarse_inverse<<<blocks_for(N, INV_COLS), INV_COLS, smem, s>>>(Lrow, N, status, X);
 }
 void launch_coarse_solve(const MgLevel& L, const double* X, int N, const int* status, const PcgScalars* S,
                          cudaStream_t s) {

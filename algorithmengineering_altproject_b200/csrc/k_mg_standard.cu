@@ -31,61 +31,88 @@ __device__ __forceinline__ int lnode(const MgLevel& L, int x, int y, int z) {
     return (z * (L.ny + 1) + y) * (L.nx + 1) + x;
 }
 
-// level-1 element matrices from the finest grid: one CTA (576 threads, thread = entry (P, Q)) per coarse
-// element (cz*ny1 + cy)*nx1 + cx
+// level-1 element matrices from the finest grid: one CTA (576 threads, thread = entry (P, Q)) per GB
+// consecutive coarse elements (cz*ny1 + cy)*nx1 + cx, so that each G_pos entry is read once per batch;
+// children are summed in position order, masked ones by the explicit product
+constexpr int GB = 8;
 __global__ void __launch_bounds__(576) k_galerkin_fine(Grid g, MgLevel L1, int s, const double* __restrict__ E,
                                                        const uint8_t* __restrict__ mask0,
                                                        const double* __restrict__ Gpos,
                                                        const double* __restrict__ Keg, double* __restrict__ Kel) {
-    __shared__ int cmask[8];
-    __shared__ double childE;
-    __shared__ int childMask[8];
-    const int ce = blockIdx.x;
-    const int cx = ce % L1.nx, cy = (ce / L1.nx) % L1.ny, cz = ce / (L1.nx * L1.ny);
+    __shared__ double Ec[GB][64];            // child moduli (0: skipped), s^3 <= 64
+    __shared__ uint8_t cmk[GB][64][8];       // child corner masks
+    __shared__ uint8_t anym[GB][64];         // child touches a fixed DOF
+    __shared__ uint8_t cmask[GB][8];         // coarse corner masks
+    const int ne1 = L1.nx * L1.ny * L1.nz, ns = s * s * s;
+    const int e0 = blockIdx.x * GB;
+    for (int q = threadIdx.x; q < GB * ns; q += blockDim.x) {
+        const int b = q / ns, p = q % ns, ce = e0 + b;
+        double Ee = 0.0;
+        uint8_t any = 0;
+        if (ce < ne1) {
+            const int cx = ce % L1.nx, cy = (ce / L1.nx) % L1.ny, cz = ce / (L1.nx * L1.ny);
+            const int i = p % s, j = (p / s) % s, k = p / (s * s);
+            const int fx = cx * s + i, fy = cy * s + j, fz = cz * s + k;
+            const double e = E[g.cell(fx, fy, fz)];
+            Ee = e <= 1.0e-16 ? 0.0 : e;   // K(E) skips these elements
+            for (int a = 0; a < 8; ++a) {
+                const uint8_t m = mask0[g.node(fx + corner_dx(a), fy + corner_dy(a), fz + corner_dz(a))];
+                cmk[b][p][a] = m;
+                any |= m;
+            }
+        }
+        Ec[b][p] = Ee;
+        anym[b][p] = any;
+    }
+    for (int q = threadIdx.x; q < GB * 8; q += blockDim.x) {
+        const int b = q / 8, A = q % 8, ce = e0 + b;
+        uint8_t m = 0;
+        if (ce < ne1) {
+            const int cx = ce % L1.nx, cy = (ce / L1.nx) % L1.ny, cz = ce / (L1.nx * L1.ny);
+            m = L1.mask[lnode(L1, cx + corner_dx(A), cy + corner_dy(A), cz + corner_dz(A))];
+        }
+        cmask[b][A] = m;
+    }
+    __syncthreads();
     const int P = threadIdx.x / 24, Q = threadIdx.x % 24;
     const int A = P / 3, r = P % 3, B = Q / 3, q = Q % 3;
-    if (threadIdx.x < 8)
-        cmask[threadIdx.x] = L1.mask[lnode(L1, cx + corner_dx(threadIdx.x), cy + corner_dy(threadIdx.x),
-                                           cz + corner_dz(threadIdx.x))];
-    double acc = 0.0;
-    for (int k = 0; k < s; ++k)
-        for (int j = 0; j < s; ++j)
-            for (int i = 0; i < s; ++i) {
-                const int fx = cx * s + i, fy = cy * s + j, fz = cz * s + k;
-                __syncthreads();
-                if (threadIdx.x == 0) {
-                    const double Ee = E[g.cell(fx, fy, fz)];
-                    childE = Ee <= 1.0e-16 ? 0.0 : Ee;   // K(E) skips these elements
-                }
-                if (threadIdx.x < 8)
-                    childMask[threadIdx.x] = mask0[g.node(fx + corner_dx(threadIdx.x), fy + corner_dy(threadIdx.x),
-                                                          fz + corner_dz(threadIdx.x))];
-                __syncthreads();
-                const double Ee = childE;
-                if (Ee == 0.0) continue;
-                int any = 0;
-                for (int a = 0; a < 8; ++a) any |= childMask[a];
-                if (!any) {
-                    acc = acc + Ee * Gpos[((k * s + j) * s + i) * 576 + threadIdx.x];
-                } else {   // sum_{a,b} w_aA w_bB M_ar M_bq E Ke[3a+r][3b+q]
-                    double t = 0.0;
-                    for (int a = 0; a < 8; ++a) {
-                        if ((childMask[a] >> r) & 1) continue;
-                        const double wa = tri_w(s, i + corner_dx(a), j + corner_dy(a), k + corner_dz(a), A);
-                        double u = 0.0;
-                        for (int b = 0; b < 8; ++b) {
-                            if ((childMask[b] >> q) & 1) continue;
-                            const double wb = tri_w(s, i + corner_dx(b), j + corner_dy(b), k + corner_dz(b), B);
-                            u = u + wb * Keg[(3 * a + r) * 24 + 3 * b + q];
-                        }
-                        t = t + wa * u;
+    double acc[GB];
+#pragma unroll
+    for (int b = 0; b < GB; ++b) acc[b] = 0.0;
+    for (int p = 0; p < ns; ++p) {
+        const double gp = Gpos[p * 576 + threadIdx.x];
+        const int i = p % s, j = (p / s) % s, k = p / (s * s);
+#pragma unroll
+        for (int b = 0; b < GB; ++b) {
+            const double Ee = Ec[b][p];
+            if (Ee == 0.0) continue;
+            if (!anym[b][p]) {
+                acc[b] = acc[b] + Ee * gp;
+            } else {   // sum_{a,b'} w_aA w_b'B M_ar M_b'q E Ke[3a+r][3b'+q]
+                double t = 0.0;
+                for (int a = 0; a < 8; ++a) {
+                    if ((cmk[b][p][a] >> r) & 1) continue;
+                    const double wa = tri_w(s, i + corner_dx(a), j + corner_dy(a), k + corner_dz(a), A);
+                    double u = 0.0;
+                    for (int c = 0; c < 8; ++c) {
+                        if ((cmk[b][p][c] >> q) & 1) continue;
+                        const double wc = tri_w(s, i + corner_dx(c), j + corner_dy(c), k + corner_dz(c), B);
+                        u = u + wc * Keg[(3 * a + r) * 24 + 3 * c + q];
                     }
-                    acc = acc + Ee * t;
+                    t = t + wa * u;
                 }
+                acc[b] = acc[b] + Ee * t;
             }
-    __syncthreads();
-    if (((cmask[A] >> r) & 1) || ((cmask[B] >> q) & 1)) acc = 0.0;
-    Kel[(int64_t)ce * 576 + threadIdx.x] = acc;
+        }
+    }
+#pragma unroll
+    for (int b = 0; b < GB; ++b) {
+        const int ce = e0 + b;
+        if (ce >= ne1) continue;
+        double v = acc[b];
+        if (((cmask[b][A] >> r) & 1) || ((cmask[b][B] >> q) & 1)) v = 0.0;
+        Kel[(int64_t)ce * 576 + threadIdx.x] = v;
+    }
 }
 
 // level-l element matrices from level l-1's (already masked): sum over the s^3 children of W^T K_c W
@@ -300,7 +327,8 @@ void galerkin_positions(int s, const double* Ke, double* G) {
 
 void launch_galerkin_fine(const Grid& g, const MgLevel& L1, const double* E, const uint8_t* mask0, const double* Gpos,
                           const double* Ke, double* Kel, cudaStream_t s) {
-    k_galerkin_fine<<<L1.nx * L1.ny * L1.nz, 576, 0, s>>>(g, L1, L1.span, E, mask0, Gpos, Ke, Kel);
+    k_galerkin_fine<<<blocks_of((int64_t)L1.nx * L1.ny * L1.nz, GB), 576, 0, s>>>(g, L1, L1.span, E, mask0, Gpos, Ke,
+                                                                              Kel);
 }
 void launch_galerkin_coarse(const MgLevel& Lf, const MgLevel& Lc, const double* Kf, double* Kc, cudaStream_t s) {
     k_galerkin_coarse<<<Lc.nx * Lc.ny * Lc.nz, 576, 0, s>>>(Lf, Lc, Kf, Kc);
