@@ -62,6 +62,10 @@ def parse_args():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default=DEFAULT_CONFIG, choices=sorted(CONFIGS))
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--vcycle", default="adapted", choices=["adapted", "standard"],
+                    help="standard: residual smoothing with Galerkin coarse operators (FP64 only; not the reference's)")
+    ap.add_argument("--mg-rebuild-period", type=int, default=5,
+                    help="design iterations between MG rebuilds (5 = the reference's schedule)")
     ap.add_argument("--compare-steps", type=int, default=2,
                     help="design iterations run by both forms from the same density (mixed vs FP64 errors)")
     ap.add_argument("--kernels-only", action="store_true",
@@ -324,7 +328,9 @@ def run_b200(args):
     comparison = compare_forms(cfg, dev, args.compare_steps) if (mixed and args.compare_steps > 0) else None
 
     P = t3d.Problem(cfg["nely"], cfg["nelx"], cfg["nelz"], device=dev, mg_max_levels=cfg["max_levels"],
-                    oc_sum_order=t3d.T3D_SUM_FP64, precision=t3d.T3D_MIXED if mixed else t3d.T3D_FP64)
+                    oc_sum_order=t3d.T3D_SUM_FP64, precision=t3d.T3D_MIXED if mixed else t3d.T3D_FP64,
+                    mg_vcycle=t3d.T3D_VCYCLE_STANDARD if args.vcycle == "standard" else t3d.T3D_VCYCLE_ADAPTED,
+                    mg_rebuild_period=args.mg_rebuild_period)
     P.design_init(cfg["V0"])
     for _ in range(args.warmup):
         P.design_step()
@@ -381,6 +387,8 @@ def run_b200(args):
                        "precision": ("mixed: FP32 inner MG-PCG in FP64 defect correction" if mixed
                                      else "fp64 (plain GPU form)"),
                        "oc_volume_sum": "fp64", "parallelism": "replicas" if world > 1 else "single GPU",
+                       "vcycle": args.vcycle + ("" if args.vcycle == "adapted" else " (not the reference's algorithm)"),
+                       "mg_rebuild_period": args.mg_rebuild_period,
                        "l2": "inputs larger than L2 (node vectors %.0f MB each)" % (3 * P.nn * (4 if mixed else 8) / 1e6)},
             "pcg_iterations": pcg_its,
             "per_kernel_ms": {"matvec": mv_ms, "vcycle": vc_ms, "pcg_iteration": it_ms},
@@ -414,6 +422,9 @@ def run_b200(args):
 
 def main():
     args = parse_args()
+    if args.vcycle == "standard" and args.precision != "fp64" and args.impl == "b200":
+        print(json.dumps({"error": "--vcycle standard is built for --precision fp64 only"}), flush=True)
+        return 2
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.kernels_only:
