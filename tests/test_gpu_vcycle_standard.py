@@ -169,3 +169,17 @@ def test_standard_vcycle_design_loop_and_precision_guard():
     with pytest.raises(t3d.T3DError) as e:
         t3d.Problem(8, 16, 8, precision=t3d.T3D_MIXED, mg_vcycle=t3d.T3D_VCYCLE_STANDARD)
     assert e.value.code == t3d.T3D_ERR_UNSUPPORTED
+
+
+def test_multigrid_parameters_are_validated():
+    import algorithmengineering_altproject_b200 as t3d
+    for kw, code in ((dict(mg_rebuild_period=-1), t3d.T3D_ERR_INVALID),
+                     (dict(mg_vcycle=t3d.T3D_VCYCLE_STANDARD, mg_standard_weight=-0.1), t3d.T3D_ERR_INVALID),
+                     (dict(mg_vcycle=7), t3d.T3D_ERR_UNSUPPORTED)):
+        with pytest.raises(t3d.T3DError) as e:
+            t3d.Problem(8, 16, 8, **kw)
+        assert e.value.code == code, (kw, e.value.code)
+    # 0 in the fields that were reserved before means the default (5 and 0.35)
+    P = t3d.Problem(8, 16, 8, mg_rebuild_period=0, mg_standard_weight=0.0, mg_vcycle=t3d.T3D_VCYCLE_STANDARD)
+    assert P.design_init(0.3) > 0
+    P.close()
