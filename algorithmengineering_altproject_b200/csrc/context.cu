@@ -1094,7 +1094,7 @@ static int design_step(Context* c, t3d_iter_record* rec) {
     T3D_CUDA_OK(cudaEventRecord(e0, c->st));
     launch_simp(g, c->solid, c->x, P.E0, P.Emin, P.penal, c->E, c->st);
     c->launches += 4;   // simp, objective, sensitivities, dc scale
-    if (c->loop == 1 || c->loop % c->prm.mg_rebuild_period == 0) CHECK(mg_setup(c));
+    if (!c->mg_ready || c->loop == 1 || c->loop % c->prm.mg_rebuild_period == 0) CHECK(mg_setup(c));
     int its = 0;
     CHECK(solve_all(c, (double)P.cg_tol, P.cg_max_it, &its, c->scal + 0));
     T3D_CUDA_OK(cudaEventRecord(e1, c->st));
@@ -1279,6 +1279,7 @@ int t3d_set_ke(t3d_context* ctx, const double* ke) {
     T3D_CUDA_OK(cudaMemcpy(ctx->Ke, ctx->Ke_h, sizeof ctx->Ke_h, cudaMemcpyHostToDevice));
     CHECK(t3d::update_ke_pattern(ctx));
     if (ctx->standard) CHECK(t3d::upload_gpos(ctx));   // the Standard V-cycle's level-1 Galerkin products
+    ctx->mg_ready = false;   // the hierarchy was built with the old Ke: rebuilt by the next design step or t3d_mg_setup
     T3D_CUDA_OK(cudaStreamSynchronize(ctx->st));
     if (ctx->Ke32) {
         float k32[576];

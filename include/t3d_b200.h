@@ -150,7 +150,9 @@ const char* t3d_last_error(void);
 
 /* --------------------------------------------------------------- model data (reference layouts) */
 int  t3d_get_ke(const struct t3d_context* ctx, double* ke576);            /* ComputeVoxelKe fea.cpp:117 */
-int  t3d_set_ke(struct t3d_context* ctx, const double* ke576);
+int  t3d_set_ke(struct t3d_context* ctx, const double* ke576);   /* invalidates the MG hierarchy: the next
+                                                                     design step rebuilds it, t3d_pcg / t3d_vcycle
+                                                                     need t3d_mg_setup first */
 int  t3d_get_element_map(struct t3d_context* ctx, int32_t* ele_map_back); /* mesh.eleMapBack core.hpp:60 */
 int  t3d_get_free_dofs(struct t3d_context* ctx, int32_t* free_dofs);      /* Problem::freeDofIndex core.hpp:88 */
 int  t3d_get_load(struct t3d_context* ctx, double* b_free);               /* restrict_to_free(F) solver.cpp:12 */

@@ -183,3 +183,20 @@ def test_multigrid_parameters_are_validated():
     P = t3d.Problem(8, 16, 8, mg_rebuild_period=0, mg_standard_weight=0.0, mg_vcycle=t3d.T3D_VCYCLE_STANDARD)
     assert P.design_init(0.3) > 0
     P.close()
+
+
+def test_set_ke_invalidates_the_hierarchy():
+    # a hierarchy built with the old Ke is not used with the new one: the per-call solvers ask for a new set-up,
+    # the design loop rebuilds by itself
+    import algorithmengineering_altproject_b200 as t3d
+    for cyc in (t3d.T3D_VCYCLE_ADAPTED, t3d.T3D_VCYCLE_STANDARD):
+        P = t3d.Problem(8, 16, 8, mg_vcycle=cyc)
+        E = np.full(P.ne, 0.5)
+        P.make_diagonal_preconditioner_from_static(E)
+        P.set_ke(2.0 * P.ke())
+        with pytest.raises(t3d.T3DError) as e:
+            P.vcycle(np.ones(P.nf))
+        assert "set up" in str(e.value) or "mg_setup" in str(e.value), str(e.value)
+        P.make_diagonal_preconditioner_from_static(E)
+        assert np.all(np.isfinite(P.vcycle(np.ones(P.nf))))
+        P.close()
