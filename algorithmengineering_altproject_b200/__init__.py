@@ -393,11 +393,17 @@ class Problem:
         _check(self._lib.t3d_design_step(self._h, C.byref(rec)))
         return rec.as_dict()
 
-    def design_step_host(self, x_in):
+    def design_step_host(self, x_in, out=None):
+        """One design iteration with the design field passed through host memory: x_in (reference element
+        order) in, the updated field out.  `out`, when given, is a caller-owned float32 array of ne values
+        (e.g. pinned memory reused across iterations) that receives the result; else a new array does."""
         rec = IterRecord()
-        xo = np.zeros(self.ne, dtype=np.float32)
-        _check(self._lib.t3d_design_step_host(self._h, _f32(x_in), xo, C.byref(rec)))
-        return xo, rec.as_dict()
+        if out is None:
+            out = np.zeros(self.ne, dtype=np.float32)
+        elif out.dtype != np.float32 or out.shape != (self.ne,) or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous float32 array of %d values" % self.ne)
+        _check(self._lib.t3d_design_step_host(self._h, _f32(x_in), out, C.byref(rec)))
+        return out, rec.as_dict()
 
     def density(self):
         x = np.zeros(self.ne, dtype=np.float32)

@@ -11,8 +11,8 @@ iterations are run by both the mixed and the plain FP64 form from the same densi
 `value` = design iterations/s
 over the whole job, timed on the device (CUDA events recorded by the library on its stream; max
 over ranks); `e2e` = the same metric through the host-buffer C-ABI call t3d_design_step_host
-(H2D of the design field, D2H of the updated field, wall clock).  Multi-GPU runs are independent
-replicas (one design per GPU, no collective on the data path).
+(H2D of the design field, D2H of the updated field, between two pinned host buffers, wall clock).
+Multi-GPU runs are independent replicas (one design per GPU, no collective on the data path).
 
 --impl reference times the reference's own CPU implementation (oracle/_ref/libt3d_ref.so, the
 unmodified reference sources) on this host's cores with a bounded sample of the same workload:
@@ -356,16 +356,18 @@ def run_b200(args):
     mv_ms = P.profile(t3d.T3D_PROFILE_MATVEC32 if mixed else t3d.T3D_PROFILE_MATVEC, args.reps)
     vc_ms = P.profile(t3d.T3D_PROFILE_VCYCLE32 if mixed else t3d.T3D_PROFILE_VCYCLE, max(1, args.reps // 2))
 
-    # end to end through host buffers: the design field goes host -> device -> host every iteration
+    # end to end through host buffers: the design field goes host -> device -> host every iteration, between
+    # two pinned host buffers that trade roles (this iteration's output is the next one's input)
     e2e = None
     if not args.no_e2e:
         x = torch.empty(P.ne, dtype=torch.float32, pin_memory=True).numpy()
+        xo = torch.empty(P.ne, dtype=torch.float32, pin_memory=True).numpy()
         x[:] = P.density()
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            xo, _ = P.design_step_host(x)
-            x[:] = xo
+            P.design_step_host(x, out=xo)
+            x, xo = xo, x
         barrier()
         e2e = time.perf_counter() - t0
 

@@ -120,3 +120,25 @@ def test_fp32_breakdown_stops_the_inner_solve_without_nan():
     r = M.design_step()
     assert np.isfinite(cs) and np.isfinite(r["obj"])
     M.close()
+
+
+def test_host_buffer_design_step_matches_the_resident_one():
+    # t3d_design_step_host (the design field through host memory, as a caller without device buffers uses
+    # it) gives the resident design step's result bit for bit, into a caller-owned output buffer reused
+    # across iterations
+    import algorithmengineering_altproject_b200 as t3d
+    A = t3d.Problem(10, 20, 10, precision=t3d.T3D_MIXED)
+    B = t3d.Problem(10, 20, 10, precision=t3d.T3D_MIXED)
+    assert A.design_init(0.3) == B.design_init(0.3)
+    x, out = A.density(), np.empty(A.ne, dtype=np.float32)
+    for _ in range(3):
+        xo, ra = A.design_step_host(x, out=out)
+        rb = B.design_step()
+        assert xo is out
+        np.testing.assert_array_equal(out, B.density())
+        assert ra["obj"] == rb["obj"] and ra["pcg_iters"] == rb["pcg_iters"], (ra, rb)
+        x = out.copy()
+    with pytest.raises(ValueError):
+        A.design_step_host(x, out=np.empty(A.ne, dtype=np.float64))
+    A.close()
+    B.close()
