@@ -137,8 +137,7 @@ struct Context {
     float* E32 = nullptr;
     float *r32 = nullptr, *d32 = nullptr, *z32 = nullptr, *p32 = nullptr, *Ap32 = nullptr;
     MgLevel32 lv32[8]{};
-    float* ra1_32[8]{};
-    float* ra2_32[8]{};
+    float* ra1_32[8]{};         // x-pass buffer of the FP32 restriction (its y and z passes are fused)
     PcgScalars* S32 = nullptr;
     cudaGraphExec_t pcg32_graph = nullptr;
     int64_t pcg32_graph_launches = 0;
@@ -308,7 +307,6 @@ static int build_mixed(Context* c) {
     for (int l = 0; l + 1 < c->nlev; ++l) {
         const MgLevel &Lf = c->lv[l], &Lc = c->lv[l + 1];
         CHECK(c->alloc(&c->ra1_32[l], (size_t)3 * (Lf.nz + 1) * (Lf.ny + 1) * (Lc.nx + 1)));
-        CHECK(c->alloc(&c->ra2_32[l], (size_t)3 * (Lf.nz + 1) * (Lc.ny + 1) * (Lc.nx + 1)));
     }
     float k32[576];
     for (int i = 0; i < 576; ++i) k32[i] = (float)c->Ke_h[i];
@@ -859,8 +857,8 @@ static void vcycle32(Context* c, const float* r, float* z, PcgScalars* S, RedSlo
     for (int l = 0; l + 1 < L; ++l) c->launches += c->lv32[l + 1].span == 2 ? 2 : 3;
     c->launches += 1;
     for (int l = 0; l + 1 < L; ++l)
-        launch_restrict32(c->lv32[l + 1], c->lv32[l], l == 0 ? r : c->lv32[l].r, c->lv32[l + 1].r, c->ra1_32[l],
-                          c->ra2_32[l], S, c->st);
+        launch_restrict32(c->lv32[l + 1], c->lv32[l], l == 0 ? r : c->lv32[l].r, c->lv32[l + 1].r, c->ra1_32[l], S,
+                          c->st);
     launch_coarse_solve32(c->lv32[L - 1], c->Xc, c->Nc, c->chol_status, S, c->st);
     for (int l = L - 2; l >= 1; --l)
         launch_prolong_smooth32(c->lv32[l + 1], c->lv32[l], c->lv32[l + 1].x, c->lv32[l].r, c->lv32[l].x,

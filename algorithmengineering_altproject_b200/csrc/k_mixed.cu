@@ -521,9 +521,8 @@ void launch_matvec32(const Grid& g, const float* Ke, const float* E, const uint8
 }
 // x pass then a fused y-z pass on the finest transition (span 4); one fused x-y-z pass on the
 // coarser ones (span 2), whose fine residual sits in L2.
-void launch_restrict32(const MgLevel32& Lc, const MgLevel32& Lf, const float* rf, float* rc, float* a1, float* a2,
+void launch_restrict32(const MgLevel32& Lc, const MgLevel32& Lf, const float* rf, float* rc, float* a1,
                        const PcgScalars* S, cudaStream_t s) {
-    (void)a2;
     const int64_t n1 = (int64_t)(Lf.nz + 1) * (Lf.ny + 1) * (Lc.nx + 1);
     if (Lc.span == 4) {
         k_restrict_x32<<<blocks_for(n1, 256), 256, 0, s>>>(Lc, Lf, rf, a1, S);

@@ -220,7 +220,8 @@ void launch_mixed_residual(const Grid& g, const double* b, const double* Au, flo
 void launch_mixed_accumulate(const Grid& g, double* u, const float* d, cudaStream_t s);
 void launch_matvec32(const Grid& g, const float* Ke, const float* E, const uint8_t* mask, const float* u, float* y,
                      RedSlot dot, PcgScalars* S, cudaStream_t s);
-void launch_restrict32(const MgLevel32& Lc, const MgLevel32& Lf, const float* rf, float* rc, float* a1, float* a2,
+// rc = normalised restriction of rf; a1 holds the x-pass result on span-4 transitions
+void launch_restrict32(const MgLevel32& Lc, const MgLevel32& Lf, const float* rf, float* rc, float* a1,
                        const PcgScalars* S, cudaStream_t s);
 void launch_prolong_smooth32(const MgLevel32& Lc, const MgLevel32& Lf, const float* xc, const float* rf, float* xf,
                              float w, const PcgScalars* S, cudaStream_t s);
