@@ -465,8 +465,10 @@ static int create(int nely, int nelx, int nelz, const t3d_params* prm, const t3d
     for (auto& e : c->ev) T3D_CUDA_OK(cudaEventCreate(&e));
     c->use_graph = std::getenv("T3D_NO_GRAPH") == nullptr;
 
-    // padding (padding.hpp:42-53, fea.cpp:189-197)
-    const uint64_t nvox = (uint64_t)nelx * nely * nelz;
+    // padding (padding.hpp:42-53, fea.cpp:189-197): the level count comes from the number of solid voxels,
+    // the whole cuboid for the built-in problems, the file's solid voxels for an external model
+    // (numel(find(voxelizedVolume_)), TOP3D_XL.m:1765-1774)
+    const uint64_t nvox = c->vox ? (uint64_t)c->vox->num_solid : (uint64_t)nelx * nely * nelz;
     const int L = pad_levels(nvox);
     const int nx = pad_dim(nelx, L), ny = pad_dim(nely, L), nz = pad_dim(nelz, L);
     if ((int64_t)(nx + 1) * (ny + 1) * (nz + 1) * 3 >= (int64_t)INT32_MAX)

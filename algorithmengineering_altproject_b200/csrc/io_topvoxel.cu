@@ -205,6 +205,11 @@ static bool parse_topvoxel_impl(const char* path, VoxelModel* out, std::string* 
             for (int c = 0; c < 3; ++c) m.case_f[(size_t)(idx - 2)].push_back(kv.second[c]);
         }
     }
+    // A node loaded in any load case is not fixed: FEA_ApplyBoundaryCondition removes, case after case,
+    // every fixation row whose node carries that case's load (setdiff, TOP3D_XL.m:1326-1331)
+    for (const auto& kv : load) fix.erase(kv.first);
+    for (const auto& nodes : m.case_node)
+        for (int64_t nd : nodes) fix.erase(nd);
     for (const auto& kv : fix) {
         const uint8_t bits = (uint8_t)((kv.second[0] ? 1 : 0) | (kv.second[1] ? 2 : 0) | (kv.second[2] ? 4 : 0));
         if (!bits) continue;

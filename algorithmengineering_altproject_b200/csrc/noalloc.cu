@@ -17,6 +17,7 @@
 #include "kernels.hpp"
 #include "red.cuh"
 
+#include <atomic>
 #include <cstdint>
 #include <string>
 
@@ -31,8 +32,10 @@ constexpr int NOALLOC_MAX_DEVICES = 64;
 // partials[0 .. NOALLOC_MAX_BLOCKS-1], then the arrival counter (as the first 4 bytes of the last slot)
 static __device__ __align__(256) double g_scratch[NOALLOC_MAX_BLOCKS + 1];
 
-// device address of g_scratch per device ordinal, filled by the first call on each device
-double* g_scratch_addr[NOALLOC_MAX_DEVICES];
+// device address of g_scratch per device ordinal, filled by the first call on each device.  Atomic slots:
+// host threads may make their first calls concurrently (each stores the same address).  The address is the
+// one in the device's primary context, the context the CUDA runtime makes current.
+std::atomic<double*> g_scratch_addr[NOALLOC_MAX_DEVICES];
 
 struct KeArg {
     double k[576];
@@ -91,13 +94,15 @@ int scratch_for_current_device(double** out) {
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return set_cuda_error(e, "cudaGetDevice", __FILE__, __LINE__);
     if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return set_error(T3D_ERR_UNSUPPORTED, "device ordinal too large");
-    if (!g_scratch_addr[dev]) {
+    double* addr = g_scratch_addr[dev].load(std::memory_order_acquire);
+    if (!addr) {
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_scratch);
         if (e != cudaSuccess) return set_cuda_error(e, "cudaGetSymbolAddress(g_scratch)", __FILE__, __LINE__);
-        g_scratch_addr[dev] = static_cast<double*>(p);
+        addr = static_cast<double*>(p);
+        g_scratch_addr[dev].store(addr, std::memory_order_release);
     }
-    *out = g_scratch_addr[dev];
+    *out = addr;
     return T3D_OK;
 }
 

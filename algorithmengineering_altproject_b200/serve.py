@@ -38,6 +38,18 @@ DEFAULT_BYTES_PER_NODE = {T3D_FP64: 900.0, T3D_MIXED: 1100.0}
 MARGIN = 1.15
 
 
+def padded_dims(nelx, nely, nelz, solid=None):
+    """The reference's padded grid (padding.hpp:23-53): L = number of times the solid voxel count (the whole
+    cuboid unless `solid` is given, as for a TopVoxel domain, TOP3D_XL.m:1765-1774), while at least 50,000, is
+    divided by 8 (rounding to nearest), at least 3; each side rounded up to a multiple of 2^L."""
+    nvox, L = (nelx * nely * nelz if solid is None else solid), 0
+    while nvox >= 50000:
+        L += 1
+        nvox = (nvox + 4) // 8
+    step = 1 << max(L, 3)
+    return tuple((n + step - 1) // step * step for n in (nelx, nely, nelz))
+
+
 class DesignRequest:
     def __init__(self, nely, nelx, nelz, V0, load_case=0, voids=(), iters=40, rid=None, keep_density=False):
         self.nely, self.nelx, self.nelz = int(nely), int(nelx), int(nelz)
@@ -50,6 +62,7 @@ class DesignRequest:
         self.arrival = None
         self.topvoxel = None        # path of a TopVoxel design domain (replaces dims, load case and voids)
         self.load_cases = 1
+        self.solid = None           # solid voxels of a TopVoxel domain (they set its padding)
 
     @classmethod
     def from_topvoxel(cls, path, V0, iters=40, rid=None, keep_density=False):
@@ -58,11 +71,12 @@ class DesignRequest:
         req = cls(info["nely"], info["nelx"], info["nelz"], V0, iters=iters, rid=rid, keep_density=keep_density)
         req.topvoxel = str(path)
         req.load_cases = 1 + info["additional_load_cases"]
+        req.solid = info["solid"]
         return req
 
     def padded_nodes(self):
-        # dims of multiples of 8 are never padded (the reference's rule pads to multiples of 2^L)
-        return (self.nelx + 1) * (self.nely + 1) * (self.nelz + 1)
+        nx, ny, nz = padded_dims(self.nelx, self.nely, self.nelz, self.solid)
+        return (nx + 1) * (ny + 1) * (nz + 1)
 
     def spec(self):
         return ProblemSpec.make(self.load_case, self.voids)

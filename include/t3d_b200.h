@@ -232,8 +232,9 @@ int  t3d_profile(struct t3d_context* ctx, int what, int reps, double* ms);
  * 65536+1 doubles (512 KiB per GPU that loads the library, held until exit), one partial per 256
  * padded cells, so grids above 16,777,216 padded cells are rejected with T3D_ERR_UNSUPPORTED.  The
  * first call on a device looks up the array's address for that device (do it before any stream
- * capture).  Every call shares the array: calls that overlap on the GPU race.  Asynchronous on
- * `stream`. */
+ * capture); the address is the one in the device's primary context, so callers that make another
+ * driver context current, or reset the device, are not supported.  Every call shares the array:
+ * calls that overlap on the GPU race.  Asynchronous on `stream`. */
 int  t3d_compliance_noalloc(int nely, int nelx, int nelz, const double* ke576, const double* d_E, const double* d_u,
                             double* d_ce, double* d_C, void* stream);
 

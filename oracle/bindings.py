@@ -154,7 +154,8 @@ def voxel_model_from_rows(nelx, nely, nelz, solid, passive=(), fixations=(), loa
     """The arrays of an external model for `Oracle(..., voxel_model=...)` from 0-based rows: solid and passive
     voxels (x, y, z), fixations (x, y, z, fx, fy, fz) with 0/1 flags, load cases of (x, y, z, Fx, Fy, Fz).
     As in the MATLAB reader (TOP3D_XL.m:529-545): duplicate nodes keep their first row, nodes ascending;
-    all-zero fixation rows fix nothing."""
+    all-zero fixation rows fix nothing.  As in FEA_ApplyBoundaryCondition (TOP3D_XL.m:1326-1331): a node that
+    any load case loads loses its fixation row."""
     vox = np.zeros(nelx * nely * nelz, dtype=np.uint8)
     for x, y, z in solid:
         vox[y + nely * (x + nelx * z)] = 1
@@ -174,6 +175,8 @@ def voxel_model_from_rows(nelx, nely, nelz, solid, passive=(), fixations=(), loa
         nodes += keys
         forces += [v for k in keys for v in rows[k]]
         counts.append(len(keys))
+    for k in nodes:
+        fix.pop(k, None)
     keys = sorted(fix)
     return {"voxel": vox, "fix_node": np.array(keys, dtype=np.int64), "fix_bits": np.array([fix[k] for k in keys],
             dtype=np.uint8), "case_n": np.array(counts, dtype=np.int32), "load_node": np.array(nodes, dtype=np.int64),

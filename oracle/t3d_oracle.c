@@ -1518,7 +1518,14 @@ orc_problem* orc_create_voxel(int nely, int nelx, int nelz, const orc_params* pr
 
 static orc_problem* create_common(orc_problem* P, int nely, int nelx, int nelz) {
     P->nelx = nelx; P->nely = nely; P->nelz = nelz;
-    const int L = pad_levels((uint64_t)nelx * nely * nelz);
+    /* L from the solid voxel count (fea.cpp:190 for the cuboid; numel(find(voxelizedVolume_)) for an external
+     * model, TOP3D_XL.m:1765-1774) */
+    uint64_t nsolid = (uint64_t)nelx * nely * nelz;
+    if (P->voxel) {
+        nsolid = 0;
+        for (int64_t k = 0; k < (int64_t)nelx * nely * nelz; ++k) nsolid += P->voxel[k] != 0;
+    }
+    const int L = pad_levels(nsolid);
     P->nx = pad_dim(nelx, L); P->ny = pad_dim(nely, L); P->nz = pad_dim(nelz, L);
     P->nnx = P->nx + 1; P->nny = P->ny + 1; P->nnz = P->nz + 1;
     P->nn = (int64_t)P->nnx * P->nny * P->nnz;

@@ -14,7 +14,8 @@ Runs the UNMODIFIED reference sources (oracle/_ref/libt3d_ref.so, built by
   few design iterations: per iteration the SIMP moduli, PCG warm start/result/iteration count,
   element compliances, filter input/output and warm-start state, and the final densities.
 
-Usage:  python tests/golden/make_golden.py          (needs /root/reference via oracle/_ref)
+Usage:  python tests/golden/make_golden.py   (needs the reference build oracle/_ref:
+        make -C oracle ref REF=<reference root>)
 """
 import hashlib
 import os

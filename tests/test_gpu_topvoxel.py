@@ -14,6 +14,8 @@
 * The whole design loop on an external domain with passive elements and two load cases matches the
   oracle's restatement (oracle/t3d_oracle.c, external-model path) bit for bit: solid compliance, every
   iteration's objective, PCG count and change, and the final densities.
+  A variant whose fixation list also fixes loaded nodes (of either load case) checks the MATLAB rule that a
+  loaded node loses its fixation (FEA_ApplyBoundaryCondition, TOP3D_XL.m:1326-1331) on both sides.
 * Files the design loop cannot run are refused: no fixation, no load.
 """
 import numpy as np
@@ -166,8 +168,8 @@ def test_two_load_cases_average_the_compliance(tmp_path):
     assert abs(cs[2] - 0.5 * (cs[0] + cs[1])) <= 1e-12 * cs[2], cs
 
 
-@pytest.mark.parametrize("two_cases", [False, True])
-def test_external_design_loop_matches_the_oracle(tmp_path, two_cases):
+@pytest.mark.parametrize("two_cases, fix_loaded", [(False, False), (True, False), (True, True)])
+def test_external_design_loop_matches_the_oracle(tmp_path, two_cases, fix_loaded):
     import algorithmengineering_altproject_b200 as t3d
     from algorithmengineering_altproject_b200.topvoxel import write_topvoxel
     from oracle.bindings import Oracle, voxel_model_from_rows
@@ -175,6 +177,8 @@ def test_external_design_loop_matches_the_oracle(tmp_path, two_cases):
     solid, passive, fix, loads = l_domain(nelx, nely, nelz)
     side = [(nelx, y, 2, 0.0, 1.0 / (nely + 1), 0.0) for y in range(nely + 1)]
     cases = [loads, side] if two_cases else [loads]
+    if fix_loaded:   # fixations on a node of each load case: both rows must be dropped
+        fix = fix + [(nelx, 1, 0, 1, 1, 1), (nelx, 2, 2, 0, 1, 0)]
     path = str(tmp_path / "l.TopVoxel")
     write_topvoxel(path, nelx, nely, nelz, solid, passive=passive, fixations=fix, loads=loads,
                    extra_load_cases=cases[1:])

@@ -89,6 +89,20 @@ def test_topvoxel_requests_are_sized_from_the_file(tmp_path):
     assert srv.log == [0, 1]
 
 
+def test_projection_uses_the_reference_padding():
+    """Admission sizes a request by the padded grid of padding.hpp:23-53, not by its raw sides: sides that are
+    not multiples of 2^L grow, and grids of 25.6M voxels or more pad to multiples of 16 (L = 4)."""
+    assert serve.padded_dims(60, 30, 30) == (64, 32, 32)          # the reference CLI demo's grid
+    assert serve.padded_dims(10, 4, 6) == (16, 8, 8)
+    assert serve.padded_dims(512, 256, 256) == (512, 256, 256)
+    assert serve.padded_dims(500, 250, 250) == (512, 256, 256)    # L = 4: multiples of 16
+    assert serve.padded_dims(200, 100, 100) == (200, 104, 104)    # 2.0M voxels: L = 3
+    assert serve.padded_dims(292, 300, 300) == (304, 304, 304)    # 26M voxels: L = 4, multiples of 16
+    assert serve.padded_dims(292, 300, 300, solid=20_000_000) == (296, 304, 304)   # L = 3 from the solid count
+    r = serve.DesignRequest(4, 10, 6, 0.3)
+    assert r.padded_nodes() == 17 * 9 * 9
+
+
 def test_unexpected_failures_are_reported_on_the_request():
     class Failing(FakeServer):
         def _execute(self, req, res):

@@ -34,6 +34,19 @@ def test_duplicates_zero_rows_passive_and_extra_cases(tmp_path):
     assert info["additional_load_cases"] == 1
 
 
+def test_loaded_nodes_lose_their_fixation(tmp_path):
+    """FEA_ApplyBoundaryCondition (TOP3D_XL.m:1326-1331) drops, for every load case, the fixation rows of the
+    nodes that case loads: a node both fixed and loaded ends up loaded and free."""
+    p = str(tmp_path / "fl.TopVoxel")
+    solid = [(x, y, z) for z in range(2) for x in range(4) for y in range(2)]
+    fix = [(0, y, z, 1, 1, 1) for z in range(3) for y in range(3)] + [(4, 0, 0, 1, 1, 1), (4, 1, 2, 0, 1, 0)]
+    loads = [(4, 0, 0, 0.0, 0.0, -1.0), (4, 2, 0, 0.0, 0.0, -1.0)]
+    write_topvoxel(p, 4, 2, 2, solid, fixations=fix, loads=loads, extra_load_cases=[[(4, 1, 2, 0.0, 1.0, 0.0)]])
+    info = t3d.topvoxel_info(p)
+    assert info["fixed_nodes"] == 9            # the x = 0 face only: both loaded nodes lost their rows
+    assert info["loaded_nodes"] == 2
+
+
 def test_density_column_is_read(tmp_path):
     p = tmp_path / "d.TopVoxel"
     p.write_text("# TopVoxel design domain\nVersion: 1.0\nResolution: 2 2 2\nDensity values: 1\n"
