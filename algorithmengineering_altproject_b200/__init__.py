@@ -100,6 +100,7 @@ _SIGS = {
     "t3d_destroy": (C.c_int, [_CTX]),
     "t3d_get_info": (C.c_int, [_CTX, C.POINTER(Info)]),
     "t3d_last_error": (C.c_char_p, []),
+    "t3d_voxel_ke": (C.c_int, [C.c_double, C.c_double, _f64p]),
     "t3d_get_ke": (C.c_int, [_CTX, _f64p]),
     "t3d_set_ke": (C.c_int, [_CTX, _f64p]),
     "t3d_get_element_map": (C.c_int, [_CTX, _i32p]),
@@ -116,6 +117,7 @@ _SIGS = {
     "t3d_mg_get_mask": (C.c_int, [_CTX, C.c_int, _u8p]),
     "t3d_mg_coarse_matrix": (C.c_int, [_CTX, _f64p, _f64p]),
     "t3d_filter_apply": (C.c_int, [_CTX, _f32p, _f32p]),
+    "t3d_filter_setup": (C.c_int, [_CTX, C.c_float]),
     "t3d_filter_get_state": (C.c_int, [_CTX, _f64p, _f64p, _f64p]),
     "t3d_filter_set_state": (C.c_int, [_CTX, _f64p, _f64p]),
     "t3d_simp": (C.c_int, [_CTX, _f32p, _f64p]),
@@ -169,6 +171,13 @@ def topvoxel_info(path):
     _check(library().t3d_topvoxel_info(os.fsencode(path), v))
     keys = ("nelx", "nely", "nelz", "solid", "passive", "fixed_nodes", "loaded_nodes", "additional_load_cases")
     return dict(zip(keys, (int(x) for x in v)))
+
+
+def ComputeVoxelKe(nu=0.3, cellSize=1.0):
+    """The reference's ComputeVoxelKe (fea.hpp:37): unit-modulus hex8 stiffness, 24x24 (host only)."""
+    Ke = np.zeros(576)
+    _check(library().t3d_voxel_ke(float(nu), float(cellSize), Ke))
+    return Ke.reshape(24, 24)
 
 
 def default_params(**kw):
@@ -351,6 +360,10 @@ class Problem:
         dst = np.zeros(self.ne, dtype=np.float32)
         _check(self._lib.t3d_filter_apply(self._h, _f32(src), dst))
         return dst
+
+    def SetupPDEFilter(self, filterRadius):
+        """SetupPDEFilter (filter.hpp:17) for another radius; resets the filter's warm start."""
+        _check(self._lib.t3d_filter_setup(self._h, float(filterRadius)))
 
     def filter_state(self):
         lx, lr, dg = np.zeros(self.nn), np.zeros(self.nn), np.zeros(self.nn)

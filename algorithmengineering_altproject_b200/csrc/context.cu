@@ -1266,6 +1266,14 @@ int t3d_get_info(const t3d_context* ctx, t3d_info* info) {
     return T3D_OK;
 }
 
+int t3d_voxel_ke(double nu, double cell_size, double* ke) {
+    if (!ke) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    if (!(cell_size > 0.0) || !std::isfinite(cell_size) || !(nu > -1.0 && nu < 0.5))
+        return t3d::set_error(T3D_ERR_INVALID, "need cell_size > 0 and -1 < nu < 0.5");
+    t3d::hex8_stiffness(nu, cell_size, ke);
+    return T3D_OK;
+}
+
 int t3d_get_ke(const t3d_context* ctx, double* ke) {
     if (!ctx || !ke) return t3d::set_error(T3D_ERR_INVALID, "null argument");
     std::memcpy(ke, ctx->Ke_h, sizeof ctx->Ke_h);
@@ -1454,6 +1462,20 @@ int t3d_filter_apply(t3d_context* ctx, const float* src, float* dst) {
     CHECK(t3d::upload_cells_f32(ctx, src, ctx->xdc));
     CHECK(t3d::filter_apply(ctx, ctx->xdc, ctx->dcf));
     return t3d::download_cells_f32(ctx, ctx->dcf, dst);
+}
+
+int t3d_filter_setup(t3d_context* ctx, float rmin) {
+    API_GUARD(ctx);
+    if (!(rmin > 0.0f) || !std::isfinite(rmin)) return t3d::set_error(T3D_ERR_INVALID, "filter radius must be positive");
+    ctx->prm.filter_rmin = rmin;
+    double kf[72];
+    t3d::filter_kernel(rmin, kf);
+    T3D_CUDA_OK(cudaMemcpyAsync(ctx->kf, kf, sizeof kf, cudaMemcpyHostToDevice, ctx->st));
+    t3d::launch_filter_diag(ctx->g, ctx->solid, ctx->kf, ctx->fdiag, ctx->st);
+    CHECK(t3d::launch_check("filter set-up"));
+    T3D_CUDA_OK(cudaMemsetAsync(ctx->flastx, 0, ctx->g.NN * sizeof(double), ctx->st));
+    T3D_CUDA_OK(cudaMemsetAsync(ctx->flastrhs, 0, ctx->g.NN * sizeof(double), ctx->st));
+    return t3d::sync(ctx);
 }
 
 int t3d_filter_get_state(t3d_context* ctx, double* last_x, double* last_rhs, double* diag) {

@@ -149,6 +149,9 @@ int  t3d_get_info(const struct t3d_context* ctx, t3d_info* info);
 const char* t3d_last_error(void);
 
 /* --------------------------------------------------------------- model data (reference layouts) */
+/* ComputeVoxelKe (fea.hpp:37, fea.cpp:117-179): unit-modulus hex8 stiffness of a cubic voxel of edge
+ * cell_size, row-major 24x24, local DOF 3a+c; host only, no device or context needed */
+int  t3d_voxel_ke(double nu, double cell_size, double* ke576);
 int  t3d_get_ke(const struct t3d_context* ctx, double* ke576);            /* ComputeVoxelKe fea.cpp:117 */
 int  t3d_set_ke(struct t3d_context* ctx, const double* ke576);   /* invalidates the MG hierarchy: the next
                                                                      design step rebuilds it, t3d_pcg / t3d_vcycle
@@ -182,6 +185,9 @@ int  t3d_mg_get_mask(struct t3d_context* ctx, int level, uint8_t* mask);
 int  t3d_mg_coarse_matrix(struct t3d_context* ctx, const double* ele_E, double* Kc);
 /* ApplyPDEFilter (filter.hpp:28, filter.cpp:175-275); warm-start state lives in the context */
 int  t3d_filter_apply(struct t3d_context* ctx, const float* src, float* dst);
+/* SetupPDEFilter (filter.hpp:17, filter.cpp:9-75) for radius rmin (cells): kernel r^2 KEF0 + KEF1,
+ * inverse-row-sum preconditioner, zero warm start (t3d_create sets it up for params.filter_rmin) */
+int  t3d_filter_setup(struct t3d_context* ctx, float rmin);
 int  t3d_filter_get_state(struct t3d_context* ctx, double* last_x, double* last_rhs, double* diag_precond);
 int  t3d_filter_set_state(struct t3d_context* ctx, const double* last_x, const double* last_rhs);
 /* SIMP moduli (driver.cpp:117-121) and sensitivities (driver.cpp:151-157) */

@@ -18,7 +18,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "_build", "libt3d_oracle.so")
-REF_SO = os.path.join(HERE, "_ref", "libt3d_ref.so")
+# T3D_REF_SO selects another build of the same reference sources (the fixture scripts use the build
+# without -ffast-math, oracle/_ref/nofm, to measure the reference's build-to-build drift)
+REF_SO = os.environ.get("T3D_REF_SO") or os.path.join(HERE, "_ref", "libt3d_ref.so")
 
 _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _f32p = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
