@@ -285,12 +285,13 @@ static int build_levels(Context* c) {
 
 static int build_mixed(Context* c) {
     const Grid& g = c->g;
+    // finest-level FP32 images are pitched (Grid::px, Grid::pex); their pads stay zero
     CHECK(c->alloc(&c->Ke32, 576));
-    CHECK(c->alloc(&c->E32, g.NE));
-    T3D_CUDA_OK(cudaMemsetAsync(c->E32, 0, g.NE * sizeof(float), c->st));
+    CHECK(c->alloc(&c->E32, g.NEp));
+    T3D_CUDA_OK(cudaMemsetAsync(c->E32, 0, g.NEp * sizeof(float), c->st));
     for (float** v : {&c->r32, &c->d32, &c->z32, &c->p32, &c->Ap32}) {
-        CHECK(c->alloc(v, 3 * g.NN));
-        T3D_CUDA_OK(cudaMemsetAsync(*v, 0, 3 * g.NN * sizeof(float), c->st));
+        CHECK(c->alloc(v, 3 * g.NNp));
+        T3D_CUDA_OK(cudaMemsetAsync(*v, 0, 3 * g.NNp * sizeof(float), c->st));
     }
     CHECK(c->alloc(&c->S32, 1));
     T3D_CUDA_OK(cudaMemsetAsync(c->S32, 0, sizeof(PcgScalars), c->st));
@@ -298,7 +299,10 @@ static int build_mixed(Context* c) {
         const MgLevel& L = c->lv[l];
         MgLevel32& M = c->lv32[l];
         M.nx = L.nx; M.ny = L.ny; M.nz = L.nz; M.span = L.span; M.nn = L.nn; M.mask = L.mask;
-        CHECK(c->alloc(&M.diag, 3 * L.nn));
+        M.pitch = l == 0 ? g.px : L.nx + 1;
+        M.cs = l == 0 ? g.NNp : L.nn;
+        CHECK(c->alloc(&M.diag, 3 * M.cs));
+        T3D_CUDA_OK(cudaMemsetAsync(M.diag, 0, 3 * M.cs * sizeof(float), c->st));
         if (l > 0) {
             CHECK(c->alloc(&M.r, 3 * L.nn));
             CHECK(c->alloc(&M.x, 3 * L.nn));
@@ -703,7 +707,10 @@ static int mg_setup(Context* c) {
         launch_coarse_inverse(c->Lrow, c->Nc, c->chol_status, c->Xc, c->st);
     }
     if (c->mixed) {
-        for (int l = 0; l < c->nlev; ++l) launch_recip_diag32(3 * c->lv[l].nn, c->lv[l].diag, c->lv32[l].diag, c->st);
+        for (int l = 0; l < c->nlev; ++l) {
+            const MgLevel32& M = c->lv32[l];
+            launch_recip_diag32(3 * (int64_t)(M.ny + 1) * (M.nz + 1), M.nx + 1, M.pitch, c->lv[l].diag, M.diag, c->st);
+        }
         c->launches += c->nlev;
     }
     c->mg_ready = true;
@@ -899,7 +906,7 @@ static int mixed_solve(Context* c, double tol, int maxit, int* iters) {
     if (!c->mg_ready) return set_error(T3D_ERR_INVALID, "multigrid preconditioner not set up");
     CHECK(ensure_pcg32_graph(c));
     const Grid& g = c->g;
-    launch_cast(g.NE, c->E, c->E32, c->st);
+    launch_cells_to32(g, c->E, c->E32, c->st);
     launch_dot(g, 3, c->b, c->b, c->slot[3], c->scal + 5, c->st);
     c->launches += 2;
     T3D_CUDA_OK(cudaMemcpyAsync(c->scal_h + 5, c->scal + 5, sizeof(double), cudaMemcpyDeviceToHost, c->st));
@@ -923,7 +930,7 @@ static int mixed_solve(Context* c, double tol, int maxit, int* iters) {
         init.first = 1;
         T3D_CUDA_OK(cudaMemcpyAsync(c->S32, &init, sizeof init, cudaMemcpyHostToDevice, c->st));
         vcycle32(c, c->r32, c->z32, c->S32, c->slot[2]);
-        T3D_CUDA_OK(cudaMemcpyAsync(c->p32, c->z32, 3 * g.NN * sizeof(float), cudaMemcpyDeviceToDevice, c->st));
+        T3D_CUDA_OK(cudaMemcpyAsync(c->p32, c->z32, 3 * g.NNp * sizeof(float), cudaMemcpyDeviceToDevice, c->st));
         int queued = 0, chunk = 0;
         bool done = false;
         while (queued < budget && !done) {
@@ -1347,11 +1354,11 @@ int t3d_matvec32(t3d_context* ctx, const double* E, const double* u, double* y) 
     if (!ctx->mixed) return t3d::set_error(T3D_ERR_INVALID, "FP32 kernels need precision T3D_MIXED");
     CHECK(t3d::upload_cells_f64(ctx, E, ctx->E));
     CHECK(t3d::upload_free(ctx, u, ctx->p));
-    t3d::launch_cast(ctx->g.NE, ctx->E, ctx->E32, ctx->st);
-    t3d::launch_cast(3 * ctx->g.NN, ctx->p, ctx->p32, ctx->st);
+    t3d::launch_cells_to32(ctx->g, ctx->E, ctx->E32, ctx->st);
+    t3d::launch_nodes_to32(ctx->g, ctx->p, ctx->p32, ctx->st);
     ctx->launches += 2;
     t3d::matvec32(ctx, ctx->p32, ctx->Ap32, t3d::RedSlot{nullptr, nullptr}, nullptr);
-    t3d::launch_widen(3 * ctx->g.NN, ctx->Ap32, ctx->Ap, ctx->st);
+    t3d::launch_nodes_from32(ctx->g, ctx->Ap32, ctx->Ap, ctx->st);
     ctx->launches += 1;
     CHECK(t3d::launch_check("matvec32"));
     return t3d::download_free(ctx, ctx->Ap, y);
@@ -1382,11 +1389,11 @@ int t3d_vcycle32(t3d_context* ctx, const double* r, double* z) {
     if (!ctx->mixed) return t3d::set_error(T3D_ERR_INVALID, "FP32 kernels need precision T3D_MIXED");
     if (!ctx->mg_ready) return t3d::set_error(T3D_ERR_INVALID, "t3d_mg_setup not called");
     CHECK(t3d::upload_free(ctx, r, ctx->r));
-    t3d::launch_cast(3 * ctx->g.NN, ctx->r, ctx->r32, ctx->st);
+    t3d::launch_nodes_to32(ctx->g, ctx->r, ctx->r32, ctx->st);
     T3D_CUDA_OK(cudaMemsetAsync(ctx->S32, 0, sizeof(t3d::PcgScalars), ctx->st));
     ctx->launches += 1;
     t3d::vcycle32(ctx, ctx->r32, ctx->z32, ctx->S32, ctx->slot[2]);
-    t3d::launch_widen(3 * ctx->g.NN, ctx->z32, ctx->z, ctx->st);
+    t3d::launch_nodes_from32(ctx->g, ctx->z32, ctx->z, ctx->st);
     ctx->launches += 1;
     CHECK(t3d::launch_check("vcycle32"));
     return t3d::download_free(ctx, ctx->z, z);
@@ -1611,9 +1618,9 @@ int t3d_profile(t3d_context* ctx, int what, int reps, double* ms) {
     T3D_CUDA_OK(cudaMemsetAsync(ctx->S, 0, sizeof(t3d::PcgScalars), ctx->st));
     if (ctx->mixed) {   // the FP32 kernels see the FP32 images of the current E, p and r
         T3D_CUDA_OK(cudaMemsetAsync(ctx->S32, 0, sizeof(t3d::PcgScalars), ctx->st));
-        t3d::launch_cast(ctx->g.NE, ctx->E, ctx->E32, ctx->st);
-        t3d::launch_cast(3 * ctx->g.NN, ctx->p, ctx->p32, ctx->st);
-        t3d::launch_cast(3 * ctx->g.NN, ctx->r, ctx->r32, ctx->st);
+        t3d::launch_cells_to32(ctx->g, ctx->E, ctx->E32, ctx->st);
+        t3d::launch_nodes_to32(ctx->g, ctx->p, ctx->p32, ctx->st);
+        t3d::launch_nodes_to32(ctx->g, ctx->r, ctx->r32, ctx->st);
     }
     auto once = [&]() {
         if (what == T3D_PROFILE_MATVEC) {

@@ -133,7 +133,9 @@ __global__ void __launch_bounds__(BX * BY, MINB)
     if (S != nullptr && blockIdx.x == 0 && threadIdx.x == 0) S->xit = S->it;   // last alpha is in x
     if (S != nullptr && S->done) return;
     const int tx = threadIdx.x % BX, ty = threadIdx.x / BX;
-    const int64_t NN = g.NN, NXY = (int64_t)g.nnx * g.nny, EXY = (int64_t)g.ex * g.ey;
+    // FP32 images are pitched (rows of g.px nodes, g.pex cells); the node mask is not
+    const int64_t NN = g.NNp, NXY = (int64_t)g.px * g.nny, EXY = (int64_t)g.pex * g.ey;
+    const int64_t MXY = (int64_t)g.nnx * g.nny;
     // besides its own node, thread row 0 loads the footprint's last row, thread row 1 its last column
     const int ex_kind = (ty == 0) ? 1 : ((ty == 1 && tx < PY) ? 2 : 0);
     double part = 0.0;
@@ -153,9 +155,9 @@ __global__ void __launch_bounds__(BX * BY, MINB)
         const bool owner = tx > 0 && ty > 0 && own_xy;
         // plane-0 offsets (32-bit: 3 NN < 2^31); plane q adds q * NXY (nodes) or q * EXY (the layer
         // below plane q is q-1)
-        const int own_off = own_xy ? cy * g.nnx + cx : 0;
-        const int ext_off = ext_xy ? exy * g.nnx + exx : 0;
-        const int e_off = e_in ? (int)g.cell(cx, cy, -1) : 0;
+        const int own_off = own_xy ? cy * g.px + cx : 0;
+        const int ext_off = ext_xy ? exy * g.px + exx : 0;
+        const int e_off = e_in ? (int)g.pcell(cx, cy, -1) : 0;
         const unsigned own_s = (unsigned)__cvta_generic_to_shared(&sm.plane[0][ty][tx].x);
         const unsigned ext_s = (unsigned)__cvta_generic_to_shared(
             ex_kind == 1 ? &sm.plane[0][BY][tx].x : &sm.plane[0][min(tx, PY - 1)][BX].x);
@@ -189,7 +191,8 @@ __global__ void __launch_bounds__(BX * BY, MINB)
         float4 h1 = make_float4(0.f, 0.f, 0.f, 0.f), h2 = h1;     // own node values of planes pz-1, pz-2
         float k0 = 0.f, k1 = 0.f, k2 = 0.f;                      // own element's corner (0,0) of plane pz-2
         int mk_next = 0;                                         // mask byte of plane pz-1
-        const int node_off = owner ? cy * g.nnx + cx : 0;
+        const int node_off = owner ? cy * g.px + cx : 0;
+        const int mask_off = owner ? cy * g.nnx + cx : 0;
 #pragma unroll 2
         for (int it = 0; it <= nplanes; ++it) {
             const int pz = Z0 - 1 + it;
@@ -214,7 +217,7 @@ __global__ void __launch_bounds__(BX * BY, MINB)
                 if (dot.partial)   // the node's 3 FP32 products summed in FP32, accumulated in FP64
                     part += (double)fmaf(h2.z, y2, fmaf(h2.y, y1, h2.x * y0));
             }
-            if (owner && pz - 1 >= Z0 && pz - 1 < Z1) mk_next = mask[node_off + (pz - 1) * (int)NXY];
+            if (owner && pz - 1 >= Z0 && pz - 1 < Z1) mk_next = mask[mask_off + (pz - 1) * (int)MXY];
             if (!PACK && it < nplanes) {
                 const int s = it % STAGES;
                 const float4 a = sm.plane[s][ty][tx], b = sm.plane[s][ty][tx + 1], c = sm.plane[s][ty + 1][tx],

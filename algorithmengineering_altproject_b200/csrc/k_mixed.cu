@@ -21,44 +21,64 @@ __device__ __forceinline__ float hatf(int i, int s) {   // 1 - |i-(s-1)|/s, exac
     return 1.0f - fabsf((float)(i - (s - 1))) * (1.0f / s);
 }
 
-__global__ void k_cast(int64_t n, const double* __restrict__ a, float* __restrict__ b) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        b[i] = (float)a[i];
+// Row remaps between the unpadded FP64 layouts and the pitched FP32 images: `rows` rows of `len` values
+// at pitch `sp` in the source and `dp` in the destination.  Pads of an FP32 destination are written zero.
+template <class A, class B>
+__global__ void k_rows_convert(int64_t rows, int len, int sp, int dp, const A* __restrict__ a, B* __restrict__ b) {
+    const int w = dp > len ? dp : len;   // FP32 destinations cover their pads
+    const int64_t total = rows * w;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = t / w;
+        const int i = (int)(t - row * w);
+        if (i < len) b[row * dp + i] = (B)a[row * sp + i];
+        else if (i < dp) b[row * dp + i] = (B)0;
+    }
 }
 
-// r64 = b - A u64; r32 = (float)r64; d32 = 0; |r64|^2 into *rn2 (FP64)
 // FP32 image of a level diagonal as the reciprocal 1 / max(1e-30, D) used by the FP32 smoother
-__global__ void k_recip_diag32(int64_t n, const double* __restrict__ d, float* __restrict__ rd) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        rd[i] = (float)(1.0 / (1.0e-30 < d[i] ? d[i] : 1.0e-30));
+__global__ void k_recip_diag32(int64_t rows, int len, int pitch, const double* __restrict__ d, float* __restrict__ rd) {
+    const int64_t total = rows * pitch;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = t / pitch;
+        const int i = (int)(t - row * pitch);
+        const double v = i < len ? d[row * len + i] : 1.0;
+        rd[t] = i < len ? (float)(1.0 / (1.0e-30 < v ? v : 1.0e-30)) : 0.0f;
+    }
 }
 
-__global__ void k_widen(int64_t n, const float* __restrict__ a, double* __restrict__ b) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        b[i] = (double)a[i];
-}
-
+// r64 = b - A u64; r32 = (float)r64 (pitched, pads zero); d32 = 0; |r64|^2 into *rn2 (FP64)
 __global__ void __launch_bounds__(RED_THREADS) k_mixed_residual(Grid g, const double* __restrict__ b,
                                                                 const double* __restrict__ Au,
                                                                 float* __restrict__ r32, float* __restrict__ d32,
                                                                 RedSlot red, double* __restrict__ rn2) {
     __shared__ double sh[32];
-    const int64_t n3 = 3 * g.NN;
+    const int64_t total = 3 * g.NNp;
     double part = 0.0;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (int64_t)gridDim.x * blockDim.x) {
-        const double rv = b[i] - Au[i];
-        r32[i] = (float)rv;
-        d32[i] = 0.0f;
-        part = fma(rv, rv, part);
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total; t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = t / g.px;
+        const int i = (int)(t - row * g.px);
+        float rv32 = 0.0f;
+        if (i < g.nnx) {
+            const int64_t k = row * g.nnx + i;
+            const double rv = b[k] - Au[k];
+            rv32 = (float)rv;
+            part = fma(rv, rv, part);
+        }
+        r32[t] = rv32;
+        d32[t] = 0.0f;
     }
     double tot;
     if (grid_fold(part, red, sh, &tot) && threadIdx.x == 0) *rn2 = tot;
 }
 
-// u64 += d32
-__global__ void k_mixed_accumulate(int64_t n3, double* __restrict__ u, const float* __restrict__ d) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (int64_t)gridDim.x * blockDim.x)
-        u[i] = u[i] + (double)d[i];
+// u64 += d32 (d32 pitched)
+__global__ void k_mixed_accumulate(Grid g, double* __restrict__ u, const float* __restrict__ d) {
+    const int64_t total = 3 * g.NN;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < total; k += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t row = k / g.nnx;
+        const int i = (int)(k - row * g.nnx);
+        u[k] = u[k] + (double)d[row * g.px + i];
+    }
 }
 
 // ---------------------------------------------------------------- K(E) p in FP32
@@ -75,27 +95,28 @@ __global__ void __launch_bounds__(RED_THREADS) k_matvec32(Grid g, const float* _
     if (S != nullptr && S->done) return;
     for (int i = threadIdx.x; i < 576; i += blockDim.x) Ke[i] = Keg[i];
     __syncthreads();
-    const int NN = (int)g.NN;
+    const int NN = (int)g.NN, NP = (int)g.NNp;
     const float* __restrict__ u0 = u;
-    const float* __restrict__ u1 = u + NN;
-    const float* __restrict__ u2 = u + 2 * (int64_t)NN;
+    const float* __restrict__ u1 = u + NP;
+    const float* __restrict__ u2 = u + 2 * (int64_t)NP;
     double part = 0.0;
     for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < NN; n += gridDim.x * blockDim.x) {
         int ix, iy, iz;
         node_ijk(g, n, ix, iy, iz);
+        const int np = (int)g.pnode(ix, iy, iz);
         float y0 = 0.0f, y1 = 0.0f, y2 = 0.0f;
 #pragma unroll 1
         for (int col = 0; col < 8; ++col) {
             const int cx = (((ix - 1) & 1) == (col & 1)) ? ix - 1 : ix;
             const int cy = (((g.ny - iy) & 1) == ((col >> 1) & 1)) ? iy - 1 : iy;
             const int cz = (((iz - 1) & 1) == ((col >> 2) & 1)) ? iz - 1 : iz;
-            const float Ee = E[g.cell(cx, cy, cz)];
+            const float Ee = E[g.pcell(cx, cy, cz)];
             if (Ee <= 1.0e-16f) continue;
             const int a = corner_of(ix - cx, iy - cy, iz - cz);
             float ue[24];
 #pragma unroll
             for (int b = 0; b < 8; ++b) {
-                const int m = (int)g.node(cx + corner_dx(b), cy + corner_dy(b), cz + corner_dz(b));
+                const int m = (int)g.pnode(cx + corner_dx(b), cy + corner_dy(b), cz + corner_dz(b));
                 ue[3 * b + 0] = u0[m];
                 ue[3 * b + 1] = u1[m];
                 ue[3 * b + 2] = u2[m];
@@ -120,13 +141,13 @@ __global__ void __launch_bounds__(RED_THREADS) k_matvec32(Grid g, const float* _
         if (mk & 1) y0 = 0.0f;
         if (mk & 2) y1 = 0.0f;
         if (mk & 4) y2 = 0.0f;
-        y[n] = y0;
-        y[NN + n] = y1;
-        y[2 * (int64_t)NN + n] = y2;
+        y[np] = y0;
+        y[NP + np] = y1;
+        y[2 * (int64_t)NP + np] = y2;
         if (dot.partial) {
-            part = fma((double)u0[n], (double)y0, part);
-            part = fma((double)u1[n], (double)y1, part);
-            part = fma((double)u2[n], (double)y2, part);
+            part = fma((double)u0[np], (double)y0, part);
+            part = fma((double)u1[np], (double)y1, part);
+            part = fma((double)u2[np], (double)y2, part);
         }
     }
     if (dot.partial) {
@@ -146,8 +167,8 @@ __global__ void k_restrict_x32(MgLevel32 Lc, MgLevel32 Lf, const float* __restri
     const int cx = (int)(t % cnx);
     const int64_t row = t / cnx;
     const int s = Lc.span, ws = 2 * s - 1;
-    const int64_t fNN = Lf.nn;
-    const float* __restrict__ src = rf + row * fnx;
+    const int64_t fNN = Lf.cs;
+    const float* __restrict__ src = rf + row * Lf.pitch;
     float v0 = 0.0f, v1 = 0.0f, v2 = 0.0f;
     for (int ix = 0; ix < ws; ++ix) {
         const int fx = cx * s + ix - (s - 1);
@@ -226,7 +247,7 @@ __global__ void __launch_bounds__(256) k_restrict_xyz32(MgLevel32 Lc, MgLevel32 
     const int cnx = Lc.nx + 1, cny = Lc.ny + 1;
     const int fnx = Lf.nx + 1, fny = Lf.ny + 1, fnz = Lf.nz + 1;
     const int cx = n % cnx, cy = (n / cnx) % cny, cz = n / (cnx * cny);
-    const int fNN = (int)Lf.nn;
+    const int fNN = (int)Lf.cs;
     float v0 = 0.0f, v1 = 0.0f, v2 = 0.0f;
 #pragma unroll
     for (int iz = 0; iz < WS; ++iz) {
@@ -237,7 +258,7 @@ __global__ void __launch_bounds__(256) k_restrict_xyz32(MgLevel32 Lc, MgLevel32 
         for (int iy = 0; iy < WS; ++iy) {
             const int fy = cy * SP + iy - (SP - 1);
             if (fy < 0 || fy >= fny) continue;
-            const float* __restrict__ src = rf + (fz * fny + fy) * fnx;
+            const float* __restrict__ src = rf + (fz * fny + fy) * Lf.pitch;
             float s0 = 0.0f, s1 = 0.0f, s2 = 0.0f;
 #pragma unroll
             for (int ix = 0; ix < WS; ++ix) {
@@ -270,7 +291,7 @@ __global__ void __launch_bounds__(256) k_restrict_xyz32(MgLevel32 Lc, MgLevel32 
 __device__ __forceinline__ void prolong_node32(const MgLevel32& Lc, const float* __restrict__ xc, int fx, int fy,
                                                int fz, int sh, float P[3]) {
     const int s = 1 << sh;
-    const int cnx = Lc.nx + 1, cny = Lc.ny + 1;
+    const int cny = Lc.ny + 1;
     int cx = fx >> sh, cy = fy >> sh, cz = fz >> sh;
     int rx = fx & (s - 1), ry = fy & (s - 1), rz = fz & (s - 1);
     if (cx >= Lc.nx) { cx = Lc.nx - 1; rx = s; }
@@ -280,13 +301,14 @@ __device__ __forceinline__ void prolong_node32(const MgLevel32& Lc, const float*
     const float wx1 = rx * inv, wx0 = 1.0f - wx1;
     const float wy1 = ry * inv, wy0 = 1.0f - wy1;
     const float wz1 = rz * inv, wz0 = 1.0f - wz1;
-    const int b = (cz * cny + cy) * cnx + cx;
-    const int pz = cnx * cny;
+    const int b = (cz * cny + cy) * Lc.pitch + cx;
+    const int pz = Lc.pitch * cny;
+    const int cnx_ = Lc.pitch;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        const float* X = xc + c * Lc.nn;
-        const float lo = fmaf(wy1, fmaf(wx1, X[b + cnx + 1], wx0 * X[b + cnx]), wy0 * fmaf(wx1, X[b + 1], wx0 * X[b]));
-        const float hi = fmaf(wy1, fmaf(wx1, X[b + pz + cnx + 1], wx0 * X[b + pz + cnx]),
+        const float* X = xc + c * Lc.cs;
+        const float lo = fmaf(wy1, fmaf(wx1, X[b + cnx_ + 1], wx0 * X[b + cnx_]), wy0 * fmaf(wx1, X[b + 1], wx0 * X[b]));
+        const float hi = fmaf(wy1, fmaf(wx1, X[b + pz + cnx_ + 1], wx0 * X[b + pz + cnx_]),
                               wy0 * fmaf(wx1, X[b + pz + 1], wx0 * X[b + pz]));
         P[c] = fmaf(wz1, hi, wz0 * lo);
     }
@@ -303,9 +325,10 @@ __global__ void k_prolong_smooth32(MgLevel32 Lc, MgLevel32 Lf, const float* __re
     float P[3];
     prolong_node32(Lc, xc, fx, fy, fz, __ffs(Lc.span) - 1, P);
     const int m = Lf.mask[n];
+    const int64_t np = (int64_t)(n / fnx) * Lf.pitch + fx;
     for (int c = 0; c < 3; ++c) {
-        const float t = (w * rf[c * Lf.nn + n]) * Lf.diag[c * Lf.nn + n];
-        xf[c * Lf.nn + n] = ((m >> c) & 1) ? 0.0f : (t + P[c]) + t;
+        const float t = (w * rf[c * Lf.cs + np]) * Lf.diag[c * Lf.cs + np];
+        xf[c * Lf.cs + np] = ((m >> c) & 1) ? 0.0f : (t + P[c]) + t;
     }
 }
 
@@ -321,9 +344,9 @@ __global__ void __launch_bounds__(RED_THREADS) k_prolong_smooth0_32(MgLevel32 Lc
                                                                     PcgScalars* S) {
     __shared__ double sh[32];
     if (S->done) return;
-    const int NN = (int)Lf.nn;
+    const int CS = (int)Lf.cs;
     const int fnx = Lf.nx + 1, fny = Lf.ny + 1;
-    const int cnx = Lc.nx + 1, cny = Lc.ny + 1, cnn = (int)Lc.nn;
+    const int cnx = Lc.pitch, cny = Lc.ny + 1, cnn = (int)Lc.cs;
     const int runs = Lf.nx / SP + 1;                 // runs per row (the last one is the single node x = nx)
     const int chunks = (runs + 31) >> 5;
     const int items = chunks * fny * (Lf.nz + 1);
@@ -353,21 +376,21 @@ __global__ void __launch_bounds__(RED_THREADS) k_prolong_smooth0_32(MgLevel32 Lc
             L[c] = fmaf(wz1, fmaf(wy1, y01, wy0 * y00), wz0 * fmaf(wy1, x01, wy0 * x00));
             R[c] = fmaf(wz1, fmaf(wy1, y11, wy0 * y10), wz0 * fmaf(wy1, x11, wy0 * x10));
         }
-        const int nb = row * fnx + SP * j;
+        const int nb = row * fnx + SP * j, npb = row * Lf.pitch + SP * j;
         const int nk = last ? 1 : SP;
 #pragma unroll
         for (int k = 0; k < SP; ++k) {
             if (k >= nk) break;
-            const int n = nb + k;
+            const int n = nb + k, np = npb + k;
             const float wx1 = last ? 1.0f : k * inv, wx0 = 1.0f - wx1;
             const int m = Lf.mask[n];
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-                const float rv = r[c * NN + n];
-                const float t = (w * rv) * Lf.diag[c * NN + n];
+                const float rv = r[c * CS + np];
+                const float t = (w * rv) * Lf.diag[c * CS + np];
                 const float P = fmaf(wx1, R[c], wx0 * L[c]);
                 const float zv = ((m >> c) & 1) ? 0.0f : (t + P) + t;
-                z[c * NN + n] = zv;
+                z[c * CS + np] = zv;
                 part = fma((double)rv, (double)zv, part);
             }
         }
@@ -431,9 +454,9 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_update32(Grid g, float* __r
     }
     const float alpha = (float)(S->rz / den);
     if (blockIdx.x == 0 && threadIdx.x == 0) S->alpha = alpha;
-    // the three component planes are contiguous: one flat vector of 3 NN floats, 16-byte accesses
-    // (cudaMalloc bases are 256-byte aligned) and a scalar tail
-    const int n3 = (int)(3 * g.NN), n4 = n3 >> 2;
+    // the three component planes are contiguous: one flat vector of 3 NNp floats (pads stay zero), 16-byte
+    // accesses (cudaMalloc bases are 256-byte aligned; NNp is a multiple of 4)
+    const int n3 = (int)(3 * g.NNp), n4 = n3 >> 2;
     const int stride = gridDim.x * blockDim.x;
     float4* __restrict__ r4 = reinterpret_cast<float4*>(r);
     const float4* __restrict__ a4 = reinterpret_cast<const float4*>(Ap);
@@ -469,7 +492,7 @@ __global__ void k_pcg_direction32(Grid g, const float* __restrict__ z, float* __
     if (S->xit == S->it) return;
     const bool move = !S->done;
     const float beta = (float)S->beta, alpha = S->alpha;
-    const int n3 = (int)(3 * g.NN), n4 = n3 >> 2;
+    const int n3 = (int)(3 * g.NNp), n4 = n3 >> 2;
     const int stride = gridDim.x * blockDim.x;
     float4* __restrict__ p4 = reinterpret_cast<float4*>(p);
     float4* __restrict__ x4 = reinterpret_cast<float4*>(x);
@@ -497,22 +520,24 @@ inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t
 
 }  // namespace
 
-void launch_cast(int64_t n, const double* a, float* b, cudaStream_t s) {
-    k_cast<<<RED_BLOCKS, 256, 0, s>>>(n, a, b);
+void launch_nodes_to32(const Grid& g, const double* a, float* b, cudaStream_t s) {
+    k_rows_convert<double, float><<<RED_BLOCKS, 256, 0, s>>>(3 * (int64_t)g.nny * g.nnz, g.nnx, g.nnx, g.px, a, b);
+}
+void launch_nodes_from32(const Grid& g, const float* a, double* b, cudaStream_t s) {
+    k_rows_convert<float, double><<<RED_BLOCKS, 256, 0, s>>>(3 * (int64_t)g.nny * g.nnz, g.nnx, g.px, g.nnx, a, b);
+}
+void launch_cells_to32(const Grid& g, const double* a, float* b, cudaStream_t s) {
+    k_rows_convert<double, float><<<RED_BLOCKS, 256, 0, s>>>((int64_t)g.ey * g.ez, g.ex, g.ex, g.pex, a, b);
 }
 void launch_mixed_residual(const Grid& g, const double* b, const double* Au, float* r32, float* d32, RedSlot red,
                            double* rn2, cudaStream_t s) {
     k_mixed_residual<<<RED_BLOCKS, RED_THREADS, 0, s>>>(g, b, Au, r32, d32, red, rn2);
 }
 void launch_mixed_accumulate(const Grid& g, double* u, const float* d, cudaStream_t s) {
-    k_mixed_accumulate<<<RED_BLOCKS, 256, 0, s>>>(3 * g.NN, u, d);
+    k_mixed_accumulate<<<RED_BLOCKS, 256, 0, s>>>(g, u, d);
 }
-void launch_recip_diag32(int64_t n, const double* d, float* rd, cudaStream_t s) {
-    k_recip_diag32<<<RED_BLOCKS, 256, 0, s>>>(n, d, rd);
-}
-
-void launch_widen(int64_t n, const float* a, double* b, cudaStream_t s) {
-    k_widen<<<RED_BLOCKS, 256, 0, s>>>(n, a, b);
+void launch_recip_diag32(int64_t rows, int len, int pitch, const double* d, float* rd, cudaStream_t s) {
+    k_recip_diag32<<<RED_BLOCKS, 256, 0, s>>>(rows, len, pitch, d, rd);
 }
 
 void launch_matvec32(const Grid& g, const float* Ke, const float* E, const uint8_t* mask, const float* u, float* y,

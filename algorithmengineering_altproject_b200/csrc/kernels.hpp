@@ -42,11 +42,13 @@ struct MgLevel {         // one structured multigrid level (hierarchy.cpp:45-81)
 
 struct MgLevel32 {       // FP32 copy of a level's vectors for the mixed-precision inner solve
     int nx, ny, nz, span;
-    int64_t nn;
+    int64_t nn;           // nodes (the mask's length)
+    int pitch;            // row pitch of the vectors: the grid's px on the finest level, nx + 1 on the others
+    int64_t cs;           // component stride of the vectors: pitch * (ny + 1) * (nz + 1)
     float* r;
     float* x;
     float* diag;          // reciprocal diagonal 1 / max(1e-30, D) in FP32
-    const uint8_t* mask;  // shared with the FP64 level
+    const uint8_t* mask;  // shared with the FP64 level (unpadded, nn bytes)
 };
 
 // ---- model set-up (fea.cpp:181-447)
@@ -212,9 +214,13 @@ void launch_oc_finish(const Grid& g, const uint8_t* solid, float* x, const float
 void launch_oc_vec8_stats(int64_t ne, const int32_t* morton_cells, const float* x, OcState* st, cudaStream_t s);
 
 // ---- mixed precision (k_mixed.cu)
-void launch_cast(int64_t n, const double* a, float* b, cudaStream_t s);
-void launch_widen(int64_t n, const float* a, double* b, cudaStream_t s);
-void launch_recip_diag32(int64_t n, const double* d, float* rd, cudaStream_t s);
+// FP64 node vector (3 planes, rows of nnx) -> FP32 image (rows of px, pads zero), and back
+void launch_nodes_to32(const Grid& g, const double* a, float* b, cudaStream_t s);
+void launch_nodes_from32(const Grid& g, const float* a, double* b, cudaStream_t s);
+// FP64 moduli (cells, rows of ex) -> FP32 image (rows of pex, pads zero)
+void launch_cells_to32(const Grid& g, const double* a, float* b, cudaStream_t s);
+// reciprocal FP32 diagonal 1 / max(1e-30, D) of a level: rows of `len` values (3 planes) -> rows of `pitch`
+void launch_recip_diag32(int64_t rows, int len, int pitch, const double* d, float* rd, cudaStream_t s);
 void launch_mixed_residual(const Grid& g, const double* b, const double* Au, float* r32, float* d32, RedSlot red,
                            double* rn2, cudaStream_t s);
 void launch_mixed_accumulate(const Grid& g, double* u, const float* d, cudaStream_t s);

@@ -8,6 +8,10 @@
 //                  ((cz+1)*(ny+2) + cy+1)*(nx+2) + cx+1.  Cell (cx,cy,cz) is the reference element
 //                  (ex,ey,ez) = (cx, ny-1-cy, cz) (fea.cpp:222).  Non-solid cells hold E = 0.
 //   node masks     one byte per node, bit c = DOF c fixed.
+//   FP32 images    the mixed-precision inner solve keeps its finest-level node vectors and moduli with
+//                  rows padded to a multiple of 4 values (pitch px for nodes, pex for cells; the pads
+//                  hold zeros), so that every row starts on a 16-byte boundary: TMA tensor maps need
+//                  16-byte row strides, and 257 nodes per row (1028 bytes) is not one.
 //
 // Every floating-point kernel is compiled with -fmad=false; fused multiply-adds are written out
 // with fma() where the algorithm uses them, so the CPU oracle can mirror each operation.
@@ -41,12 +45,22 @@ struct Grid {
     int64_t NN;          // nodes per plane
     int ex, ey, ez;      // cell-array dims with ghost ring (nx+2, ...)
     int64_t NE;          // cell-array length
+    int px;              // FP32 node row pitch: nnx rounded up to a multiple of 4
+    int64_t NNp;         // px * nny * nnz: one component plane of an FP32 node vector
+    int pex;             // FP32 cell row pitch: ex rounded up to a multiple of 4
+    int64_t NEp;         // pex * ey * ez
 
     __host__ __device__ int64_t node(int ix, int iy, int iz) const {
         return ((int64_t)iz * nny + iy) * nnx + ix;
     }
     __host__ __device__ int64_t cell(int cx, int cy, int cz) const {
         return ((int64_t)(cz + 1) * ey + (cy + 1)) * ex + (cx + 1);
+    }
+    __host__ __device__ int64_t pnode(int ix, int iy, int iz) const {   // FP32 node vectors
+        return ((int64_t)iz * nny + iy) * px + ix;
+    }
+    __host__ __device__ int64_t pcell(int cx, int cy, int cz) const {   // FP32 moduli
+        return ((int64_t)(cz + 1) * ey + (cy + 1)) * pex + (cx + 1);
     }
 };
 
@@ -57,6 +71,10 @@ inline Grid make_grid(int nx, int ny, int nz) {
     g.NN = (int64_t)g.nnx * g.nny * g.nnz;
     g.ex = nx + 2; g.ey = ny + 2; g.ez = nz + 2;
     g.NE = (int64_t)g.ex * g.ey * g.ez;
+    g.px = (g.nnx + 3) / 4 * 4;
+    g.NNp = (int64_t)g.px * g.nny * g.nnz;
+    g.pex = (g.ex + 3) / 4 * 4;
+    g.NEp = (int64_t)g.pex * g.ey * g.ez;
     return g;
 }
 
