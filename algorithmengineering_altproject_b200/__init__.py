@@ -47,7 +47,7 @@ class Params(C.Structure):
                 ("oc_sum_order", C.c_int), ("precision", C.c_int), ("device", C.c_int),
                 ("matvec32_form", C.c_int), ("mg_coarse_assembly", C.c_int), ("matvec64_form", C.c_int),
                 ("mg_vcycle", C.c_int), ("mg_standard_weight", C.c_float),
-                ("mg_rebuild_period", C.c_int), ("reserved", C.c_int * 1)]
+                ("mg_rebuild_period", C.c_int), ("matvec32_tile", C.c_int)]
 
 
 T3D_LOAD_TIP_LINE, T3D_LOAD_TOP_TRACTION, T3D_LOAD_TORSION = 0, 1, 2
@@ -75,7 +75,8 @@ class Info(C.Structure):
                 ("num_nodes", C.c_int64), ("num_free", C.c_int64), ("num_levels", C.c_int64),
                 ("levels", (C.c_int64 * 4) * 8), ("coarse_n", C.c_int64), ("coarse_cholesky_ok", C.c_int64),
                 ("device_bytes", C.c_int64), ("kernel_launches", C.c_int64), ("matvec32_modal", C.c_int64),
-                ("matvec32_tile", C.c_int64 * 4), ("matvec64_kernel", C.c_int64)]
+                ("matvec32_tile", C.c_int64 * 4), ("matvec64_kernel", C.c_int64),
+                ("matvec32_variant", C.c_int64)]
 
 
 class IterRecord(C.Structure):

@@ -139,6 +139,7 @@ struct Context {
     MgLevel32 lv32[8]{};
     float* ra1_32[8]{};         // x-pass buffer of the FP32 restriction (its y and z passes are fused)
     PcgScalars* S32 = nullptr;
+    int* tma_err = nullptr;     // set by a TMA-staged K(E)p whose mbarrier wait gave up (checked after solves)
     cudaGraphExec_t pcg32_graph = nullptr;
     int64_t pcg32_graph_launches = 0;
     int last_outer = 0;
@@ -283,6 +284,16 @@ static int build_levels(Context* c) {
     return launch_check("mask restriction");
 }
 
+// A TMA-staged K(E)p records a bounded mbarrier wait that gave up in c->tma_err (the kernel went on and
+// returned); its results are then void.  Reads the flag (synchronising the stream).
+static int check_tma(Context* c) {
+    int e = 0;
+    T3D_CUDA_OK(cudaMemcpyAsync(&e, c->tma_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    T3D_CUDA_OK(cudaStreamSynchronize(c->st));
+    if (e) return set_error(T3D_ERR_CUDA, "TMA-staged K(E)p: an mbarrier wait timed out");
+    return T3D_OK;
+}
+
 static int build_mixed(Context* c) {
     const Grid& g = c->g;
     // finest-level FP32 images are pitched (Grid::px, Grid::pex); their pads stay zero
@@ -295,6 +306,8 @@ static int build_mixed(Context* c) {
     }
     CHECK(c->alloc(&c->S32, 1));
     T3D_CUDA_OK(cudaMemsetAsync(c->S32, 0, sizeof(PcgScalars), c->st));
+    CHECK(c->alloc(&c->tma_err, 1));
+    T3D_CUDA_OK(cudaMemsetAsync(c->tma_err, 0, sizeof(int), c->st));
     for (int l = 0; l < c->nlev; ++l) {
         const MgLevel& L = c->lv[l];
         MgLevel32& M = c->lv32[l];
@@ -317,14 +330,16 @@ static int build_mixed(Context* c) {
     T3D_CUDA_OK(cudaMemcpyAsync(c->Ke32, k32, sizeof k32, cudaMemcpyHostToDevice, c->st));
     c->modal = c->prm.matvec32_form == T3D_MATVEC32_AUTO && modal_ke_from(c->Ke_h, &c->kh, &c->modal_off);
     // the tile shape of the modal kernel is chosen by timing each one on this grid (zero vectors)
-    CHECK(modal_autotune(g, c->dev, c->kh, c->E32, c->mask0, c->p32, c->Ap32, c->st, &c->mt));
-    return sync(c);
+    if (c->prm.matvec32_tile > 0) CHECK(modal_tiling(g, c->dev, c->prm.matvec32_tile - 1, &c->mt));
+    else CHECK(modal_autotune(g, c->dev, c->kh, c->E32, c->mask0, c->p32, c->Ap32, c->tma_err, c->st, &c->mt));
+    CHECK(sync(c));
+    return check_tma(c);
 }
 
 // FP32 K(E)p on the FP32 images (E32, x -> y); with dot.partial, x.y goes to S->denom
 static void matvec32(Context* c, const float* x, float* y, RedSlot dot, PcgScalars* S) {
     c->launches += 1;
-    if (c->modal) launch_matvec32_modal(c->g, c->kh, c->mt, c->E32, c->mask0, x, y, dot, S, c->st);
+    if (c->modal) launch_matvec32_modal(c->g, c->kh, c->mt, c->E32, c->mask0, x, y, dot, S, c->tma_err, c->st);
     else launch_matvec32(c->g, c->Ke32, c->E32, c->mask0, x, y, dot, S, c->st);
 }
 
@@ -961,7 +976,7 @@ static int mixed_solve(Context* c, double tol, int maxit, int* iters) {
     }
     c->last_outer = outer;
     *iters = converged ? used : maxit;
-    return T3D_OK;
+    return check_tma(c);
 }
 
 static int solve(Context* c, double tol, int maxit, int* iters) {
@@ -1269,6 +1284,7 @@ int t3d_get_info(const t3d_context* ctx, t3d_info* info) {
         int d[4];
         t3d::modal_variant_desc(ctx->mt.variant, d);
         for (int k = 0; k < 4; ++k) info->matvec32_tile[k] = d[k];
+        info->matvec32_variant = ctx->mt.variant;
     }
     return T3D_OK;
 }
@@ -1361,6 +1377,7 @@ int t3d_matvec32(t3d_context* ctx, const double* E, const double* u, double* y) 
     t3d::launch_nodes_from32(ctx->g, ctx->Ap32, ctx->Ap, ctx->st);
     ctx->launches += 1;
     CHECK(t3d::launch_check("matvec32"));
+    CHECK(t3d::check_tma(ctx));
     return t3d::download_free(ctx, ctx->Ap, y);
 }
 
@@ -1642,7 +1659,7 @@ int t3d_profile(t3d_context* ctx, int what, int reps, double* ms) {
     float t = 0;
     T3D_CUDA_OK(cudaEventElapsedTime(&t, ctx->ev[6], ctx->ev[7]));
     *ms = (double)t / reps;
-    return T3D_OK;
+    return ctx->mixed ? t3d::check_tma(ctx) : T3D_OK;
 }
 
 int t3d_export_stl(t3d_context* ctx, const float* xphys, float iso, const char* path, int64_t* ntri) {

@@ -23,81 +23,23 @@
 //   * fixed DOFs are zeroed by the node mask (their inputs are exact zeros); p.Ap is folded in FP64.
 // Work items (tile, slab) are walked by a persistent grid in x-fastest order so that concurrent CTAs
 // share their halo planes through L2.
+#include <cuda.h>
+
 #include <algorithm>
 #include <cmath>
 #include <map>
 #include <mutex>
 #include <tuple>
 
+#include "k_matvec_tma.cuh"
 #include "kernels.hpp"
+#include "modal.cuh"
 #include "red.cuh"
 #include "t3d_b200.h"
 
 namespace t3d {
 
 namespace {
-
-// modal index = component * 8 + mode, mode bit 0 = x, bit 1 = y, bit 2 = z (constant mode 0 unused)
-// X(dst, src) for each of the 45 nonzeros, in the order of ModalKe::v
-#define T3D_KH_PATTERN(X)                                                                          \
-    /* normal strains: (0,x) (1,y) (2,z) */                                                        \
-    X(1, 1) X(1, 10) X(1, 20) X(10, 1) X(10, 10) X(10, 20) X(20, 1) X(20, 10) X(20, 20)            \
-    /* shears xy, xz, yz */                                                                        \
-    X(9, 9) X(9, 2) X(2, 9) X(2, 2) X(17, 17) X(17, 4) X(4, 17) X(4, 4)                            \
-    X(18, 18) X(18, 12) X(12, 18) X(12, 12)                                                        \
-    /* bilinear pairs */                                                                           \
-    X(3, 3) X(3, 22) X(22, 3) X(22, 22) X(11, 11) X(11, 21) X(21, 11) X(21, 21)                    \
-    X(5, 5) X(5, 14) X(14, 5) X(14, 14)                                                            \
-    /* bilinear triple (2,xy) (1,xz) (0,yz) */                                                     \
-    X(19, 19) X(19, 13) X(19, 6) X(13, 19) X(13, 13) X(13, 6) X(6, 19) X(6, 13) X(6, 6)            \
-    /* trilinear */                                                                                \
-    X(7, 7) X(15, 15) X(23, 23)
-
-struct KhEntry {
-    int dst, src;
-};
-#define T3D_KH_ENTRY(d, s) {d, s},
-constexpr KhEntry KH_PATTERN_HOST[45] = {T3D_KH_PATTERN(T3D_KH_ENTRY)};
-#undef T3D_KH_ENTRY
-
-// x-y Hadamard stage of one component on one node plane: corners (dx,dy) -> modes (i,j)
-struct Modes2 {
-    float m00, m10, m01, m11;
-};
-
-__device__ __forceinline__ Modes2 fwd2(float u00, float u10, float u01, float u11) {
-    const float s0 = u00 + u10, d0 = u10 - u00, s1 = u01 + u11, d1 = u11 - u01;
-    return Modes2{s0 + s1, d0 + d1, s1 - s0, d1 - d0};
-}
-
-// inverse x-y stage: modes (i,j) -> corner values (dx,dy) = sum s_x^i s_y^j w_ij
-__device__ __forceinline__ void inv2(const Modes2& w, float& v00, float& v10, float& v01, float& v11) {
-    const float p = w.m00 - w.m01, q = w.m10 - w.m11, pp = w.m00 + w.m01, qq = w.m10 + w.m11;
-    v00 = p - q;
-    v10 = p + q;
-    v01 = pp - qq;
-    v11 = pp + qq;
-}
-
-// The same two stages on components 0 and 1 at once (packed FP32x2 arithmetic, .x = component 0,
-// .y = component 1); a - b is fma(b, -1, a), which is exact.
-struct Modes2x2 {
-    float2 m00, m10, m01, m11;
-};
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ Modes2x2 fwd2x2(float2 u00, float2 u10, float2 u01, float2 u11) {
-    const float2 s0 = add2(u00, u10), d0 = sub2(u10, u00), s1 = add2(u01, u11), d1 = sub2(u11, u01);
-    return Modes2x2{add2(s0, s1), add2(d0, d1), sub2(s1, s0), sub2(d1, d0)};
-}
-__device__ __forceinline__ void inv2x2(const Modes2x2& w, float2& v00, float2& v10, float2& v01, float2& v11) {
-    const float2 p = sub2(w.m00, w.m01), q = sub2(w.m10, w.m11), pp = add2(w.m00, w.m01), qq = add2(w.m10, w.m11);
-    v00 = sub2(p, q);
-    v10 = add2(p, q);
-    v01 = sub2(pp, qq);
-    v11 = add2(pp, qq);
-}
 
 __device__ __forceinline__ void cp_async4(unsigned s, const float* gsrc, bool valid) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(s), "l"(gsrc), "r"(valid ? 4 : 0)
@@ -353,35 +295,97 @@ __global__ void __launch_bounds__(BX * BY, MINB)
     }
 }
 
-// Tile shapes the autotuner chooses from: CTA of BX x BY element columns, MINB CTAs per SM, ring depth.
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda)
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
+
+// Tensor maps of the pitched FP32 displacement image u (x, y, z, component; box rw x py x 1 x 3) and moduli
+// E (x, y, z; box rw x by x 1).  Strides are multiples of 16 bytes because the rows are pitched; elements
+// outside the arrays read as zero.
+bool modal_tensor_maps(const Grid& g, const float* u, const float* E, int rw, int py, int by, CUtensorMap* um,
+                       CUtensorMap* em) {
+    const EncodeTiledFn fn = encode_tiled();
+    if (!fn) return false;
+    const cuuint64_t ud[4] = {(cuuint64_t)g.px, (cuuint64_t)g.nny, (cuuint64_t)g.nnz, 3};
+    const cuuint64_t us[3] = {(cuuint64_t)g.px * 4, (cuuint64_t)g.px * g.nny * 4, (cuuint64_t)g.NNp * 4};
+    const cuuint32_t ub[4] = {(cuuint32_t)rw, (cuuint32_t)py, 1, 3};
+    const cuuint32_t one[4] = {1, 1, 1, 1};
+    if (fn(um, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<float*>(u), ud, us, ub, one, CU_TENSOR_MAP_INTERLEAVE_NONE,
+           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) !=
+        CUDA_SUCCESS)
+        return false;
+    const cuuint64_t ed[3] = {(cuuint64_t)g.pex, (cuuint64_t)g.ey, (cuuint64_t)g.ez};
+    const cuuint64_t es[2] = {(cuuint64_t)g.pex * 4, (cuuint64_t)g.pex * g.ey * 4};
+    const cuuint32_t eb[3] = {(cuuint32_t)rw, (cuuint32_t)by, 1};
+    return fn(em, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(E), ed, es, eb, one,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Tile shapes the autotuner chooses from: CTA of BX x BY element columns, MINB CTAs per SM, ring depth;
+// planes staged by per-thread cp.async (ModalShape) or by the Tensor Memory Accelerator (TmaShape).
+// launch() returns false when the shape cannot run on these buffers (no tensor map could be made).
 template <int BX, int BY, int MINB, int ST, int PACK = 0>
 struct ModalShape {
-    static constexpr int bx = BX, by = BY, stages = ST, packed = PACK;
+    static constexpr int bx = BX, by = BY, stages = ST, packed = PACK, tma = 0;
     static constexpr size_t smem = sizeof(ModalSmem<BX, BY, ST>);
     static const void* fn() { return reinterpret_cast<const void*>(k_matvec32_modal<BX, BY, MINB, ST, PACK>); }
-    static void launch(const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E, const uint8_t* mask,
-                       const float* u, float* y, RedSlot dot, PcgScalars* S, cudaStream_t s) {
+    static bool launch(const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E, const uint8_t* mask,
+                       const float* u, float* y, RedSlot dot, PcgScalars* S, int* err, cudaStream_t s) {
+        (void)err;
         k_matvec32_modal<BX, BY, MINB, ST, PACK><<<t.grid, BX * BY, smem, s>>>(g, kh, t, E, mask, u, y, dot, S);
+        return true;
+    }
+};
+template <int BX, int BY, int MINB, int ST>
+struct TmaShape {
+    using SM = TmaSmem<BX, BY, ST>;
+    static constexpr int bx = BX, by = BY, stages = ST, packed = 1, tma = 1;
+    static constexpr size_t smem = sizeof(SM) + 128;   // + slack for the 128-byte alignment of the ring
+    static const void* fn() { return reinterpret_cast<const void*>(k_matvec32_tma<BX, BY, MINB, ST>); }
+    static bool launch(const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E, const uint8_t* mask,
+                       const float* u, float* y, RedSlot dot, PcgScalars* S, int* err, cudaStream_t s) {
+        CUtensorMap um, em;
+        if (!modal_tensor_maps(g, u, E, SM::RW, SM::PY, BY, &um, &em)) return false;
+        k_matvec32_tma<BX, BY, MINB, ST><<<t.grid, BX * BY, smem, s>>>(um, em, g, kh, t, mask, y, dot, S, err);
+        return true;
     }
 };
 struct ModalVariant {
-    int bx, by, stages, packed;
+    int bx, by, stages, packed, tma;
     size_t smem;
     const void* (*fn)();
-    void (*launch)(const Grid&, const ModalKe&, const ModalTiling&, const float*, const uint8_t*, const float*,
-                   float*, RedSlot, PcgScalars*, cudaStream_t);
+    bool (*launch)(const Grid&, const ModalKe&, const ModalTiling&, const float*, const uint8_t*, const float*,
+                   float*, RedSlot, PcgScalars*, int*, cudaStream_t);
 };
 template <class V>
 constexpr ModalVariant variant_of() {
-    return ModalVariant{V::bx, V::by, V::stages, V::packed, V::smem, &V::fn, &V::launch};
+    return ModalVariant{V::bx, V::by, V::stages, V::packed, V::tma, V::smem, &V::fn, &V::launch};
 }
 const ModalVariant MODAL_VARIANTS[] = {
-    variant_of<ModalShape<32, 8, 2, 4, 1>>(),
+    variant_of<ModalShape<32, 8, 2, 4, 1>>(),   // variant 0: the fallback of a TMA shape without tensor maps
     variant_of<ModalShape<32, 8, 2, 4>>(),
     variant_of<ModalShape<32, 8, 2, 3>>(),
     variant_of<ModalShape<32, 8, 3, 3>>(),
     variant_of<ModalShape<32, 16, 2, 3>>(),
     variant_of<ModalShape<32, 16, 1, 4>>(),
+    variant_of<TmaShape<32, 8, 2, 4>>(),
+    variant_of<TmaShape<32, 8, 3, 3>>(),
+    variant_of<TmaShape<32, 16, 1, 4>>(),
+    variant_of<TmaShape<32, 16, 2, 3>>(),
 };
 constexpr int MODAL_NVARIANTS = sizeof(MODAL_VARIANTS) / sizeof(MODAL_VARIANTS[0]);
 constexpr int MODAL_SLAB_MIN = 8;
@@ -427,7 +431,7 @@ void modal_variant_desc(int variant, int out[4]) {
     out[0] = v.bx;
     out[1] = v.by;
     out[2] = v.stages;
-    out[3] = v.packed;
+    out[3] = v.tma ? 2 : v.packed;
 }
 
 int modal_tiling(const Grid& g, int dev, int variant, ModalTiling* t) {
@@ -459,7 +463,7 @@ int modal_tiling(const Grid& g, int dev, int variant, ModalTiling* t) {
 // size uses the same tile shape: results then do not depend on which contexts ran before or beside it
 // (the shape fixes the block order of the FP64 p.Ap partial sums).
 int modal_autotune(const Grid& g, int dev, const ModalKe& kh, const float* E, const uint8_t* mask, const float* u,
-                   float* y, cudaStream_t s, ModalTiling* best) {
+                   float* y, int* err, cudaStream_t s, ModalTiling* best) {
     static std::mutex mu;
     static std::map<std::tuple<int, int, int, int>, ModalTiling> cache;
     const auto key = std::make_tuple(dev, g.nx, g.ny, g.nz);
@@ -479,13 +483,14 @@ int modal_autotune(const Grid& g, int dev, const ModalKe& kh, const float* E, co
     }
     float best_ms = 0.f;
     int rc = 0;
+    bool have = false;
     for (int v = 0; v < MODAL_NVARIANTS && rc == 0; ++v) {
         ModalTiling t{};
         if ((rc = modal_tiling(g, dev, v, &t)) != 0) break;
         const RedSlot none{nullptr, nullptr};
-        MODAL_VARIANTS[v].launch(g, kh, t, E, mask, u, y, none, nullptr, s);   // warm-up
+        if (!MODAL_VARIANTS[v].launch(g, kh, t, E, mask, u, y, none, nullptr, err, s)) continue;   // warm-up
         cudaEventRecord(e0, s);
-        for (int r = 0; r < 3; ++r) MODAL_VARIANTS[v].launch(g, kh, t, E, mask, u, y, none, nullptr, s);
+        for (int r = 0; r < 3; ++r) MODAL_VARIANTS[v].launch(g, kh, t, E, mask, u, y, none, nullptr, err, s);
         cudaEventRecord(e1, s);
         if ((e = cudaEventSynchronize(e1)) != cudaSuccess) {
             rc = set_cuda_error(e, "modal autotune", __FILE__, __LINE__);
@@ -493,9 +498,10 @@ int modal_autotune(const Grid& g, int dev, const ModalKe& kh, const float* E, co
         }
         float ms = 0.f;
         cudaEventElapsedTime(&ms, e0, e1);
-        if (v == 0 || ms < best_ms) {
+        if (!have || ms < best_ms) {
             best_ms = ms;
             *best = t;
+            have = true;
         }
     }
     cudaEventDestroy(e0);
@@ -505,9 +511,15 @@ int modal_autotune(const Grid& g, int dev, const ModalKe& kh, const float* E, co
 }
 
 void launch_matvec32_modal(const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E,
-                           const uint8_t* mask, const float* u, float* y, RedSlot dot, PcgScalars* S,
+                           const uint8_t* mask, const float* u, float* y, RedSlot dot, PcgScalars* S, int* err,
                            cudaStream_t s) {
-    MODAL_VARIANTS[t.variant].launch(g, kh, t, E, mask, u, y, dot, S, s);
+    if (MODAL_VARIANTS[t.variant].launch(g, kh, t, E, mask, u, y, dot, S, err, s)) return;
+    // no tensor map for these buffers: the cp.async form of the same arithmetic (bit-identical results)
+    ModalTiling t0 = t;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    modal_tiling(g, dev, 0, &t0);
+    MODAL_VARIANTS[0].launch(g, kh, t0, E, mask, u, y, dot, S, err, s);
 }
 
 }  // namespace t3d

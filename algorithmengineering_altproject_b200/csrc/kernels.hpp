@@ -257,10 +257,11 @@ void modal_variant_desc(int variant, int out[4]);
 int modal_tiling(const Grid& g, int dev, int variant, ModalTiling* t);
 // Times every tile shape on the given buffers (3 launches each, stream-ordered, CUDA events) and returns
 // the fastest one's tiling.  y is overwritten.
+// err: device int set to 1 by a TMA-staged shape whose mbarrier wait gave up (never expected; checked by the host)
 int modal_autotune(const Grid& g, int dev, const ModalKe& kh, const float* E, const uint8_t* mask, const float* u,
-                   float* y, cudaStream_t s, ModalTiling* best);
+                   float* y, int* err, cudaStream_t s, ModalTiling* best);
 void launch_matvec32_modal(const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E,
-                           const uint8_t* mask, const float* u, float* y, RedSlot dot, PcgScalars* S,
+                           const uint8_t* mask, const float* u, float* y, RedSlot dot, PcgScalars* S, int* err,
                            cudaStream_t s);
 
 // ---- surface export (k_stl.cu, io.cpp:80-87)

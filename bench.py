@@ -71,6 +71,8 @@ def parse_args():
     ap.add_argument("--kernels-only", action="store_true",
                     help="time the matvec and V-cycle alone on the config's grid (for ncu captures)")
     ap.add_argument("--reps", type=int, default=20)
+    ap.add_argument("--tile", type=int, default=0,
+                    help="modal FP32 K(E)p tile shape: 0 = autotuned, k = shape k-1 (--kernels-only timing)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
@@ -264,7 +266,7 @@ def run_kernels_only(args):
     cfg = CONFIGS[args.config]
     mixed = args.precision == "mixed"
     P = t3d.Problem(cfg["nely"], cfg["nelx"], cfg["nelz"], mg_max_levels=cfg["max_levels"],
-                    precision=t3d.T3D_MIXED if mixed else t3d.T3D_FP64)
+                    precision=t3d.T3D_MIXED if mixed else t3d.T3D_FP64, matvec32_tile=args.tile)
     rng = np.random.default_rng(7)
     E = np.full(P.ne, 1e-9 + cfg["V0"] ** 3 * (1.0 - 1e-9))
     P.make_diagonal_preconditioner_from_static(E)
@@ -274,6 +276,7 @@ def run_kernels_only(args):
     vc = P.profile(t3d.T3D_PROFILE_VCYCLE32 if mixed else t3d.T3D_PROFILE_VCYCLE, args.reps)
     print(json.dumps({"config": cfg["name"], "precision": args.precision, "matvec_ms": mv, "vcycle_ms": vc,
                       "matvec32_tile": list(P.info().matvec32_tile) if mixed else None,
+                      "matvec32_variant": int(P.info().matvec32_variant) if mixed else None,
                       "roofline": matvec_roofline(P, mixed, mv)}), flush=True)
     P.close()
     return 0

@@ -77,7 +77,8 @@ typedef struct t3d_params {
                                      so its residual smoother converges; the reference's 0.6 does not */
     int   mg_rebuild_period;      /* design iterations between MG rebuilds: 5 = the reference's loop 1 and every
                                      5th (driver.cpp:132); 1 = every iteration; 0 = the default (5) */
-    int   reserved[1];
+    int   matvec32_tile;          /* tile shape of the modal FP32 K(E)p: 0 = chosen by timing every shape on the
+                                     grid (the default); k >= 1 = shape k-1 (all shapes give identical results) */
 } t3d_params;
 
 /* Problem spec beyond the reference's built-in cantilever (the reference hard-codes one load case and a
@@ -110,7 +111,9 @@ typedef struct t3d_info {
     int64_t kernel_launches;      /* kernels launched by this context so far (graph nodes included) */
     int64_t matvec32_modal;       /* 1 when the mixed form's FP32 K(E)p uses the modal kernel */
     int64_t matvec32_tile[4];     /* tile shape the modal kernel's autotuner chose: threads in x, threads in y,
-                                     plane-ring slots, packed FP32x2 arithmetic (0/1) */
+                                     plane-ring slots, plane staging (0 per-thread cp.async, 1 the same with packed
+                                     FP32x2 arithmetic, 2 packed arithmetic with TMA bulk tensor copies) */
+    int64_t matvec32_variant;     /* index of that shape (params.matvec32_tile - 1 selects it) */
     int64_t matvec64_kernel;      /* FP64 K(E)u kernel: 0 node-centric, 1 streaming with Ke from the constant bank,
                                      2 streaming with the built-in Ke's magnitudes in registers */
 } t3d_info;

@@ -6,6 +6,8 @@ K_times_u_finest (fea.cpp:763-837) with FP32 inputs, so each must agree with the
 FP32 accuracy: ||y32 - y64|| <= 2e-6 ||y64|| on random moduli and displacements.  The grids cover a
 padded one (30x60x30 -> 64x32x32 elements) and ones that do not divide the kernel's node tiles.
 The FP32 V-cycle of the same inner solve is checked against the FP64 V-cycle the same way (1e-5).
+Every tile shape of the modal kernel -- per-thread cp.async staging and TMA bulk-tensor staging alike -- runs
+the same arithmetic in the same order, so all shapes must give bit-identical products.
 """
 import numpy as np
 import pytest
@@ -84,3 +86,27 @@ def test_fp32_vcycle_matches_fp64(dims):
     z32 = P.vcycle32(r)
     assert np.linalg.norm(z32 - z64) <= 1e-5 * np.linalg.norm(z64), np.linalg.norm(z32 - z64) / np.linalg.norm(z64)
     P.close()
+
+
+@pytest.mark.parametrize("dims", [(6, 12, 6), (17, 40, 23), (30, 60, 30)])
+def test_every_modal_tile_shape_gives_identical_results(dims):
+    import algorithmengineering_altproject_b200 as t3d
+    rng = np.random.default_rng(21)
+    ref = None
+    shapes = []
+    for v in range(64):
+        try:
+            P = t3d.Problem(*dims, precision=t3d.T3D_MIXED, matvec32_tile=v + 1)
+        except t3d.T3DError:
+            break
+        assert P.info().matvec32_variant == v
+        shapes.append(tuple(P.info().matvec32_tile))
+        if ref is None:
+            E = np.where(rng.random(P.ne) < 0.5, 1e-9, rng.uniform(0.01, 1.0, P.ne))
+            u = rng.standard_normal(P.nf)
+        y = P.K_times_u_finest32(E, u)
+        if ref is None:
+            ref = y
+        np.testing.assert_array_equal(y, ref, err_msg="tile shape %d %s" % (v, shapes[-1]))
+        P.close()
+    assert len(shapes) >= 6 and any(s[3] == 2 for s in shapes), shapes   # the TMA-staged shapes are among them
