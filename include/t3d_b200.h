@@ -113,9 +113,9 @@ typedef struct t3d_info {
     int64_t matvec32_tile[4];     /* tile shape the modal kernel's autotuner chose: threads in x, threads in y,
                                      plane-ring slots, plane staging (0 per-thread cp.async, 1 the same with packed
                                      FP32x2 arithmetic, 2 packed arithmetic with TMA bulk tensor copies) */
-    int64_t matvec32_variant;     /* index of that shape (params.matvec32_tile - 1 selects it) */
     int64_t matvec64_kernel;      /* FP64 K(E)u kernel: 0 node-centric, 1 streaming with Ke from the constant bank,
                                      2 streaming with the built-in Ke's magnitudes in registers */
+    int64_t matvec32_variant;     /* index of the modal tile shape (params.matvec32_tile - 1 selects it) */
 } t3d_info;
 
 typedef struct t3d_iter_record {  /* one design iteration (driver.cpp:205-216) */
