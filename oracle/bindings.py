@@ -152,12 +152,14 @@ class _Common:
         self._fss(self.h, np.ascontiguousarray(lastx, np.float64), np.ascontiguousarray(lastrhs, np.float64))
 
 
-def voxel_model_from_rows(nelx, nely, nelz, solid, passive=(), fixations=(), load_cases=((),)):
+def voxel_model_from_rows(nelx, nely, nelz, solid, passive=(), fixations=(), load_cases=((),),
+                          loaded_nodes_free=True):
     """The arrays of an external model for `Oracle(..., voxel_model=...)` from 0-based rows: solid and passive
     voxels (x, y, z), fixations (x, y, z, fx, fy, fz) with 0/1 flags, load cases of (x, y, z, Fx, Fy, Fz).
     As in the MATLAB reader (TOP3D_XL.m:529-545): duplicate nodes keep their first row, nodes ascending;
-    all-zero fixation rows fix nothing.  As in FEA_ApplyBoundaryCondition (TOP3D_XL.m:1326-1331): a node that
-    any load case loads loses its fixation row."""
+    all-zero fixation rows fix nothing.  With loaded_nodes_free (a TopVoxel file, FEA_ApplyBoundaryCondition
+    TOP3D_XL.m:1326-1331) a node that any load case loads loses its fixation row; without it (the restatement
+    of a built-in problem spec) fixations stay and loads on fixed DOFs are dropped."""
     vox = np.zeros(nelx * nely * nelz, dtype=np.uint8)
     for x, y, z in solid:
         vox[y + nely * (x + nelx * z)] = 1
@@ -177,8 +179,9 @@ def voxel_model_from_rows(nelx, nely, nelz, solid, passive=(), fixations=(), loa
         nodes += keys
         forces += [v for k in keys for v in rows[k]]
         counts.append(len(keys))
-    for k in nodes:
-        fix.pop(k, None)
+    if loaded_nodes_free:
+        for k in nodes:
+            fix.pop(k, None)
     keys = sorted(fix)
     return {"voxel": vox, "fix_node": np.array(keys, dtype=np.int64), "fix_bits": np.array([fix[k] for k in keys],
             dtype=np.uint8), "case_n": np.array(counts, dtype=np.int32), "load_node": np.array(nodes, dtype=np.int64),

@@ -144,7 +144,7 @@ def spec_as_voxel_model(P, nely, nelx, nelz, load_case, voids):
         f = 1.0 / (nely + 1)
         loads = [(nelx, y, nelz, 0.0, f, 0.0) for y in range(nely + 1)] + \
                 [(nelx, y, 0, 0.0, -f, 0.0) for y in range(nely + 1)]
-    return voxel_model_from_rows(nelx, nely, nelz, solid, fixations=fix, load_cases=[loads])
+    return voxel_model_from_rows(nelx, nely, nelz, solid, fixations=fix, load_cases=[loads], loaded_nodes_free=False)
 
 
 @pytest.mark.parametrize("load_case", [0, 1, 2])
