@@ -184,6 +184,11 @@ def cfg1_traj():
         shutil.rmtree(work, ignore_errors=True)
         for k, v in r.items():
             d["%s_%s" % (tag, k)] = v
+    # final densities: the full-field build-to-build drift and seeded samples of both builds
+    idx = sample_indices(seed, 10, len(d["ref_xfinal"]))
+    d["idx_x"] = idx
+    d["xdrift_full"] = float(np.abs(d["ref_xfinal"] - d["nofm_xfinal"]).max())
+    d["ref_xfinal"], d["nofm_xfinal"] = d["ref_xfinal"][idx], d["nofm_xfinal"][idx]
     np.savez_compressed(os.path.join(HERE, "cfg1_traj.npz"), **d)
     print("cfg1 traj: ref C", d["ref_C"], "nofm C", d["nofm_C"], "iters", d["ref_iters"])
 
