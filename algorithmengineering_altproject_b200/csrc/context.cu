@@ -138,6 +138,10 @@ struct Context {
     float *r32 = nullptr, *d32 = nullptr, *z32 = nullptr, *p32 = nullptr, *Ap32 = nullptr;
     MgLevel32 lv32[8]{};
     float* ra1_32[8]{};         // x-pass buffer of the FP32 restriction (its y and z passes are fused)
+    // the Standard V-cycle in FP32: element-matrix images and scratch per coarse level, level-0 moduli image
+    float* Kel32[8]{};
+    float* vtmp32[8]{};
+    float* E_mg32 = nullptr;
     PcgScalars* S32 = nullptr;
     int* tma_err = nullptr;     // set by a TMA-staged K(E)p whose mbarrier wait gave up (checked after solves)
     cudaGraphExec_t pcg32_graph = nullptr;
@@ -325,6 +329,15 @@ static int build_mixed(Context* c) {
         const MgLevel &Lf = c->lv[l], &Lc = c->lv[l + 1];
         CHECK(c->alloc(&c->ra1_32[l], (size_t)3 * (Lf.nz + 1) * (Lf.ny + 1) * (Lc.nx + 1)));
     }
+    if (c->standard) {
+        CHECK(c->alloc(&c->E_mg32, g.NEp));
+        T3D_CUDA_OK(cudaMemsetAsync(c->E_mg32, 0, g.NEp * sizeof(float), c->st));
+        for (int l = 1; l < c->nlev; ++l) {
+            const MgLevel& L = c->lv[l];
+            CHECK(c->alloc(&c->Kel32[l], (size_t)L.nx * L.ny * L.nz * 576));
+            CHECK(c->alloc(&c->vtmp32[l], 3 * L.nn));
+        }
+    }
     float k32[576];
     for (int i = 0; i < 576; ++i) k32[i] = (float)c->Ke_h[i];
     T3D_CUDA_OK(cudaMemcpyAsync(c->Ke32, k32, sizeof k32, cudaMemcpyHostToDevice, c->st));
@@ -336,11 +349,14 @@ static int build_mixed(Context* c) {
     return check_tma(c);
 }
 
-// FP32 K(E)p on the FP32 images (E32, x -> y); with dot.partial, x.y goes to S->denom
-static void matvec32(Context* c, const float* x, float* y, RedSlot dot, PcgScalars* S) {
+// FP32 K(E)p on the FP32 images (moduli E, default E32; x -> y); with dot.partial, x.y goes to S->denom.
+// mark = 0 for the operator inside the Standard V-cycle (leaves the PCG's S->xit alone).
+static void matvec32(Context* c, const float* x, float* y, RedSlot dot, PcgScalars* S, int mark = 1,
+                     const float* E = nullptr) {
     c->launches += 1;
-    if (c->modal) launch_matvec32_modal(c->g, c->kh, c->mt, c->E32, c->mask0, x, y, dot, S, c->tma_err, c->st);
-    else launch_matvec32(c->g, c->Ke32, c->E32, c->mask0, x, y, dot, S, c->st);
+    if (!E) E = c->E32;
+    if (c->modal) launch_matvec32_modal(c->g, c->kh, c->mt, E, c->mask0, x, y, dot, S, mark, c->tma_err, c->st);
+    else launch_matvec32(c->g, c->Ke32, E, c->mask0, x, y, dot, S, mark, c->st);
 }
 
 // Load vector b of the context's load case on its free DOFs (fixed DOFs are skipped).
@@ -469,8 +485,6 @@ static int create(int nely, int nelx, int nelz, const t3d_params* prm, const t3d
         return set_error(T3D_ERR_UNSUPPORTED, "matvec64_form must be T3D_MATVEC64_AUTO or T3D_MATVEC64_NODES");
     if (c->prm.mg_vcycle != T3D_VCYCLE_ADAPTED && c->prm.mg_vcycle != T3D_VCYCLE_STANDARD)
         return set_error(T3D_ERR_UNSUPPORTED, "mg_vcycle must be T3D_VCYCLE_ADAPTED or T3D_VCYCLE_STANDARD");
-    if (c->prm.mg_vcycle == T3D_VCYCLE_STANDARD && c->prm.precision != T3D_FP64)
-        return set_error(T3D_ERR_UNSUPPORTED, "the Standard V-cycle is built for precision T3D_FP64 only");
     // fields that were reserved (zero) in earlier versions of t3d_params: 0 selects the default
     if (c->prm.mg_rebuild_period == 0) c->prm.mg_rebuild_period = 5;
     if (c->prm.mg_standard_weight == 0.0f) c->prm.mg_standard_weight = 0.35f;
@@ -705,6 +719,19 @@ static int mg_setup(Context* c) {
             launch_cholesky(c->Kc, c->LT, c->Lrow, c->Nc, c->chol_status, c->st);
             launch_coarse_inverse(c->Lrow, c->Nc, c->chol_status, c->Xc, c->st);
         }
+        if (c->mixed) {   // FP32 images: level-0 moduli, coarse element matrices, reciprocal diagonals
+            launch_cells_to32(c->g, c->E_mg, c->E_mg32, c->st);
+            for (int l = 1; l < c->nlev; ++l) {
+                const MgLevel& L = c->lv[l];
+                launch_rows_to32((int64_t)L.nx * L.ny * L.nz, 576, c->Kel[l], c->Kel32[l], c->st);
+            }
+            for (int l = 0; l < c->nlev; ++l) {
+                const MgLevel32& M = c->lv32[l];
+                launch_recip_diag32(3 * (int64_t)(M.ny + 1) * (M.nz + 1), M.nx + 1, M.pitch, c->lv[l].diag, M.diag,
+                                    c->st);
+            }
+            c->launches += 2 * c->nlev;
+        }
         c->mg_ready = true;
         return launch_check("mg set-up");
     }
@@ -875,7 +902,48 @@ static int pcg_solve(Context* c, double tol, int maxit, int* iters) {
 }
 
 // ------------------------------------------------------------------ mixed-precision solve
+// The Standard cycle in FP32 (k_mg_standard32.cu): the same steps as vcycle_standard; level 0 uses Ap32 as
+// scratch and the modal FP32 K(E) of the hierarchy's moduli as its operator
+static void vcycle32_standard(Context* c, const float* r, float* z, PcgScalars* S, RedSlot dot) {
+    const int L = c->nlev;
+    const float w = c->prm.mg_standard_weight;
+    auto level_op = [&](int l, const float* x, float* y) {
+        if (l == 0) matvec32(c, x, y, RedSlot{nullptr, nullptr}, S, 0, c->E_mg32);
+        else {
+            launch_level_matvec32(c->lv32[l], c->Kel32[l], x, y, S, c->st);
+            c->launches += 1;
+        }
+    };
+    for (int l = 0; l + 1 < L; ++l) {
+        const float* rl = l == 0 ? r : c->lv32[l].r;
+        float* xl = l == 0 ? z : c->lv32[l].x;
+        float* t = l == 0 ? c->Ap32 : c->vtmp32[l];
+        launch_jacobi_init32(c->lv32[l], rl, xl, w, S, c->st);
+        level_op(l, xl, t);
+        launch_residual32(c->lv32[l], rl, t, S, c->st);
+        launch_restrict32(c->lv32[l + 1], c->lv32[l], t, c->lv32[l + 1].r, c->ra1_32[l], S, c->st, false);
+        c->launches += 2 + (c->lv32[l + 1].span == 4 ? 2 : 1);
+    }
+    launch_coarse_solve32(c->lv32[L - 1], c->Xc, c->Nc, c->chol_status, S, c->st);
+    c->launches += 1;
+    for (int l = L - 2; l >= 0; --l) {
+        const float* rl = l == 0 ? r : c->lv32[l].r;
+        float* xl = l == 0 ? z : c->lv32[l].x;
+        float* t = l == 0 ? c->Ap32 : c->vtmp32[l];
+        launch_prolong_add32(c->lv32[l + 1], c->lv32[l], c->lv32[l + 1].x, xl, S, c->st);
+        level_op(l, xl, t);
+        launch_jacobi_correct32(c->lv32[l], rl, t, xl, w, S, c->st);
+        c->launches += 2;
+    }
+    launch_dot_rz32(3 * c->g.NNp, r, z, dot, S, c->st);
+    c->launches += 1;
+}
+
 static void vcycle32(Context* c, const float* r, float* z, PcgScalars* S, RedSlot dot) {
+    if (c->standard) {
+        vcycle32_standard(c, r, z, S, dot);
+        return;
+    }
     const int L = c->nlev;
     // per transition: restriction (x + y-z passes for span 4, one x-y-z pass for span 2) and prolongation
     for (int l = 0; l + 1 < L; ++l) c->launches += c->lv32[l + 1].span == 2 ? 2 : 3;

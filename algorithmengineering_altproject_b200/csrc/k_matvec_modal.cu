@@ -66,13 +66,14 @@ template <int BX, int BY, int MINB, int STAGES, int PACK>
 __global__ void __launch_bounds__(BX * BY, MINB)
     k_matvec32_modal(Grid g, ModalKe kh, ModalTiling t, const float* __restrict__ E,
                      const uint8_t* __restrict__ mask, const float* __restrict__ u, float* __restrict__ y,
-                     RedSlot dot, PcgScalars* S) {
+                     RedSlot dot, PcgScalars* S, int mark) {
     constexpr int PX = BX + 1, PY = BY + 1;
     static_assert(PY <= BX, "the footprint column is loaded by one row of BX threads");
     static_assert(STAGES >= 2, "ring needs two slots at least");
     extern __shared__ __align__(16) unsigned char smem_raw[];
     ModalSmem<BX, BY, STAGES>& sm = *reinterpret_cast<ModalSmem<BX, BY, STAGES>*>(smem_raw);
-    if (S != nullptr && blockIdx.x == 0 && threadIdx.x == 0) S->xit = S->it;   // last alpha is in x
+    // mark: the PCG product (not an operator inside the V-cycle) records that the last alpha is in x
+    if (S != nullptr && mark && blockIdx.x == 0 && threadIdx.x == 0) S->xit = S->it;
     if (S != nullptr && S->done) return;
     const int tx = threadIdx.x % BX, ty = threadIdx.x / BX;
     // FP32 images are pitched (rows of g.px nodes, g.pex cells); the node mask is not
@@ -344,9 +345,9 @@ struct ModalShape {
     static constexpr size_t smem = sizeof(ModalSmem<BX, BY, ST>);
     static const void* fn() { return reinterpret_cast<const void*>(k_matvec32_modal<BX, BY, MINB, ST, PACK>); }
     static bool launch(const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E, const uint8_t* mask,
-                       const float* u, float* y, RedSlot dot, PcgScalars* S, int* err, cudaStream_t s) {
+                       const float* u, float* y, RedSlot dot, PcgScalars* S, int mark, int* err, cudaStream_t s) {
         (void)err;
-        k_matvec32_modal<BX, BY, MINB, ST, PACK><<<t.grid, BX * BY, smem, s>>>(g, kh, t, E, mask, u, y, dot, S);
+        k_matvec32_modal<BX, BY, MINB, ST, PACK><<<t.grid, BX * BY, smem, s>>>(g, kh, t, E, mask, u, y, dot, S, mark);
         return true;
     }
 };
@@ -357,10 +358,10 @@ struct TmaShape {
     static constexpr size_t smem = sizeof(SM) + 128;   // + slack for the 128-byte alignment of the ring
     static const void* fn() { return reinterpret_cast<const void*>(k_matvec32_tma<BX, BY, MINB, ST>); }
     static bool launch(const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E, const uint8_t* mask,
-                       const float* u, float* y, RedSlot dot, PcgScalars* S, int* err, cudaStream_t s) {
+                       const float* u, float* y, RedSlot dot, PcgScalars* S, int mark, int* err, cudaStream_t s) {
         CUtensorMap um, em;
         if (!modal_tensor_maps(g, u, E, SM::RW, SM::PY, BY, &um, &em)) return false;
-        k_matvec32_tma<BX, BY, MINB, ST><<<t.grid, BX * BY, smem, s>>>(um, em, g, kh, t, mask, y, dot, S, err);
+        k_matvec32_tma<BX, BY, MINB, ST><<<t.grid, BX * BY, smem, s>>>(um, em, g, kh, t, mask, y, dot, S, mark, err);
         return true;
     }
 };
@@ -369,7 +370,7 @@ struct ModalVariant {
     size_t smem;
     const void* (*fn)();
     bool (*launch)(const Grid&, const ModalKe&, const ModalTiling&, const float*, const uint8_t*, const float*,
-                   float*, RedSlot, PcgScalars*, int*, cudaStream_t);
+                   float*, RedSlot, PcgScalars*, int, int*, cudaStream_t);
 };
 template <class V>
 constexpr ModalVariant variant_of() {
@@ -488,9 +489,9 @@ int modal_autotune(const Grid& g, int dev, const ModalKe& kh, const float* E, co
         ModalTiling t{};
         if ((rc = modal_tiling(g, dev, v, &t)) != 0) break;
         const RedSlot none{nullptr, nullptr};
-        if (!MODAL_VARIANTS[v].launch(g, kh, t, E, mask, u, y, none, nullptr, err, s)) continue;   // warm-up
+        if (!MODAL_VARIANTS[v].launch(g, kh, t, E, mask, u, y, none, nullptr, 0, err, s)) continue;   // warm-up
         cudaEventRecord(e0, s);
-        for (int r = 0; r < 3; ++r) MODAL_VARIANTS[v].launch(g, kh, t, E, mask, u, y, none, nullptr, err, s);
+        for (int r = 0; r < 3; ++r) MODAL_VARIANTS[v].launch(g, kh, t, E, mask, u, y, none, nullptr, 0, err, s);
         cudaEventRecord(e1, s);
         if ((e = cudaEventSynchronize(e1)) != cudaSuccess) {
             rc = set_cuda_error(e, "modal autotune", __FILE__, __LINE__);
@@ -511,15 +512,15 @@ int modal_autotune(const Grid& g, int dev, const ModalKe& kh, const float* E, co
 }
 
 void launch_matvec32_modal(const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E,
-                           const uint8_t* mask, const float* u, float* y, RedSlot dot, PcgScalars* S, int* err,
-                           cudaStream_t s) {
-    if (MODAL_VARIANTS[t.variant].launch(g, kh, t, E, mask, u, y, dot, S, err, s)) return;
+                           const uint8_t* mask, const float* u, float* y, RedSlot dot, PcgScalars* S, int mark,
+                           int* err, cudaStream_t s) {
+    if (MODAL_VARIANTS[t.variant].launch(g, kh, t, E, mask, u, y, dot, S, mark, err, s)) return;
     // no tensor map for these buffers: the cp.async form of the same arithmetic (bit-identical results)
     ModalTiling t0 = t;
     int dev = 0;
     cudaGetDevice(&dev);
     modal_tiling(g, dev, 0, &t0);
-    MODAL_VARIANTS[0].launch(g, kh, t0, E, mask, u, y, dot, S, err, s);
+    MODAL_VARIANTS[0].launch(g, kh, t0, E, mask, u, y, dot, S, mark, err, s);
 }
 
 }  // namespace t3d

@@ -102,14 +102,15 @@ template <int BX, int BY, int MINB, int STAGES>
 __global__ void __launch_bounds__(BX * BY, MINB)
     k_matvec32_tma(const __grid_constant__ CUtensorMap umap, const __grid_constant__ CUtensorMap emap, Grid g,
                    ModalKe kh, ModalTiling t, const uint8_t* __restrict__ mask, float* __restrict__ y, RedSlot dot,
-                   PcgScalars* S, int* err) {
+                   PcgScalars* S, int mark, int* err) {
     using SM = TmaSmem<BX, BY, STAGES>;
     constexpr int RW = SM::RW, PY = SM::PY;
     static_assert(STAGES >= 2, "ring needs two slots at least");
     extern __shared__ __align__(128) unsigned char tma_smem_raw[];
     // TMA destinations must be 128-byte aligned: the launch adds 128 bytes of slack for this shift
     SM& sm = *reinterpret_cast<SM*>(tma_smem_raw + ((128u - (smem_u32(tma_smem_raw) & 127u)) & 127u));
-    if (S != nullptr && blockIdx.x == 0 && threadIdx.x == 0) S->xit = S->it;   // last alpha is in x
+    // mark: the PCG product (not an operator inside the V-cycle) records that the last alpha is in x
+    if (S != nullptr && mark && blockIdx.x == 0 && threadIdx.x == 0) S->xit = S->it;
     if (S != nullptr && S->done) return;
     const int tx = threadIdx.x % BX, ty = threadIdx.x / BX;
     const bool producer = threadIdx.x == 0;

@@ -1,0 +1,191 @@
+// The 'Standard' V-cycle (TOP3D_XL.m:772-807; FP64 form and derivation in k_mg_standard.cu) in FP32 for the
+// mixed-precision inner solve:
+//
+//   down, l = 0..L-2:  x_l = w r_l / D_l;  r_{l+1} = P^T (r_l - K_l x_l)
+//   coarsest:          x_L = K_L^{-1} r_L  (the FP64 inverse of the Galerkin coarsest matrix)
+//   up,   l = L-2..0:  x_l += P x_{l+1};  x_l += w (r_l - K_l x_l) / D_l
+//
+// FP32 storage and arithmetic: the level vectors, the reciprocal diagonals 1/D_l, the Galerkin element
+// matrices of the coarse levels (FP32 images of the FP64 set-up), and K_0 = the modal FP32 K(E) of the moduli
+// the hierarchy was built from.  Level 0's vectors are pitched (Grid::px rows, MgLevel32::pitch/cs); the
+// coarse levels' are not.  Every kernel skips its work once S->done (the inner PCG converged).
+#include "kernels.hpp"
+#include "red.cuh"
+
+namespace t3d {
+
+namespace {
+
+__device__ __forceinline__ float tri_wf(int s, int fx, int fy, int fz, int A) {
+    const float is = 1.0f / (float)s;   // s is 2 or 4: exact
+    const float wx = corner_dx(A) ? fx * is : (s - fx) * is;
+    const float wy = corner_dy(A) ? fy * is : (s - fy) * is;
+    const float wz = corner_dz(A) ? fz * is : (s - fz) * is;
+    return wx * wy * wz;
+}
+
+// node n (unpadded, the mask's index) of level L -> index into its (possibly pitched) vectors
+__device__ __forceinline__ int64_t vidx(const MgLevel32& L, int64_t n) {
+    const int nnx = L.nx + 1;
+    return (n / nnx) * L.pitch + n % nnx;
+}
+
+// x = w r / D
+__global__ void k_jacobi_init32(MgLevel32 L, const float* __restrict__ r, float* __restrict__ x, float w,
+                                const PcgScalars* S) {
+    if (S->done) return;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < L.nn; n += (int64_t)gridDim.x * blockDim.x) {
+        const int m = L.mask[n];
+        const int64_t v = vidx(L, n);
+        for (int c = 0; c < 3; ++c) {
+            const int64_t i = c * L.cs + v;
+            x[i] = ((m >> c) & 1) ? 0.0f : (w * r[i]) * L.diag[i];
+        }
+    }
+}
+
+// kx <- r - kx
+__global__ void k_residual32(MgLevel32 L, const float* __restrict__ r, float* __restrict__ kx, const PcgScalars* S) {
+    if (S->done) return;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < L.nn; n += (int64_t)gridDim.x * blockDim.x) {
+        const int m = L.mask[n];
+        const int64_t v = vidx(L, n);
+        for (int c = 0; c < 3; ++c) {
+            const int64_t i = c * L.cs + v;
+            kx[i] = ((m >> c) & 1) ? 0.0f : r[i] - kx[i];
+        }
+    }
+}
+
+// x += w (r - kx) / D
+__global__ void k_jacobi_correct32(MgLevel32 L, const float* __restrict__ r, const float* __restrict__ kx,
+                                   float* __restrict__ x, float w, const PcgScalars* S) {
+    if (S->done) return;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < L.nn; n += (int64_t)gridDim.x * blockDim.x) {
+        const int m = L.mask[n];
+        const int64_t v = vidx(L, n);
+        for (int c = 0; c < 3; ++c) {
+            const int64_t i = c * L.cs + v;
+            x[i] = ((m >> c) & 1) ? 0.0f : x[i] + (w * (r[i] - kx[i])) * L.diag[i];
+        }
+    }
+}
+
+// xf += P xc (trilinear from the coarse cell floor(f/s), clamped to the last cell), fixed DOFs 0
+__global__ void k_prolong_add32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ xc, float* __restrict__ xf,
+                                const PcgScalars* S) {
+    if (S->done) return;
+    const int s = Lc.span;
+    const int fnx = Lf.nx + 1, fny = Lf.ny + 1, cnx = Lc.nx + 1, cny = Lc.ny + 1;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < Lf.nn; n += (int64_t)gridDim.x * blockDim.x) {
+        const int fx = (int)(n % fnx), fy = (int)((n / fnx) % fny), fz = (int)(n / ((int64_t)fnx * fny));
+        int cx = fx / s, cy = fy / s, cz = fz / s;
+        if (cx >= Lc.nx) cx = Lc.nx - 1;
+        if (cy >= Lc.ny) cy = Lc.ny - 1;
+        if (cz >= Lc.nz) cz = Lc.nz - 1;
+        const int m = Lf.mask[n];
+        const int64_t v = vidx(Lf, n);
+        for (int c = 0; c < 3; ++c) {
+            float p = 0.0f;
+            for (int A = 0; A < 8; ++A)
+                p = fmaf(tri_wf(s, fx - cx * s, fy - cy * s, fz - cz * s, A),
+                         xc[c * Lc.cs + ((int64_t)(cz + corner_dz(A)) * cny + cy + corner_dy(A)) * cnx + cx + corner_dx(A)],
+                         p);
+            const int64_t i = c * Lf.cs + v;
+            xf[i] = ((m >> c) & 1) ? 0.0f : xf[i] + p;
+        }
+    }
+}
+
+// y = K_l x from the FP32 element matrices of a coarse level (node-centric gather: each node reads the three
+// rows of its corner in the 8 element matrices around it, so every matrix entry is read once), fixed DOFs 0
+__global__ void k_level_matvec32(MgLevel32 L, const float* __restrict__ Kel, const float* __restrict__ x,
+                                 float* __restrict__ y, const PcgScalars* S) {
+    if (S->done) return;
+    const int nnx = L.nx + 1, nny = L.ny + 1;
+    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < L.nn; n += (int64_t)gridDim.x * blockDim.x) {
+        const int X = (int)(n % nnx), Y = (int)((n / nnx) % nny), Z = (int)(n / ((int64_t)nnx * nny));
+        float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f;
+        for (int dz = 0; dz <= 1; ++dz)
+            for (int dy = 0; dy <= 1; ++dy)
+                for (int dx = 0; dx <= 1; ++dx) {
+                    const int ex = X - dx, ey = Y - dy, ez = Z - dz;
+                    if (ex < 0 || ey < 0 || ez < 0 || ex >= L.nx || ey >= L.ny || ez >= L.nz) continue;
+                    const int a = corner_of(dx, dy, dz);
+                    const float* K = Kel + ((int64_t)((ez * L.ny + ey) * L.nx + ex)) * 576 + (3 * a) * 24;
+#pragma unroll
+                    for (int b = 0; b < 8; ++b) {
+                        const int64_t m = ((int64_t)(ez + corner_dz(b)) * nny + ey + corner_dy(b)) * nnx + ex + corner_dx(b);
+#pragma unroll
+                        for (int c = 0; c < 3; ++c) {
+                            const float xv = x[c * L.cs + m];
+                            acc0 = fmaf(K[3 * b + c], xv, acc0);
+                            acc1 = fmaf(K[24 + 3 * b + c], xv, acc1);
+                            acc2 = fmaf(K[48 + 3 * b + c], xv, acc2);
+                        }
+                    }
+                }
+        const int mk = L.mask[n];
+        y[n] = (mk & 1) ? 0.0f : acc0;
+        y[L.cs + n] = (mk & 2) ? 0.0f : acc1;
+        y[2 * L.cs + n] = (mk & 4) ? 0.0f : acc2;
+    }
+}
+
+// r.z over pitched FP32 vectors (pads zero), accumulated in FP64; the last block sets rz (first use) or
+// beta = rz_new / max(1e-30, rz), rz = rz_new
+__global__ void __launch_bounds__(RED_THREADS) k_dot_rz32(int64_t n3, const float* __restrict__ r,
+                                                          const float* __restrict__ z, RedSlot red, PcgScalars* S) {
+    __shared__ double sh[32];
+    if (S->done) return;
+    const int64_t n4 = n3 >> 2;
+    const float4* r4 = reinterpret_cast<const float4*>(r);
+    const float4* z4 = reinterpret_cast<const float4*>(z);
+    double part = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x) {
+        const float4 a = r4[i], b = z4[i];
+        part += (double)fmaf(a.w, b.w, fmaf(a.z, b.z, fmaf(a.y, b.y, a.x * b.x)));
+    }
+    double tot;
+    if (grid_fold(part, red, sh, &tot) && threadIdx.x == 0) {
+        if (S->first) {
+            S->rz = tot;
+            S->first = 0;
+        } else {
+            const double rz = S->rz;
+            S->beta = tot / (1.0e-30 < rz ? rz : 1.0e-30);
+            S->rz = tot;
+        }
+    }
+}
+
+inline unsigned blocks_of(int64_t n, int t) {
+    const int64_t b = (n + t - 1) / t;
+    return (unsigned)(b < 8 * RED_BLOCKS ? (b > 0 ? b : 1) : 8 * RED_BLOCKS);
+}
+
+}  // namespace
+
+void launch_jacobi_init32(const MgLevel32& L, const float* r, float* x, float w, const PcgScalars* S, cudaStream_t s) {
+    k_jacobi_init32<<<blocks_of(L.nn, 256), 256, 0, s>>>(L, r, x, w, S);
+}
+void launch_residual32(const MgLevel32& L, const float* r, float* kx, const PcgScalars* S, cudaStream_t s) {
+    k_residual32<<<blocks_of(L.nn, 256), 256, 0, s>>>(L, r, kx, S);
+}
+void launch_jacobi_correct32(const MgLevel32& L, const float* r, const float* kx, float* x, float w,
+                             const PcgScalars* S, cudaStream_t s) {
+    k_jacobi_correct32<<<blocks_of(L.nn, 256), 256, 0, s>>>(L, r, kx, x, w, S);
+}
+void launch_prolong_add32(const MgLevel32& Lc, const MgLevel32& Lf, const float* xc, float* xf, const PcgScalars* S,
+                          cudaStream_t s) {
+    k_prolong_add32<<<blocks_of(Lf.nn, 256), 256, 0, s>>>(Lc, Lf, xc, xf, S);
+}
+void launch_level_matvec32(const MgLevel32& L, const float* Kel, const float* x, float* y, const PcgScalars* S,
+                           cudaStream_t s) {
+    k_level_matvec32<<<blocks_of(L.nn, 128), 128, 0, s>>>(L, Kel, x, y, S);
+}
+void launch_dot_rz32(int64_t n3, const float* r, const float* z, RedSlot red, PcgScalars* S, cudaStream_t s) {
+    k_dot_rz32<<<RED_BLOCKS, RED_THREADS, 0, s>>>(n3, r, z, red, S);
+}
+
+}  // namespace t3d

@@ -88,10 +88,10 @@ __global__ void __launch_bounds__(RED_THREADS) k_matvec32(Grid g, const float* _
                                                           const float* __restrict__ E,
                                                           const uint8_t* __restrict__ mask,
                                                           const float* __restrict__ u, float* __restrict__ y,
-                                                          RedSlot dot, PcgScalars* S) {
+                                                          RedSlot dot, PcgScalars* S, int mark) {
     __shared__ __align__(16) float Ke[576];
     __shared__ double sh[32];
-    if (S != nullptr && blockIdx.x == 0 && threadIdx.x == 0) S->xit = S->it;   // last alpha is in x
+    if (S != nullptr && mark && blockIdx.x == 0 && threadIdx.x == 0) S->xit = S->it;   // the PCG product
     if (S != nullptr && S->done) return;
     for (int i = threadIdx.x; i < 576; i += blockDim.x) Ke[i] = Keg[i];
     __syncthreads();
@@ -199,7 +199,7 @@ __device__ __forceinline__ float hat_sum(int c, int n) {
 // weights and masked (the k_restrict_y32 + k_restrict_z32 pair fused; one thread per coarse node).
 template <int SP>
 __global__ void __launch_bounds__(256) k_restrict_yz32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ a1,
-                                                       float* __restrict__ rc, const PcgScalars* S) {
+                                                       float* __restrict__ rc, const PcgScalars* S, int normalize) {
     if (S->done) return;
     constexpr int WS = 2 * SP - 1;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -229,7 +229,8 @@ __global__ void __launch_bounds__(256) k_restrict_yz32(MgLevel32 Lc, MgLevel32 L
         v1 = fmaf(w, s1, v1);
         v2 = fmaf(w, s2, v2);
     }
-    const float iw = 1.0f / (hat_sum<SP>(cz, fnz) * hat_sum<SP>(cy, fny) * hat_sum<SP>(cx, fnx));
+    // normalised average (transfers.cpp:520-528) or, for the Standard cycle, the transposed prolongation
+    const float iw = normalize ? 1.0f / (hat_sum<SP>(cz, fnz) * hat_sum<SP>(cy, fny) * hat_sum<SP>(cx, fnx)) : 1.0f;
     const int m = Lc.mask[n];
     rc[n] = (m & 1) ? 0.0f : v0 * iw;
     rc[Lc.nn + n] = (m & 2) ? 0.0f : v1 * iw;
@@ -239,7 +240,7 @@ __global__ void __launch_bounds__(256) k_restrict_yz32(MgLevel32 Lc, MgLevel32 L
 // The whole 3D window of the fine residual in one pass (levels small enough to sit in L2).
 template <int SP>
 __global__ void __launch_bounds__(256) k_restrict_xyz32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ rf,
-                                                        float* __restrict__ rc, const PcgScalars* S) {
+                                                        float* __restrict__ rc, const PcgScalars* S, int normalize) {
     if (S->done) return;
     constexpr int WS = 2 * SP - 1;
     const int n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -279,7 +280,8 @@ __global__ void __launch_bounds__(256) k_restrict_xyz32(MgLevel32 Lc, MgLevel32 
         v1 = fmaf(w, t1, v1);
         v2 = fmaf(w, t2, v2);
     }
-    const float iw = 1.0f / (hat_sum<SP>(cz, fnz) * hat_sum<SP>(cy, fny) * hat_sum<SP>(cx, fnx));
+    // normalised average (transfers.cpp:520-528) or, for the Standard cycle, the transposed prolongation
+    const float iw = normalize ? 1.0f / (hat_sum<SP>(cz, fnz) * hat_sum<SP>(cy, fny) * hat_sum<SP>(cx, fnx)) : 1.0f;
     const int m = Lc.mask[n];
     rc[n] = (m & 1) ? 0.0f : v0 * iw;
     rc[Lc.nn + n] = (m & 2) ? 0.0f : v1 * iw;
@@ -541,20 +543,23 @@ void launch_recip_diag32(int64_t rows, int len, int pitch, const double* d, floa
 }
 
 void launch_matvec32(const Grid& g, const float* Ke, const float* E, const uint8_t* mask, const float* u, float* y,
-                     RedSlot dot, PcgScalars* S, cudaStream_t s) {
-    k_matvec32<<<RED_BLOCKS, RED_THREADS, 0, s>>>(g, Ke, E, mask, u, y, dot, S);
+                     RedSlot dot, PcgScalars* S, int mark, cudaStream_t s) {
+    k_matvec32<<<RED_BLOCKS, RED_THREADS, 0, s>>>(g, Ke, E, mask, u, y, dot, S, mark);
 }
 // x pass then a fused y-z pass on the finest transition (span 4); one fused x-y-z pass on the
 // coarser ones (span 2), whose fine residual sits in L2.
 void launch_restrict32(const MgLevel32& Lc, const MgLevel32& Lf, const float* rf, float* rc, float* a1,
-                       const PcgScalars* S, cudaStream_t s) {
+                       const PcgScalars* S, cudaStream_t s, bool normalize) {
     const int64_t n1 = (int64_t)(Lf.nz + 1) * (Lf.ny + 1) * (Lc.nx + 1);
     if (Lc.span == 4) {
         k_restrict_x32<<<blocks_for(n1, 256), 256, 0, s>>>(Lc, Lf, rf, a1, S);
-        k_restrict_yz32<4><<<blocks_for(Lc.nn, 256), 256, 0, s>>>(Lc, Lf, a1, rc, S);
+        k_restrict_yz32<4><<<blocks_for(Lc.nn, 256), 256, 0, s>>>(Lc, Lf, a1, rc, S, normalize ? 1 : 0);
     } else {
-        k_restrict_xyz32<2><<<blocks_for(Lc.nn, 256), 256, 0, s>>>(Lc, Lf, rf, rc, S);
+        k_restrict_xyz32<2><<<blocks_for(Lc.nn, 256), 256, 0, s>>>(Lc, Lf, rf, rc, S, normalize ? 1 : 0);
     }
+}
+void launch_rows_to32(int64_t rows, int len, const double* a, float* b, cudaStream_t s) {
+    k_rows_convert<double, float><<<RED_BLOCKS, 256, 0, s>>>(rows, len, len, len, a, b);
 }
 void launch_prolong_smooth32(const MgLevel32& Lc, const MgLevel32& Lf, const float* xc, const float* rf, float* xf,
                              float w, const PcgScalars* S, cudaStream_t s) {

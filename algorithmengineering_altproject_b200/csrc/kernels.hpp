@@ -224,11 +224,25 @@ void launch_recip_diag32(int64_t rows, int len, int pitch, const double* d, floa
 void launch_mixed_residual(const Grid& g, const double* b, const double* Au, float* r32, float* d32, RedSlot red,
                            double* rn2, cudaStream_t s);
 void launch_mixed_accumulate(const Grid& g, double* u, const float* d, cudaStream_t s);
+// mark = 1 for the PCG's own K(E)p (records S->xit), 0 for the operator inside the Standard V-cycle
 void launch_matvec32(const Grid& g, const float* Ke, const float* E, const uint8_t* mask, const float* u, float* y,
-                     RedSlot dot, PcgScalars* S, cudaStream_t s);
-// rc = normalised restriction of rf; a1 holds the x-pass result on span-4 transitions
+                     RedSlot dot, PcgScalars* S, int mark, cudaStream_t s);
+// rc = normalised restriction of rf (normalize = false: the transposed prolongation); a1 holds the x-pass
+// result on span-4 transitions
 void launch_restrict32(const MgLevel32& Lc, const MgLevel32& Lf, const float* rf, float* rc, float* a1,
-                       const PcgScalars* S, cudaStream_t s);
+                       const PcgScalars* S, cudaStream_t s, bool normalize = true);
+// FP32 image of `rows` rows of `len` doubles (same layout)
+void launch_rows_to32(int64_t rows, int len, const double* a, float* b, cudaStream_t s);
+// ---- the Standard V-cycle in FP32 (k_mg_standard32.cu)
+void launch_jacobi_init32(const MgLevel32& L, const float* r, float* x, float w, const PcgScalars* S, cudaStream_t s);
+void launch_residual32(const MgLevel32& L, const float* r, float* kx, const PcgScalars* S, cudaStream_t s);
+void launch_jacobi_correct32(const MgLevel32& L, const float* r, const float* kx, float* x, float w,
+                             const PcgScalars* S, cudaStream_t s);
+void launch_prolong_add32(const MgLevel32& Lc, const MgLevel32& Lf, const float* xc, float* xf, const PcgScalars* S,
+                          cudaStream_t s);
+void launch_level_matvec32(const MgLevel32& L, const float* Kel, const float* x, float* y, const PcgScalars* S,
+                           cudaStream_t s);
+void launch_dot_rz32(int64_t n3, const float* r, const float* z, RedSlot red, PcgScalars* S, cudaStream_t s);
 void launch_prolong_smooth32(const MgLevel32& Lc, const MgLevel32& Lf, const float* xc, const float* rf, float* xf,
                              float w, const PcgScalars* S, cudaStream_t s);
 void launch_prolong_smooth0_32(const MgLevel32& Lc, const MgLevel32& Lf, const float* xc, const float* r, float* z,
@@ -261,8 +275,8 @@ int modal_tiling(const Grid& g, int dev, int variant, ModalTiling* t);
 int modal_autotune(const Grid& g, int dev, const ModalKe& kh, const float* E, const uint8_t* mask, const float* u,
                    float* y, int* err, cudaStream_t s, ModalTiling* best);
 void launch_matvec32_modal(const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E,
-                           const uint8_t* mask, const float* u, float* y, RedSlot dot, PcgScalars* S, int* err,
-                           cudaStream_t s);
+                           const uint8_t* mask, const float* u, float* y, RedSlot dot, PcgScalars* S, int mark,
+                           int* err, cudaStream_t s);
 
 // ---- surface export (k_stl.cu, io.cpp:80-87)
 int stl_chunks(const Grid& g);

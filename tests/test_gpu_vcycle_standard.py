@@ -166,9 +166,45 @@ def test_standard_vcycle_design_loop_and_precision_guard():
     assert all(i < 5000 for i in its[t3d.T3D_VCYCLE_STANDARD]), its
     # the first step starts from the same density in both; later steps follow different OC trajectories
     np.testing.assert_allclose(objs[t3d.T3D_VCYCLE_STANDARD][0], objs[t3d.T3D_VCYCLE_ADAPTED][0], rtol=1e-5)
-    with pytest.raises(t3d.T3DError) as e:
-        t3d.Problem(8, 16, 8, precision=t3d.T3D_MIXED, mg_vcycle=t3d.T3D_VCYCLE_STANDARD)
-    assert e.value.code == t3d.T3D_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("dims", [(8, 16, 8), (17, 40, 23), (30, 60, 30)])
+def test_fp32_standard_vcycle_matches_fp64(dims):
+    # the FP32 Standard cycle (modal FP32 K(E) on level 0, FP32 Galerkin element matrices on the coarse levels,
+    # FP64 coarsest inverse) against the FP64 cycle on the same FP32-rounded residual: 1e-5 relative
+    import algorithmengineering_altproject_b200 as t3d
+    P = t3d.Problem(*dims, precision=t3d.T3D_MIXED, mg_vcycle=t3d.T3D_VCYCLE_STANDARD)
+    rng = np.random.default_rng(13)
+    E = np.where(rng.random(P.ne) < 0.3, 1e-6, rng.uniform(0.05, 1.0, P.ne))
+    P.make_diagonal_preconditioner_from_static(E)
+    r = rng.standard_normal(P.nf).astype(np.float32).astype(np.float64)
+    z64 = P.vcycle(r)
+    z32 = P.vcycle32(r)
+    assert np.linalg.norm(z32 - z64) <= 1e-5 * np.linalg.norm(z64), np.linalg.norm(z32 - z64) / np.linalg.norm(z64)
+    P.close()
+
+
+@pytest.mark.parametrize("tol", [1e-6, 1e-8])
+def test_mixed_standard_converged_design_steps_match_fp64(tol):
+    # both forms on the Standard cycle, MG rebuilt every design iteration, solved to |r| < tol |b|: every
+    # design iteration started from the same density gives compliances within 1e-6 relative (the bound of the
+    # mixed-precision target) and the displacement within 1e-4
+    import algorithmengineering_altproject_b200 as t3d
+    kw = dict(mg_vcycle=t3d.T3D_VCYCLE_STANDARD, mg_rebuild_period=1, cg_tol=tol, cg_max_it=5000,
+              oc_sum_order=t3d.T3D_SUM_FP64)
+    F = t3d.Problem(30, 60, 30, precision=t3d.T3D_FP64, **kw)
+    M = t3d.Problem(30, 60, 30, precision=t3d.T3D_MIXED, **kw)
+    csF, csM = F.design_init(0.12), M.design_init(0.12)
+    assert abs(csM - csF) <= 1e-6 * csF, (csF, csM)
+    for _ in range(4):
+        M.set_density(F.density())
+        rF, rM = F.design_step(), M.design_step()
+        assert rF["pcg_iters"] < 5000 and rM["pcg_iters"] < 5000, (rF, rM)
+        assert abs(rM["obj"] - rF["obj"]) <= 1e-6 * abs(rF["obj"]), (rF["obj"], rM["obj"])
+        uF, uM = F.displacement(), M.displacement()
+        assert np.linalg.norm(uM - uF) <= 1e-4 * np.linalg.norm(uF)
+    F.close()
+    M.close()
 
 
 def test_multigrid_parameters_are_validated():
