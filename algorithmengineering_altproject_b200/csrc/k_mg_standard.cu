@@ -11,6 +11,8 @@
 // non-positive entries -> 1.  Level-1 element matrices are sums of E_c G_pos over the s^3 children, with
 // G_pos = W_pos^T Ke W_pos precomputed per child position (W_pos: trilinear weights of the child's corners);
 // children touching a fixed DOF take the masked product explicitly.  All FP64, deterministic orders.
+// Element matrices are stored entry-major (kel_index): entry k of element e at k * ne + e, so that threads
+// working on consecutive elements read consecutive addresses.
 #include "kernels.hpp"
 #include "red.cuh"
 
@@ -111,7 +113,7 @@ __global__ void __launch_bounds__(576) k_galerkin_fine(Grid g, MgLevel L1, int s
         if (ce >= ne1) continue;
         double v = acc[b];
         if (((cmask[b][A] >> r) & 1) || ((cmask[b][B] >> q) & 1)) v = 0.0;
-        Kel[(int64_t)ce * 576 + threadIdx.x] = v;
+        Kel[kel_index(ce, threadIdx.x, ne1)] = v;
     }
 }
 
@@ -121,6 +123,7 @@ __global__ void __launch_bounds__(576) k_galerkin_coarse(MgLevel Lf, MgLevel Lc,
     __shared__ int cmask[8];
     const int s = Lc.span;
     const int ce = blockIdx.x;
+    const int64_t nef = (int64_t)Lf.nx * Lf.ny * Lf.nz, nec = (int64_t)Lc.nx * Lc.ny * Lc.nz;
     const int cx = ce % Lc.nx, cy = (ce / Lc.nx) % Lc.ny, cz = ce / (Lc.nx * Lc.ny);
     const int P = threadIdx.x / 24, Q = threadIdx.x % 24;
     const int A = P / 3, r = P % 3, B = Q / 3, q = Q % 3;
@@ -132,14 +135,13 @@ __global__ void __launch_bounds__(576) k_galerkin_coarse(MgLevel Lf, MgLevel Lc,
         for (int j = 0; j < s; ++j)
             for (int i = 0; i < s; ++i) {
                 const int fe = ((cz * s + k) * Lf.ny + cy * s + j) * Lf.nx + cx * s + i;
-                const double* K = Kf + (int64_t)fe * 576;
                 double t = 0.0;
                 for (int a = 0; a < 8; ++a) {
                     const double wa = tri_w(s, i + corner_dx(a), j + corner_dy(a), k + corner_dz(a), A);
                     double u = 0.0;
                     for (int b = 0; b < 8; ++b) {
                         const double wb = tri_w(s, i + corner_dx(b), j + corner_dy(b), k + corner_dz(b), B);
-                        u = u + wb * K[(3 * a + r) * 24 + 3 * b + q];
+                        u = u + wb * Kf[kel_index(fe, (3 * a + r) * 24 + 3 * b + q, nef)];
                     }
                     t = t + wa * u;
                 }
@@ -147,7 +149,7 @@ __global__ void __launch_bounds__(576) k_galerkin_coarse(MgLevel Lf, MgLevel Lc,
             }
     __syncthreads();
     if (((cmask[A] >> r) & 1) || ((cmask[B] >> q) & 1)) acc = 0.0;
-    Kc[(int64_t)ce * 576 + threadIdx.x] = acc;
+    Kc[kel_index(ce, threadIdx.x, nec)] = acc;
 }
 
 // D = diag of the assembled level operator; fixed or non-positive -> 1
@@ -157,6 +159,7 @@ __global__ void k_level_diag(MgLevel L, const double* __restrict__ Kel) {
     const int nnx = L.nx + 1, nny = L.ny + 1;
     const int x = n % nnx, y = (n / nnx) % nny, z = n / (nnx * nny);
     const int m = L.mask[n];
+    const int64_t ne = (int64_t)L.nx * L.ny * L.nz;
     for (int c = 0; c < 3; ++c) {
         double d = 0.0;
         for (int dz = 0; dz <= 1; ++dz)
@@ -165,7 +168,7 @@ __global__ void k_level_diag(MgLevel L, const double* __restrict__ Kel) {
                     const int ex = x - dx, ey = y - dy, ez = z - dz;
                     if (ex < 0 || ey < 0 || ez < 0 || ex >= L.nx || ey >= L.ny || ez >= L.nz) continue;
                     const int a = corner_of(dx, dy, dz), e = (ez * L.ny + ey) * L.nx + ex;
-                    d = d + Kel[(int64_t)e * 576 + (3 * a + c) * 24 + 3 * a + c];
+                    d = d + Kel[kel_index(e, (3 * a + c) * 24 + 3 * a + c, ne)];
                 }
         L.diag[c * L.nn + n] = (((m >> c) & 1) || !(d > 0.0)) ? 1.0 : d;
     }
@@ -179,6 +182,7 @@ __global__ void k_level_matvec(MgLevel L, const double* __restrict__ Kel, const 
     if (n >= L.nn) return;
     const int nnx = L.nx + 1, nny = L.ny + 1;
     const int X = n % nnx, Y = (n / nnx) % nny, Z = n / (nnx * nny);
+    const int64_t ne = (int64_t)L.nx * L.ny * L.nz;
     double acc[3] = {0.0, 0.0, 0.0};
     for (int dz = 0; dz <= 1; ++dz)
         for (int dy = 0; dy <= 1; ++dy)
@@ -186,12 +190,12 @@ __global__ void k_level_matvec(MgLevel L, const double* __restrict__ Kel, const 
                 const int ex = X - dx, ey = Y - dy, ez = Z - dz;
                 if (ex < 0 || ey < 0 || ez < 0 || ex >= L.nx || ey >= L.ny || ez >= L.nz) continue;
                 const int a = corner_of(dx, dy, dz);
-                const double* K = Kel + ((int64_t)((ez * L.ny + ey) * L.nx + ex)) * 576;
+                const double* K = Kel + ((ez * L.ny + ey) * L.nx + ex);   // entry k at K[k * ne]
                 for (int b = 0; b < 8; ++b) {
                     const int m = lnode(L, ex + corner_dx(b), ey + corner_dy(b), ez + corner_dz(b));
                     for (int c = 0; c < 3; ++c) {
                         const double xv = x[c * L.nn + m];
-                        for (int r = 0; r < 3; ++r) acc[r] = acc[r] + K[(3 * a + r) * 24 + 3 * b + c] * xv;
+                        for (int r = 0; r < 3; ++r) acc[r] = acc[r] + K[((3 * a + r) * 24 + 3 * b + c) * ne] * xv;
                     }
                 }
             }
@@ -290,7 +294,7 @@ __global__ void k_to_coarse_layout(MgLevel L, const double* __restrict__ Kel, do
     const int e = (int)(t / 576), k = (int)(t % 576);
     const int cx = e % L.nx, cy = (e / L.nx) % L.ny, cz = e / (L.nx * L.ny);
     const int cel = (cz * L.nx + cx) * L.ny + (L.ny - 1 - cy);
-    Kce[(int64_t)cel * 576 + k] = Kel[t];
+    Kce[(int64_t)cel * 576 + k] = Kel[kel_index(e, k, ne)];
 }
 
 inline unsigned blocks_of(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }

@@ -98,11 +98,13 @@ __global__ void k_prolong_add32(MgLevel32 Lc, MgLevel32 Lf, const float* __restr
 }
 
 // y = K_l x from the FP32 element matrices of a coarse level (node-centric gather: each node reads the three
-// rows of its corner in the 8 element matrices around it, so every matrix entry is read once), fixed DOFs 0
+// rows of its corner in the 8 element matrices around it, so every matrix entry is read once; entry-major
+// storage makes the reads of consecutive nodes consecutive), fixed DOFs 0
 __global__ void k_level_matvec32(MgLevel32 L, const float* __restrict__ Kel, const float* __restrict__ x,
                                  float* __restrict__ y, const PcgScalars* S) {
     if (S->done) return;
     const int nnx = L.nx + 1, nny = L.ny + 1;
+    const int64_t ne = (int64_t)L.nx * L.ny * L.nz;
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < L.nn; n += (int64_t)gridDim.x * blockDim.x) {
         const int X = (int)(n % nnx), Y = (int)((n / nnx) % nny), Z = (int)(n / ((int64_t)nnx * nny));
         float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f;
@@ -112,16 +114,17 @@ __global__ void k_level_matvec32(MgLevel32 L, const float* __restrict__ Kel, con
                     const int ex = X - dx, ey = Y - dy, ez = Z - dz;
                     if (ex < 0 || ey < 0 || ez < 0 || ex >= L.nx || ey >= L.ny || ez >= L.nz) continue;
                     const int a = corner_of(dx, dy, dz);
-                    const float* K = Kel + ((int64_t)((ez * L.ny + ey) * L.nx + ex)) * 576 + (3 * a) * 24;
+                    // entry-major element matrices: row 3a+r, column 3b+c of element e at ((3a+r)*24 + 3b+c) * ne + e
+                    const float* K = Kel + ((int64_t)(ez * L.ny + ey) * L.nx + ex) + (int64_t)(3 * a) * 24 * ne;
 #pragma unroll
                     for (int b = 0; b < 8; ++b) {
                         const int64_t m = ((int64_t)(ez + corner_dz(b)) * nny + ey + corner_dy(b)) * nnx + ex + corner_dx(b);
 #pragma unroll
                         for (int c = 0; c < 3; ++c) {
                             const float xv = x[c * L.cs + m];
-                            acc0 = fmaf(K[3 * b + c], xv, acc0);
-                            acc1 = fmaf(K[24 + 3 * b + c], xv, acc1);
-                            acc2 = fmaf(K[48 + 3 * b + c], xv, acc2);
+                            acc0 = fmaf(K[(3 * b + c) * ne], xv, acc0);
+                            acc1 = fmaf(K[(24 + 3 * b + c) * ne], xv, acc1);
+                            acc2 = fmaf(K[(48 + 3 * b + c) * ne], xv, acc2);
                         }
                     }
                 }

@@ -128,7 +128,9 @@ void launch_coarse_solve(const MgLevel& L, const double* X, int N, const int* st
                          cudaStream_t s);
 
 // ---- 'Standard' V-cycle option (TOP3D_XL.m:772-807): Galerkin element matrices per level, smoothing with
-// the true residual; FP64
+// the true residual; FP64.  Element matrices are stored entry-major: entry k (row-major 24x24, local DOF
+// 3a+c) of element e of a level with ne elements at k * ne + e.
+__host__ __device__ inline int64_t kel_index(int64_t e, int k, int64_t ne) { return (int64_t)k * ne + e; }
 // G[pos][576] = W_pos^T Ke W_pos for the s^3 child positions of a span-s coarse element (host)
 void galerkin_positions(int s, const double* Ke, double* G);
 void launch_galerkin_fine(const Grid& g, const MgLevel& L1, const double* E, const uint8_t* mask0, const double* Gpos,
