@@ -76,7 +76,7 @@ class Info(C.Structure):
                 ("levels", (C.c_int64 * 4) * 8), ("coarse_n", C.c_int64), ("coarse_cholesky_ok", C.c_int64),
                 ("device_bytes", C.c_int64), ("kernel_launches", C.c_int64), ("matvec32_modal", C.c_int64),
                 ("matvec32_tile", C.c_int64 * 4), ("matvec64_kernel", C.c_int64),
-                ("matvec32_variant", C.c_int64)]
+                ("matvec32_variant", C.c_int64), ("last_outer_passes", C.c_int64)]
 
 
 class IterRecord(C.Structure):

@@ -1353,6 +1353,7 @@ int t3d_get_info(const t3d_context* ctx, t3d_info* info) {
         t3d::modal_variant_desc(ctx->mt.variant, d);
         for (int k = 0; k < 4; ++k) info->matvec32_tile[k] = d[k];
         info->matvec32_variant = ctx->mt.variant;
+        info->last_outer_passes = ctx->last_outer;
     }
     return T3D_OK;
 }

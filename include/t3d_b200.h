@@ -116,6 +116,7 @@ typedef struct t3d_info {
     int64_t matvec64_kernel;      /* FP64 K(E)u kernel: 0 node-centric, 1 streaming with Ke from the constant bank,
                                      2 streaming with the built-in Ke's magnitudes in registers */
     int64_t matvec32_variant;     /* index of the modal tile shape (params.matvec32_tile - 1 selects it) */
+    int64_t last_outer_passes;    /* mixed precision: FP64 defect-correction passes of the last solve */
 } t3d_info;
 
 typedef struct t3d_iter_record {  /* one design iteration (driver.cpp:205-216) */
