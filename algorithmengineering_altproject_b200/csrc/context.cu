@@ -115,7 +115,8 @@ struct Context {
     // Ke for level 1, and one scratch vector per level
     bool standard = false;
     double* E_mg = nullptr;     // the moduli the hierarchy was built from (the cycle's level-0 operator)
-    double* Kel[8]{};
+    double* Kel[8]{};           // element-major (assembly)
+    double* KelT[8]{};          // entry-major copies read by the level products
     double* Gpos = nullptr;
     double* vtmp[8]{};
     bool ke_pat = false;        // Ke has the built-in coefficient pattern: its magnitudes are in Kd
@@ -278,6 +279,7 @@ static int build_levels(Context* c) {
         for (int l = 1; l < c->nlev; ++l) {
             const MgLevel& L = c->lv[l];
             CHECK(c->alloc(&c->Kel[l], (size_t)L.nx * L.ny * L.nz * 576));
+            CHECK(c->alloc(&c->KelT[l], (size_t)L.nx * L.ny * L.nz * 576));
             CHECK(c->alloc(&c->vtmp[l], 3 * L.nn));
         }
         const int s1 = c->lv[1].span;
@@ -710,8 +712,12 @@ static int mg_setup(Context* c) {
         T3D_CUDA_OK(cudaMemcpyAsync(c->E_mg, c->E, c->g.NE * sizeof(double), cudaMemcpyDeviceToDevice, c->st));
         launch_galerkin_fine(c->g, c->lv[1], c->E, c->mask0, c->Gpos, c->Ke, c->Kel[1], c->st);
         for (int l = 2; l < c->nlev; ++l) launch_galerkin_coarse(c->lv[l - 1], c->lv[l], c->Kel[l - 1], c->Kel[l], c->st);
-        for (int l = 1; l < c->nlev; ++l) launch_level_diag(c->lv[l], c->Kel[l], c->st);
-        c->launches += 2 * (c->nlev - 1);
+        for (int l = 1; l < c->nlev; ++l) {
+            launch_level_diag(c->lv[l], c->Kel[l], c->st);
+            const MgLevel& L = c->lv[l];
+            launch_kel_transpose((int64_t)L.nx * L.ny * L.nz, c->Kel[l], c->KelT[l], c->st);
+        }
+        c->launches += 3 * (c->nlev - 1);
         if (c->Nc) {
             const MgLevel& Lc = c->lv[c->nlev - 1];
             launch_to_coarse_layout(Lc, c->Kel[c->nlev - 1], c->Kce, c->st);
@@ -723,7 +729,7 @@ static int mg_setup(Context* c) {
             launch_cells_to32(c->g, c->E_mg, c->E_mg32, c->st);
             for (int l = 1; l < c->nlev; ++l) {
                 const MgLevel& L = c->lv[l];
-                launch_rows_to32((int64_t)L.nx * L.ny * L.nz, 576, c->Kel[l], c->Kel32[l], c->st);
+                launch_kel_transpose32((int64_t)L.nx * L.ny * L.nz, c->Kel[l], c->Kel32[l], c->st);
             }
             for (int l = 0; l < c->nlev; ++l) {
                 const MgLevel32& M = c->lv32[l];
@@ -787,7 +793,7 @@ static void level_matvec(Context* c, int l, const double* x, double* y, const Pc
         launch_matvec64_stream(c->g, c->st64, c->Ke_h, c->ke_pat ? c->Kd : nullptr, c->E_mg, c->mask0, x, y, S,
                                c->st);
     else
-        launch_level_matvec(c->lv[l], c->Kel[l], x, y, S, c->st);
+        launch_level_matvec(c->lv[l], c->KelT[l], x, y, S, c->st);
 }
 
 // kernels of one V-cycle

@@ -11,8 +11,9 @@
 // non-positive entries -> 1.  Level-1 element matrices are sums of E_c G_pos over the s^3 children, with
 // G_pos = W_pos^T Ke W_pos precomputed per child position (W_pos: trilinear weights of the child's corners);
 // children touching a fixed DOF take the masked product explicitly.  All FP64, deterministic orders.
-// Element matrices are stored entry-major (kel_index): entry k of element e at k * ne + e, so that threads
-// working on consecutive elements read consecutive addresses.
+// The assembly keeps element matrices element-major (576 consecutive entries per element); the level products
+// read an entry-major copy (kel_index: entry k of element e at k * ne + e), in which threads working on
+// consecutive nodes read consecutive addresses.
 #include "kernels.hpp"
 #include "red.cuh"
 
@@ -113,7 +114,7 @@ __global__ void __launch_bounds__(576) k_galerkin_fine(Grid g, MgLevel L1, int s
         if (ce >= ne1) continue;
         double v = acc[b];
         if (((cmask[b][A] >> r) & 1) || ((cmask[b][B] >> q) & 1)) v = 0.0;
-        Kel[kel_index(ce, threadIdx.x, ne1)] = v;
+        Kel[(int64_t)ce * 576 + threadIdx.x] = v;
     }
 }
 
@@ -123,7 +124,6 @@ __global__ void __launch_bounds__(576) k_galerkin_coarse(MgLevel Lf, MgLevel Lc,
     __shared__ int cmask[8];
     const int s = Lc.span;
     const int ce = blockIdx.x;
-    const int64_t nef = (int64_t)Lf.nx * Lf.ny * Lf.nz, nec = (int64_t)Lc.nx * Lc.ny * Lc.nz;
     const int cx = ce % Lc.nx, cy = (ce / Lc.nx) % Lc.ny, cz = ce / (Lc.nx * Lc.ny);
     const int P = threadIdx.x / 24, Q = threadIdx.x % 24;
     const int A = P / 3, r = P % 3, B = Q / 3, q = Q % 3;
@@ -141,7 +141,7 @@ __global__ void __launch_bounds__(576) k_galerkin_coarse(MgLevel Lf, MgLevel Lc,
                     double u = 0.0;
                     for (int b = 0; b < 8; ++b) {
                         const double wb = tri_w(s, i + corner_dx(b), j + corner_dy(b), k + corner_dz(b), B);
-                        u = u + wb * Kf[kel_index(fe, (3 * a + r) * 24 + 3 * b + q, nef)];
+                        u = u + wb * Kf[(int64_t)fe * 576 + (3 * a + r) * 24 + 3 * b + q];
                     }
                     t = t + wa * u;
                 }
@@ -149,7 +149,7 @@ __global__ void __launch_bounds__(576) k_galerkin_coarse(MgLevel Lf, MgLevel Lc,
             }
     __syncthreads();
     if (((cmask[A] >> r) & 1) || ((cmask[B] >> q) & 1)) acc = 0.0;
-    Kc[kel_index(ce, threadIdx.x, nec)] = acc;
+    Kc[(int64_t)ce * 576 + threadIdx.x] = acc;
 }
 
 // D = diag of the assembled level operator; fixed or non-positive -> 1
@@ -159,7 +159,6 @@ __global__ void k_level_diag(MgLevel L, const double* __restrict__ Kel) {
     const int nnx = L.nx + 1, nny = L.ny + 1;
     const int x = n % nnx, y = (n / nnx) % nny, z = n / (nnx * nny);
     const int m = L.mask[n];
-    const int64_t ne = (int64_t)L.nx * L.ny * L.nz;
     for (int c = 0; c < 3; ++c) {
         double d = 0.0;
         for (int dz = 0; dz <= 1; ++dz)
@@ -168,13 +167,13 @@ __global__ void k_level_diag(MgLevel L, const double* __restrict__ Kel) {
                     const int ex = x - dx, ey = y - dy, ez = z - dz;
                     if (ex < 0 || ey < 0 || ez < 0 || ex >= L.nx || ey >= L.ny || ez >= L.nz) continue;
                     const int a = corner_of(dx, dy, dz), e = (ez * L.ny + ey) * L.nx + ex;
-                    d = d + Kel[kel_index(e, (3 * a + c) * 24 + 3 * a + c, ne)];
+                    d = d + Kel[(int64_t)e * 576 + (3 * a + c) * 24 + 3 * a + c];
                 }
         L.diag[c * L.nn + n] = (((m >> c) & 1) || !(d > 0.0)) ? 1.0 : d;
     }
 }
 
-// y = K_l x from the element matrices (node-centric gather), fixed DOFs 0
+// y = K_l x from the entry-major element matrices KelT (node-centric gather), fixed DOFs 0
 __global__ void k_level_matvec(MgLevel L, const double* __restrict__ Kel, const double* __restrict__ x,
                                double* __restrict__ y, const PcgScalars* S) {
     if (S != nullptr && S->done) return;
@@ -294,12 +293,39 @@ __global__ void k_to_coarse_layout(MgLevel L, const double* __restrict__ Kel, do
     const int e = (int)(t / 576), k = (int)(t % 576);
     const int cx = e % L.nx, cy = (e / L.nx) % L.ny, cz = e / (L.nx * L.ny);
     const int cel = (cz * L.nx + cx) * L.ny + (L.ny - 1 - cy);
-    Kce[(int64_t)cel * 576 + k] = Kel[kel_index(e, k, ne)];
+    Kce[(int64_t)cel * 576 + k] = Kel[t];
+}
+
+// element-major -> entry-major (dst[k * ne + e] = src[e * 576 + k]) through 32 x 32 shared-memory tiles, with
+// the FP32 image written instead when B is float
+template <class B>
+__global__ void k_kel_transpose(int64_t ne, const double* __restrict__ src, B* __restrict__ dst) {
+    __shared__ double tile[32][33];
+    const int64_t e0 = (int64_t)blockIdx.x * 32;
+    const int k0 = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {   // rows = elements, columns = entries (coalesced in k)
+        const int64_t e = e0 + j;
+        const int k = k0 + threadIdx.x;
+        tile[j][threadIdx.x] = (e < ne && k < 576) ? src[e * 576 + k] : 0.0;
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {   // rows = entries, columns = elements (coalesced in e)
+        const int k = k0 + j;
+        const int64_t e = e0 + threadIdx.x;
+        if (e < ne && k < 576) dst[(int64_t)k * ne + e] = (B)tile[threadIdx.x][j];
+    }
 }
 
 inline unsigned blocks_of(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
+
+void launch_kel_transpose(int64_t ne, const double* Kel, double* KelT, cudaStream_t s) {
+    k_kel_transpose<double><<<dim3((unsigned)((ne + 31) / 32), 18), dim3(32, 8), 0, s>>>(ne, Kel, KelT);
+}
+void launch_kel_transpose32(int64_t ne, const double* Kel, float* KelT32, cudaStream_t s) {
+    k_kel_transpose<float><<<dim3((unsigned)((ne + 31) / 32), 18), dim3(32, 8), 0, s>>>(ne, Kel, KelT32);
+}
 
 void galerkin_positions(int s, const double* Ke, double* G) {
     for (int k = 0; k < s; ++k)

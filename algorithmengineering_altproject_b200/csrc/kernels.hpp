@@ -128,16 +128,20 @@ void launch_coarse_solve(const MgLevel& L, const double* X, int N, const int* st
                          cudaStream_t s);
 
 // ---- 'Standard' V-cycle option (TOP3D_XL.m:772-807): Galerkin element matrices per level, smoothing with
-// the true residual; FP64.  Element matrices are stored entry-major: entry k (row-major 24x24, local DOF
-// 3a+c) of element e of a level with ne elements at k * ne + e.
+// the true residual; FP64.  The assembly stores element matrices element-major (576 entries per element,
+// row-major 24x24, local DOF 3a+c); the level products read an entry-major copy, entry k of element e of a
+// level with ne elements at kel_index(e, k, ne) = k * ne + e.
 __host__ __device__ inline int64_t kel_index(int64_t e, int k, int64_t ne) { return (int64_t)k * ne + e; }
+void launch_kel_transpose(int64_t ne, const double* Kel, double* KelT, cudaStream_t s);
+void launch_kel_transpose32(int64_t ne, const double* Kel, float* KelT32, cudaStream_t s);
 // G[pos][576] = W_pos^T Ke W_pos for the s^3 child positions of a span-s coarse element (host)
 void galerkin_positions(int s, const double* Ke, double* G);
 void launch_galerkin_fine(const Grid& g, const MgLevel& L1, const double* E, const uint8_t* mask0, const double* Gpos,
                           const double* Ke, double* Kel, cudaStream_t s);
 void launch_galerkin_coarse(const MgLevel& Lf, const MgLevel& Lc, const double* Kf, double* Kc, cudaStream_t s);
 void launch_level_diag(const MgLevel& L, const double* Kel, cudaStream_t s);
-void launch_level_matvec(const MgLevel& L, const double* Kel, const double* x, double* y, const PcgScalars* S,
+// KelT: the level's entry-major element matrices
+void launch_level_matvec(const MgLevel& L, const double* KelT, const double* x, double* y, const PcgScalars* S,
                          cudaStream_t s);
 void launch_jacobi_init(const MgLevel& L, const double* r, double* x, double w, const PcgScalars* S, cudaStream_t s);
 void launch_residual(const MgLevel& L, const double* r, double* kx, const PcgScalars* S, cudaStream_t s);

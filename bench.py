@@ -2,22 +2,25 @@
 sensitivities -> PDE filter -> OC) on the reference's cantilever.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--config c2]
-                    [--precision mixed|fp64] [--compare-steps S] [--kernels-only --reps R]
+                    [--precision mixed|fp64] [--regime converged|reference] [--compare-steps S]
+                    [--kernels-only --reps R --tile T]
 
-Prints ONE JSON line (rank 0).  A step is one design iteration.  The default form is the mixed-
-precision one (FP32 inner MG-PCG inside FP64 defect correction); before the timed run, S design
-iterations are run by both the mixed and the plain FP64 form from the same densities, and
-`vs_fp64` reports the speed ratio and the compliance / displacement / density errors.
-`value` = design iterations/s
-over the whole job, timed on the device (CUDA events recorded by the library on its stream; max
-over ranks); `e2e` = the same metric through the host-buffer C-ABI call t3d_design_step_host
-(H2D of the design field, D2H of the updated field, between two pinned host buffers, wall clock).
-Multi-GPU runs are independent replicas (one design per GPU, no collective on the data path).
+Prints ONE JSON line (rank 0).  A step is one design iteration of 256x512x256 (101.6M DOF).  The default
+form is the mixed-precision one (FP32 inner MG-PCG inside FP64 defect correction) in the "converged"
+regime: every solve reaches |r| < 1e-6 |b| with the Standard V-cycle rebuilt every design iteration, so
+mixed and FP64 approximate the same solution; `vs_fp64` runs S design iterations of both forms from the
+same densities and reports the speed ratio and the compliance / displacement / density errors there, and
+`reference_regime` the same for the reference CLI's own solver settings (Adapted cycle, tol 1e-3,
+800-iteration cap, which both forms hit at this size).  `value` = design iterations/s over the whole job,
+timed on the device (CUDA events recorded by the library on its stream; max over ranks); `e2e` = the same
+metric through the host-buffer C-ABI call t3d_design_step_host (H2D of the design field, D2H of the updated
+field, between two pinned host buffers, wall clock).  Multi-GPU runs are independent replicas (one design
+per GPU, no collective on the data path).
 
 --impl reference times the reference's own CPU implementation (oracle/_ref/libt3d_ref.so, the
-unmodified reference sources) on this host's cores with a bounded sample of the same workload:
-design iterations with PCG capped at a few iterations, extrapolated to the iteration count of a
-full solve.
+unmodified reference sources) on this host's physical cores with a bounded sample of the same workload:
+design iterations with PCG capped at 1 and 3 iterations, extrapolated to the 800 iterations its solves
+take at this size.
 """
 from __future__ import annotations
 
@@ -62,11 +65,10 @@ def parse_args():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--config", default=DEFAULT_CONFIG, choices=sorted(CONFIGS))
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
-    ap.add_argument("--vcycle", default="adapted", choices=["adapted", "standard"],
-                    help="standard: residual smoothing with Galerkin coarse operators (FP64 only; not the reference's)")
-    ap.add_argument("--mg-rebuild-period", type=int, default=5,
-                    help="design iterations between MG rebuilds (5 = the reference's schedule)")
-    ap.add_argument("--compare-steps", type=int, default=2,
+    ap.add_argument("--regime", default="converged", choices=sorted(REGIMES),
+                    help="converged: both forms solve to 1e-6 with the Standard V-cycle rebuilt every iteration; "
+                         "reference: the reference CLI's Adapted cycle, tol 1e-3, 800-iteration cap")
+    ap.add_argument("--compare-steps", type=int, default=3,
                     help="design iterations run by both forms from the same density (mixed vs FP64 errors)")
     ap.add_argument("--kernels-only", action="store_true",
                     help="time the matvec and V-cycle alone on the config's grid (for ncu captures)")
@@ -149,57 +151,81 @@ def traffic_per_launch(kernel):
 
 
 # ---------------------------------------------------------------- CPU baseline / reference arm
-def reference_sample(cfg, steps, warmup, n_pcg, threads):
-    """Bounded sample of the reference's CPU design iteration: `steps` iterations with PCG capped at
-    3 iterations (after `warmup` untimed ones), extrapolated to n_pcg PCG iterations per design
-    iteration with the per-iteration PCG cost measured from caps of 1 and 3."""
+CPU_SAMPLES = 10   # PCG-cost samples in both the reference arm and the cpu_baseline leg
+
+
+def setup_cpu_env():
+    """OpenMP placement of the reference's own runs (run_cubic_test_top3d_GLOBAL.sbatch:54-56): threads bound
+    close, one per physical core.  Must be set before the reference library (libgomp) is loaded."""
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    os.environ.setdefault("OMP_PLACES", "cores")
+
+
+def physical_cores():
+    try:
+        import psutil
+        n = psutil.cpu_count(logical=False)
+    except Exception:
+        n = None
+    return int(n or os.cpu_count() or 1)
+
+
+def reference_sample(cfg, samples, n_pcg, threads):
+    """Bounded sample of the reference's CPU design iteration (the reference build of oracle/_ref): `samples`
+    pairs of design iterations with PCG capped at 1 and 3 iterations give the per-PCG-iteration cost (their
+    PCG-time difference / 2), extrapolated to n_pcg PCG iterations per design iteration, plus the measured
+    SIMP / compliance / filter / OC time and 1/5 of an MG rebuild (the reference rebuilds at loop 1 and every
+    5th, driver.cpp:132).  PCG_free, the MG preconditioner, ComputeCompliance and ApplyPDEFilter are the
+    reference's own; SIMP, dc and OC are the harness's restatement of driver.cpp:117-183."""
     from oracle.bindings import Reference, reference_available
-    if reference_available():
-        Reference.set_threads(threads)
-        r = Reference(cfg["nely"], cfg["nelx"], cfg["nelz"], max_levels=cfg["max_levels"])
-        kind, cores = "reference", threads
-    else:
+    if not reference_available():
         raise RuntimeError("reference build oracle/_ref/libt3d_ref.so is not present")
+    Reference.set_threads(threads)
+    r = Reference(cfg["nely"], cfg["nelx"], cfg["nelz"], max_levels=cfg["max_levels"])
     V0 = cfg["V0"]
-    for k in range(max(1, warmup)):
-        r.sample_iteration(V0, 1, k == 0)
-    per_iter = []
-    rest = []
-    for k in range(max(1, steps)):
+    r.sample_iteration(V0, 1, True)   # warm-up: filter set-up, first MG build
+    per_iter, rest = [], []
+    for _ in range(samples):
         _, a = r.sample_iteration(V0, 1, False)
         _, b = r.sample_iteration(V0, 3, False)
         per_iter.append((b[2] - a[2]) / 2.0)
-        rest.append(b[0] + b[3] + b[4] + b[5] + a[1])
+        rest.append(b[0] + b[3] + b[4] + b[5])
     _, mg = r.sample_iteration(V0, 1, True)
     t_iter = statistics.median(per_iter)
-    t_pcg_full = max(t_iter, 0.0) * n_pcg
-    t_design = t_pcg_full + statistics.median(rest) + mg[1] / 5.0
-    return dict(value=1.0 / t_design, seconds_per_design_iteration=t_design, pcg_iteration_s=t_iter,
-                kind=kind, cores=cores,
-                sample="%d reference design iterations with PCG capped at 1 and 3 iterations "
-                       "(per-PCG-iteration cost %.3f s); extrapolated to %d PCG iterations per design iteration "
-                       "plus the measured SIMP/compliance/filter/OC time and 1/5 of an MG rebuild"
-                       % (2 * max(1, steps), t_iter, n_pcg))
+    t_design = max(t_iter, 0.0) * n_pcg + statistics.median(rest) + mg[1] / 5.0
+    spread = {"min": min(per_iter), "median": t_iter, "max": max(per_iter)}
+    return dict(value=1.0 / t_design, seconds_per_design_iteration=t_design, pcg_iteration_s=spread,
+                kind="reference", cores=threads,
+                sample="%d pairs of reference design iterations (%s) with PCG capped at 1 and 3 iterations: "
+                       "per-PCG-iteration cost median %.3f s (min %.3f, max %.3f), extrapolated to %d PCG iterations "
+                       "(cgMaxIt, core.hpp:36; the reference's Adapted-cycle solves hit it at this size), plus the "
+                       "measured SIMP/compliance/filter/OC time and 1/5 of an MG rebuild; OpenMP %d threads on "
+                       "physical cores (OMP_PROC_BIND=%s, OMP_PLACES=%s); PCG, MG, compliance and filter are the "
+                       "reference's own code, SIMP/dc/OC the harness's restatement of driver.cpp:117-183"
+                       % (samples, cfg["name"], t_iter, spread["min"], spread["max"], n_pcg, threads,
+                          os.environ.get("OMP_PROC_BIND"), os.environ.get("OMP_PLACES")))
 
 
 def run_reference_arm(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
+    setup_cpu_env()
     cfg = CONFIGS[args.config]
-    threads = os.cpu_count() or 1
+    threads = physical_cores()
     n_pcg = 800   # cgMaxIt (core.hpp:36): the reference's solves hit the cap at these sizes
     t0 = time.time()
-    s = reference_sample(cfg, args.steps, args.warmup, n_pcg, threads)
+    s = reference_sample(cfg, CPU_SAMPLES, n_pcg, threads)
     line = {
         "impl": "reference", "metric": METRIC, "value": s["value"], "unit": "design iter/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1000.0 * s["seconds_per_design_iteration"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (built-in cantilever load case)",
         "config": {"workload": cfg["name"], "V0": cfg["V0"], "mg_max_levels": cfg["max_levels"],
-                   "precision": "fp64 (reference OpenMP CPU path)", "pcg_iterations_assumed": n_pcg},
+                   "precision": "fp64 (reference OpenMP CPU path)", "vcycle": "adapted (the reference's only cycle)",
+                   "pcg_iterations_assumed": n_pcg},
         "cpu_baseline": {"value": s["value"], "unit": "design iter/s", "cores": s["cores"], "kind": s["kind"],
-                         "sample": s["sample"]},
+                         "sample": s["sample"], "pcg_iteration_s": s["pcg_iteration_s"]},
         "e2e": {"value": s["value"], "unit": "design iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "wall_s": time.time() - t0,
     }
@@ -223,6 +249,30 @@ def job_throughput(world, steps, seconds):
 
 
 # ---------------------------------------------------------------- B200 arm
+# Solver regimes of the design loop.  "converged": both forms solve every design iteration to |r| < 1e-6 |b| with
+# the Standard V-cycle (the MATLAB original's 'Standard', TOP3D_XL.m:772-807) rebuilt every iteration -- the
+# regime in which "compliance within 1e-6 of FP64" is a property of the solution; "reference": the reference
+# CLI's algorithm (Adapted V-cycle, rebuilt at loop 1 and every 5th, tol 1e-3, 800-iteration cap), in which the
+# solves stop at the cap unconverged at this size, as the reference's do.
+REGIMES = {
+    "converged": dict(mg_vcycle="standard", mg_rebuild_period=1, cg_tol=1e-6, cg_max_it=2000,
+                      desc="converged: every solve to |r| < 1e-6 |b| (PCG cap 2000), Standard V-cycle rebuilt every "
+                           "design iteration, both forms"),
+    "reference": dict(mg_vcycle="adapted", mg_rebuild_period=5, cg_tol=1e-3, cg_max_it=800,
+                      desc="reference: the reference CLI's solver (Adapted V-cycle rebuilt at loop 1 and every 5th, "
+                           "tol 1e-3, 800-iteration cap; unconverged at the cap at this size)"),
+}
+
+
+def problem_kw(t3d, cfg, regime, precision, dev, tile=0):
+    R = REGIMES[regime]
+    return dict(device=dev, mg_max_levels=cfg["max_levels"], oc_sum_order=t3d.T3D_SUM_FP64,
+                precision=t3d.T3D_MIXED if precision == "mixed" else t3d.T3D_FP64,
+                mg_vcycle=t3d.T3D_VCYCLE_STANDARD if R["mg_vcycle"] == "standard" else t3d.T3D_VCYCLE_ADAPTED,
+                mg_rebuild_period=R["mg_rebuild_period"], cg_tol=R["cg_tol"], cg_max_it=R["cg_max_it"],
+                matvec32_tile=tile)
+
+
 def matvec_roofline(P, mixed, mv_ms):
     """roofline of K(E)p (+ p.Ap): algorithmic bytes = w*(2 n_free + n_elements), w = 4 (FP32) or 8."""
     w = 4 if mixed else 8
@@ -230,27 +280,34 @@ def matvec_roofline(P, mixed, mv_ms):
     achieved = alg_bytes / (mv_ms * 1e-3) / 1e9
     peak, peak_kind = hbm_peak()
     flops = 1152 * P.ne
+    info = P.info()
+    staging = {0: "per-thread cp.async", 1: "per-thread cp.async, packed FP32x2",
+               2: "TMA bulk tensor copies, packed FP32x2"}.get(int(info.matvec32_tile[3]), "?")
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic_per_launch("matvec32" if mixed else "matvec64"), "peak_source": peak_kind,
-            "kernel": (("k_matvec32_modal" if P.info().matvec32_modal else "k_matvec32") +
-                       " (FP32 K(E)p + FP64 p.Ap)" if mixed
-                       else "k_matvec64_stream + k_dot_pcg (FP64 K(E)p, then p.Ap)"),
+            "kernel": (("k_matvec32_tma" if info.matvec32_tile[3] == 2 else "k_matvec32_modal"
+                        if info.matvec32_modal else "k_matvec32") + " (FP32 K(E)p + FP64 p.Ap; %s)" % staging
+                       if mixed else "k_matvec64_stream + k_dot_pcg (FP64 K(E)p, then p.Ap)"),
             "algorithmic_bytes_per_launch": alg_bytes, "flops_per_launch": flops,
             "tflops": flops / (mv_ms * 1e-3) / 1e12, "ms": mv_ms}
 
 
-def throughput_fractions(P, mixed, mv_ms, vc_ms, it_ms):
-    """DOF-matvecs/s, V-cycles/s and PCG iterations/s with the HBM-roofline fraction of each, from the
-    algorithmic bytes per unit: V-cycle w*4*(n + sum of the coarse levels' 3*nodes) (down: read r; up: read
-    r and D, write z), PCG iteration w*(15n + N_e) (K(E)p 2n + N_e, update 6n, V-cycle 4n, p-update 3n);
-    n = free DOFs, w = bytes per value of the inner solve."""
+def throughput_fractions(P, mixed, vcycle, mv_ms, vc_ms, it_ms):
+    """DOF-matvecs/s, V-cycles/s and PCG iterations/s with the HBM-roofline fraction of each, from algorithmic
+    bytes per unit (n = free DOFs, N_e = elements, w = bytes per value of the inner solve, c = the coarse levels'
+    3 * nodes):
+      Adapted V-cycle   w * 4 (n + c)            (down: read r; up: read r and D, write z)
+      Standard V-cycle  w * (22 n + 2 N_e + 8 c) (level 0: Jacobi start r, D -> x; K x (2n + N_e); residual r, Kx
+                        -> t; restriction reads t; prolongation x -> x; K x; correction r, t, x, D -> x; r.z)
+      PCG iteration     the V-cycle + w * (11 n + N_e) (K(E)p 2n + N_e, update 3n, direction and x update 6n)"""
     w = 4 if mixed else 8
     peak, _ = hbm_peak()
     coarse = sum(3 * (nx + 1) * (ny + 1) * (nz + 1) for nx, ny, nz, _ in P.levels[1:])
-    vc_bytes = w * 4 * (P.nf + coarse)
-    it_bytes = w * (15 * P.nf + P.ne)
-    out = {"dof_matvecs_per_s": P.nf / (mv_ms * 1e-3), "vcycles_per_s": 1.0 / (vc_ms * 1e-3),
-           "vcycle_bytes": vc_bytes, "vcycle_gbs": vc_bytes / (vc_ms * 1e-3) / 1e9,
+    n, ne = P.nf, P.ne
+    vc_bytes = w * (22 * n + 2 * ne + 8 * coarse) if vcycle == "standard" else w * 4 * (n + coarse)
+    it_bytes = vc_bytes + w * (11 * n + ne)
+    out = {"dof_matvecs_per_s": n / (mv_ms * 1e-3), "vcycles_per_s": 1.0 / (vc_ms * 1e-3),
+           "vcycle": vcycle, "vcycle_bytes": vc_bytes, "vcycle_gbs": vc_bytes / (vc_ms * 1e-3) / 1e9,
            "pcg_iteration_bytes": it_bytes}
     out["vcycle_frac"] = out["vcycle_gbs"] / peak
     if it_ms and it_ms > 0:
@@ -265,8 +322,8 @@ def run_kernels_only(args):
     import algorithmengineering_altproject_b200 as t3d
     cfg = CONFIGS[args.config]
     mixed = args.precision == "mixed"
-    P = t3d.Problem(cfg["nely"], cfg["nelx"], cfg["nelz"], mg_max_levels=cfg["max_levels"],
-                    precision=t3d.T3D_MIXED if mixed else t3d.T3D_FP64, matvec32_tile=args.tile)
+    P = t3d.Problem(cfg["nely"], cfg["nelx"], cfg["nelz"], **problem_kw(t3d, cfg, args.regime, args.precision, 0,
+                                                                       args.tile))
     rng = np.random.default_rng(7)
     E = np.full(P.ne, 1e-9 + cfg["V0"] ** 3 * (1.0 - 1e-9))
     P.make_diagonal_preconditioner_from_static(E)
@@ -274,7 +331,8 @@ def run_kernels_only(args):
     P.vcycle(rng.standard_normal(P.nf))                  # leaves r on the device
     mv = P.profile(t3d.T3D_PROFILE_MATVEC32 if mixed else t3d.T3D_PROFILE_MATVEC, args.reps)
     vc = P.profile(t3d.T3D_PROFILE_VCYCLE32 if mixed else t3d.T3D_PROFILE_VCYCLE, args.reps)
-    print(json.dumps({"config": cfg["name"], "precision": args.precision, "matvec_ms": mv, "vcycle_ms": vc,
+    print(json.dumps({"config": cfg["name"], "precision": args.precision, "regime": args.regime,
+                      "matvec_ms": mv, "vcycle_ms": vc,
                       "matvec32_tile": list(P.info().matvec32_tile) if mixed else None,
                       "matvec32_variant": int(P.info().matvec32_variant) if mixed else None,
                       "roofline": matvec_roofline(P, mixed, mv)}), flush=True)
@@ -282,29 +340,33 @@ def run_kernels_only(args):
     return 0
 
 
-def compare_forms(cfg, dev, steps):
-    """Mixed vs plain FP64 on the same designs: both forms run `steps` design iterations, the mixed one
-    starting each iteration from the FP64 one's density.  Returns speeds and relative errors."""
+def compare_forms(cfg, regime, dev, steps, warm=1):
+    """Mixed vs plain FP64 on the same designs: both forms run `warm` untimed and `steps` compared design
+    iterations, the mixed one starting each iteration from the FP64 one's density.  Returns speeds (device time
+    of the compared iterations) and relative errors."""
     import algorithmengineering_altproject_b200 as t3d
-    kw = dict(device=dev, mg_max_levels=cfg["max_levels"], oc_sum_order=t3d.T3D_SUM_FP64)
-    F = t3d.Problem(cfg["nely"], cfg["nelx"], cfg["nelz"], precision=t3d.T3D_FP64, **kw)
-    M = t3d.Problem(cfg["nely"], cfg["nelx"], cfg["nelz"], precision=t3d.T3D_MIXED, **kw)
+    F = t3d.Problem(cfg["nely"], cfg["nelx"], cfg["nelz"], **problem_kw(t3d, cfg, regime, "fp64", dev))
+    M = t3d.Problem(cfg["nely"], cfg["nelx"], cfg["nelz"], **problem_kw(t3d, cfg, regime, "mixed", dev))
     csF, csM = F.design_init(cfg["V0"]), M.design_init(cfg["V0"])
-    out = {"c_solid_rel_err": abs(csM - csF) / abs(csF), "iterations": []}
+    out = {"regime": REGIMES[regime]["desc"], "c_solid_rel_err": abs(csM - csF) / abs(csF), "iterations": []}
     tF = tM = 0.0
-    for _ in range(steps):
+    for k in range(warm + steps):
         M.set_density(F.density())
         rF, rM = F.design_step(), M.design_step()
+        if k < warm:
+            continue
         uF, uM = F.displacement(), M.displacement()
         xF, xM = F.density(), M.density()
         tF += rF["t_total"]
         tM += rM["t_total"]
         out["iterations"].append({
             "loop": rF["loop"], "pcg_iters_fp64": rF["pcg_iters"], "pcg_iters_mixed": rM["pcg_iters"],
+            "outer_passes_mixed": int(M.info().last_outer_passes),
             "compliance_rel_err": abs(rM["obj"] - rF["obj"]) / abs(rF["obj"]),
             "displacement_rel_l2_err": float(np.linalg.norm(uM - uF) / np.linalg.norm(uF)),
             "density_max_abs_err": float(np.max(np.abs(xM.astype(np.float64) - xF))),
             "s_fp64": rF["t_total"], "s_mixed": rM["t_total"]})
+    out["max_compliance_rel_err"] = max(i["compliance_rel_err"] for i in out["iterations"])
     out["fp64_design_iter_per_s"] = steps / tF
     out["mixed_design_iter_per_s"] = steps / tM
     out["speedup_mixed_vs_fp64"] = tF / tM
@@ -327,13 +389,15 @@ def run_b200(args):
     torch.cuda.set_device(dev)
     cfg = CONFIGS[args.config]
     mixed = args.precision == "mixed"
+    regime = args.regime
 
-    comparison = compare_forms(cfg, dev, args.compare_steps) if (mixed and args.compare_steps > 0) else None
+    comparison = compare_forms(cfg, regime, dev, args.compare_steps) if (mixed and args.compare_steps > 0) else None
+    # the other regime, briefly, for context (no FP64 comparison in the reference regime: 1 warm + 1 compared step)
+    other = None
+    if mixed and regime == "converged" and args.compare_steps > 0:
+        other = compare_forms(cfg, "reference", dev, 1)
 
-    P = t3d.Problem(cfg["nely"], cfg["nelx"], cfg["nelz"], device=dev, mg_max_levels=cfg["max_levels"],
-                    oc_sum_order=t3d.T3D_SUM_FP64, precision=t3d.T3D_MIXED if mixed else t3d.T3D_FP64,
-                    mg_vcycle=t3d.T3D_VCYCLE_STANDARD if args.vcycle == "standard" else t3d.T3D_VCYCLE_ADAPTED,
-                    mg_rebuild_period=args.mg_rebuild_period)
+    P = t3d.Problem(cfg["nely"], cfg["nelx"], cfg["nelz"], **problem_kw(t3d, cfg, regime, args.precision, dev))
     P.design_init(cfg["V0"])
     for _ in range(args.warmup):
         P.design_step()
@@ -380,6 +444,7 @@ def run_b200(args):
         ne = P.ne
         pcg_its = [r["pcg_iters"] for r in recs]
         it_ms = 1000.0 * sum(r["t_cg"] for r in recs) / max(1, sum(pcg_its))
+        R = REGIMES[regime]
         line = {
             "metric": METRIC, "value": job_throughput(world, args.steps, dev_time), "unit": "design iter/s",
             "n_gpus": world,
@@ -388,16 +453,19 @@ def run_b200(args):
             "dtype": "f32+f64 (mixed)" if mixed else "f64",
             "data": "synthetic (the reference's built-in cantilever load case; no dataset involved)",
             "config": {"workload": cfg["name"], "V0": cfg["V0"], "mg_max_levels": cfg["max_levels"],
-                       "mg_levels": P.nlev, "coarse_dofs": P.coarse_n,
+                       "mg_levels": P.nlev, "coarse_dofs": P.coarse_n, "regime": R["desc"],
                        "precision": ("mixed: FP32 inner MG-PCG in FP64 defect correction" if mixed
                                      else "fp64 (plain GPU form)"),
                        "oc_volume_sum": "fp64", "parallelism": "replicas" if world > 1 else "single GPU",
-                       "vcycle": args.vcycle + ("" if args.vcycle == "adapted" else " (not the reference's algorithm)"),
-                       "mg_rebuild_period": args.mg_rebuild_period,
+                       "vcycle": R["mg_vcycle"] + ("" if R["mg_vcycle"] == "adapted" else
+                                                  " (the MATLAB original's Standard cycle; the C++ reference has "
+                                                  "only the Adapted one)"),
+                       "mg_rebuild_period": R["mg_rebuild_period"], "cg_tol": R["cg_tol"],
+                       "cg_max_it": R["cg_max_it"],
                        "l2": "inputs larger than L2 (node vectors %.0f MB each)" % (3 * P.nn * (4 if mixed else 8) / 1e6)},
             "pcg_iterations": pcg_its,
             "per_kernel_ms": {"matvec": mv_ms, "vcycle": vc_ms, "pcg_iteration": it_ms},
-            "throughput": throughput_fractions(P, mixed, mv_ms, vc_ms, it_ms),
+            "throughput": throughput_fractions(P, mixed, R["mg_vcycle"], mv_ms, vc_ms, it_ms),
             "roofline": matvec_roofline(P, mixed, mv_ms),
             "matvec32_tile": list(P.info().matvec32_tile) if mixed else None,
             "clocks": clk,
@@ -406,15 +474,17 @@ def run_b200(args):
         }
         if comparison is not None:
             line["vs_fp64"] = comparison
+        if other is not None:
+            line["reference_regime"] = other
         if e2e:
             line["e2e"] = {"value": job_throughput(world, args.steps, e2e), "unit": "design iter/s",
                            "h2d_bytes_per_step": 4 * ne, "d2h_bytes_per_step": 4 * ne + 64}
         if not args.no_cpu_baseline and world == 1:
             try:
-                s = reference_sample(CONFIGS[args.config], 1, 1, int(round(statistics.mean(pcg_its))),
-                                     os.cpu_count() or 1)
+                s = reference_sample(CONFIGS[args.config], CPU_SAMPLES, 800, physical_cores())
                 line["cpu_baseline"] = {"value": s["value"], "unit": "design iter/s", "cores": s["cores"],
-                                        "kind": s["kind"], "sample": s["sample"]}
+                                        "kind": s["kind"], "sample": s["sample"],
+                                        "pcg_iteration_s": s["pcg_iteration_s"]}
             except Exception as e:  # baseline is reported, never required for the GPU number
                 line["cpu_baseline"] = {"value": None, "unit": "design iter/s", "cores": 0, "kind": "reference",
                                         "sample": "unavailable: %s" % e}
@@ -427,9 +497,7 @@ def run_b200(args):
 
 def main():
     args = parse_args()
-    if args.vcycle == "standard" and args.precision != "fp64" and args.impl == "b200":
-        print(json.dumps({"error": "--vcycle standard is built for --precision fp64 only"}), flush=True)
-        return 2
+    setup_cpu_env()
     if args.impl == "reference":
         return run_reference_arm(args)
     if args.kernels_only:
