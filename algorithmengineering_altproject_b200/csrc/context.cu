@@ -336,7 +336,7 @@ static int build_mixed(Context* c) {
         T3D_CUDA_OK(cudaMemsetAsync(c->E_mg32, 0, g.NEp * sizeof(float), c->st));
         for (int l = 1; l < c->nlev; ++l) {
             const MgLevel& L = c->lv[l];
-            CHECK(c->alloc(&c->Kel32[l], (size_t)L.nx * L.ny * L.nz * 576));
+            CHECK(c->alloc(&c->Kel32[l], (size_t)L.nx * L.ny * L.nz * 300));   // symmetric-packed
             CHECK(c->alloc(&c->vtmp32[l], 3 * L.nn));
         }
     }
@@ -729,7 +729,7 @@ static int mg_setup(Context* c) {
             launch_cells_to32(c->g, c->E_mg, c->E_mg32, c->st);
             for (int l = 1; l < c->nlev; ++l) {
                 const MgLevel& L = c->lv[l];
-                launch_kel_transpose32((int64_t)L.nx * L.ny * L.nz, c->Kel[l], c->Kel32[l], c->st);
+                launch_kel_pack32((int64_t)L.nx * L.ny * L.nz, c->Kel[l], c->Kel32[l], c->st);
             }
             for (int l = 0; l < c->nlev; ++l) {
                 const MgLevel32& M = c->lv32[l];
@@ -913,6 +913,8 @@ static int pcg_solve(Context* c, double tol, int maxit, int* iters) {
 static void vcycle32_standard(Context* c, const float* r, float* z, PcgScalars* S, RedSlot dot) {
     const int L = c->nlev;
     const float w = c->prm.mg_standard_weight;
+    // level 0 with the modal TMA kernel: the residual and the correction (with r.z) run in its epilogue
+    const bool fuse = c->modal && modal_fused_available(c->mt);
     auto level_op = [&](int l, const float* x, float* y) {
         if (l == 0) matvec32(c, x, y, RedSlot{nullptr, nullptr}, S, 0, c->E_mg32);
         else {
@@ -925,24 +927,42 @@ static void vcycle32_standard(Context* c, const float* r, float* z, PcgScalars* 
         float* xl = l == 0 ? z : c->lv32[l].x;
         float* t = l == 0 ? c->Ap32 : c->vtmp32[l];
         launch_jacobi_init32(c->lv32[l], rl, xl, w, S, c->st);
-        level_op(l, xl, t);
-        launch_residual32(c->lv32[l], rl, t, S, c->st);
+        c->launches += 1;
+        if (l == 0 && fuse) {
+            launch_matvec32_fused(1, c->g, c->kh, c->mt, c->E_mg32, c->mask0, xl, t, rl, nullptr, w,
+                                  RedSlot{nullptr, nullptr}, S, c->tma_err, c->st);
+            c->launches += 1;
+        } else {
+            level_op(l, xl, t);
+            launch_residual32(c->lv32[l], rl, t, S, c->st);
+            c->launches += 1;
+        }
         launch_restrict32(c->lv32[l + 1], c->lv32[l], t, c->lv32[l + 1].r, c->ra1_32[l], S, c->st, false);
-        c->launches += 2 + (c->lv32[l + 1].span == 4 ? 2 : 1);
+        c->launches += c->lv32[l + 1].span == 4 ? 2 : 1;
     }
     launch_coarse_solve32(c->lv32[L - 1], c->Xc, c->Nc, c->chol_status, S, c->st);
     c->launches += 1;
-    for (int l = L - 2; l >= 0; --l) {
-        const float* rl = l == 0 ? r : c->lv32[l].r;
-        float* xl = l == 0 ? z : c->lv32[l].x;
-        float* t = l == 0 ? c->Ap32 : c->vtmp32[l];
-        launch_prolong_add32(c->lv32[l + 1], c->lv32[l], c->lv32[l + 1].x, xl, S, c->st);
-        level_op(l, xl, t);
-        launch_jacobi_correct32(c->lv32[l], rl, t, xl, w, S, c->st);
+    for (int l = L - 2; l >= 1; --l) {
+        const float* rl = c->lv32[l].r;
+        float* xl = c->lv32[l].x;
+        launch_prolong_add32(c->lv32[l + 1], c->lv32[l], c->lv32[l + 1].x, xl, xl, S, c->st);
+        level_op(l, xl, c->vtmp32[l]);
+        launch_jacobi_correct32(c->lv32[l], rl, c->vtmp32[l], xl, w, S, c->st);
         c->launches += 2;
     }
+    // level 0: T = z + P x_1 into Ap32, then z = T + w (r - K T) / D with r.z, fused; else the separate steps
+    if (fuse) {
+        launch_prolong_add32(c->lv32[1], c->lv32[0], c->lv32[1].x, z, c->Ap32, S, c->st);
+        launch_matvec32_fused(2, c->g, c->kh, c->mt, c->E_mg32, c->mask0, c->Ap32, z, r, c->lv32[0].diag, w, dot, S,
+                              c->tma_err, c->st);
+        c->launches += 2;
+        return;
+    }
+    launch_prolong_add32(c->lv32[1], c->lv32[0], c->lv32[1].x, z, z, S, c->st);
+    level_op(0, z, c->Ap32);
+    launch_jacobi_correct32(c->lv32[0], r, c->Ap32, z, w, S, c->st);
     launch_dot_rz32(3 * c->g.NNp, r, z, dot, S, c->st);
-    c->launches += 1;
+    c->launches += 3;
 }
 
 static void vcycle32(Context* c, const float* r, float* z, PcgScalars* S, RedSlot dot) {

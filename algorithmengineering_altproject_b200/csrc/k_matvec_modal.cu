@@ -361,7 +361,25 @@ struct TmaShape {
                        const float* u, float* y, RedSlot dot, PcgScalars* S, int mark, int* err, cudaStream_t s) {
         CUtensorMap um, em;
         if (!modal_tensor_maps(g, u, E, SM::RW, SM::PY, BY, &um, &em)) return false;
-        k_matvec32_tma<BX, BY, MINB, ST><<<t.grid, BX * BY, smem, s>>>(um, em, g, kh, t, mask, y, dot, S, mark, err);
+        k_matvec32_tma<BX, BY, MINB, ST, 0><<<t.grid, BX * BY, smem, s>>>(um, em, g, kh, t, mask, y, dot, S, mark, err,
+                                                                         nullptr, nullptr, 0.0f);
+        return true;
+    }
+    static const void* fn_mode(int mode) {
+        return mode == 1 ? reinterpret_cast<const void*>(k_matvec32_tma<BX, BY, MINB, ST, 1>)
+                         : reinterpret_cast<const void*>(k_matvec32_tma<BX, BY, MINB, ST, 2>);
+    }
+    static bool fused(int mode, const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E,
+                      const uint8_t* mask, const float* u, float* y, const float* r, const float* rd, float w,
+                      RedSlot dot, PcgScalars* S, int* err, cudaStream_t s) {
+        CUtensorMap um, em;
+        if (!modal_tensor_maps(g, u, E, SM::RW, SM::PY, BY, &um, &em)) return false;
+        if (mode == 1)
+            k_matvec32_tma<BX, BY, MINB, ST, 1><<<t.grid, BX * BY, smem, s>>>(um, em, g, kh, t, mask, y, dot, S, 0, err,
+                                                                             r, rd, w);
+        else
+            k_matvec32_tma<BX, BY, MINB, ST, 2><<<t.grid, BX * BY, smem, s>>>(um, em, g, kh, t, mask, y, dot, S, 0, err,
+                                                                             r, rd, w);
         return true;
     }
 };
@@ -371,10 +389,18 @@ struct ModalVariant {
     const void* (*fn)();
     bool (*launch)(const Grid&, const ModalKe&, const ModalTiling&, const float*, const uint8_t*, const float*,
                    float*, RedSlot, PcgScalars*, int, int*, cudaStream_t);
+    // the fused Standard-cycle epilogues (TMA shapes only)
+    const void* (*fn_mode)(int);
+    bool (*fused)(int, const Grid&, const ModalKe&, const ModalTiling&, const float*, const uint8_t*, const float*,
+                  float*, const float*, const float*, float, RedSlot, PcgScalars*, int*, cudaStream_t);
 };
 template <class V>
 constexpr ModalVariant variant_of() {
-    return ModalVariant{V::bx, V::by, V::stages, V::packed, V::tma, V::smem, &V::fn, &V::launch};
+    if constexpr (V::tma)
+        return ModalVariant{V::bx, V::by, V::stages, V::packed, V::tma, V::smem, &V::fn, &V::launch, &V::fn_mode,
+                            &V::fused};
+    else
+        return ModalVariant{V::bx, V::by, V::stages, V::packed, V::tma, V::smem, &V::fn, &V::launch, nullptr, nullptr};
 }
 const ModalVariant MODAL_VARIANTS[] = {
     variant_of<ModalShape<32, 8, 2, 4, 1>>(),   // variant 0: the fallback of a TMA shape without tensor maps
@@ -443,6 +469,10 @@ int modal_tiling(const Grid& g, int dev, int variant, ModalTiling* t) {
     if (e != cudaSuccess) return set_cuda_error(e, "cudaDeviceGetAttribute", __FILE__, __LINE__);
     e = cudaFuncSetAttribute(v.fn(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem);
     if (e != cudaSuccess) return set_cuda_error(e, "cudaFuncSetAttribute", __FILE__, __LINE__);
+    for (int mode = 1; v.fn_mode && mode <= 2; ++mode) {
+        e = cudaFuncSetAttribute(v.fn_mode(mode), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem);
+        if (e != cudaSuccess) return set_cuda_error(e, "cudaFuncSetAttribute", __FILE__, __LINE__);
+    }
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn(), v.bx * v.by, v.smem);
     if (e != cudaSuccess) return set_cuda_error(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor", __FILE__, __LINE__);
     const int resident = std::max(1, std::min(sms * std::max(per_sm, 1), RED_BLOCKS));
@@ -509,6 +539,17 @@ int modal_autotune(const Grid& g, int dev, const ModalKe& kh, const float* E, co
     cudaEventDestroy(e1);
     if (rc == 0) cache[key] = *best;
     return rc;
+}
+
+bool modal_fused_available(const ModalTiling& t) {
+    return t.variant >= 0 && t.variant < MODAL_NVARIANTS && MODAL_VARIANTS[t.variant].fused != nullptr;
+}
+
+bool launch_matvec32_fused(int mode, const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E,
+                           const uint8_t* mask, const float* u, float* y, const float* r, const float* rd, float w,
+                           RedSlot dot, PcgScalars* S, int* err, cudaStream_t s) {
+    const ModalVariant& v = MODAL_VARIANTS[t.variant];
+    return v.fused != nullptr && v.fused(mode, g, kh, t, E, mask, u, y, r, rd, w, dot, S, err, s);
 }
 
 void launch_matvec32_modal(const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E,

@@ -98,11 +98,17 @@ struct TmaSmem {
     unsigned long long bar[STAGES];
 };
 
-template <int BX, int BY, int MINB, int STAGES>
+// Epilogue of an owned node (K x at the node in y0..y2, x's own values in h):
+//   MODE 0  the PCG's K(E)p: y = K x (fixed DOFs 0); with dot.partial, x.(K x) folded into S->denom;
+//   MODE 1  the Standard V-cycle's residual: y = r - K x (fixed DOFs 0);
+//   MODE 2  the Standard V-cycle's correction: y = x + w (r - K x) / D (rd = 1/D; fixed DOFs 0) written to a
+//           buffer other than x, with r.y folded into S (rz, or beta and rz, as the V-cycle's r.z).
+template <int BX, int BY, int MINB, int STAGES, int MODE = 0>
 __global__ void __launch_bounds__(BX * BY, MINB)
     k_matvec32_tma(const __grid_constant__ CUtensorMap umap, const __grid_constant__ CUtensorMap emap, Grid g,
                    ModalKe kh, ModalTiling t, const uint8_t* __restrict__ mask, float* __restrict__ y, RedSlot dot,
-                   PcgScalars* S, int mark, int* err) {
+                   PcgScalars* S, int mark, int* err, const float* __restrict__ rv, const float* __restrict__ rd,
+                   float w) {
     using SM = TmaSmem<BX, BY, STAGES>;
     constexpr int RW = SM::RW, PY = SM::PY;
     static_assert(STAGES >= 2, "ring needs two slots at least");
@@ -172,14 +178,29 @@ __global__ void __launch_bounds__(BX * BY, MINB)
                 float y0 = ((k0 + s1.x) + s2.x) + s3.x;
                 float y1 = ((k1 + s1.y) + s2.y) + s3.y;
                 float y2 = ((k2 + s1.z) + s2.z) + s3.z;
+                const int n = node_off + (pz - 2) * (int)NXY;
+                const int NP = (int)g.NNp;
+                if (MODE == 1) {
+                    y0 = rv[n] - y0;
+                    y1 = rv[NP + n] - y1;
+                    y2 = rv[2 * NP + n] - y2;
+                } else if (MODE == 2) {
+                    const float r0 = rv[n], r1 = rv[NP + n], r2 = rv[2 * NP + n];
+                    y0 = h2.x + (w * (r0 - y0)) * rd[n];
+                    y1 = h2.y + (w * (r1 - y1)) * rd[NP + n];
+                    y2 = h2.z + (w * (r2 - y2)) * rd[2 * NP + n];
+                    if (mk_next & 1) y0 = 0.f;
+                    if (mk_next & 2) y1 = 0.f;
+                    if (mk_next & 4) y2 = 0.f;
+                    part += (double)fmaf(r2, y2, fmaf(r1, y1, r0 * y0));
+                }
                 if (mk_next & 1) y0 = 0.f;
                 if (mk_next & 2) y1 = 0.f;
                 if (mk_next & 4) y2 = 0.f;
-                const int n = node_off + (pz - 2) * (int)NXY;
                 y[n] = y0;
-                y[(int)g.NNp + n] = y1;
-                y[2 * (int)g.NNp + n] = y2;
-                if (dot.partial)   // the node's 3 FP32 products summed in FP32, accumulated in FP64
+                y[NP + n] = y1;
+                y[2 * NP + n] = y2;
+                if (MODE == 0 && dot.partial)   // the node's 3 FP32 products summed in FP32, accumulated in FP64
                     part += (double)fmaf(h2.z, y2, fmaf(h2.y, y1, h2.x * y0));
             }
             if (owner && pz - 1 >= Z0 && pz - 1 < Z1) mk_next = mask[mask_off + (pz - 1) * (int)MXY];
@@ -259,9 +280,22 @@ __global__ void __launch_bounds__(BX * BY, MINB)
         }
         gp += (unsigned)nplanes;
     }
-    if (dot.partial) {
+    if (MODE == 0 && dot.partial) {
         double tot;
         if (grid_fold(part, dot, sm.sh, &tot) && threadIdx.x == 0) S->denom = tot;
+    }
+    if (MODE == 2) {
+        double tot;
+        if (grid_fold(part, dot, sm.sh, &tot) && threadIdx.x == 0) {
+            if (S->first) {
+                S->rz = tot;
+                S->first = 0;
+            } else {
+                const double rz = S->rz;
+                S->beta = tot / (1.0e-30 < rz ? rz : 1.0e-30);
+                S->rz = tot;
+            }
+        }
     }
 }
 

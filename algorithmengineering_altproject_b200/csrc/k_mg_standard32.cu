@@ -71,8 +71,8 @@ __global__ void k_jacobi_correct32(MgLevel32 L, const float* __restrict__ r, con
     }
 }
 
-// xf += P xc (trilinear from the coarse cell floor(f/s), clamped to the last cell), fixed DOFs 0
-__global__ void k_prolong_add32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ xc, float* __restrict__ xf,
+// xo = xi + P xc (trilinear from the coarse cell floor(f/s), clamped to the last cell), fixed DOFs 0; xo may be xi
+__global__ void k_prolong_add32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ xc, const float* xi, float* xo,
                                 const PcgScalars* S) {
     if (S->done) return;
     const int s = Lc.span;
@@ -92,14 +92,21 @@ __global__ void k_prolong_add32(MgLevel32 Lc, MgLevel32 Lf, const float* __restr
                          xc[c * Lc.cs + ((int64_t)(cz + corner_dz(A)) * cny + cy + corner_dy(A)) * cnx + cx + corner_dx(A)],
                          p);
             const int64_t i = c * Lf.cs + v;
-            xf[i] = ((m >> c) & 1) ? 0.0f : xf[i] + p;
+            xo[i] = ((m >> c) & 1) ? 0.0f : xi[i] + p;
         }
     }
 }
 
-// y = K_l x from the FP32 element matrices of a coarse level (node-centric gather: each node reads the three
-// rows of its corner in the 8 element matrices around it, so every matrix entry is read once; entry-major
-// storage makes the reads of consecutive nodes consecutive), fixed DOFs 0
+// packed position of entry (i, j) of a symmetric 24x24 matrix: the upper triangle row by row, 300 entries
+__host__ __device__ constexpr int sym_pack(int i, int j) {
+    return i <= j ? i * 24 - i * (i - 1) / 2 + (j - i) : j * 24 - j * (j - 1) / 2 + (i - j);
+}
+constexpr int SYM_N = 300;
+
+// y = K_l x from the FP32 element matrices of a coarse level, stored symmetric-packed and entry-major (entry p of
+// element e at p * ne + e; the Galerkin operators P^T K P are symmetric).  Node-centric gather: each node reads
+// the three rows of its corner in the 8 element matrices around it (all loops unrolled, so the packed positions
+// are constants); consecutive nodes read consecutive addresses.  Fixed DOFs 0.
 __global__ void k_level_matvec32(MgLevel32 L, const float* __restrict__ Kel, const float* __restrict__ x,
                                  float* __restrict__ y, const PcgScalars* S) {
     if (S->done) return;
@@ -108,23 +115,25 @@ __global__ void k_level_matvec32(MgLevel32 L, const float* __restrict__ Kel, con
     for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < L.nn; n += (int64_t)gridDim.x * blockDim.x) {
         const int X = (int)(n % nnx), Y = (int)((n / nnx) % nny), Z = (int)(n / ((int64_t)nnx * nny));
         float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f;
+#pragma unroll
         for (int dz = 0; dz <= 1; ++dz)
+#pragma unroll
             for (int dy = 0; dy <= 1; ++dy)
+#pragma unroll
                 for (int dx = 0; dx <= 1; ++dx) {
                     const int ex = X - dx, ey = Y - dy, ez = Z - dz;
                     if (ex < 0 || ey < 0 || ez < 0 || ex >= L.nx || ey >= L.ny || ez >= L.nz) continue;
                     const int a = corner_of(dx, dy, dz);
-                    // entry-major element matrices: row 3a+r, column 3b+c of element e at ((3a+r)*24 + 3b+c) * ne + e
-                    const float* K = Kel + ((int64_t)(ez * L.ny + ey) * L.nx + ex) + (int64_t)(3 * a) * 24 * ne;
+                    const float* K = Kel + ((int64_t)(ez * L.ny + ey) * L.nx + ex);
 #pragma unroll
                     for (int b = 0; b < 8; ++b) {
                         const int64_t m = ((int64_t)(ez + corner_dz(b)) * nny + ey + corner_dy(b)) * nnx + ex + corner_dx(b);
 #pragma unroll
                         for (int c = 0; c < 3; ++c) {
                             const float xv = x[c * L.cs + m];
-                            acc0 = fmaf(K[(3 * b + c) * ne], xv, acc0);
-                            acc1 = fmaf(K[(24 + 3 * b + c) * ne], xv, acc1);
-                            acc2 = fmaf(K[(48 + 3 * b + c) * ne], xv, acc2);
+                            acc0 = fmaf(K[sym_pack(3 * a, 3 * b + c) * ne], xv, acc0);
+                            acc1 = fmaf(K[sym_pack(3 * a + 1, 3 * b + c) * ne], xv, acc1);
+                            acc2 = fmaf(K[sym_pack(3 * a + 2, 3 * b + c) * ne], xv, acc2);
                         }
                     }
                 }
@@ -133,6 +142,24 @@ __global__ void k_level_matvec32(MgLevel32 L, const float* __restrict__ Kel, con
         y[L.cs + n] = (mk & 2) ? 0.0f : acc1;
         y[2 * L.cs + n] = (mk & 4) ? 0.0f : acc2;
     }
+}
+
+// FP32 symmetric-packed, entry-major image of element-major FP64 element matrices (the upper triangle):
+// dst[p * ne + e] = src[e * 576 + 24 i + j], (i, j) the p-th upper-triangle entry
+__global__ void k_kel_pack32(int64_t ne, const double* __restrict__ src, float* __restrict__ dst) {
+    __shared__ short ij[SYM_N];
+    for (int p = threadIdx.x + threadIdx.y * 32; p < SYM_N; p += 32 * blockDim.y) {
+        int i = 0, q = p;
+        while (q >= 24 - i) {
+            q -= 24 - i;
+            ++i;
+        }
+        ij[p] = (short)(i * 24 + i + q);
+    }
+    __syncthreads();
+    const int64_t e = (int64_t)blockIdx.x * 32 + threadIdx.x;
+    if (e >= ne) return;
+    for (int p = threadIdx.y; p < SYM_N; p += blockDim.y) dst[(int64_t)p * ne + e] = (float)src[e * 576 + ij[p]];
 }
 
 // r.z over pitched FP32 vectors (pads zero), accumulated in FP64; the last block sets rz (first use) or
@@ -179,13 +206,16 @@ void launch_jacobi_correct32(const MgLevel32& L, const float* r, const float* kx
                              const PcgScalars* S, cudaStream_t s) {
     k_jacobi_correct32<<<blocks_of(L.nn, 256), 256, 0, s>>>(L, r, kx, x, w, S);
 }
-void launch_prolong_add32(const MgLevel32& Lc, const MgLevel32& Lf, const float* xc, float* xf, const PcgScalars* S,
-                          cudaStream_t s) {
-    k_prolong_add32<<<blocks_of(Lf.nn, 256), 256, 0, s>>>(Lc, Lf, xc, xf, S);
+void launch_prolong_add32(const MgLevel32& Lc, const MgLevel32& Lf, const float* xc, const float* xi, float* xo,
+                          const PcgScalars* S, cudaStream_t s) {
+    k_prolong_add32<<<blocks_of(Lf.nn, 256), 256, 0, s>>>(Lc, Lf, xc, xi, xo, S);
 }
 void launch_level_matvec32(const MgLevel32& L, const float* Kel, const float* x, float* y, const PcgScalars* S,
                            cudaStream_t s) {
     k_level_matvec32<<<blocks_of(L.nn, 128), 128, 0, s>>>(L, Kel, x, y, S);
+}
+void launch_kel_pack32(int64_t ne, const double* Kel, float* KelP32, cudaStream_t s) {
+    k_kel_pack32<<<(unsigned)((ne + 31) / 32), dim3(32, 8), 0, s>>>(ne, Kel, KelP32);
 }
 void launch_dot_rz32(int64_t n3, const float* r, const float* z, RedSlot red, PcgScalars* S, cudaStream_t s) {
     k_dot_rz32<<<RED_BLOCKS, RED_THREADS, 0, s>>>(n3, r, z, red, S);

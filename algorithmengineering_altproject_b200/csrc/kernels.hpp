@@ -244,10 +244,13 @@ void launch_jacobi_init32(const MgLevel32& L, const float* r, float* x, float w,
 void launch_residual32(const MgLevel32& L, const float* r, float* kx, const PcgScalars* S, cudaStream_t s);
 void launch_jacobi_correct32(const MgLevel32& L, const float* r, const float* kx, float* x, float w,
                              const PcgScalars* S, cudaStream_t s);
-void launch_prolong_add32(const MgLevel32& Lc, const MgLevel32& Lf, const float* xc, float* xf, const PcgScalars* S,
-                          cudaStream_t s);
-void launch_level_matvec32(const MgLevel32& L, const float* Kel, const float* x, float* y, const PcgScalars* S,
+// xo = xi + P xc (fixed DOFs 0); xo may be xi
+void launch_prolong_add32(const MgLevel32& Lc, const MgLevel32& Lf, const float* xc, const float* xi, float* xo,
+                          const PcgScalars* S, cudaStream_t s);
+// KelP32: the level's element matrices as FP32, symmetric-packed (300 upper-triangle entries), entry-major
+void launch_level_matvec32(const MgLevel32& L, const float* KelP32, const float* x, float* y, const PcgScalars* S,
                            cudaStream_t s);
+void launch_kel_pack32(int64_t ne, const double* Kel, float* KelP32, cudaStream_t s);
 void launch_dot_rz32(int64_t n3, const float* r, const float* z, RedSlot red, PcgScalars* S, cudaStream_t s);
 void launch_prolong_smooth32(const MgLevel32& Lc, const MgLevel32& Lf, const float* xc, const float* rf, float* xf,
                              float w, const PcgScalars* S, cudaStream_t s);
@@ -283,6 +286,14 @@ int modal_autotune(const Grid& g, int dev, const ModalKe& kh, const float* E, co
 void launch_matvec32_modal(const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E,
                            const uint8_t* mask, const float* u, float* y, RedSlot dot, PcgScalars* S, int mark,
                            int* err, cudaStream_t s);
+
+// The Standard V-cycle's level-0 operator with its elementwise step fused into the epilogue (TMA tile shapes only;
+// false when the tiling's shape has no fused form, then nothing was launched):
+//   mode 1: y = r - K(E)u;  mode 2: y = u + w (r - K(E)u) rd (rd = 1/D; y must not alias u), r.y -> S (rz / beta)
+bool modal_fused_available(const ModalTiling& t);
+bool launch_matvec32_fused(int mode, const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E,
+                           const uint8_t* mask, const float* u, float* y, const float* r, const float* rd, float w,
+                           RedSlot dot, PcgScalars* S, int* err, cudaStream_t s);
 
 // ---- surface export (k_stl.cu, io.cpp:80-87)
 int stl_chunks(const Grid& g);
