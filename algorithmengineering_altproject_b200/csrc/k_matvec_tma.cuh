@@ -101,14 +101,14 @@ struct TmaSmem {
 // Epilogue of an owned node (K x at the node in y0..y2, x's own values in h):
 //   MODE 0  the PCG's K(E)p: y = K x (fixed DOFs 0); with dot.partial, x.(K x) folded into S->denom;
 //   MODE 1  the Standard V-cycle's residual: y = r - K x (fixed DOFs 0);
-//   MODE 2  the Standard V-cycle's correction: y = x + w (r - K x) / D (rd = 1/D; fixed DOFs 0) written to a
+//   MODE 2  the Standard V-cycle's correction: y = x + omega (r - K x) / D (rd = 1/D; fixed DOFs 0) written to a
 //           buffer other than x, with r.y folded into S (rz, or beta and rz, as the V-cycle's r.z).
 template <int BX, int BY, int MINB, int STAGES, int MODE = 0>
 __global__ void __launch_bounds__(BX * BY, MINB)
     k_matvec32_tma(const __grid_constant__ CUtensorMap umap, const __grid_constant__ CUtensorMap emap, Grid g,
                    ModalKe kh, ModalTiling t, const uint8_t* __restrict__ mask, float* __restrict__ y, RedSlot dot,
                    PcgScalars* S, int mark, int* err, const float* __restrict__ rv, const float* __restrict__ rd,
-                   float w) {
+                   float omega) {
     using SM = TmaSmem<BX, BY, STAGES>;
     constexpr int RW = SM::RW, PY = SM::PY;
     static_assert(STAGES >= 2, "ring needs two slots at least");
@@ -186,9 +186,9 @@ __global__ void __launch_bounds__(BX * BY, MINB)
                     y2 = rv[2 * NP + n] - y2;
                 } else if (MODE == 2) {
                     const float r0 = rv[n], r1 = rv[NP + n], r2 = rv[2 * NP + n];
-                    y0 = h2.x + (w * (r0 - y0)) * rd[n];
-                    y1 = h2.y + (w * (r1 - y1)) * rd[NP + n];
-                    y2 = h2.z + (w * (r2 - y2)) * rd[2 * NP + n];
+                    y0 = h2.x + (omega * (r0 - y0)) * rd[n];
+                    y1 = h2.y + (omega * (r1 - y1)) * rd[NP + n];
+                    y2 = h2.z + (omega * (r2 - y2)) * rd[2 * NP + n];
                     if (mk_next & 1) y0 = 0.f;
                     if (mk_next & 2) y1 = 0.f;
                     if (mk_next & 4) y2 = 0.f;
