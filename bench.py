@@ -50,6 +50,9 @@ CONFIGS = {
     # kernel-capture size: vectors above L2, a few GB on the device
     "k1": dict(nely=160, nelx=320, nelz=160, V0=0.08, max_levels=5,
                name="cantilever 160x320x160 (8,192,000 elements)"),
+    # DRAM-traffic capture size: FP32 node vectors 273 MB each, 2.2x the 126 MB L2
+    "k2": dict(nely=224, nelx=448, nelz=224, V0=0.08, max_levels=6,
+               name="cantilever 224x448x224 (22,478,848 elements)"),
 }
 DEFAULT_CONFIG = "c2"
 METRIC = "design iterations/s"
