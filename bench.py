@@ -5,6 +5,9 @@ sensitivities -> PDE filter -> OC) on the reference's cantilever.
                     [--precision mixed|fp64] [--regime converged|reference] [--compare-steps S]
                     [--kernels-only --reps R --tile T]
 
+`serving` (N=1, after the timed region) runs the request loop (serve.py) on Poisson arrivals at 0.5 and 8
+requests/s and the same requests one at a time in FP64: designs/s and p50/p95/p99 latency.
+
 Prints ONE JSON line (rank 0).  A step is one design iteration of 256x512x256 (101.6M DOF).  The default
 form is the mixed-precision one (FP32 inner MG-PCG inside FP64 defect correction) in the "converged"
 regime: every solve reaches |r| < 1e-6 |b| with the Standard V-cycle rebuilt every design iteration, so
@@ -80,6 +83,8 @@ def parse_args():
                     help="modal FP32 K(E)p tile shape: 0 = autotuned, k = shape k-1 (--kernels-only timing)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=8,
+                    help="requests per arrival rate in the serving sample (0 = no serving sample)")
     return ap.parse_args()
 
 
@@ -267,6 +272,37 @@ REGIMES = {
 }
 
 
+# Serving sample: Poisson arrivals at the two ends of the 0.5-8 requests/s sweep, request sizes lognormal (median
+# 0.5M elements, clipped to [30k, 16M]) with shapes, V0, load cases and voids drawn as in the batched workload,
+# 40 OC iterations per request, 160 GB admission budget; the same seeded requests one at a time in plain FP64 as
+# the baseline.
+SERVE_RATES = (0.5, 8.0)
+SERVE_SEED = 20251203
+SERVE_ITERS = 40
+
+
+def serving_sample(dev, n):
+    """designs/s and p50/p95/p99 end-to-end latency of the request loop (serve.DesignServer: admission by
+    projected HBM footprint, concurrent contexts on their own streams) for n requests at each rate, and of the
+    same requests served one at a time in FP64."""
+    import algorithmengineering_altproject_b200 as t3d
+    from algorithmengineering_altproject_b200 import serve
+
+    def run(rate, precision, max_active):
+        with serve.DesignServer(device=dev, hbm_budget=160e9, max_active=max_active, precision=precision) as srv:
+            res, wall = serve.run_poisson(srv, np.random.default_rng(SERVE_SEED), rate, n, SERVE_ITERS)
+        s = serve.summary(res, wall)
+        s["elements"] = int(sum(r.request.nelx * r.request.nely * r.request.nelz for r in res))
+        return {"rate_per_s": rate, **s}
+
+    out = {"requests_per_rate": n, "iters_per_request": SERVE_ITERS, "seed": SERVE_SEED, "budget_gb": 160,
+           "max_active": 8, "precision": "mixed",
+           "note": "p99 of %d requests is their maximum latency; latency = arrival to result" % n,
+           "rates": [run(r, t3d.T3D_MIXED, 8) for r in SERVE_RATES]}
+    out["sequential_fp64"] = run(SERVE_RATES[0], t3d.T3D_FP64, 1)
+    return out
+
+
 def problem_kw(t3d, cfg, regime, precision, dev, tile=0):
     R = REGIMES[regime]
     return dict(device=dev, mg_max_levels=cfg["max_levels"], oc_sum_order=t3d.T3D_SUM_FP64,
@@ -300,14 +336,17 @@ def throughput_fractions(P, mixed, vcycle, mv_ms, vc_ms, it_ms):
     bytes per unit (n = free DOFs, N_e = elements, w = bytes per value of the inner solve, c = the coarse levels'
     3 * nodes):
       Adapted V-cycle   w * 4 (n + c)            (down: read r; up: read r and D, write z)
-      Standard V-cycle  w * (22 n + 2 N_e + 8 c) (level 0: Jacobi start r, D -> x; K x (2n + N_e); residual r, Kx
-                        -> t; restriction reads t; prolongation x -> x; K x; correction r, t, x, D -> x; r.z)
+      Standard V-cycle  w * (22 n + 2 N_e + 8 c) + 2 k Σ N_l (level 0: Jacobi start r, D -> x; K x (2n + N_e);
+                        residual r, Kx -> t; restriction reads t; prolongation x -> x; K x; correction r, t, x, D
+                        -> x; r.z; each level l between the finest and the coarsest: two products with its N_l
+                        stored Galerkin element matrices of k bytes each, 300 FP32 (symmetric-packed) or 576 FP64)
       PCG iteration     the V-cycle + w * (11 n + N_e) (K(E)p 2n + N_e, update 3n, direction and x update 6n)"""
     w = 4 if mixed else 8
     peak, _ = hbm_peak()
     coarse = sum(3 * (nx + 1) * (ny + 1) * (nz + 1) for nx, ny, nz, _ in P.levels[1:])
     n, ne = P.nf, P.ne
-    vc_bytes = w * (22 * n + 2 * ne + 8 * coarse) if vcycle == "standard" else w * 4 * (n + coarse)
+    kel = (300 * 4 if mixed else 576 * 8) * sum(nx * ny * nz for nx, ny, nz, _ in P.levels[1:-1])
+    vc_bytes = w * (22 * n + 2 * ne + 8 * coarse) + 2 * kel if vcycle == "standard" else w * 4 * (n + coarse)
     it_bytes = vc_bytes + w * (11 * n + ne)
     out = {"dof_matvecs_per_s": n / (mv_ms * 1e-3), "vcycles_per_s": 1.0 / (vc_ms * 1e-3),
            "vcycle": vcycle, "vcycle_bytes": vc_bytes, "vcycle_gbs": vc_bytes / (vc_ms * 1e-3) / 1e9,
@@ -379,6 +418,8 @@ def compare_forms(cfg, regime, dev, steps, warm=1):
 
 
 def run_b200(args):
+    # the serving sample runs concurrent contexts in this process: load every kernel module at CUDA start-up
+    os.environ.setdefault("CUDA_MODULE_LOADING", "EAGER")
     import torch
     import algorithmengineering_altproject_b200 as t3d
 
@@ -488,8 +529,14 @@ def run_b200(args):
             except Exception as e:  # baseline is reported, never required for the GPU number
                 line["cpu_baseline"] = {"value": None, "unit": "design iter/s", "cores": 0, "kind": "reference",
                                         "sample": "unavailable: %s" % e}
-        print(json.dumps(line), flush=True)
     P.close()
+    if rank == 0:
+        if args.serve_requests > 0 and world == 1 and mixed:
+            try:
+                line["serving"] = serving_sample(dev, args.serve_requests)
+            except Exception as e:  # reported beside the headline, never required for it
+                line["serving"] = {"unavailable": "%s: %s" % (type(e).__name__, e)}
+        print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
     return 0
