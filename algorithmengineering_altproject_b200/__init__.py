@@ -14,7 +14,7 @@ import os
 
 import numpy as np
 
-__all__ = ["Problem", "T3DError", "library", "IterRecord", "Params", "LIB_PATH", "HEADER_PATH"]
+__all__ = ["Problem", "Batch", "T3DError", "library", "IterRecord", "Params", "LIB_PATH", "HEADER_PATH"]
 
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(PKG_DIR, "libt3d_b200.so")
@@ -90,6 +90,7 @@ class IterRecord(C.Structure):
 
 
 _CTX = C.c_void_p
+_BATCH = C.c_void_p
 # name -> (restype, argtypes); every function declared in include/t3d_b200.h
 _SIGS = {
     "t3d_params_default": (C.c_int, [C.POINTER(Params)]),
@@ -139,7 +140,15 @@ _SIGS = {
     "t3d_profile": (C.c_int, [_CTX, C.c_int, C.c_int, C.POINTER(C.c_double)]),
     "t3d_compliance_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_int, _f64p, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_void_p]),
+    "t3d_batch_create": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(Params), C.POINTER(ProblemSpec),
+                                   C.POINTER(_BATCH)]),
+    "t3d_batch_member": (C.c_int, [_BATCH, C.c_int, C.POINTER(_CTX)]),
+    "t3d_batch_design_init": (C.c_int, [_BATCH, _f32p, _f64p]),
+    "t3d_batch_design_step": (C.c_int, [_BATCH, C.POINTER(IterRecord)]),
+    "t3d_batch_info": (C.c_int, [_BATCH, C.POINTER(C.c_int64)]),
+    "t3d_batch_destroy": (C.c_int, [_BATCH]),
 }
+T3D_BATCH_TILE = 7
 T3D_PROFILE_MATVEC, T3D_PROFILE_VCYCLE, T3D_PROFILE_MATVEC32, T3D_PROFILE_VCYCLE32 = 0, 1, 2, 3
 
 _lib = None
@@ -245,7 +254,8 @@ class Problem:
 
     def close(self):
         if getattr(self, "_h", None):
-            self._lib.t3d_destroy(self._h)
+            if getattr(self, "_owned", True):
+                self._lib.t3d_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -454,3 +464,85 @@ class Problem:
 
     def kernel_launches(self):
         return int(self.info().kernel_launches)
+
+
+class Batch:
+    """Many designs of uneven grid size stepping together (t3d_batch_*; no reference counterpart -- the
+    reference runs one design per process, driver.cpp:23).  Members share one device arena; every kernel of
+    their inner FP32 MG-PCG iteration is one persistent launch over an (instance, block) work list with
+    per-instance convergence masks, and each member's results equal those of a Problem created alone with
+    the same parameters and ``matvec32_tile=T3D_BATCH_TILE``.
+
+    dims: [(nely, nelx, nelz), ...]; problems: ProblemSpec per member or None (the reference cantilever);
+    params: common keyword parameters (precision is T3D_MIXED), or ``member_params``: one dict per member.
+    ``members[i]`` is a Problem view of member i (queries only; the batch owns it).
+    """
+
+    def __init__(self, dims, problems=None, member_params=None, **params):
+        self._lib = library()
+        n = len(dims)
+        P = (Params * n)()
+        for i in range(n):
+            kw = dict(params, precision=T3D_MIXED)
+            if member_params is not None:
+                kw.update(member_params[i])
+            P[i] = default_params(**kw)
+        D = (C.c_int * (3 * n))(*[int(v) for d in dims for v in d])
+        Q = None
+        if problems is not None:
+            Q = (ProblemSpec * n)()
+            for i, q in enumerate(problems):
+                Q[i] = q if q is not None else ProblemSpec.make()
+        h = _BATCH()
+        _check(self._lib.t3d_batch_create(n, D, P, Q, C.byref(h)))
+        self._h = h
+        self.n = n
+        self.members = []
+        for i in range(n):
+            c = _CTX()
+            _check(self._lib.t3d_batch_member(self._h, i, C.byref(c)))
+            m = Problem.__new__(Problem)
+            m._lib = self._lib
+            m.params = P[i]
+            m._owned = False
+            m._attach(c)
+            self.members.append(m)
+
+    def design_init(self, V0):
+        """t3d_design_init of every member; V0: one value per member; returns the solid compliances"""
+        v = np.ascontiguousarray(np.broadcast_to(np.asarray(V0, dtype=np.float32), (self.n,)))
+        cs = np.zeros(self.n)
+        _check(self._lib.t3d_batch_design_init(self._h, v, cs))
+        return cs
+
+    def design_step(self):
+        """one design iteration of every member; returns their records"""
+        recs = (IterRecord * self.n)()
+        _check(self._lib.t3d_batch_design_step(self._h, recs))
+        return [recs[i].as_dict() for i in range(self.n)]
+
+    def info(self):
+        v = (C.c_int64 * 6)()
+        _check(self._lib.t3d_batch_info(self._h, v))
+        keys = ("arena_bytes", "members", "batched_launches", "kernels_per_iteration", "blocks_per_iteration",
+                "member_launches")
+        return {k: int(v[i]) for i, k in enumerate(keys)}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            for m in self.members:
+                m._h = None
+            self._lib.t3d_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -6,6 +6,7 @@
 #include "hex8.hpp"
 #include "kernels.hpp"
 #include "topvoxel.hpp"
+#include "context.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -77,128 +78,6 @@ static int pad_dim(int n, int L) {
     return ((n + s - 1) / s) * s;
 }
 
-// ------------------------------------------------------------------ context
-struct Context {
-    t3d_params prm{};
-    Grid g{};
-    Cuboid cub{};
-    VoidSet voids{};            // passive-void ellipsoids (absent voxels)
-    int load_case = T3D_LOAD_TIP_LINE;
-    int dev = 0;
-    cudaStream_t st = nullptr;
-    int nlev = 0;
-    MgLevel lv[8]{};
-    int Nc = 0;                 // dense coarsest size (0: Jacobi coarsest)
-    int64_t ne = 0;             // solid elements
-    size_t bytes = 0;
-    std::vector<void*> allocs;
-
-    double* Ke = nullptr;       // 576
-    double* kf = nullptr;       // 72
-    double Ke_h[576];
-    uint8_t* solid = nullptr;   // cells
-    uint8_t* mask0 = nullptr;   // nodes
-    double *E = nullptr, *ce = nullptr;                       // cells
-    float *x = nullptr, *xnew = nullptr, *dc = nullptr, *xdc = nullptr, *dcf = nullptr;   // cells
-    double *b = nullptr, *u = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *Ap = nullptr;  // 3 NN
-    PcgScalars* S = nullptr;
-    FilterScalars* FS = nullptr;
-    OcState* OC = nullptr;
-    double* scal = nullptr;     // [0] C, [1] Csolid, [2] objective
-    bool mv64_stream = false;   // FP64 K(E)u by the element-streaming kernel (else node-centric)
-    Stream64Tiling st64{};
-    std::shared_ptr<const VoxelModel> vox;   // external (TopVoxel) model, else the built-in cuboid
-    // several load cases (external models): per-case loads and warm starts, weighted element compliance
-    int ncases = 1;
-    double *b_cases = nullptr, *u_cases = nullptr, *ce_acc = nullptr, *one = nullptr;
-    // 'Standard' V-cycle option: Galerkin element matrices per level (l >= 1), child-position products of
-    // Ke for level 1, and one scratch vector per level
-    bool standard = false;
-    double* E_mg = nullptr;     // the moduli the hierarchy was built from (the cycle's level-0 operator)
-    double* Kel[8]{};           // element-major (assembly)
-    double* KelT[8]{};          // entry-major copies read by the level products
-    double* Gpos = nullptr;
-    double* vtmp[8]{};
-    bool ke_pat = false;        // Ke has the built-in coefficient pattern: its magnitudes are in Kd
-    double* Kd = nullptr;       // [KE_MAX_DISTINCT]
-    RedSlot slot[4]{};
-    double *Kce = nullptr, *Kc = nullptr, *LT = nullptr, *Lrow = nullptr, *Xc = nullptr;
-    double* ra1[8]{};           // separable-restriction pass buffers per level transition
-    double* ra2[8]{};
-    int* chol_status = nullptr;
-    double *frhs = nullptr, *fx = nullptr, *fr = nullptr, *fz = nullptr, *fp = nullptr, *fAp = nullptr,
-           *flastx = nullptr, *flastrhs = nullptr, *fdiag = nullptr;
-    // mixed precision (T3D_MIXED): FP32 inner-solve state
-    bool mixed = false;
-    float* Ke32 = nullptr;
-    ModalKe kh{};               // modal form of Ke for the FP32 K(E)p (valid when `modal`)
-    ModalTiling mt{};
-    bool modal = false;
-    double modal_off = 0.0;     // largest relative off-pattern entry of T^T Ke T
-    float* E32 = nullptr;
-    float *r32 = nullptr, *d32 = nullptr, *z32 = nullptr, *p32 = nullptr, *Ap32 = nullptr;
-    MgLevel32 lv32[8]{};
-    float* ra1_32[8]{};         // x-pass buffer of the FP32 restriction (its y and z passes are fused)
-    // the Standard V-cycle in FP32: element-matrix images and scratch per coarse level, level-0 moduli image
-    float* Kel32[8]{};
-    float* vtmp32[8]{};
-    float* E_mg32 = nullptr;
-    PcgScalars* S32 = nullptr;
-    int* tma_err = nullptr;     // set by a TMA-staged K(E)p whose mbarrier wait gave up (checked after solves)
-    cudaGraphExec_t pcg32_graph = nullptr;
-    int64_t pcg32_graph_launches = 0;
-    int last_outer = 0;
-    // lazily built maps between the reference's layouts and the grid
-    int32_t* morton = nullptr;          // [ne] cell index of the k-th element in Morton order
-    std::vector<int32_t> morton_h;
-    int32_t* free_d = nullptr;
-    std::vector<int32_t> free_h;
-    double* stage = nullptr;            // staging buffer for host<->device conversions
-    size_t stage_n = 0;
-    // pinned host mirror of small device state
-    PcgScalars* S_h = nullptr;
-    OcState* OC_h = nullptr;
-    FilterScalars* FS_h = nullptr;
-    double* scal_h = nullptr;
-    int* flag_h = nullptr;              // two done-flag slots for pipelined polling
-    // CUDA graph of a chunk of PCG iterations
-    cudaGraphExec_t pcg_graph = nullptr;
-    int pcg_graph_len = 0;
-    bool use_graph = true;
-    // design state
-    bool mg_ready = false;
-    bool design_ready = false;
-    float V0 = 0.0f;
-    int loop = 0;
-    cudaEvent_t ev[8]{};
-    int64_t launches = 0;   // kernels launched (graph replays counted per node)
-
-    template <class T>
-    int alloc(T** ptr, size_t n) {
-        void* q = nullptr;
-        const size_t nb = std::max<size_t>(n, 1) * sizeof(T);
-        cudaError_t e = cudaMalloc(&q, nb);
-        if (e != cudaSuccess) return set_cuda_error(e, "cudaMalloc", __FILE__, __LINE__);
-        allocs.push_back(q);
-        bytes += nb;
-        *ptr = static_cast<T*>(q);
-        return T3D_OK;
-    }
-
-    ~Context() {
-        if (pcg_graph) cudaGraphExecDestroy(pcg_graph);
-        if (pcg32_graph) cudaGraphExecDestroy(pcg32_graph);
-        for (auto& e : ev)
-            if (e) cudaEventDestroy(e);
-        for (void* q : allocs) cudaFree(q);
-        if (S_h) cudaFreeHost(S_h);
-        if (OC_h) cudaFreeHost(OC_h);
-        if (FS_h) cudaFreeHost(FS_h);
-        if (scal_h) cudaFreeHost(scal_h);
-        if (flag_h) cudaFreeHost(flag_h);
-        if (st) cudaStreamDestroy(st);
-    }
-};
 
 static int update_ke_pattern(Context* c);
 
@@ -211,19 +90,13 @@ static int upload_gpos(Context* c) {
     return T3D_OK;
 }
 
-#define CHECK(call)                       \
-    do {                                  \
-        int rc_ = (call);                 \
-        if (rc_ != T3D_OK) return rc_;    \
-    } while (0)
-
-static int launch_check(const char* what) {
+int launch_check(const char* what) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_cuda_error(e, what, __FILE__, __LINE__);
     return T3D_OK;
 }
 
-static int sync(Context* c) {
+int sync(Context* c) {
     T3D_CUDA_OK(cudaStreamSynchronize(c->st));
     return T3D_OK;
 }
@@ -292,7 +165,7 @@ static int build_levels(Context* c) {
 
 // A TMA-staged K(E)p records a bounded mbarrier wait that gave up in c->tma_err (the kernel went on and
 // returned); its results are then void.  Reads the flag (synchronising the stream).
-static int check_tma(Context* c) {
+int check_tma(Context* c) {
     int e = 0;
     T3D_CUDA_OK(cudaMemcpyAsync(&e, c->tma_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
     T3D_CUDA_OK(cudaStreamSynchronize(c->st));
@@ -453,7 +326,7 @@ static int setup_voxel_model(Context* c) {
     return T3D_OK;
 }
 
-static int create(int nely, int nelx, int nelz, const t3d_params* prm, const t3d_problem* pb, Context* c) {
+int create(int nely, int nelx, int nelz, const t3d_params* prm, const t3d_problem* pb, Context* c) {
     if (nely <= 0 || nelx <= 0 || nelz <= 0) return set_error(T3D_ERR_INVALID, "element counts must be positive");
     if (pb) {
         if (pb->load_case < T3D_LOAD_TIP_LINE || pb->load_case > T3D_LOAD_TORSION)
@@ -618,7 +491,7 @@ static void morton_walk(const Context* c, int x0, int y0, int z0, int h, std::ve
     for (int k = 0; k < 8; ++k) morton_walk(c, x0 + ((k >> 2) & 1) * m, y0 + ((k >> 1) & 1) * m, z0 + (k & 1) * m, m, out);
 }
 
-static int ensure_morton(Context* c) {
+int ensure_morton(Context* c) {
     if (c->morton) return T3D_OK;
     int h = 1;
     while (h < std::max(c->cub.nelx, std::max(c->cub.nely, c->cub.nelz))) h *= 2;
@@ -776,7 +649,7 @@ static int update_ke_pattern(Context* c) {
 
 // FP64 y = K(E) u on c->E (bit-identical in both forms); with dot.partial, u.y goes to S->denom unless
 // S->done.  Returns the number of kernels launched.
-static int matvec64(Context* c, const double* u, double* y, RedSlot dot, PcgScalars* S) {
+int matvec64(Context* c, const double* u, double* y, RedSlot dot, PcgScalars* S) {
     if (!c->mv64_stream) {
         launch_matvec64(c->g, c->Ke, c->E, c->mask0, u, y, dot, S, c->st);
         return 1;
@@ -1037,6 +910,7 @@ static int mixed_solve(Context* c, double tol, int maxit, int* iters) {
         init.stop = std::max(stop, 1e-5 * rn);
         init.tol = tol;
         init.first = 1;
+        init.maxit = budget;
         T3D_CUDA_OK(cudaMemcpyAsync(c->S32, &init, sizeof init, cudaMemcpyHostToDevice, c->st));
         vcycle32(c, c->r32, c->z32, c->S32, c->slot[2]);
         T3D_CUDA_OK(cudaMemcpyAsync(c->p32, c->z32, 3 * g.NNp * sizeof(float), cudaMemcpyDeviceToDevice, c->st));
@@ -1176,7 +1050,7 @@ static int solve_all(Context* c, double tol, int maxit, int* iters, double* C) {
     return launch_check("load cases");
 }
 
-static int design_init(Context* c, float V0, double* Csolid) {
+int design_init(Context* c, float V0, double* Csolid) {
     CHECK(ensure_morton(c));
     c->V0 = V0;
     c->loop = 0;
@@ -1201,18 +1075,28 @@ static int design_init(Context* c, float V0, double* Csolid) {
     return T3D_OK;
 }
 
-static int design_step(Context* c, t3d_iter_record* rec) {
+int design_pre(Context* c) {
     if (!c->design_ready) return set_error(T3D_ERR_INVALID, "t3d_design_init not called");
-    const Grid& g = c->g;
     const t3d_params& P = c->prm;
     ++c->loop;
-    cudaEvent_t e0 = c->ev[2], e1 = c->ev[3], e2 = c->ev[4], e3 = c->ev[5], e4 = c->ev[6];
-    T3D_CUDA_OK(cudaEventRecord(e0, c->st));
-    launch_simp(g, c->solid, c->x, P.E0, P.Emin, P.penal, c->E, c->st);
+    T3D_CUDA_OK(cudaEventRecord(c->ev[2], c->st));
+    launch_simp(c->g, c->solid, c->x, P.E0, P.Emin, P.penal, c->E, c->st);
     c->launches += 4;   // simp, objective, sensitivities, dc scale
     if (!c->mg_ready || c->loop == 1 || c->loop % c->prm.mg_rebuild_period == 0) CHECK(mg_setup(c));
+    return T3D_OK;
+}
+
+static int design_step(Context* c, t3d_iter_record* rec) {
+    CHECK(design_pre(c));
     int its = 0;
-    CHECK(solve_all(c, (double)P.cg_tol, P.cg_max_it, &its, c->scal + 0));
+    CHECK(solve_all(c, (double)c->prm.cg_tol, c->prm.cg_max_it, &its, c->scal + 0));
+    return design_post(c, its, rec);
+}
+
+int design_post(Context* c, int its, t3d_iter_record* rec) {
+    const Grid& g = c->g;
+    const t3d_params& P = c->prm;
+    cudaEvent_t e0 = c->ev[2], e1 = c->ev[3], e2 = c->ev[4], e3 = c->ev[5], e4 = c->ev[6];
     T3D_CUDA_OK(cudaEventRecord(e1, c->st));
     launch_objective(g, c->E, c->ce, c->scal + 1, c->slot[1], c->scal + 2, c->st);
     launch_sens(g, c->solid, c->x, c->ce, c->scal + 1, P.E0, P.Emin, P.penal, c->dc, c->xdc, c->st);
@@ -1251,7 +1135,6 @@ static int design_step(Context* c, t3d_iter_record* rec) {
 }  // namespace t3d
 
 // ====================================================================== C-ABI
-struct t3d_context : public t3d::Context {};
 
 #define API_GUARD(ctx)                                                                  \
     if (!(ctx)) return t3d::set_error(T3D_ERR_INVALID, "null context");                \

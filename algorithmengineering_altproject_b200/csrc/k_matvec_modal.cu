@@ -357,6 +357,14 @@ struct TmaShape {
     static constexpr int bx = BX, by = BY, stages = ST, packed = 1, tma = 1;
     static constexpr size_t smem = sizeof(SM) + 128;   // + slack for the 128-byte alignment of the ring
     static const void* fn() { return reinterpret_cast<const void*>(k_matvec32_tma<BX, BY, MINB, ST>); }
+    static const void* fn_batched() { return reinterpret_cast<const void*>(k_matvec32_tma_batched<BX, BY, MINB, ST>); }
+    static bool maps(const Grid& g, const float* u, const float* E, CUtensorMap* um, CUtensorMap* em) {
+        return modal_tensor_maps(g, u, E, SM::RW, SM::PY, BY, um, em);
+    }
+    static void batched(const BatchMatvec* a, const int* vstart, int n, const ModalKe& kh, int grid, int* err,
+                        cudaStream_t s) {
+        k_matvec32_tma_batched<BX, BY, MINB, ST><<<grid, BX * BY, smem, s>>>(a, vstart, n, kh, err);
+    }
     static bool launch(const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E, const uint8_t* mask,
                        const float* u, float* y, RedSlot dot, PcgScalars* S, int mark, int* err, cudaStream_t s) {
         CUtensorMap um, em;
@@ -393,14 +401,19 @@ struct ModalVariant {
     const void* (*fn_mode)(int);
     bool (*fused)(int, const Grid&, const ModalKe&, const ModalTiling&, const float*, const uint8_t*, const float*,
                   float*, const float*, const float*, float, RedSlot, PcgScalars*, int*, cudaStream_t);
+    // the batched PCG product over many instances (TMA shapes only)
+    const void* (*fn_batched)();
+    bool (*maps)(const Grid&, const float*, const float*, CUtensorMap*, CUtensorMap*);
+    void (*batched)(const BatchMatvec*, const int*, int, const ModalKe&, int, int*, cudaStream_t);
 };
 template <class V>
 constexpr ModalVariant variant_of() {
     if constexpr (V::tma)
         return ModalVariant{V::bx, V::by, V::stages, V::packed, V::tma, V::smem, &V::fn, &V::launch, &V::fn_mode,
-                            &V::fused};
+                            &V::fused, &V::fn_batched, &V::maps, &V::batched};
     else
-        return ModalVariant{V::bx, V::by, V::stages, V::packed, V::tma, V::smem, &V::fn, &V::launch, nullptr, nullptr};
+        return ModalVariant{V::bx, V::by, V::stages, V::packed, V::tma, V::smem, &V::fn, &V::launch, nullptr, nullptr,
+                            nullptr, nullptr, nullptr};
 }
 const ModalVariant MODAL_VARIANTS[] = {
     variant_of<ModalShape<32, 8, 2, 4, 1>>(),   // variant 0: the fallback of a TMA shape without tensor maps
@@ -550,6 +563,37 @@ bool launch_matvec32_fused(int mode, const Grid& g, const ModalKe& kh, const Mod
                            RedSlot dot, PcgScalars* S, int* err, cudaStream_t s) {
     const ModalVariant& v = MODAL_VARIANTS[t.variant];
     return v.fused != nullptr && v.fused(mode, g, kh, t, E, mask, u, y, r, rd, w, dot, S, err, s);
+}
+
+bool modal_batched_available(int variant) {
+    return variant >= 0 && variant < MODAL_NVARIANTS && MODAL_VARIANTS[variant].batched != nullptr;
+}
+
+// resident CTAs of the batched kernel on this device (its persistent grid); sets its shared-memory size
+int modal_batched_grid(int variant, int dev, int* grid) {
+    if (!modal_batched_available(variant)) return set_error(T3D_ERR_INVALID, "tile shape has no batched form");
+    const ModalVariant& v = MODAL_VARIANTS[variant];
+    int sms = 0, per_sm = 0;
+    cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return set_cuda_error(e, "cudaDeviceGetAttribute", __FILE__, __LINE__);
+    e = cudaFuncSetAttribute(v.fn_batched(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem);
+    if (e != cudaSuccess) return set_cuda_error(e, "cudaFuncSetAttribute", __FILE__, __LINE__);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn_batched(), v.bx * v.by, v.smem);
+    if (e != cudaSuccess) return set_cuda_error(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor", __FILE__, __LINE__);
+    *grid = std::max(1, sms * std::max(per_sm, 1));
+    return T3D_OK;
+}
+
+bool modal_tensor_maps_for(int variant, const Grid& g, const float* u, const float* E, CUtensorMap* umap,
+                           CUtensorMap* emap) {
+    return modal_batched_available(variant) && MODAL_VARIANTS[variant].maps(g, u, E, umap, emap);
+}
+
+bool launch_batch_matvec32(int variant, const BatchMatvec* a, const int* vstart, int n, const ModalKe& kh, int grid,
+                           int* err, cudaStream_t s) {
+    if (!modal_batched_available(variant) || n <= 0) return false;
+    MODAL_VARIANTS[variant].batched(a, vstart, n, kh, grid, err, s);
+    return true;
 }
 
 void launch_matvec32_modal(const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E,

@@ -103,35 +103,45 @@ struct TmaSmem {
 //   MODE 1  the Standard V-cycle's residual: y = r - K x (fixed DOFs 0);
 //   MODE 2  the Standard V-cycle's correction: y = x + omega (r - K x) / D (rd = 1/D; fixed DOFs 0) written to a
 //           buffer other than x, with r.y folded into S (rz, or beta and rz, as the V-cycle's r.z).
-template <int BX, int BY, int MINB, int STAGES, int MODE = 0>
-__global__ void __launch_bounds__(BX * BY, MINB)
-    k_matvec32_tma(const __grid_constant__ CUtensorMap umap, const __grid_constant__ CUtensorMap emap, Grid g,
-                   ModalKe kh, ModalTiling t, const uint8_t* __restrict__ mask, float* __restrict__ y, RedSlot dot,
-                   PcgScalars* S, int mark, int* err, const float* __restrict__ rv, const float* __restrict__ rd,
-                   float omega) {
+// The CTA's shared memory, 128-byte aligned (the launch adds 128 bytes of slack for the shift).
+template <class SM>
+__device__ __forceinline__ SM& tma_smem() {
+    extern __shared__ __align__(128) unsigned char tma_smem_raw[];
+    return *reinterpret_cast<SM*>(tma_smem_raw + ((128u - (smem_u32(tma_smem_raw) & 127u)) & 127u));
+}
+template <class SM, int STAGES>
+__device__ __forceinline__ void tma_ring_init(SM& sm) {
+    if (threadIdx.x == 0) {
+        for (int k = 0; k < STAGES; ++k) mbar_init(smem_u32(&sm.bar[k]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+}
+__device__ __forceinline__ void tma_prefetch_maps(const CUtensorMap* umap, const CUtensorMap* emap) {
+    asm volatile("prefetch.tensormap [%0];\n" ::"l"(umap) : "memory");
+    asm volatile("prefetch.tensormap [%0];\n" ::"l"(emap) : "memory");
+}
+
+// One logical block (vb) of the product: work items vb.b, vb.b + vb.n, ... of the tiling t.  gp (planes this
+// CTA has consumed: ring slot and mbarrier phase) and failed (a wait of this thread gave up) carry over from
+// one call to the next in the same CTA.
+template <int BX, int BY, int STAGES, int MODE>
+__device__ __forceinline__ void tma_matvec_body(TmaSmem<BX, BY, STAGES>& sm, const CUtensorMap* umap,
+                                                const CUtensorMap* emap, const Grid& g, const ModalKe& kh,
+                                                const ModalTiling& t, const uint8_t* __restrict__ mask,
+                                                float* __restrict__ y, RedSlot dot, PcgScalars* S, int mark, int* err,
+                                                const float* __restrict__ rv, const float* __restrict__ rd,
+                                                float omega, VB vb, unsigned& gp, bool& failed) {
     using SM = TmaSmem<BX, BY, STAGES>;
     constexpr int RW = SM::RW, PY = SM::PY;
     static_assert(STAGES >= 2, "ring needs two slots at least");
-    extern __shared__ __align__(128) unsigned char tma_smem_raw[];
-    // TMA destinations must be 128-byte aligned: the launch adds 128 bytes of slack for this shift
-    SM& sm = *reinterpret_cast<SM*>(tma_smem_raw + ((128u - (smem_u32(tma_smem_raw) & 127u)) & 127u));
     // mark: the PCG product (not an operator inside the V-cycle) records that the last alpha is in x
-    if (S != nullptr && mark && blockIdx.x == 0 && threadIdx.x == 0) S->xit = S->it;
+    if (S != nullptr && mark && vb.b == 0 && threadIdx.x == 0) S->xit = S->it;
     if (S != nullptr && S->done) return;
     const int tx = threadIdx.x % BX, ty = threadIdx.x / BX;
     const bool producer = threadIdx.x == 0;
-    if (producer) {
-        for (int k = 0; k < STAGES; ++k) mbar_init(smem_u32(&sm.bar[k]), 1);
-        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-        asm volatile("prefetch.tensormap [%0];\n" ::"l"(&umap) : "memory");
-        asm volatile("prefetch.tensormap [%0];\n" ::"l"(&emap) : "memory");
-    }
-    __syncthreads();
     const int64_t NXY = (int64_t)g.px * g.nny, MXY = (int64_t)g.nnx * g.nny;
     double part = 0.0;
-    bool failed = false;   // a wait of this thread gave up
-    unsigned gp = 0;       // planes consumed by this CTA so far (ring slot and mbarrier phase)
-    for (int w = blockIdx.x; w < t.items; w += gridDim.x) {
+    for (int w = vb.b; w < t.items; w += vb.n) {
         const int itx = w % t.tiles_x;
         const int rest = w / t.tiles_x;
         const int ity = rest % t.tiles_y;
@@ -148,8 +158,8 @@ __global__ void __launch_bounds__(BX * BY, MINB)
             const int s = (int)((gp + (unsigned)k) % STAGES);
             const unsigned bar = smem_u32(&sm.bar[s]);
             mbar_expect_tx(bar, SM::UBYTES + SM::EBYTES);
-            tma_load_4d(smem_u32(&sm.u[s][0]), &umap, xu, Y0 - 1, q, 0, bar);
-            tma_load_3d(smem_u32(&sm.e[s][0]), &emap, xe, Y0, q, bar);   // layer q-1: cells z = q
+            tma_load_4d(smem_u32(&sm.u[s][0]), umap, xu, Y0 - 1, q, 0, bar);
+            tma_load_3d(smem_u32(&sm.e[s][0]), emap, xe, Y0, q, bar);   // layer q-1: cells z = q
         };
         __syncthreads();                                          // the previous item's readers are done
         if (producer)
@@ -282,11 +292,11 @@ __global__ void __launch_bounds__(BX * BY, MINB)
     }
     if (MODE == 0 && dot.partial) {
         double tot;
-        if (grid_fold(part, dot, sm.sh, &tot) && threadIdx.x == 0) S->denom = tot;
+        if (grid_fold(part, dot, sm.sh, &tot, vb) && threadIdx.x == 0) S->denom = tot;
     }
     if (MODE == 2) {
         double tot;
-        if (grid_fold(part, dot, sm.sh, &tot) && threadIdx.x == 0) {
+        if (grid_fold(part, dot, sm.sh, &tot, vb) && threadIdx.x == 0) {
             if (S->first) {
                 S->rz = tot;
                 S->first = 0;
@@ -296,6 +306,53 @@ __global__ void __launch_bounds__(BX * BY, MINB)
                 S->rz = tot;
             }
         }
+    }
+}
+
+template <int BX, int BY, int MINB, int STAGES, int MODE = 0>
+__global__ void __launch_bounds__(BX * BY, MINB)
+    k_matvec32_tma(const __grid_constant__ CUtensorMap umap, const __grid_constant__ CUtensorMap emap, Grid g,
+                   ModalKe kh, ModalTiling t, const uint8_t* __restrict__ mask, float* __restrict__ y, RedSlot dot,
+                   PcgScalars* S, int mark, int* err, const float* __restrict__ rv, const float* __restrict__ rd,
+                   float omega) {
+    using SM = TmaSmem<BX, BY, STAGES>;
+    SM& sm = tma_smem<SM>();
+    tma_ring_init<SM, STAGES>(sm);
+    if (threadIdx.x == 0) tma_prefetch_maps(&umap, &emap);
+    __syncthreads();
+    unsigned gp = 0;
+    bool failed = false;
+    tma_matvec_body<BX, BY, STAGES, MODE>(sm, &umap, &emap, g, kh, t, mask, y, dot, S, mark, err, rv, rd, omega,
+                                          vb_real(), gp, failed);
+}
+
+// Batched PCG product (MODE 0 with the p.Ap fold): many instances' K(E)p in one persistent launch.  The work
+// list is (instance, logical block): logical block v belongs to instance batch_instance(vstart, n, v) and
+// runs that instance's own tiling, reduction slot and scalars, so each instance's result is the one its
+// own launch gives.  The tensor maps sit in global memory, one pair per instance, written by the host
+// before the launch; they cover this GPU's own buffers and no copy uses cluster multicast.  Instances whose
+// inner solve has converged (S->done) skip their blocks: the per-instance convergence mask.
+template <int BX, int BY, int MINB, int STAGES>
+__global__ void __launch_bounds__(BX * BY, MINB)
+    k_matvec32_tma_batched(const BatchMatvec* __restrict__ a, const int* __restrict__ vstart, int n, ModalKe kh,
+                           int* err) {
+    using SM = TmaSmem<BX, BY, STAGES>;
+    SM& sm = tma_smem<SM>();
+    tma_ring_init<SM, STAGES>(sm);
+    __syncthreads();
+    unsigned gp = 0;
+    bool failed = false;
+    const int total = __ldg(vstart + n);
+    for (int v = blockIdx.x; v < total; v += gridDim.x) {
+        const int i = batch_instance(vstart, n, v);
+        const BatchMatvec& A = a[i];
+        const int v0 = __ldg(vstart + i);
+        const Grid g = A.g;
+        const ModalTiling t = A.t;
+        if (threadIdx.x == 0) tma_prefetch_maps(A.umap, A.emap);
+        tma_matvec_body<BX, BY, STAGES, 0>(sm, A.umap, A.emap, g, kh, t, A.mask, A.y, A.dot, A.S, 1, err, nullptr,
+                                           nullptr, 0.f, VB{v - v0, __ldg(vstart + i + 1) - v0}, gp, failed);
+        __syncthreads();
     }
 }
 

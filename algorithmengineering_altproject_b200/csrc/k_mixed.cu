@@ -3,6 +3,8 @@
 // inner products and alpha/beta (device scalars), the true-residual recompute b - K64 u64 (the FP64
 // matvec), the coarsest-level factor and solve, and the accumulation u64 += d32.  Same algorithm as
 // the FP64 path (solver.cpp:87-217, preconditioner.cpp:88-265); only the storage precision differs.
+#include <algorithm>
+
 #include "kernels.hpp"
 #include "red.cuh"
 
@@ -157,12 +159,14 @@ __global__ void __launch_bounds__(RED_THREADS) k_matvec32(Grid g, const float* _
 }
 
 // ---------------------------------------------------------------- V-cycle in FP32
-__global__ void k_restrict_x32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ rf, float* __restrict__ a1,
-                               const PcgScalars* S) {
+// Kernel bodies take the logical block (VB) so that the batched launches below run them unchanged.
+__device__ __forceinline__ void restrict_x32(VB vb, const MgLevel32& Lc, const MgLevel32& Lf,
+                                             const float* __restrict__ rf, float* __restrict__ a1,
+                                             const PcgScalars* S) {
     if (S->done) return;
     const int cnx = Lc.nx + 1, fnx = Lf.nx + 1, fny = Lf.ny + 1, fnz = Lf.nz + 1;
     const int64_t total = (int64_t)fnz * fny * cnx;
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t t = (int64_t)vb.b * blockDim.x + threadIdx.x;
     if (t >= total) return;
     const int cx = (int)(t % cnx);
     const int64_t row = t / cnx;
@@ -182,6 +186,10 @@ __global__ void k_restrict_x32(MgLevel32 Lc, MgLevel32 Lf, const float* __restri
     a1[total + t] = v1;
     a1[2 * total + t] = v2;
 }
+__global__ void k_restrict_x32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ rf, float* __restrict__ a1,
+                               const PcgScalars* S) {
+    restrict_x32(vb_real(), Lc, Lf, rf, a1, S);
+}
 
 // Sum of the in-range hat weights of the window of coarse index c (span SP) over n fine points.
 template <int SP>
@@ -198,11 +206,12 @@ __device__ __forceinline__ float hat_sum(int c, int n) {
 // y and z window sums of the x-pass result a1[fz][fy][cx] in one pass, normalised by the summed in-range
 // weights and masked (the k_restrict_y32 + k_restrict_z32 pair fused; one thread per coarse node).
 template <int SP>
-__global__ void __launch_bounds__(256) k_restrict_yz32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ a1,
-                                                       float* __restrict__ rc, const PcgScalars* S, int normalize) {
+__device__ __forceinline__ void restrict_yz32(VB vb, const MgLevel32& Lc, const MgLevel32& Lf,
+                                              const float* __restrict__ a1, float* __restrict__ rc,
+                                              const PcgScalars* S, int normalize) {
     if (S->done) return;
     constexpr int WS = 2 * SP - 1;
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = vb.b * blockDim.x + threadIdx.x;
     if (n >= Lc.nn) return;
     const int cnx = Lc.nx + 1, cny = Lc.ny + 1;
     const int fnx = Lf.nx + 1, fny = Lf.ny + 1, fnz = Lf.nz + 1;
@@ -236,14 +245,20 @@ __global__ void __launch_bounds__(256) k_restrict_yz32(MgLevel32 Lc, MgLevel32 L
     rc[Lc.nn + n] = (m & 2) ? 0.0f : v1 * iw;
     rc[2 * Lc.nn + n] = (m & 4) ? 0.0f : v2 * iw;
 }
+template <int SP>
+__global__ void __launch_bounds__(256) k_restrict_yz32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ a1,
+                                                       float* __restrict__ rc, const PcgScalars* S, int normalize) {
+    restrict_yz32<SP>(vb_real(), Lc, Lf, a1, rc, S, normalize);
+}
 
 // The whole 3D window of the fine residual in one pass (levels small enough to sit in L2).
 template <int SP>
-__global__ void __launch_bounds__(256) k_restrict_xyz32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ rf,
-                                                        float* __restrict__ rc, const PcgScalars* S, int normalize) {
+__device__ __forceinline__ void restrict_xyz32(VB vb, const MgLevel32& Lc, const MgLevel32& Lf,
+                                               const float* __restrict__ rf, float* __restrict__ rc,
+                                               const PcgScalars* S, int normalize) {
     if (S->done) return;
     constexpr int WS = 2 * SP - 1;
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = vb.b * blockDim.x + threadIdx.x;
     if (n >= Lc.nn) return;
     const int cnx = Lc.nx + 1, cny = Lc.ny + 1;
     const int fnx = Lf.nx + 1, fny = Lf.ny + 1, fnz = Lf.nz + 1;
@@ -287,6 +302,11 @@ __global__ void __launch_bounds__(256) k_restrict_xyz32(MgLevel32 Lc, MgLevel32 
     rc[Lc.nn + n] = (m & 2) ? 0.0f : v1 * iw;
     rc[2 * Lc.nn + n] = (m & 4) ? 0.0f : v2 * iw;
 }
+template <int SP>
+__global__ void __launch_bounds__(256) k_restrict_xyz32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ rf,
+                                                        float* __restrict__ rc, const PcgScalars* S, int normalize) {
+    restrict_xyz32<SP>(vb_real(), Lc, Lf, rf, rc, S, normalize);
+}
 
 // Trilinear prolongation at fine node (fx,fy,fz) from the coarse cell fx >> sh (span 1 << sh), clamped to the
 // last coarse cell (transfers.cpp:396-408).
@@ -316,11 +336,11 @@ __device__ __forceinline__ void prolong_node32(const MgLevel32& Lc, const float*
     }
 }
 
-__global__ void k_prolong_smooth32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ xc,
-                                   const float* __restrict__ rf, float* __restrict__ xf, float w,
-                                   const PcgScalars* S) {
+__device__ __forceinline__ void prolong_smooth32(VB vb, const MgLevel32& Lc, const MgLevel32& Lf,
+                                                 const float* __restrict__ xc, const float* __restrict__ rf,
+                                                 float* __restrict__ xf, float w, const PcgScalars* S) {
     if (S->done) return;
-    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = vb.b * blockDim.x + threadIdx.x;
     if (n >= Lf.nn) return;
     const int fnx = Lf.nx + 1, fny = Lf.ny + 1;
     const int fx = n % fnx, fy = (n / fnx) % fny, fz = n / (fnx * fny);
@@ -333,18 +353,21 @@ __global__ void k_prolong_smooth32(MgLevel32 Lc, MgLevel32 Lf, const float* __re
         xf[c * Lf.cs + np] = ((m >> c) & 1) ? 0.0f : (t + P[c]) + t;
     }
 }
+__global__ void k_prolong_smooth32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ xc,
+                                   const float* __restrict__ rf, float* __restrict__ xf, float w,
+                                   const PcgScalars* S) {
+    prolong_smooth32(vb_real(), Lc, Lf, xc, rf, xf, w, S);
+}
 
 // Finest-level prolongation + smoothing + r.z.  Each lane takes a run of SP consecutive fine nodes of one
 // row that share one coarse cell in x (fine x = SP * j + k): the 8 coarse corners are gathered once and
 // interpolated in y and z once per run; each node then only interpolates in x.  The last node of a row
 // (fine x = nx, clamped to the last coarse cell with weight 1) is its own run.
 template <int SP>
-__global__ void __launch_bounds__(RED_THREADS) k_prolong_smooth0_32(MgLevel32 Lc, MgLevel32 Lf,
-                                                                    const float* __restrict__ xc,
-                                                                    const float* __restrict__ r,
-                                                                    float* __restrict__ z, float w, RedSlot dot,
-                                                                    PcgScalars* S) {
-    __shared__ double sh[32];
+__device__ __forceinline__ void prolong_smooth0_32(VB vb, const MgLevel32& Lc, const MgLevel32& Lf,
+                                                   const float* __restrict__ xc, const float* __restrict__ r,
+                                                   float* __restrict__ z, float w, RedSlot dot, PcgScalars* S,
+                                                   double* sh) {
     if (S->done) return;
     const int CS = (int)Lf.cs;
     const int fnx = Lf.nx + 1, fny = Lf.ny + 1;
@@ -353,10 +376,10 @@ __global__ void __launch_bounds__(RED_THREADS) k_prolong_smooth0_32(MgLevel32 Lc
     const int chunks = (runs + 31) >> 5;
     const int items = chunks * fny * (Lf.nz + 1);
     const int lane = threadIdx.x & 31;
-    const int nw = (gridDim.x * blockDim.x) >> 5;
+    const int nw = (vb.n * blockDim.x) >> 5;
     constexpr float inv = 1.0f / (float)SP;          // exact: SP is a power of two
     double part = 0.0;
-    for (int it = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; it < items; it += nw) {
+    for (int it = (vb.b * blockDim.x + threadIdx.x) >> 5; it < items; it += nw) {
         const int row = it / chunks;
         const int j = (it - row * chunks) * 32 + lane;
         if (j >= runs) continue;
@@ -398,7 +421,7 @@ __global__ void __launch_bounds__(RED_THREADS) k_prolong_smooth0_32(MgLevel32 Lc
         }
     }
     double tot;
-    if (grid_fold(part, dot, sh, &tot) && threadIdx.x == 0) {
+    if (grid_fold(part, dot, sh, &tot, vb) && threadIdx.x == 0) {
         if (S->first) {
             S->rz = tot;
             S->first = 0;
@@ -409,15 +432,23 @@ __global__ void __launch_bounds__(RED_THREADS) k_prolong_smooth0_32(MgLevel32 Lc
         }
     }
 }
+template <int SP>
+__global__ void __launch_bounds__(RED_THREADS) k_prolong_smooth0_32(MgLevel32 Lc, MgLevel32 Lf,
+                                                                    const float* __restrict__ xc,
+                                                                    const float* __restrict__ r,
+                                                                    float* __restrict__ z, float w, RedSlot dot,
+                                                                    PcgScalars* S) {
+    __shared__ double sh[32];
+    prolong_smooth0_32<SP>(vb_real(), Lc, Lf, xc, r, z, w, dot, S, sh);
+}
 
 // coarsest level: FP64 inverse applied to the FP32 residual in FP64, or the Jacobi fallback
-__global__ void __launch_bounds__(128) k_coarse_solve32(MgLevel32 L, const double* __restrict__ X, int N,
-                                                        const int* __restrict__ status, const PcgScalars* S) {
-    extern __shared__ double rs[];
+__device__ __forceinline__ void coarse_solve32(VB vb, const MgLevel32& L, const double* __restrict__ X, int N,
+                                               const int* __restrict__ status, const PcgScalars* S, double* rs) {
     if (S->done) return;
     const int64_t nn = L.nn;
     if (*status != 1) {
-        for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < nn; n += (int64_t)gridDim.x * blockDim.x) {
+        for (int64_t n = (int64_t)vb.b * blockDim.x + threadIdx.x; n < nn; n += (int64_t)vb.n * blockDim.x) {
             const int m = L.mask[n];
             for (int c = 0; c < 3; ++c)
                 L.x[c * nn + n] = ((m >> c) & 1) ? 0.0f : L.r[c * nn + n] * L.diag[c * nn + n];
@@ -426,28 +457,31 @@ __global__ void __launch_bounds__(128) k_coarse_solve32(MgLevel32 L, const doubl
     }
     for (int j = threadIdx.x; j < N; j += blockDim.x) rs[j] = (double)L.r[(j % 3) * nn + j / 3];
     __syncthreads();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = vb.b * blockDim.x + threadIdx.x;
     if (i >= N) return;
     double acc = 0.0;
     for (int j = 0; j < N; ++j) acc = fma(X[(int64_t)j * N + i], rs[j], acc);
     const int ni = i / 3, ci = i % 3;
     L.x[ci * nn + ni] = ((L.mask[ni] >> ci) & 1) ? 0.0f : (float)acc;
 }
+__global__ void __launch_bounds__(128) k_coarse_solve32(MgLevel32 L, const double* __restrict__ X, int N,
+                                                        const int* __restrict__ status, const PcgScalars* S) {
+    extern __shared__ double rs[];
+    coarse_solve32(vb_real(), L, X, N, status, S, rs);
+}
 
 // ---------------------------------------------------------------- PCG vector steps in FP32
 // r -= alpha Ap and |r|^2 (alpha = r.z / p.Ap of this iteration, stored for the direction kernel, which
 // applies x += alpha p while it reads p anyway)
-__global__ void __launch_bounds__(RED_THREADS) k_pcg_update32(Grid g, float* __restrict__ r,
-                                                              const float* __restrict__ Ap, RedSlot red,
-                                                              PcgScalars* S) {
-    __shared__ double sh[32];
+__device__ __forceinline__ void pcg_update32(VB vb, int64_t NNp, float* __restrict__ r, const float* __restrict__ Ap,
+                                             RedSlot red, PcgScalars* S, double* sh) {
     if (S->done) return;
     const double den = S->denom;
     // breakdown of the FP32 recurrence (p.Ap <= 0 or r.z <= 0, e.g. an indefinite preconditioner): stop this
     // inner solve before the step; the FP64 outer loop restarts from the true residual.  Every block reads the
     // same scalars, so they all take the same branch.
     if (!(den > 0.0) || !(S->rz > 0.0)) {
-        if (blockIdx.x == 0 && threadIdx.x == 0) {
+        if (vb.b == 0 && threadIdx.x == 0) {
             S->alpha = 0.0f;
             S->done = 1;
             S->result = S->it;
@@ -455,15 +489,15 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_update32(Grid g, float* __r
         return;
     }
     const float alpha = (float)(S->rz / den);
-    if (blockIdx.x == 0 && threadIdx.x == 0) S->alpha = alpha;
+    if (vb.b == 0 && threadIdx.x == 0) S->alpha = alpha;
     // the three component planes are contiguous: one flat vector of 3 NNp floats (pads stay zero), 16-byte
     // accesses (cudaMalloc bases are 256-byte aligned; NNp is a multiple of 4)
-    const int n3 = (int)(3 * g.NNp), n4 = n3 >> 2;
-    const int stride = gridDim.x * blockDim.x;
+    const int n3 = (int)(3 * NNp), n4 = n3 >> 2;
+    const int stride = vb.n * blockDim.x;
     float4* __restrict__ r4 = reinterpret_cast<float4*>(r);
     const float4* __restrict__ a4 = reinterpret_cast<const float4*>(Ap);
     double part = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
+    for (int i = vb.b * blockDim.x + threadIdx.x; i < n4; i += stride) {
         const float4 av = a4[i];
         float4 rv = r4[i];
         rv.x = fmaf(-alpha, av.x, rv.x); rv.y = fmaf(-alpha, av.y, rv.y);
@@ -471,35 +505,43 @@ __global__ void __launch_bounds__(RED_THREADS) k_pcg_update32(Grid g, float* __r
         r4[i] = rv;
         part += (double)fmaf(rv.w, rv.w, fmaf(rv.z, rv.z, fmaf(rv.y, rv.y, rv.x * rv.x)));
     }
-    for (int i = 4 * n4 + blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += stride) {
+    for (int i = 4 * n4 + vb.b * blockDim.x + threadIdx.x; i < n3; i += stride) {
         const float rv = fmaf(-alpha, Ap[i], r[i]);
         r[i] = rv;
         part = fma((double)rv, (double)rv, part);
     }
     double tot;
-    if (grid_fold(part, red, sh, &tot) && threadIdx.x == 0) {
+    if (grid_fold(part, red, sh, &tot, vb) && threadIdx.x == 0) {
         S->rnorm2 = tot;
         S->it = S->it + 1;
         if (sqrt(tot) < S->stop) {
             S->done = 1;
             S->result = S->it;
+        } else if (S->maxit > 0 && S->it >= S->maxit) {   // iteration budget of this inner solve spent
+            S->done = 1;
         }
     }
+}
+__global__ void __launch_bounds__(RED_THREADS) k_pcg_update32(Grid g, float* __restrict__ r,
+                                                              const float* __restrict__ Ap, RedSlot red,
+                                                              PcgScalars* S) {
+    __shared__ double sh[32];
+    pcg_update32(vb_real(), g.NNp, r, Ap, red, S, sh);
 }
 
 // x += alpha p_old and, unless the update just converged, p = z + beta p_old.  Once converged, the
 // step is applied by the first launch only (xit == it afterwards).
-__global__ void k_pcg_direction32(Grid g, const float* __restrict__ z, float* __restrict__ p,
-                                  float* __restrict__ x, PcgScalars* S) {
+__device__ __forceinline__ void pcg_direction32(VB vb, int64_t NNp, const float* __restrict__ z, float* __restrict__ p,
+                                                float* __restrict__ x, const PcgScalars* S) {
     if (S->xit == S->it) return;
     const bool move = !S->done;
     const float beta = (float)S->beta, alpha = S->alpha;
-    const int n3 = (int)(3 * g.NNp), n4 = n3 >> 2;
-    const int stride = gridDim.x * blockDim.x;
+    const int n3 = (int)(3 * NNp), n4 = n3 >> 2;
+    const int stride = vb.n * blockDim.x;
     float4* __restrict__ p4 = reinterpret_cast<float4*>(p);
     float4* __restrict__ x4 = reinterpret_cast<float4*>(x);
     const float4* __restrict__ z4 = reinterpret_cast<const float4*>(z);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
+    for (int i = vb.b * blockDim.x + threadIdx.x; i < n4; i += stride) {
         float4 pv = p4[i], xv = x4[i];
         xv.x = fmaf(alpha, pv.x, xv.x); xv.y = fmaf(alpha, pv.y, xv.y);
         xv.z = fmaf(alpha, pv.z, xv.z); xv.w = fmaf(alpha, pv.w, xv.w);
@@ -511,16 +553,133 @@ __global__ void k_pcg_direction32(Grid g, const float* __restrict__ z, float* __
             p4[i] = pv;
         }
     }
-    for (int i = 4 * n4 + blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += stride) {
+    for (int i = 4 * n4 + vb.b * blockDim.x + threadIdx.x; i < n3; i += stride) {
         const float pv = p[i];
         x[i] = fmaf(alpha, pv, x[i]);
         if (move) p[i] = fmaf(beta, pv, z[i]);
     }
 }
+__global__ void k_pcg_direction32(Grid g, const float* __restrict__ z, float* __restrict__ p,
+                                  float* __restrict__ x, PcgScalars* S) {
+    pcg_direction32(vb_real(), g.NNp, z, p, x, S);
+}
 
 inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
+// ---------------------------------------------------------------- batched launches
+// A persistent grid walks the (instance, logical block) list: logical block v is block v - vstart[i] of
+// instance i = batch_instance(vstart, n, v) in a launch of vstart[i+1] - vstart[i] blocks.  The body runs as
+// in that instance's own launch; the barrier between items keeps shared scratch from being overwritten early.
+template <class A, class F>
+__device__ __forceinline__ void batch_walk(const A* __restrict__ a, const int* __restrict__ vstart, int n, F&& f) {
+    const int total = __ldg(vstart + n);
+    for (int v = blockIdx.x; v < total; v += gridDim.x) {
+        const int i = batch_instance(vstart, n, v);
+        const int v0 = __ldg(vstart + i);
+        f(a[i], VB{v - v0, __ldg(vstart + i + 1) - v0});
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(RED_THREADS) k_batch_update32(const BatchUpdate* __restrict__ a,
+                                                                const int* __restrict__ vstart, int n) {
+    __shared__ double sh[32];
+    batch_walk(a, vstart, n, [&](const BatchUpdate& A, VB vb) { pcg_update32(vb, A.NNp, A.r, A.Ap, A.red, A.S, sh); });
+}
+
+__global__ void __launch_bounds__(RED_THREADS) k_batch_direction32(const BatchDirection* __restrict__ a,
+                                                                   const int* __restrict__ vstart, int n) {
+    batch_walk(a, vstart, n, [&](const BatchDirection& A, VB vb) { pcg_direction32(vb, A.NNp, A.z, A.p, A.x, A.S); });
+}
+
+// stage 0: span-4 transitions run their x pass, span-2 ones their whole window; stage 1: the span-4 y-z pass
+__global__ void __launch_bounds__(256) k_batch_restrict32(const BatchRestrict* __restrict__ a,
+                                                          const int* __restrict__ vstart, int n, int stage) {
+    batch_walk(a, vstart, n, [&](const BatchRestrict& A, VB vb) {
+        const MgLevel32 Lc = A.Lc, Lf = A.Lf;
+        if (Lc.span == 4) {
+            if (stage == 0) restrict_x32(vb, Lc, Lf, A.rf, A.a1, A.S);
+            else restrict_yz32<4>(vb, Lc, Lf, A.a1, A.rc, A.S, 1);
+        } else {
+            restrict_xyz32<2>(vb, Lc, Lf, A.rf, A.rc, A.S, 1);
+        }
+    });
+}
+
+__global__ void __launch_bounds__(256) k_batch_prolong32(const BatchProlong* __restrict__ a,
+                                                         const int* __restrict__ vstart, int n) {
+    batch_walk(a, vstart, n, [&](const BatchProlong& A, VB vb) {
+        const MgLevel32 Lc = A.Lc, Lf = A.Lf;
+        prolong_smooth32(vb, Lc, Lf, Lc.x, Lf.r, Lf.x, A.w, A.S);
+    });
+}
+
+__global__ void __launch_bounds__(RED_THREADS) k_batch_prolong0_32(const BatchProlong0* __restrict__ a,
+                                                                   const int* __restrict__ vstart, int n) {
+    __shared__ double sh[32];
+    batch_walk(a, vstart, n, [&](const BatchProlong0& A, VB vb) {
+        const MgLevel32 Lc = A.Lc, Lf = A.Lf;
+        if (Lc.span == 4) prolong_smooth0_32<4>(vb, Lc, Lf, Lc.x, A.r, A.z, A.w, A.dot, A.S, sh);
+        else prolong_smooth0_32<2>(vb, Lc, Lf, Lc.x, A.r, A.z, A.w, A.dot, A.S, sh);
+    });
+}
+
+__global__ void __launch_bounds__(128) k_batch_coarse32(const BatchCoarse* __restrict__ a,
+                                                        const int* __restrict__ vstart, int n) {
+    extern __shared__ double rs[];
+    batch_walk(a, vstart, n, [&](const BatchCoarse& A, VB vb) {
+        const MgLevel32 L = A.L;
+        coarse_solve32(vb, L, A.X, A.N, A.status, A.S, rs);
+    });
+}
+
+// the instances' done flags gathered into one array (one copy to the host per poll)
+__global__ void k_batch_flags(PcgScalars* const* __restrict__ S, int n, int* __restrict__ out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) out[i] = S[i]->done;
+}
+
+// persistent grid of the batched launches: 8 resident blocks per SM of B200 (148 SMs), fewer for short lists
+constexpr int BATCH_GRID = 8 * 148;
+
 }  // namespace
+
+int batch_blocks_update() { return RED_BLOCKS; }
+int batch_blocks_prolong0() { return RED_BLOCKS; }
+int batch_blocks_restrict(const BatchRestrict& a, int stage) {
+    const MgLevel32& Lc = a.Lc;
+    const MgLevel32& Lf = a.Lf;
+    if (Lc.span == 4) {
+        if (stage == 0) return (int)blocks_for((int64_t)(Lf.nz + 1) * (Lf.ny + 1) * (Lc.nx + 1), 256);
+        return (int)blocks_for(Lc.nn, 256);
+    }
+    return stage == 0 ? (int)blocks_for(Lc.nn, 256) : 0;
+}
+int batch_blocks_prolong(const BatchProlong& a) { return (int)blocks_for(a.Lf.nn, 256); }
+int batch_blocks_coarse(const BatchCoarse& a) {
+    const int64_t work = a.N > 0 ? a.N : a.L.nn;
+    return (int)std::max<int64_t>(1, (work + 127) / 128);
+}
+void launch_batch_flags(PcgScalars* const* S, int n, int* out, cudaStream_t s) {
+    k_batch_flags<<<1, 256, 0, s>>>(S, n, out);
+}
+void launch_batch_update32(const BatchUpdate* a, const int* vstart, int n, cudaStream_t s) {
+    k_batch_update32<<<BATCH_GRID, RED_THREADS, 0, s>>>(a, vstart, n);
+}
+void launch_batch_direction32(const BatchDirection* a, const int* vstart, int n, cudaStream_t s) {
+    k_batch_direction32<<<BATCH_GRID, RED_THREADS, 0, s>>>(a, vstart, n);
+}
+void launch_batch_restrict32(const BatchRestrict* a, const int* vstart, int n, int stage, cudaStream_t s) {
+    k_batch_restrict32<<<BATCH_GRID, 256, 0, s>>>(a, vstart, n, stage);
+}
+void launch_batch_prolong32(const BatchProlong* a, const int* vstart, int n, cudaStream_t s) {
+    k_batch_prolong32<<<BATCH_GRID, 256, 0, s>>>(a, vstart, n);
+}
+void launch_batch_prolong0_32(const BatchProlong0* a, const int* vstart, int n, cudaStream_t s) {
+    k_batch_prolong0_32<<<BATCH_GRID, RED_THREADS, 0, s>>>(a, vstart, n);
+}
+void launch_batch_coarse32(const BatchCoarse* a, const int* vstart, int n, int max_n, cudaStream_t s) {
+    k_batch_coarse32<<<2 * BATCH_GRID, 128, (size_t)(max_n > 0 ? max_n : 1) * sizeof(double), s>>>(a, vstart, n);
+}
 
 void launch_nodes_to32(const Grid& g, const double* a, float* b, cudaStream_t s) {
     k_rows_convert<double, float><<<RED_BLOCKS, 256, 0, s>>>(3 * (int64_t)g.nny * g.nnz, g.nnx, g.nnx, g.px, a, b);

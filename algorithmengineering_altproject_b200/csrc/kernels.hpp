@@ -1,5 +1,7 @@
 // Host-side launchers of the B200 kernels.  All launches go to the given stream; none allocates.
 #pragma once
+#include <cuda.h>
+
 #include <string>
 
 #include "t3d_common.cuh"
@@ -294,6 +296,84 @@ bool modal_fused_available(const ModalTiling& t);
 bool launch_matvec32_fused(int mode, const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E,
                            const uint8_t* mask, const float* u, float* y, const float* r, const float* rd, float w,
                            RedSlot dot, PcgScalars* S, int* err, cudaStream_t s);
+
+// ---- batched launches (batch.cu): one persistent launch runs the logical launches of many instances of
+// uneven size.  Each takes a device array of per-instance arguments and vstart[0..n], the prefix sum of the
+// instances' logical block counts (each instance's count is the grid of its own launch, so its arithmetic and
+// reduction order are those of that launch); instances whose inner solve is done (S->done) skip their blocks.
+struct BatchMatvec {      // the PCG product K(E)p with p.Ap (TMA tile shapes; maps in global memory)
+    Grid g;
+    ModalTiling t;
+    const uint8_t* mask;
+    float* y;
+    RedSlot dot;
+    PcgScalars* S;
+    const CUtensorMap* umap;
+    const CUtensorMap* emap;
+};
+struct BatchUpdate {      // r -= alpha Ap with |r|^2
+    int64_t NNp;
+    float* r;
+    const float* Ap;
+    RedSlot red;
+    PcgScalars* S;
+};
+struct BatchDirection {   // x += alpha p, p = z + beta p
+    int64_t NNp;
+    const float* z;
+    float* p;
+    float* x;
+    PcgScalars* S;
+};
+struct BatchRestrict {    // restriction Lf -> Lc: span 4 x pass rf -> a1 then y-z pass a1 -> rc; span 2 rf -> rc
+    MgLevel32 Lc, Lf;
+    const float* rf;
+    float* a1;
+    float* rc;
+    PcgScalars* S;
+};
+struct BatchProlong {     // prolongation + smoothing on a level above the finest
+    MgLevel32 Lc, Lf;
+    float w;
+    PcgScalars* S;
+};
+struct BatchProlong0 {    // finest-level prolongation + smoothing with r.z
+    MgLevel32 Lc, Lf;
+    const float* r;
+    float* z;
+    float w;
+    RedSlot dot;
+    PcgScalars* S;
+};
+struct BatchCoarse {      // coarsest-level solve
+    MgLevel32 L;
+    const double* X;
+    int N;
+    const int* status;
+    PcgScalars* S;
+};
+// logical block counts of one instance's own launches
+int batch_blocks_update();
+int batch_blocks_restrict(const BatchRestrict& a, int stage);   // stage 0: x or x-y-z pass, 1: y-z pass (0 if none)
+int batch_blocks_prolong(const BatchProlong& a);
+int batch_blocks_prolong0();
+int batch_blocks_coarse(const BatchCoarse& a);
+// the launches (a, vstart on the device; n instances; total = vstart[n] logical blocks)
+void launch_batch_flags(PcgScalars* const* S, int n, int* out, cudaStream_t s);   // out[i] = S[i]->done
+void launch_batch_update32(const BatchUpdate* a, const int* vstart, int n, cudaStream_t s);
+void launch_batch_direction32(const BatchDirection* a, const int* vstart, int n, cudaStream_t s);
+void launch_batch_restrict32(const BatchRestrict* a, const int* vstart, int n, int stage, cudaStream_t s);
+void launch_batch_prolong32(const BatchProlong* a, const int* vstart, int n, cudaStream_t s);
+void launch_batch_prolong0_32(const BatchProlong0* a, const int* vstart, int n, cudaStream_t s);
+void launch_batch_coarse32(const BatchCoarse* a, const int* vstart, int n, int max_n, cudaStream_t s);
+// the batched PCG product: variant = the members' common TMA tile shape; false when it has no batched form
+bool modal_batched_available(int variant);
+int modal_batched_grid(int variant, int dev, int* grid);
+bool launch_batch_matvec32(int variant, const BatchMatvec* a, const int* vstart, int n, const ModalKe& kh, int grid,
+                           int* err, cudaStream_t s);
+// the tensor maps of one instance's PCG product (p and E images); false when they cannot be encoded
+bool modal_tensor_maps_for(int variant, const Grid& g, const float* u, const float* E, CUtensorMap* umap,
+                           CUtensorMap* emap);
 
 // ---- surface export (k_stl.cu, io.cpp:80-87)
 int stl_chunks(const Grid& g);

@@ -32,26 +32,50 @@ __device__ __forceinline__ double block_fold(double v, double* sh) {
     return t;
 }
 
+// A block of one logical launch: its index and the launch's block count.  A plain launch passes
+// (blockIdx.x, gridDim.x); a batched launch runs the logical launches of many instances as one persistent
+// grid, each real block taking (instance, virtual block) items, and passes the item's index and its
+// instance's block count, so every instance computes exactly what its own launch would.
+struct VB {
+    int b, n;
+};
+__device__ __forceinline__ VB vb_real() { return VB{(int)blockIdx.x, (int)gridDim.x}; }
+
 // Publishes the block's partial; the last block to arrive folds all partials (threads stride over
 // them in index order, then block_fold) and returns true with *total valid in warp 0.
 // Resets the arrival counter for the next use of the slot.
-__device__ __forceinline__ bool grid_fold(double v, RedSlot slot, double* sh, double* total) {
+__device__ __forceinline__ bool grid_fold(double v, RedSlot slot, double* sh, double* total, VB vb) {
     __shared__ int am_last;
     const double b = block_fold(v, sh);
     if (threadIdx.x == 0) {
-        slot.partial[blockIdx.x] = b;
+        slot.partial[vb.b] = b;
         __threadfence();
         const unsigned int t = atomicAdd(slot.counter, 1u);
-        am_last = (t == gridDim.x - 1) ? 1 : 0;
+        am_last = (t == (unsigned)vb.n - 1u) ? 1 : 0;
     }
     __syncthreads();
     if (!am_last) return false;
     __threadfence();
     double s = 0.0;
-    for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) s = s + __ldcg(slot.partial + i);
+    for (int i = threadIdx.x; i < vb.n; i += blockDim.x) s = s + __ldcg(slot.partial + i);
     *total = block_fold(s, sh);
     if (threadIdx.x == 0) *slot.counter = 0u;
     return true;
+}
+__device__ __forceinline__ bool grid_fold(double v, RedSlot slot, double* sh, double* total) {
+    return grid_fold(v, slot, sh, total, vb_real());
+}
+
+// Instance of virtual block v in a batched launch: vstart[0..n] is the prefix sum of the instances' block
+// counts (vstart[0] = 0).  Binary search; every thread of the block computes the same result.
+__device__ __forceinline__ int batch_instance(const int* __restrict__ vstart, int n, int v) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(vstart + mid) <= v) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
 }
 
 }  // namespace t3d

@@ -95,6 +95,7 @@ struct PcgScalars {
     // alpha is already in x (set by the next K(E)p launch), so a converged step is applied exactly once
     int xit;
     float alpha;      // alpha of iteration `it`, stored by the update kernel
+    int maxit;        // FP32 inner solve: done once `it` reaches it (0: no cap); the FP64 path ignores it
 };
 
 // Reduction scratch: RED_BLOCKS partials + arrival counter per reduction slot.

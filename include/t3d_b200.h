@@ -218,6 +218,32 @@ int  t3d_run_global(struct t3d_context* ctx, float V0, int n_loop, double* c_sol
                     int* n_records, float* x_final);
 int  t3d_synchronize(struct t3d_context* ctx);
 
+/* --------------------------------------------------------------- batched designs (no reference counterpart;
+ * the reference runs one design per process, driver.cpp:23).  n designs of uneven grid size share one device
+ * arena and step together: each design iteration runs the members' SIMP / MG rebuild, then ONE inner FP32
+ * MG-PCG for all members in which every kernel of the PCG iteration (K(E)p with p.Ap, update, restrictions,
+ * coarsest solve, prolongations, direction) is a single persistent launch walking an (instance, block) work
+ * list, with per-instance convergence masks and the steady iterations captured in a CUDA graph, inside the
+ * members' FP64 defect-correction loops; then the members' compliance, sensitivities, filter and OC.  Every
+ * member's results equal the ones its own context gives with the same parameters.
+ * Members: precision T3D_MIXED, the Adapted V-cycle, one load case (built-in cuboid problems); the FP32
+ * K(E)p tile shape is set to the batched one (params.matvec32_tile is overridden to T3D_BATCH_TILE).
+ *   dims: n x {nely, nelx, nelz};  params, problems: n each (problems may be NULL: the tip-line cantilever). */
+enum { T3D_BATCH_TILE = 7 };
+struct t3d_batch;
+int  t3d_batch_create(int n, const int* dims, const t3d_params* params, const t3d_problem* problems,
+                      struct t3d_batch** out);
+/* member i's context (owned by the batch; use it for queries such as t3d_get_density, not t3d_destroy) */
+int  t3d_batch_member(struct t3d_batch* b, int i, struct t3d_context** out);
+/* t3d_design_init of every member: V0[n] in, c_solid[n] out (may be NULL) */
+int  t3d_batch_design_init(struct t3d_batch* b, const float* V0, double* c_solid);
+/* one design iteration of every member: recs[n] */
+int  t3d_batch_design_step(struct t3d_batch* b, t3d_iter_record* recs);
+/* info[0] arena bytes, [1] members, [2] batched kernel launches so far, [3] kernels of one batched PCG
+ * iteration, [4] logical blocks of one batched PCG iteration, [5] member kernels launched so far */
+int  t3d_batch_info(struct t3d_batch* b, int64_t* info);
+int  t3d_batch_destroy(struct t3d_batch* b);
+
 /* --------------------------------------------------------------- profiling (no reference counterpart)
  * Times `reps` back-to-back launches of one device-resident kernel sequence with CUDA events on the
  * context's stream, after one untimed launch: T3D_PROFILE_MATVEC = K(E)p with the fused p.Ap,

@@ -85,3 +85,16 @@ def test_null_arguments_are_errors():
     assert lib.t3d_create(6, 12, 6, None, None) == t3d.T3D_ERR_INVALID
     assert lib.t3d_get_info(None, None) == t3d.T3D_ERR_INVALID
     assert lib.t3d_destroy(None) == t3d.T3D_OK
+
+
+def test_batch_arguments_are_checked_before_any_device_work():
+    import ctypes as C
+    lib = t3d.library()
+    h = C.c_void_p()
+    dims = (C.c_int * 3)(8, 16, 8)
+    assert lib.t3d_batch_create(0, dims, None, None, C.byref(h)) == t3d.T3D_ERR_INVALID
+    assert lib.t3d_batch_create(1, None, None, None, C.byref(h)) == t3d.T3D_ERR_INVALID
+    assert lib.t3d_batch_create(1, dims, None, None, None) == t3d.T3D_ERR_INVALID
+    assert lib.t3d_batch_design_step(None, None) == t3d.T3D_ERR_INVALID
+    assert lib.t3d_batch_info(None, None) == t3d.T3D_ERR_INVALID
+    assert lib.t3d_batch_destroy(None) == t3d.T3D_OK

@@ -1,0 +1,89 @@
+"""Batched designs (t3d_batch_*): designs of uneven grid size stepping together, every kernel of the inner FP32
+MG-PCG iteration one persistent launch over an (instance, block) work list with per-instance convergence
+masks.  Each member's design iterations must equal, bit for bit, those of the same design run alone with the
+same parameters (the batched launches give every instance the blocks, arithmetic and reduction order of its
+own launches); the solo path itself is pinned to the oracle by the parity tests.
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+# uneven grids, all three load cases, voids (centre ex, ey, ez, radii rx, ry, rz in element units)
+CASES = [
+    dict(dims=(16, 48, 24), load_case=0, voids=(), V0=0.12),
+    dict(dims=(24, 40, 16), load_case=1, voids=((20.0, 12.0, 8.0, 6.0, 5.0, 4.0),), V0=0.2),
+    dict(dims=(32, 64, 32), load_case=2, voids=((40.0, 10.0, 16.0, 8.0, 6.0, 6.0), (12.0, 20.0, 10.0, 5.0, 5.0, 5.0)),
+         V0=0.08),
+    dict(dims=(8, 32, 16), load_case=0, voids=(), V0=0.3),
+]
+COMMON = dict(oc_sum_order=1, mg_coarse_assembly=1)
+
+
+def spec(t3d, c):
+    return t3d.ProblemSpec.make(c["load_case"], c["voids"])
+
+
+def run_alone(t3d, c, steps, **extra):
+    P = t3d.Problem(*c["dims"], problem=spec(t3d, c), precision=t3d.T3D_MIXED, matvec32_tile=t3d.T3D_BATCH_TILE,
+                    **COMMON, **extra)
+    cs = P.design_init(c["V0"])
+    recs = [P.design_step() for _ in range(steps)]
+    x, u = P.density(), P.displacement()
+    P.close()
+    return cs, recs, x, u
+
+
+def same_records(a, b):
+    for key in ("loop", "pcg_iters", "obj", "vol", "sharp", "change", "lmid", "bisections"):
+        assert a[key] == b[key], (key, a[key], b[key])
+
+
+def test_batch_members_equal_their_solo_runs():
+    import algorithmengineering_altproject_b200 as t3d
+    steps = 3
+    B = t3d.Batch([c["dims"] for c in CASES], problems=[spec(t3d, c) for c in CASES], **COMMON)
+    info = B.info()
+    assert info["members"] == len(CASES) and info["arena_bytes"] > 0
+    assert all(m.device_bytes > 0 for m in B.members)
+    cs = B.design_init([c["V0"] for c in CASES])
+    brecs = [B.design_step() for _ in range(steps)]
+    bx = [m.density() for m in B.members]
+    bu = [m.displacement() for m in B.members]
+    info = B.info()
+    B.close()
+    # one launch per kernel of the PCG iteration for all members: far fewer than the members' own launches
+    assert 5 <= info["kernels_per_iteration"] <= 20
+    assert info["batched_launches"] > 0
+    for i, c in enumerate(CASES):
+        cs1, recs1, x1, u1 = run_alone(t3d, c, steps)
+        assert cs[i] == cs1
+        for k in range(steps):
+            same_records(brecs[k][i], recs1[k])
+        np.testing.assert_array_equal(bx[i], x1)
+        np.testing.assert_array_equal(bu[i], u1)
+
+
+def test_batch_member_budgets_and_masks():
+    """Members with their own iteration budgets (one far below its need, not a multiple of the graph chunk)
+    stop on the device at their budget while the others go on; each still equals its solo run."""
+    import algorithmengineering_altproject_b200 as t3d
+    cases = CASES[:3]
+    extra = [dict(cg_max_it=11), dict(), dict(cg_tol=1e-5)]
+    B = t3d.Batch([c["dims"] for c in cases], problems=[spec(t3d, c) for c in cases], member_params=extra, **COMMON)
+    B.design_init([c["V0"] for c in cases])
+    brecs = [B.design_step() for _ in range(2)]
+    bx = [m.density() for m in B.members]
+    B.close()
+    assert brecs[0][0]["pcg_iters"] <= 11   # its budget
+    for i, c in enumerate(cases):
+        _, recs1, x1, _ = run_alone(t3d, c, 2, **extra[i])
+        for k in range(2):
+            same_records(brecs[k][i], recs1[k])
+        np.testing.assert_array_equal(bx[i], x1)
+
+
+def test_batch_rejects_members_it_cannot_batch():
+    import algorithmengineering_altproject_b200 as t3d
+    with pytest.raises(t3d.T3DError, match="Adapted"):
+        t3d.Batch([(16, 32, 16)], mg_vcycle=t3d.T3D_VCYCLE_STANDARD)
