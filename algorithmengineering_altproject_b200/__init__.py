@@ -143,6 +143,9 @@ _SIGS = {
     "t3d_batch_create": (C.c_int, [C.c_int, C.POINTER(C.c_int), C.POINTER(Params), C.POINTER(ProblemSpec),
                                    C.POINTER(_BATCH)]),
     "t3d_batch_member": (C.c_int, [_BATCH, C.c_int, C.POINTER(_CTX)]),
+    "t3d_batch_open": (C.c_int, [C.c_int, C.POINTER(_BATCH)]),
+    "t3d_batch_adopt": (C.c_int, [_BATCH, _CTX]),
+    "t3d_batch_release": (C.c_int, [_BATCH, C.c_int, C.POINTER(_CTX)]),
     "t3d_batch_design_init": (C.c_int, [_BATCH, _f32p, _f64p]),
     "t3d_batch_design_step": (C.c_int, [_BATCH, C.POINTER(IterRecord)]),
     "t3d_batch_info": (C.c_int, [_BATCH, C.POINTER(C.c_int64)]),
@@ -507,6 +510,35 @@ class Batch:
             m._owned = False
             m._attach(c)
             self.members.append(m)
+
+    @classmethod
+    def open(cls, device=0):
+        """An empty batch for continuous batching: members join with adopt() and leave with release()."""
+        self = cls.__new__(cls)
+        self._lib = library()
+        h = _BATCH()
+        _check(self._lib.t3d_batch_open(int(device), C.byref(h)))
+        self._h = h
+        self.n = 0
+        self.members = []
+        return self
+
+    def adopt(self, problem):
+        """Moves a Problem created alone (precision T3D_MIXED, matvec32_tile=T3D_BATCH_TILE, one load case,
+        design_init done) into the batch as its last member; the batch owns it until release()."""
+        _check(self._lib.t3d_batch_adopt(self._h, problem._h))
+        problem._owned = False
+        self.members.append(problem)
+        self.n += 1
+
+    def release(self, i):
+        """Takes member i out of the batch (later members move down) and returns it; the caller closes it."""
+        c = _CTX()
+        _check(self._lib.t3d_batch_release(self._h, int(i), C.byref(c)))
+        p = self.members.pop(i)
+        p._owned = True
+        self.n -= 1
+        return p
 
     def design_init(self, V0):
         """t3d_design_init of every member; V0: one value per member; returns the solid compliances"""

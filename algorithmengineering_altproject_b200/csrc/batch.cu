@@ -7,12 +7,14 @@
 // threads (SIMP, MG rebuild, compliance, sensitivities, filter, OC).
 //
 // Work list.  Every kernel of the FP32 MG-PCG iteration is one persistent launch over (instance, logical
-// block) items (kernels.hpp, "batched launches"): logical block v of instance i is block v - vstart[i] of
-// the launch the member would make alone, so each member's arithmetic and reduction order are those of its
-// own launch and its results are identical to a solo run with the same parameters.  Members whose inner
-// solve has converged or spent its budget (S->done, set on the device) skip their items: the per-instance
-// convergence mask.  BATCH_CHUNK iterations are captured once in a CUDA graph and replayed; the host polls
-// the members' done flags (gathered into one array) after each replay.
+// block) items (kernels.hpp, "batched launches"): the logical blocks of an instance are the blocks of the
+// launch the member would make alone, so each member's arithmetic and reduction order are those of its own
+// launch and its results are identical to a solo run with the same parameters.  Per-instance convergence
+// masks: a member whose inner solve has converged or spent its budget (S->done, set on the device) skips its
+// items for the rest of that iteration, and a compaction kernel at the end of every iteration drops it from
+// the work lists, so finished members cost nothing while the others go on.  BATCH_CHUNK iterations are
+// captured once in a CUDA graph and replayed; the host polls the members' done flags (gathered into one
+// array) after each replay.
 //
 // The FP64 defect-correction loop around the inner solve (mixed_solve in context.cu) is run for all members
 // in lock step: one true-residual pass for the members still iterating, one batched inner solve, one
@@ -32,11 +34,11 @@ constexpr int BATCH_CHUNK = 16;      // inner PCG iterations per graph replay
 constexpr int BATCH_THREADS = 16;    // host threads of the per-member phases
 constexpr int BATCH_MAX_OUTER = 64;  // defect-correction passes (as the single-design solve)
 
-struct LaunchList {      // one batched launch: per-instance arguments and block prefix sums on the device
+struct LaunchList {      // one batched launch: per-instance arguments and the active-instance list on the device
     void* args = nullptr;
-    int* vstart = nullptr;
-    int n = 0;
-    int64_t blocks = 0;
+    int* act = nullptr;   // n, positions, block prefix sums (kernels.hpp)
+    int n = 0;            // instances in the list
+    int64_t blocks = 0;   // logical blocks with every instance active
 };
 
 }  // namespace
@@ -50,10 +52,13 @@ struct Batch {
     int mv_grid = 0;
     ModalKe kh{};
     std::vector<void*> dallocs;
-    LaunchList mv, up, dir, p0, co;
-    LaunchList rs0[8], rs1[8], pr[8];
+    bool standard = false;       // the members' V-cycle (all the same): Standard, else Adapted
+    LaunchList mv, up, dir, p0, co, mv1, mv2;
+    LaunchList rs0[8], rs1[8], pr[8], lop[8], lmv[8], pa[8];
     int maxL = 0, coarse_max = 0;
     CUtensorMap* maps = nullptr;
+    std::vector<BatchCompact> jobs;   // one per launch list
+    BatchCompact* djobs = nullptr;
     PcgScalars** dS = nullptr;
     int* dflags = nullptr;
     int* err = nullptr;
@@ -64,6 +69,8 @@ struct Batch {
     int64_t launches = 0;
     int iter_kernels = 0;
     int64_t iter_blocks = 0;
+    int n_arena = 0;             // members 0 .. n_arena-1 live in the arena (created with the batch)
+    bool dirty = true;           // membership changed: the launch lists and the graph are rebuilt before use
 
     template <class T>
     int dalloc(T** p, size_t n) {
@@ -75,44 +82,74 @@ struct Batch {
         return T3D_OK;
     }
 
+    // the launch lists, the graph and the polling buffers (rebuilt when membership changes)
+    void free_lists() {
+        if (graph) cudaGraphExecDestroy(graph);
+        graph = nullptr;
+        for (void* q : dallocs) cudaFree(q);
+        dallocs.clear();
+        if (hflags) cudaFreeHost(hflags);
+        if (hS) cudaFreeHost(hS);
+        if (hscal) cudaFreeHost(hscal);
+        hflags = nullptr;
+        hS = nullptr;
+        hscal = nullptr;
+        maps = nullptr;
+        jobs.clear();
+        djobs = nullptr;
+        dS = nullptr;
+        dflags = nullptr;
+        err = nullptr;
+        mv = up = dir = p0 = co = mv1 = mv2 = LaunchList{};
+        for (int l = 0; l < 8; ++l) rs0[l] = rs1[l] = pr[l] = lop[l] = lmv[l] = pa[l] = LaunchList{};
+    }
+
     ~Batch() {
         cudaSetDevice(dev);
         if (st) cudaStreamSynchronize(st);
-        if (graph) cudaGraphExecDestroy(graph);
         for (t3d_context* c : m) {
             if (!c) continue;
             cudaStreamSynchronize(c->st);
             delete c;
         }
-        for (void* q : dallocs) cudaFree(q);
+        free_lists();
         if (arena.base) cudaFree(arena.base);
-        if (hflags) cudaFreeHost(hflags);
-        if (hS) cudaFreeHost(hS);
-        if (hscal) cudaFreeHost(hscal);
         if (st) cudaStreamDestroy(st);
     }
 };
 
 namespace {
 
-// uploads one launch list: args[k] with blocks[k] logical blocks each
+// uploads one launch list: args[k] with blocks[k] logical blocks each and scalars S[k]; the active list starts
+// with every instance and its compaction job is queued
 template <class T>
-int make_list(Batch* B, const std::vector<T>& a, const std::vector<int>& blocks, LaunchList* L) {
-    L->n = (int)a.size();
+int make_list(Batch* B, const std::vector<T>& a, const std::vector<int>& blocks, const std::vector<PcgScalars*>& S,
+              LaunchList* L) {
+    const int N = (int)a.size();
+    L->n = N;
     L->blocks = 0;
-    if (L->n == 0) return T3D_OK;
-    std::vector<int> vs((size_t)L->n + 1, 0);
-    for (int k = 0; k < L->n; ++k) {
+    if (N == 0) return T3D_OK;
+    std::vector<int> act(2 * (size_t)N + 2, 0);
+    act[0] = N;
+    for (int k = 0; k < N; ++k) {
         if (blocks[k] <= 0) return set_error(T3D_ERR_INVALID, "batched launch with an empty instance");
-        vs[k + 1] = vs[k] + blocks[k];
+        act[1 + k] = k;
+        act[2 + N + k] = act[1 + N + k] + blocks[k];
     }
-    L->blocks = vs[L->n];
+    L->blocks = act[1 + 2 * N];
     T* da = nullptr;
+    int* db = nullptr;
+    PcgScalars** dS = nullptr;
     CHECK(B->dalloc(&da, a.size()));
-    CHECK(B->dalloc(&L->vstart, vs.size()));
+    CHECK(B->dalloc(&L->act, act.size()));
+    CHECK(B->dalloc(&db, blocks.size()));
+    CHECK(B->dalloc(&dS, S.size()));
     T3D_CUDA_OK(cudaMemcpy(da, a.data(), a.size() * sizeof(T), cudaMemcpyHostToDevice));
-    T3D_CUDA_OK(cudaMemcpy(L->vstart, vs.data(), vs.size() * sizeof(int), cudaMemcpyHostToDevice));
+    T3D_CUDA_OK(cudaMemcpy(L->act, act.data(), act.size() * sizeof(int), cudaMemcpyHostToDevice));
+    T3D_CUDA_OK(cudaMemcpy(db, blocks.data(), blocks.size() * sizeof(int), cudaMemcpyHostToDevice));
+    T3D_CUDA_OK(cudaMemcpy(dS, S.data(), S.size() * sizeof(PcgScalars*), cudaMemcpyHostToDevice));
     L->args = da;
+    B->jobs.push_back(BatchCompact{dS, db, N, L->act});
     return T3D_OK;
 }
 
@@ -149,10 +186,10 @@ static int batch_members_check(Batch* B) {
         const t3d_context* c = B->m[i];
         const std::string who = "batch member " + std::to_string(i) + ": ";
         if (!c->mixed) return set_error(T3D_ERR_INVALID, who + "batched designs need precision T3D_MIXED");
-        if (c->standard) return set_error(T3D_ERR_INVALID, who + "batched designs use the Adapted V-cycle");
+        if (c->standard != c0->standard) return set_error(T3D_ERR_INVALID, who + "members must share one V-cycle");
         if (c->ncases != 1) return set_error(T3D_ERR_INVALID, who + "batched designs have one load case");
         if (c->nlev < 2) return set_error(T3D_ERR_INVALID, who + "batched designs need two MG levels at least");
-        if (!c->modal || c->mt.variant != B->variant)
+        if (!c->modal || c->mt.variant != B->variant || !modal_fused_available(c->mt))
             return set_error(T3D_ERR_INVALID, who + "the batched K(E)p needs the modal TMA tile shape");
         if (c->dev != c0->dev) return set_error(T3D_ERR_INVALID, who + "members must share one device");
         if (std::memcmp(&c->kh, &c0->kh, sizeof c->kh) != 0)
@@ -164,76 +201,127 @@ static int batch_members_check(Batch* B) {
 // the launch lists of one batched PCG iteration (all arguments are fixed for the life of the batch: the
 // members' buffers never move)
 static int batch_lists(Batch* B) {
+    T3D_CUDA_OK(cudaStreamSynchronize(B->st));
+    B->free_lists();
+    B->dirty = true;
     const int n = (int)B->m.size();
-    std::vector<CUtensorMap> maps(2 * (size_t)n);
+    if (n == 0) return T3D_OK;
+    B->standard = B->m[0]->standard;
+    // tensor maps per member: the PCG product (p, E); the Standard cycle's level-0 products (z, E_mg), (Ap, E_mg)
+    const int per = B->standard ? 6 : 2;
+    std::vector<CUtensorMap> maps((size_t)per * n);
     for (int i = 0; i < n; ++i) {
         const t3d_context* c = B->m[i];
-        if (!modal_tensor_maps_for(B->variant, c->g, c->p32, c->E32, &maps[2 * i], &maps[2 * i + 1]))
-            return set_error(T3D_ERR_CUDA, "batch member " + std::to_string(i) + ": tensor maps could not be encoded");
+        CUtensorMap* q = &maps[(size_t)per * i];
+        bool ok = modal_tensor_maps_for(B->variant, c->g, c->p32, c->E32, q, q + 1);
+        if (B->standard)
+            ok = ok && modal_tensor_maps_for(B->variant, c->g, c->z32, c->E_mg32, q + 2, q + 3) &&
+                 modal_tensor_maps_for(B->variant, c->g, c->Ap32, c->E_mg32, q + 4, q + 5);
+        if (!ok) return set_error(T3D_ERR_CUDA, "batch member " + std::to_string(i) + ": tensor maps could not be encoded");
     }
     CHECK(B->dalloc(&B->maps, maps.size()));
     T3D_CUDA_OK(cudaMemcpy(B->maps, maps.data(), maps.size() * sizeof(CUtensorMap), cudaMemcpyHostToDevice));
 
-    std::vector<BatchMatvec> mv;
-    std::vector<BatchUpdate> up;
-    std::vector<BatchDirection> dir;
-    std::vector<BatchProlong0> p0;
-    std::vector<BatchCoarse> co;
-    std::vector<int> bmv, bup, bdir, bp0, bco;
-    std::vector<PcgScalars*> S;
     B->maxL = 0;
     B->coarse_max = 0;
-    for (int i = 0; i < n; ++i) {
-        t3d_context* c = B->m[i];
-        mv.push_back(BatchMatvec{c->g, c->mt, c->mask0, c->Ap32, c->slot[0], c->S32, B->maps + 2 * i, B->maps + 2 * i + 1});
-        bmv.push_back(c->mt.grid);
-        up.push_back(BatchUpdate{c->g.NNp, c->r32, c->Ap32, c->slot[1], c->S32});
-        bup.push_back(batch_blocks_update());
-        dir.push_back(BatchDirection{c->g.NNp, c->z32, c->p32, c->d32, c->S32});
-        bdir.push_back(batch_blocks_update());
-        p0.push_back(BatchProlong0{c->lv32[1], c->lv32[0], c->r32, c->z32, c->prm.mg_weight, c->slot[2], c->S32});
-        bp0.push_back(batch_blocks_prolong0());
-        const BatchCoarse bc{c->lv32[c->nlev - 1], c->Xc, c->Nc, c->chol_status, c->S32};
-        co.push_back(bc);
-        bco.push_back(batch_blocks_coarse(bc));
-        S.push_back(c->S32);
+    B->iter_kernels = 0;
+    B->iter_blocks = 0;
+    for (const t3d_context* c : B->m) {
         B->maxL = std::max(B->maxL, c->nlev);
         B->coarse_max = std::max(B->coarse_max, c->Nc);
     }
-    CHECK(make_list(B, mv, bmv, &B->mv));
-    CHECK(make_list(B, up, bup, &B->up));
-    CHECK(make_list(B, dir, bdir, &B->dir));
-    CHECK(make_list(B, p0, bp0, &B->p0));
-    CHECK(make_list(B, co, bco, &B->co));
-    B->iter_kernels = 5;
-    B->iter_blocks = B->mv.blocks + B->up.blocks + B->dir.blocks + B->p0.blocks + B->co.blocks;
-    for (int l = 0; l + 1 < B->maxL; ++l) {
-        std::vector<BatchRestrict> r0, r1;
-        std::vector<BatchProlong> pr;
-        std::vector<int> b0, b1, bp;
+    // one list: the arguments f(c, i) of the members that `take` (c, i), with their block counts
+    auto list = [&](LaunchList* L, auto take, auto f, auto blocks) -> int {
+        using A = decltype(f(B->m[0], 0));
+        std::vector<A> a;
+        std::vector<int> bl;
+        std::vector<PcgScalars*> S;
         for (int i = 0; i < n; ++i) {
             t3d_context* c = B->m[i];
-            if (c->nlev - 1 <= l) continue;
-            const BatchRestrict a{c->lv32[l + 1], c->lv32[l], l == 0 ? c->r32 : c->lv32[l].r, c->ra1_32[l],
-                                  c->lv32[l + 1].r, c->S32};
-            r0.push_back(a);
-            b0.push_back(batch_blocks_restrict(a, 0));
-            if (batch_blocks_restrict(a, 1) > 0) {
-                r1.push_back(a);
-                b1.push_back(batch_blocks_restrict(a, 1));
-            }
-            if (l >= 1) {
-                const BatchProlong p{c->lv32[l + 1], c->lv32[l], c->prm.mg_weight, c->S32};
-                pr.push_back(p);
-                bp.push_back(batch_blocks_prolong(p));
-            }
+            if (!take(c)) continue;
+            a.push_back(f(c, i));
+            bl.push_back(blocks(a.back()));
+            S.push_back(c->S32);
         }
-        CHECK(make_list(B, r0, b0, &B->rs0[l]));
-        CHECK(make_list(B, r1, b1, &B->rs1[l]));
-        CHECK(make_list(B, pr, bp, &B->pr[l]));
-        B->iter_kernels += (B->rs0[l].n > 0) + (B->rs1[l].n > 0) + (B->pr[l].n > 0);
-        B->iter_blocks += B->rs0[l].blocks + B->rs1[l].blocks + B->pr[l].blocks;
+        CHECK(make_list(B, a, bl, S, L));
+        B->iter_kernels += L->n > 0;
+        B->iter_blocks += L->blocks;
+        return T3D_OK;
+    };
+    auto all = [](const t3d_context*) { return true; };
+    auto mvb = [](const BatchMatvec& a) { return a.t.grid; };
+    CHECK(list(&B->mv, all, [&](t3d_context* c, int i) {
+        const CUtensorMap* q = B->maps + (size_t)per * i;
+        return BatchMatvec{c->g, c->mt, c->mask0, c->Ap32, c->slot[0], c->S32, q, q + 1, nullptr, nullptr, 0.f};
+    }, mvb));
+    CHECK(list(&B->up, all, [](t3d_context* c, int) {
+        return BatchUpdate{c->g.NNp, c->r32, c->Ap32, c->slot[1], c->S32};
+    }, [](const BatchUpdate&) { return batch_blocks_update(); }));
+    CHECK(list(&B->dir, all, [](t3d_context* c, int) {
+        return BatchDirection{c->g.NNp, c->z32, c->p32, c->d32, c->S32};
+    }, [](const BatchDirection&) { return batch_blocks_update(); }));
+    CHECK(list(&B->co, all, [](t3d_context* c, int) {
+        return BatchCoarse{c->lv32[c->nlev - 1], c->Xc, c->Nc, c->chol_status, c->S32};
+    }, [](const BatchCoarse& a) { return batch_blocks_coarse(a); }));
+    const int norm = B->standard ? 0 : 1;
+    for (int l = 0; l + 1 < B->maxL; ++l) {
+        auto below = [l](const t3d_context* c) { return c->nlev - 1 > l; };
+        auto rs = [&, l](t3d_context* c, int) {
+            const float* src = B->standard ? (l == 0 ? c->Ap32 : c->vtmp32[l]) : (l == 0 ? c->r32 : c->lv32[l].r);
+            return BatchRestrict{c->lv32[l + 1], c->lv32[l], src, c->ra1_32[l], c->lv32[l + 1].r, c->S32, norm};
+        };
+        CHECK(list(&B->rs0[l], below, rs, [](const BatchRestrict& a) { return batch_blocks_restrict(a, 0); }));
+        CHECK(list(&B->rs1[l], [&, l](const t3d_context* c) {
+            return c->nlev - 1 > l && c->lv32[l + 1].span == 4;
+        }, rs, [](const BatchRestrict& a) { return batch_blocks_restrict(a, 1); }));
+        if (!B->standard) {
+            if (l >= 1)
+                CHECK(list(&B->pr[l], below, [l](t3d_context* c, int) {
+                    return BatchProlong{c->lv32[l + 1], c->lv32[l], c->prm.mg_weight, c->S32};
+                }, [](const BatchProlong& a) { return batch_blocks_prolong(a); }));
+            continue;
+        }
+        // the Standard cycle's level steps, level matrices and prolongations (level 0: z, r and the TMA products)
+        CHECK(list(&B->lop[l], below, [l](t3d_context* c, int) {
+            const MgLevel32& L = c->lv32[l];
+            return l == 0 ? BatchLevelOp{L, c->r32, nullptr, c->z32, c->prm.mg_standard_weight, c->S32}
+                          : BatchLevelOp{L, L.r, c->vtmp32[l], L.x, c->prm.mg_standard_weight, c->S32};
+        }, [](const BatchLevelOp& a) { return batch_blocks_level_op(a); }));
+        CHECK(list(&B->pa[l], below, [l](t3d_context* c, int) {
+            const MgLevel32 &Lc = c->lv32[l + 1], &Lf = c->lv32[l];
+            return l == 0 ? BatchProlongAdd{Lc, Lf, Lc.x, c->z32, c->Ap32, c->S32}
+                          : BatchProlongAdd{Lc, Lf, Lc.x, Lf.x, Lf.x, c->S32};
+        }, [](const BatchProlongAdd& a) { return batch_blocks_prolong_add(a); }));
+        if (l >= 1) {
+            CHECK(list(&B->lmv[l], below, [l](t3d_context* c, int) {
+                return BatchLevelMatvec{c->lv32[l], c->Kel32[l], c->lv32[l].x, c->vtmp32[l], c->S32};
+            }, [](const BatchLevelMatvec& a) { return batch_blocks_level_matvec(a); }));
+            // each level op and level product runs twice per cycle (down and up)
+            B->iter_kernels += 2;
+            B->iter_blocks += B->lop[l].blocks + B->lmv[l].blocks;
+        }
     }
+    if (B->standard) {
+        CHECK(list(&B->mv1, all, [&](t3d_context* c, int i) {
+            const CUtensorMap* q = B->maps + (size_t)per * i + 2;
+            return BatchMatvec{c->g, c->mt, c->mask0, c->Ap32, RedSlot{nullptr, nullptr}, c->S32, q, q + 1, c->r32,
+                               nullptr, c->prm.mg_standard_weight};
+        }, mvb));
+        CHECK(list(&B->mv2, all, [&](t3d_context* c, int i) {
+            const CUtensorMap* q = B->maps + (size_t)per * i + 4;
+            return BatchMatvec{c->g, c->mt, c->mask0, c->z32, c->slot[2], c->S32, q, q + 1, c->r32, c->lv32[0].diag,
+                               c->prm.mg_standard_weight};
+        }, mvb));
+    } else {
+        CHECK(list(&B->p0, all, [](t3d_context* c, int) {
+            return BatchProlong0{c->lv32[1], c->lv32[0], c->r32, c->z32, c->prm.mg_weight, c->slot[2], c->S32};
+        }, [](const BatchProlong0&) { return batch_blocks_prolong0(); }));
+    }
+    std::vector<PcgScalars*> S;
+    for (const t3d_context* c : B->m) S.push_back(c->S32);
+    CHECK(B->dalloc(&B->djobs, B->jobs.size()));
+    T3D_CUDA_OK(cudaMemcpy(B->djobs, B->jobs.data(), B->jobs.size() * sizeof(BatchCompact), cudaMemcpyHostToDevice));
+    B->iter_kernels += 1;   // the compaction
     CHECK(B->dalloc(&B->dS, S.size()));
     T3D_CUDA_OK(cudaMemcpy(B->dS, S.data(), S.size() * sizeof(PcgScalars*), cudaMemcpyHostToDevice));
     CHECK(B->dalloc(&B->dflags, (size_t)n));
@@ -242,7 +330,9 @@ static int batch_lists(Batch* B) {
     T3D_CUDA_OK(cudaMallocHost(&B->hflags, (size_t)n * sizeof(int)));
     T3D_CUDA_OK(cudaMallocHost(&B->hS, (size_t)n * sizeof(PcgScalars)));
     T3D_CUDA_OK(cudaMallocHost(&B->hscal, (size_t)n * sizeof(double)));
-    return modal_batched_grid(B->variant, B->dev, &B->mv_grid);
+    CHECK(modal_batched_grid(B->variant, B->dev, &B->mv_grid));
+    B->dirty = false;
+    return T3D_OK;
 }
 
 static int batch_create(int n, const int* dims, const t3d_params* params, const t3d_problem* problems, Batch* B) {
@@ -284,35 +374,68 @@ static int batch_create(int n, const int* dims, const t3d_params* params, const 
     }
     CHECK(batch_members_check(B));
     B->kh = B->m[0]->kh;
-    B->variant = B->m[0]->mt.variant;
+    B->n_arena = n;
     T3D_CUDA_OK(cudaStreamCreateWithFlags(&B->st, cudaStreamNonBlocking));
     return batch_lists(B);
 }
 
 // ------------------------------------------------------------------ the batched inner solve
+template <class T>
+static const T* args_of(const LaunchList& L) {
+    return static_cast<const T*>(L.args);
+}
+
+static void batch_restrict(Batch* B, int l) {
+    if (B->rs0[l].n) launch_batch_restrict32(args_of<BatchRestrict>(B->rs0[l]), B->rs0[l].act, B->rs0[l].n, 0, B->st);
+    if (B->rs1[l].n) launch_batch_restrict32(args_of<BatchRestrict>(B->rs1[l]), B->rs1[l].act, B->rs1[l].n, 1, B->st);
+}
+
+static void batch_product(Batch* B, int mode, const LaunchList& L) {
+    launch_batch_matvec32(B->variant, mode, args_of<BatchMatvec>(L), L.act, L.n, B->kh, B->mv_grid, B->err, B->st);
+}
+
+// vcycle32 (context.cu) for every member: the Adapted cycle, or the Standard one (vcycle32_standard) with its
+// level-0 residual and correction fused into the TMA products
 static void batch_vcycle(Batch* B) {
-    for (int l = 0; l + 1 < B->maxL; ++l) {
-        if (B->rs0[l].n)
-            launch_batch_restrict32(static_cast<const BatchRestrict*>(B->rs0[l].args), B->rs0[l].vstart, B->rs0[l].n, 0,
-                                    B->st);
-        if (B->rs1[l].n)
-            launch_batch_restrict32(static_cast<const BatchRestrict*>(B->rs1[l].args), B->rs1[l].vstart, B->rs1[l].n, 1,
-                                    B->st);
+    if (!B->standard) {
+        for (int l = 0; l + 1 < B->maxL; ++l) batch_restrict(B, l);
+        launch_batch_coarse32(args_of<BatchCoarse>(B->co), B->co.act, B->co.n, B->coarse_max, B->st);
+        for (int l = B->maxL - 2; l >= 1; --l)
+            if (B->pr[l].n) launch_batch_prolong32(args_of<BatchProlong>(B->pr[l]), B->pr[l].act, B->pr[l].n, B->st);
+        launch_batch_prolong0_32(args_of<BatchProlong0>(B->p0), B->p0.act, B->p0.n, B->st);
+        return;
     }
-    launch_batch_coarse32(static_cast<const BatchCoarse*>(B->co.args), B->co.vstart, B->co.n, B->coarse_max, B->st);
-    for (int l = B->maxL - 2; l >= 1; --l)
-        if (B->pr[l].n)
-            launch_batch_prolong32(static_cast<const BatchProlong*>(B->pr[l].args), B->pr[l].vstart, B->pr[l].n, B->st);
-    launch_batch_prolong0_32(static_cast<const BatchProlong0*>(B->p0.args), B->p0.vstart, B->p0.n, B->st);
+    for (int l = 0; l + 1 < B->maxL; ++l) {
+        const LaunchList& op = B->lop[l];
+        launch_batch_level_op32(args_of<BatchLevelOp>(op), op.act, op.n, 0, B->st);          // x = w r / D
+        if (l == 0) {
+            batch_product(B, 1, B->mv1);                                                     // t = r - K x
+        } else {
+            const LaunchList& mv = B->lmv[l];
+            launch_batch_level_matvec32(args_of<BatchLevelMatvec>(mv), mv.act, mv.n, B->st);   // t = K x
+            launch_batch_level_op32(args_of<BatchLevelOp>(op), op.act, op.n, 1, B->st);      // t = r - t
+        }
+        batch_restrict(B, l);                                                                // r' = P^T t
+    }
+    launch_batch_coarse32(args_of<BatchCoarse>(B->co), B->co.act, B->co.n, B->coarse_max, B->st);
+    for (int l = B->maxL - 2; l >= 1; --l) {
+        const LaunchList &pa = B->pa[l], &mv = B->lmv[l], &op = B->lop[l];
+        launch_batch_prolong_add32(args_of<BatchProlongAdd>(pa), pa.act, pa.n, B->st);       // x += P x'
+        launch_batch_level_matvec32(args_of<BatchLevelMatvec>(mv), mv.act, mv.n, B->st);     // t = K x
+        launch_batch_level_op32(args_of<BatchLevelOp>(op), op.act, op.n, 2, B->st);          // x += w (r - t) / D
+    }
+    launch_batch_prolong_add32(args_of<BatchProlongAdd>(B->pa[0]), B->pa[0].act, B->pa[0].n, B->st);   // T = z + P x'
+    batch_product(B, 2, B->mv2);                                      // z = T + w (r - K T) / D, with r.z
 }
 
 // one PCG iteration of every member (pcg32_iteration in context.cu, batched)
 static void batch_iteration(Batch* B) {
-    launch_batch_matvec32(B->variant, static_cast<const BatchMatvec*>(B->mv.args), B->mv.vstart, B->mv.n, B->kh,
-                          B->mv_grid, B->err, B->st);
-    launch_batch_update32(static_cast<const BatchUpdate*>(B->up.args), B->up.vstart, B->up.n, B->st);
+    batch_product(B, 0, B->mv);
+    launch_batch_update32(args_of<BatchUpdate>(B->up), B->up.act, B->up.n, B->st);
     batch_vcycle(B);
-    launch_batch_direction32(static_cast<const BatchDirection*>(B->dir.args), B->dir.vstart, B->dir.n, B->st);
+    launch_batch_direction32(args_of<BatchDirection>(B->dir), B->dir.act, B->dir.n, B->st);
+    // members whose solve ended in this iteration (their last step applied above) leave the work lists
+    launch_batch_compact(B->djobs, (int)B->jobs.size(), B->st);
 }
 
 static int batch_graph(Batch* B) {
@@ -406,7 +529,8 @@ static int batch_solve(Batch* B, int* iters) {
             }
             T3D_CUDA_OK(cudaMemcpyAsync(B->m[i]->S32, &h, sizeof h, cudaMemcpyHostToDevice, B->st));
         }
-        batch_vcycle(B);   // z = M r for the members iterating
+        launch_batch_compact(B->djobs, (int)B->jobs.size(), B->st);   // the members iterating in this pass
+        batch_vcycle(B);   // z = M r for them
         B->launches += B->iter_kernels - 3;
         for (int i = 0; i < n; ++i)
             if (active[(size_t)i]) {
@@ -455,6 +579,8 @@ static int batch_solve(Batch* B, int* iters) {
 }
 
 static int batch_design_step(Batch* B, t3d_iter_record* recs) {
+    if (B->m.empty()) return T3D_OK;
+    if (B->dirty) CHECK(batch_lists(B));
     CHECK(for_members(B, [&](int i) -> int {
         t3d_context* c = B->m[i];
         CHECK(design_pre(c));
@@ -489,6 +615,51 @@ int t3d_batch_create(int n, const int* dims, const t3d_params* params, const t3d
         return rc;
     }
     *out = b;
+    return T3D_OK;
+}
+
+int t3d_batch_open(int device, t3d_batch** out) {
+    if (!out) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    *out = nullptr;
+    t3d_batch* b = new (std::nothrow) t3d_batch();
+    if (!b) return t3d::set_error(T3D_ERR_OOM, "host allocation failed");
+    b->dev = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete b;
+        return t3d::set_cuda_error(e, "t3d_batch_open", __FILE__, __LINE__);
+    }
+    *out = b;
+    return T3D_OK;
+}
+
+int t3d_batch_adopt(t3d_batch* b, t3d_context* ctx) {
+    if (!b || !ctx) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    if (!ctx->design_ready) return t3d::set_error(T3D_ERR_INVALID, "t3d_design_init not called on the context");
+    for (const t3d_context* c : b->m)
+        if (c == ctx) return t3d::set_error(T3D_ERR_INVALID, "context is already a batch member");
+    if (cudaSetDevice(b->dev) != cudaSuccess) return t3d::set_error(T3D_ERR_CUDA, "cudaSetDevice failed");
+    if (ctx->dev != b->dev) return t3d::set_error(T3D_ERR_INVALID, "context is on another device");
+    b->m.push_back(ctx);
+    const int rc = t3d::batch_members_check(b);
+    if (rc != T3D_OK) {
+        b->m.pop_back();
+        return rc;
+    }
+    if (b->m.size() == 1) b->kh = ctx->kh;
+    b->dirty = true;
+    return T3D_OK;
+}
+
+int t3d_batch_release(t3d_batch* b, int i, t3d_context** out) {
+    if (!b || !out || i < 0 || i >= (int)b->m.size()) return t3d::set_error(T3D_ERR_INVALID, "bad batch member");
+    if (i < b->n_arena) return t3d::set_error(T3D_ERR_INVALID, "member lives in the batch arena");
+    if (cudaSetDevice(b->dev) != cudaSuccess) return t3d::set_error(T3D_ERR_CUDA, "cudaSetDevice failed");
+    if (cudaStreamSynchronize(b->st) != cudaSuccess) return t3d::set_error(T3D_ERR_CUDA, "batch stream failed");
+    *out = b->m[(size_t)i];
+    b->m.erase(b->m.begin() + i);
+    b->dirty = true;
     return T3D_OK;
 }
 

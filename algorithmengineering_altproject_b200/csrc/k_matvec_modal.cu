@@ -357,13 +357,19 @@ struct TmaShape {
     static constexpr int bx = BX, by = BY, stages = ST, packed = 1, tma = 1;
     static constexpr size_t smem = sizeof(SM) + 128;   // + slack for the 128-byte alignment of the ring
     static const void* fn() { return reinterpret_cast<const void*>(k_matvec32_tma<BX, BY, MINB, ST>); }
-    static const void* fn_batched() { return reinterpret_cast<const void*>(k_matvec32_tma_batched<BX, BY, MINB, ST>); }
+    static const void* fn_batched(int mode) {
+        return mode == 0   ? reinterpret_cast<const void*>(k_matvec32_tma_batched<BX, BY, MINB, ST, 0>)
+               : mode == 1 ? reinterpret_cast<const void*>(k_matvec32_tma_batched<BX, BY, MINB, ST, 1>)
+                           : reinterpret_cast<const void*>(k_matvec32_tma_batched<BX, BY, MINB, ST, 2>);
+    }
     static bool maps(const Grid& g, const float* u, const float* E, CUtensorMap* um, CUtensorMap* em) {
         return modal_tensor_maps(g, u, E, SM::RW, SM::PY, BY, um, em);
     }
-    static void batched(const BatchMatvec* a, const int* vstart, int n, const ModalKe& kh, int grid, int* err,
+    static void batched(int mode, const BatchMatvec* a, const int* act, int N, const ModalKe& kh, int grid, int* err,
                         cudaStream_t s) {
-        k_matvec32_tma_batched<BX, BY, MINB, ST><<<grid, BX * BY, smem, s>>>(a, vstart, n, kh, err);
+        if (mode == 0) k_matvec32_tma_batched<BX, BY, MINB, ST, 0><<<grid, BX * BY, smem, s>>>(a, act, N, kh, err);
+        else if (mode == 1) k_matvec32_tma_batched<BX, BY, MINB, ST, 1><<<grid, BX * BY, smem, s>>>(a, act, N, kh, err);
+        else k_matvec32_tma_batched<BX, BY, MINB, ST, 2><<<grid, BX * BY, smem, s>>>(a, act, N, kh, err);
     }
     static bool launch(const Grid& g, const ModalKe& kh, const ModalTiling& t, const float* E, const uint8_t* mask,
                        const float* u, float* y, RedSlot dot, PcgScalars* S, int mark, int* err, cudaStream_t s) {
@@ -402,9 +408,9 @@ struct ModalVariant {
     bool (*fused)(int, const Grid&, const ModalKe&, const ModalTiling&, const float*, const uint8_t*, const float*,
                   float*, const float*, const float*, float, RedSlot, PcgScalars*, int*, cudaStream_t);
     // the batched PCG product over many instances (TMA shapes only)
-    const void* (*fn_batched)();
+    const void* (*fn_batched)(int);
     bool (*maps)(const Grid&, const float*, const float*, CUtensorMap*, CUtensorMap*);
-    void (*batched)(const BatchMatvec*, const int*, int, const ModalKe&, int, int*, cudaStream_t);
+    void (*batched)(int, const BatchMatvec*, const int*, int, const ModalKe&, int, int*, cudaStream_t);
 };
 template <class V>
 constexpr ModalVariant variant_of() {
@@ -576,9 +582,11 @@ int modal_batched_grid(int variant, int dev, int* grid) {
     int sms = 0, per_sm = 0;
     cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return set_cuda_error(e, "cudaDeviceGetAttribute", __FILE__, __LINE__);
-    e = cudaFuncSetAttribute(v.fn_batched(), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem);
-    if (e != cudaSuccess) return set_cuda_error(e, "cudaFuncSetAttribute", __FILE__, __LINE__);
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn_batched(), v.bx * v.by, v.smem);
+    for (int mode = 0; mode <= 2; ++mode) {
+        e = cudaFuncSetAttribute(v.fn_batched(mode), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v.smem);
+        if (e != cudaSuccess) return set_cuda_error(e, "cudaFuncSetAttribute", __FILE__, __LINE__);
+    }
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, v.fn_batched(0), v.bx * v.by, v.smem);
     if (e != cudaSuccess) return set_cuda_error(e, "cudaOccupancyMaxActiveBlocksPerMultiprocessor", __FILE__, __LINE__);
     *grid = std::max(1, sms * std::max(per_sm, 1));
     return T3D_OK;
@@ -589,10 +597,10 @@ bool modal_tensor_maps_for(int variant, const Grid& g, const float* u, const flo
     return modal_batched_available(variant) && MODAL_VARIANTS[variant].maps(g, u, E, umap, emap);
 }
 
-bool launch_batch_matvec32(int variant, const BatchMatvec* a, const int* vstart, int n, const ModalKe& kh, int grid,
-                           int* err, cudaStream_t s) {
-    if (!modal_batched_available(variant) || n <= 0) return false;
-    MODAL_VARIANTS[variant].batched(a, vstart, n, kh, grid, err, s);
+bool launch_batch_matvec32(int variant, int mode, const BatchMatvec* a, const int* act, int N, const ModalKe& kh,
+                           int grid, int* err, cudaStream_t s) {
+    if (!modal_batched_available(variant) || N <= 0) return false;
+    MODAL_VARIANTS[variant].batched(mode, a, act, N, kh, grid, err, s);
     return true;
 }
 

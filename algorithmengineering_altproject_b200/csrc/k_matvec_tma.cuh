@@ -326,15 +326,15 @@ __global__ void __launch_bounds__(BX * BY, MINB)
                                           vb_real(), gp, failed);
 }
 
-// Batched PCG product (MODE 0 with the p.Ap fold): many instances' K(E)p in one persistent launch.  The work
-// list is (instance, logical block): logical block v belongs to instance batch_instance(vstart, n, v) and
-// runs that instance's own tiling, reduction slot and scalars, so each instance's result is the one its
-// own launch gives.  The tensor maps sit in global memory, one pair per instance, written by the host
+// Batched K(E)u (MODE 0 the PCG product with the p.Ap fold; 1, 2 the Standard cycle's fused residual and
+// correction): many instances in one persistent launch.  The work
+// list is (active instance, logical block) (act, kernels.hpp): each logical block runs its instance's own
+// tiling, reduction slot and scalars, so each instance's result is the one its own launch gives.  The tensor maps sit in global memory, one pair per instance, written by the host
 // before the launch; they cover this GPU's own buffers and no copy uses cluster multicast.  Instances whose
 // inner solve has converged (S->done) skip their blocks: the per-instance convergence mask.
-template <int BX, int BY, int MINB, int STAGES>
+template <int BX, int BY, int MINB, int STAGES, int MODE = 0>
 __global__ void __launch_bounds__(BX * BY, MINB)
-    k_matvec32_tma_batched(const BatchMatvec* __restrict__ a, const int* __restrict__ vstart, int n, ModalKe kh,
+    k_matvec32_tma_batched(const BatchMatvec* __restrict__ a, const int* __restrict__ act, int N, ModalKe kh,
                            int* err) {
     using SM = TmaSmem<BX, BY, STAGES>;
     SM& sm = tma_smem<SM>();
@@ -342,16 +342,20 @@ __global__ void __launch_bounds__(BX * BY, MINB)
     __syncthreads();
     unsigned gp = 0;
     bool failed = false;
-    const int total = __ldg(vstart + n);
+    const int n = __ldg(act);                      // the active instances (layout: kernels.hpp)
+    const int* __restrict__ pos = act + 1;
+    const int* __restrict__ vs = act + 1 + N;
+    const int total = __ldg(vs + n);
     for (int v = blockIdx.x; v < total; v += gridDim.x) {
-        const int i = batch_instance(vstart, n, v);
-        const BatchMatvec& A = a[i];
-        const int v0 = __ldg(vstart + i);
+        const int k = batch_instance(vs, n, v);
+        const BatchMatvec& A = a[__ldg(pos + k)];
+        const int v0 = __ldg(vs + k);
         const Grid g = A.g;
         const ModalTiling t = A.t;
         if (threadIdx.x == 0) tma_prefetch_maps(A.umap, A.emap);
-        tma_matvec_body<BX, BY, STAGES, 0>(sm, A.umap, A.emap, g, kh, t, A.mask, A.y, A.dot, A.S, 1, err, nullptr,
-                                           nullptr, 0.f, VB{v - v0, __ldg(vstart + i + 1) - v0}, gp, failed);
+        tma_matvec_body<BX, BY, STAGES, MODE>(sm, A.umap, A.emap, g, kh, t, A.mask, A.y, A.dot, A.S, MODE == 0 ? 1 : 0,
+                                              err, A.rv, A.rd, A.omega, VB{v - v0, __ldg(vs + k + 1) - v0}, gp,
+                                              failed);
         __syncthreads();
     }
 }

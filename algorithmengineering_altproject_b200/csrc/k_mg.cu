@@ -533,7 +533,10 @@ void launch_cholesky(const double* A, double* LT, double* Lrow, int N, int* stat
 }
 void launch_coarse_inverse(const double* Lrow, int N, const int* status, double* X, cudaStream_t s) {
     const size_t smem = (size_t)N * INV_COLS * sizeof(double);   // N <= 1000: at most 128 KB
-    cudaFuncSetAttribute(k_coarse_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // the attribute is per function, not per launch: always the bound for the largest N, so that contexts set
+    // up concurrently from several host threads never lower it under another thread's launch
+    cudaFuncSetAttribute(k_coarse_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(1000 * INV_COLS * sizeof(double)));
     k_coarse_inverse<<<blocks_for(N, INV_COLS), INV_COLS, smem, s>>>(Lrow, N, status, X);
 }
 void launch_coarse_solve(const MgLevel& L, const double* X, int N, const int* status, const PcgScalars* S,

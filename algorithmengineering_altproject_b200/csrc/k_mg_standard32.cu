@@ -31,10 +31,11 @@ __device__ __forceinline__ int64_t vidx(const MgLevel32& L, int64_t n) {
 }
 
 // x = w r / D
-__global__ void k_jacobi_init32(MgLevel32 L, const float* __restrict__ r, float* __restrict__ x, float w,
-                                const PcgScalars* S) {
+// (kernel bodies take the logical block VB, so that the batched launches below run them unchanged)
+__device__ __forceinline__ void jacobi_init32(VB vb, const MgLevel32& L, const float* __restrict__ r,
+                                              float* __restrict__ x, float w, const PcgScalars* S) {
     if (S->done) return;
-    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < L.nn; n += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t n = (int64_t)vb.b * blockDim.x + threadIdx.x; n < L.nn; n += (int64_t)vb.n * blockDim.x) {
         const int m = L.mask[n];
         const int64_t v = vidx(L, n);
         for (int c = 0; c < 3; ++c) {
@@ -44,10 +45,16 @@ __global__ void k_jacobi_init32(MgLevel32 L, const float* __restrict__ r, float*
     }
 }
 
+__global__ void k_jacobi_init32(MgLevel32 L, const float* __restrict__ r, float* __restrict__ x, float w,
+                                const PcgScalars* S) {
+    jacobi_init32(vb_real(), L, r, x, w, S);
+}
+
 // kx <- r - kx
-__global__ void k_residual32(MgLevel32 L, const float* __restrict__ r, float* __restrict__ kx, const PcgScalars* S) {
+__device__ __forceinline__ void residual32(VB vb, const MgLevel32& L, const float* __restrict__ r,
+                                           float* __restrict__ kx, const PcgScalars* S) {
     if (S->done) return;
-    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < L.nn; n += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t n = (int64_t)vb.b * blockDim.x + threadIdx.x; n < L.nn; n += (int64_t)vb.n * blockDim.x) {
         const int m = L.mask[n];
         const int64_t v = vidx(L, n);
         for (int c = 0; c < 3; ++c) {
@@ -57,11 +64,16 @@ __global__ void k_residual32(MgLevel32 L, const float* __restrict__ r, float* __
     }
 }
 
+__global__ void k_residual32(MgLevel32 L, const float* __restrict__ r, float* __restrict__ kx, const PcgScalars* S) {
+    residual32(vb_real(), L, r, kx, S);
+}
+
 // x += w (r - kx) / D
-__global__ void k_jacobi_correct32(MgLevel32 L, const float* __restrict__ r, const float* __restrict__ kx,
-                                   float* __restrict__ x, float w, const PcgScalars* S) {
+__device__ __forceinline__ void jacobi_correct32(VB vb, const MgLevel32& L, const float* __restrict__ r,
+                                                 const float* __restrict__ kx, float* __restrict__ x, float w,
+                                                 const PcgScalars* S) {
     if (S->done) return;
-    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < L.nn; n += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t n = (int64_t)vb.b * blockDim.x + threadIdx.x; n < L.nn; n += (int64_t)vb.n * blockDim.x) {
         const int m = L.mask[n];
         const int64_t v = vidx(L, n);
         for (int c = 0; c < 3; ++c) {
@@ -71,13 +83,19 @@ __global__ void k_jacobi_correct32(MgLevel32 L, const float* __restrict__ r, con
     }
 }
 
+__global__ void k_jacobi_correct32(MgLevel32 L, const float* __restrict__ r, const float* __restrict__ kx,
+                                   float* __restrict__ x, float w, const PcgScalars* S) {
+    jacobi_correct32(vb_real(), L, r, kx, x, w, S);
+}
+
 // xo = xi + P xc (trilinear from the coarse cell floor(f/s), clamped to the last cell), fixed DOFs 0; xo may be xi
-__global__ void k_prolong_add32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ xc, const float* xi, float* xo,
-                                const PcgScalars* S) {
+__device__ __forceinline__ void prolong_add32(VB vb, const MgLevel32& Lc, const MgLevel32& Lf,
+                                              const float* __restrict__ xc, const float* xi, float* xo,
+                                              const PcgScalars* S) {
     if (S->done) return;
     const int s = Lc.span;
     const int fnx = Lf.nx + 1, fny = Lf.ny + 1, cnx = Lc.nx + 1, cny = Lc.ny + 1;
-    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < Lf.nn; n += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t n = (int64_t)vb.b * blockDim.x + threadIdx.x; n < Lf.nn; n += (int64_t)vb.n * blockDim.x) {
         const int fx = (int)(n % fnx), fy = (int)((n / fnx) % fny), fz = (int)(n / ((int64_t)fnx * fny));
         int cx = fx / s, cy = fy / s, cz = fz / s;
         if (cx >= Lc.nx) cx = Lc.nx - 1;
@@ -96,6 +114,10 @@ __global__ void k_prolong_add32(MgLevel32 Lc, MgLevel32 Lf, const float* __restr
         }
     }
 }
+__global__ void k_prolong_add32(MgLevel32 Lc, MgLevel32 Lf, const float* __restrict__ xc, const float* xi, float* xo,
+                                const PcgScalars* S) {
+    prolong_add32(vb_real(), Lc, Lf, xc, xi, xo, S);
+}
 
 // packed position of entry (i, j) of a symmetric 24x24 matrix: the upper triangle row by row, 300 entries
 __host__ __device__ constexpr int sym_pack(int i, int j) {
@@ -107,12 +129,13 @@ constexpr int SYM_N = 300;
 // element e at p * ne + e; the Galerkin operators P^T K P are symmetric).  Node-centric gather: each node reads
 // the three rows of its corner in the 8 element matrices around it (all loops unrolled, so the packed positions
 // are constants); consecutive nodes read consecutive addresses.  Fixed DOFs 0.
-__global__ void k_level_matvec32(MgLevel32 L, const float* __restrict__ Kel, const float* __restrict__ x,
-                                 float* __restrict__ y, const PcgScalars* S) {
+__device__ __forceinline__ void level_matvec32(VB vb, const MgLevel32& L, const float* __restrict__ Kel,
+                                               const float* __restrict__ x, float* __restrict__ y,
+                                               const PcgScalars* S) {
     if (S->done) return;
     const int nnx = L.nx + 1, nny = L.ny + 1;
     const int64_t ne = (int64_t)L.nx * L.ny * L.nz;
-    for (int64_t n = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; n < L.nn; n += (int64_t)gridDim.x * blockDim.x) {
+    for (int64_t n = (int64_t)vb.b * blockDim.x + threadIdx.x; n < L.nn; n += (int64_t)vb.n * blockDim.x) {
         const int X = (int)(n % nnx), Y = (int)((n / nnx) % nny), Z = (int)(n / ((int64_t)nnx * nny));
         float acc0 = 0.0f, acc1 = 0.0f, acc2 = 0.0f;
 #pragma unroll
@@ -142,6 +165,10 @@ __global__ void k_level_matvec32(MgLevel32 L, const float* __restrict__ Kel, con
         y[L.cs + n] = (mk & 2) ? 0.0f : acc1;
         y[2 * L.cs + n] = (mk & 4) ? 0.0f : acc2;
     }
+}
+__global__ void k_level_matvec32(MgLevel32 L, const float* __restrict__ Kel, const float* __restrict__ x,
+                                 float* __restrict__ y, const PcgScalars* S) {
+    level_matvec32(vb_real(), L, Kel, x, y, S);
 }
 
 // FP32 symmetric-packed, entry-major image of element-major FP64 element matrices (the upper triangle):
@@ -194,7 +221,46 @@ inline unsigned blocks_of(int64_t n, int t) {
     return (unsigned)(b < 8 * RED_BLOCKS ? (b > 0 ? b : 1) : 8 * RED_BLOCKS);
 }
 
+// ---------------------------------------------------------------- batched launches (persistent grids)
+__global__ void __launch_bounds__(256) k_batch_level_op32(const BatchLevelOp* __restrict__ a,
+                                                          const int* __restrict__ act, int N, int op) {
+    batch_walk(a, act, N, [&](const BatchLevelOp& A, VB vb) {
+        const MgLevel32 L = A.L;
+        if (op == 0) jacobi_init32(vb, L, A.r, A.x, A.w, A.S);
+        else if (op == 1) residual32(vb, L, A.r, A.kx, A.S);
+        else jacobi_correct32(vb, L, A.r, A.kx, A.x, A.w, A.S);
+    });
+}
+__global__ void __launch_bounds__(256) k_batch_prolong_add32(const BatchProlongAdd* __restrict__ a,
+                                                             const int* __restrict__ act, int N) {
+    batch_walk(a, act, N, [&](const BatchProlongAdd& A, VB vb) {
+        const MgLevel32 Lc = A.Lc, Lf = A.Lf;
+        prolong_add32(vb, Lc, Lf, A.xc, A.xi, A.xo, A.S);
+    });
+}
+__global__ void __launch_bounds__(128) k_batch_level_matvec32(const BatchLevelMatvec* __restrict__ a,
+                                                              const int* __restrict__ act, int N) {
+    batch_walk(a, act, N, [&](const BatchLevelMatvec& A, VB vb) {
+        const MgLevel32 L = A.L;
+        level_matvec32(vb, L, A.Kel, A.x, A.y, A.S);
+    });
+}
+constexpr int BATCH_GRID256 = 8 * 148, BATCH_GRID128 = 16 * 148;
+
 }  // namespace
+
+int batch_blocks_level_op(const BatchLevelOp& a) { return (int)blocks_of(a.L.nn, 256); }
+int batch_blocks_prolong_add(const BatchProlongAdd& a) { return (int)blocks_of(a.Lf.nn, 256); }
+int batch_blocks_level_matvec(const BatchLevelMatvec& a) { return (int)blocks_of(a.L.nn, 128); }
+void launch_batch_level_op32(const BatchLevelOp* a, const int* act, int N, int op, cudaStream_t s) {
+    k_batch_level_op32<<<BATCH_GRID256, 256, 0, s>>>(a, act, N, op);
+}
+void launch_batch_prolong_add32(const BatchProlongAdd* a, const int* act, int N, cudaStream_t s) {
+    k_batch_prolong_add32<<<BATCH_GRID256, 256, 0, s>>>(a, act, N);
+}
+void launch_batch_level_matvec32(const BatchLevelMatvec* a, const int* act, int N, cudaStream_t s) {
+    k_batch_level_matvec32<<<BATCH_GRID128, 128, 0, s>>>(a, act, N);
+}
 
 void launch_jacobi_init32(const MgLevel32& L, const float* r, float* x, float w, const PcgScalars* S, cudaStream_t s) {
     k_jacobi_init32<<<blocks_of(L.nn, 256), 256, 0, s>>>(L, r, x, w, S);

@@ -567,57 +567,60 @@ __global__ void k_pcg_direction32(Grid g, const float* __restrict__ z, float* __
 inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 // ---------------------------------------------------------------- batched launches
-// A persistent grid walks the (instance, logical block) list: logical block v is block v - vstart[i] of
-// instance i = batch_instance(vstart, n, v) in a launch of vstart[i+1] - vstart[i] blocks.  The body runs as
-// in that instance's own launch; the barrier between items keeps shared scratch from being overwritten early.
-template <class A, class F>
-__device__ __forceinline__ void batch_walk(const A* __restrict__ a, const int* __restrict__ vstart, int n, F&& f) {
-    const int total = __ldg(vstart + n);
-    for (int v = blockIdx.x; v < total; v += gridDim.x) {
-        const int i = batch_instance(vstart, n, v);
-        const int v0 = __ldg(vstart + i);
-        f(a[i], VB{v - v0, __ldg(vstart + i + 1) - v0});
-        __syncthreads();
+// one thread per launch list: the positions of its instances still iterating and their block prefix sums
+__global__ void k_batch_compact(const BatchCompact* __restrict__ jobs, int njobs) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= njobs) return;
+    const BatchCompact J = jobs[j];
+    int n = 0, acc = 0;
+    J.act[1 + J.N] = 0;
+    for (int p = 0; p < J.N; ++p) {
+        if (J.S[p]->done) continue;
+        J.act[1 + n] = p;
+        acc += J.blocks[p];
+        ++n;
+        J.act[1 + J.N + n] = acc;
     }
+    J.act[0] = n;
 }
 
 __global__ void __launch_bounds__(RED_THREADS) k_batch_update32(const BatchUpdate* __restrict__ a,
-                                                                const int* __restrict__ vstart, int n) {
+                                                                const int* __restrict__ act, int N) {
     __shared__ double sh[32];
-    batch_walk(a, vstart, n, [&](const BatchUpdate& A, VB vb) { pcg_update32(vb, A.NNp, A.r, A.Ap, A.red, A.S, sh); });
+    batch_walk(a, act, N, [&](const BatchUpdate& A, VB vb) { pcg_update32(vb, A.NNp, A.r, A.Ap, A.red, A.S, sh); });
 }
 
 __global__ void __launch_bounds__(RED_THREADS) k_batch_direction32(const BatchDirection* __restrict__ a,
-                                                                   const int* __restrict__ vstart, int n) {
-    batch_walk(a, vstart, n, [&](const BatchDirection& A, VB vb) { pcg_direction32(vb, A.NNp, A.z, A.p, A.x, A.S); });
+                                                                   const int* __restrict__ act, int N) {
+    batch_walk(a, act, N, [&](const BatchDirection& A, VB vb) { pcg_direction32(vb, A.NNp, A.z, A.p, A.x, A.S); });
 }
 
 // stage 0: span-4 transitions run their x pass, span-2 ones their whole window; stage 1: the span-4 y-z pass
 __global__ void __launch_bounds__(256) k_batch_restrict32(const BatchRestrict* __restrict__ a,
-                                                          const int* __restrict__ vstart, int n, int stage) {
-    batch_walk(a, vstart, n, [&](const BatchRestrict& A, VB vb) {
+                                                          const int* __restrict__ act, int N, int stage) {
+    batch_walk(a, act, N, [&](const BatchRestrict& A, VB vb) {
         const MgLevel32 Lc = A.Lc, Lf = A.Lf;
         if (Lc.span == 4) {
             if (stage == 0) restrict_x32(vb, Lc, Lf, A.rf, A.a1, A.S);
-            else restrict_yz32<4>(vb, Lc, Lf, A.a1, A.rc, A.S, 1);
+            else restrict_yz32<4>(vb, Lc, Lf, A.a1, A.rc, A.S, A.normalize);
         } else {
-            restrict_xyz32<2>(vb, Lc, Lf, A.rf, A.rc, A.S, 1);
+            restrict_xyz32<2>(vb, Lc, Lf, A.rf, A.rc, A.S, A.normalize);
         }
     });
 }
 
 __global__ void __launch_bounds__(256) k_batch_prolong32(const BatchProlong* __restrict__ a,
-                                                         const int* __restrict__ vstart, int n) {
-    batch_walk(a, vstart, n, [&](const BatchProlong& A, VB vb) {
+                                                         const int* __restrict__ act, int N) {
+    batch_walk(a, act, N, [&](const BatchProlong& A, VB vb) {
         const MgLevel32 Lc = A.Lc, Lf = A.Lf;
         prolong_smooth32(vb, Lc, Lf, Lc.x, Lf.r, Lf.x, A.w, A.S);
     });
 }
 
 __global__ void __launch_bounds__(RED_THREADS) k_batch_prolong0_32(const BatchProlong0* __restrict__ a,
-                                                                   const int* __restrict__ vstart, int n) {
+                                                                   const int* __restrict__ act, int N) {
     __shared__ double sh[32];
-    batch_walk(a, vstart, n, [&](const BatchProlong0& A, VB vb) {
+    batch_walk(a, act, N, [&](const BatchProlong0& A, VB vb) {
         const MgLevel32 Lc = A.Lc, Lf = A.Lf;
         if (Lc.span == 4) prolong_smooth0_32<4>(vb, Lc, Lf, Lc.x, A.r, A.z, A.w, A.dot, A.S, sh);
         else prolong_smooth0_32<2>(vb, Lc, Lf, Lc.x, A.r, A.z, A.w, A.dot, A.S, sh);
@@ -625,9 +628,9 @@ __global__ void __launch_bounds__(RED_THREADS) k_batch_prolong0_32(const BatchPr
 }
 
 __global__ void __launch_bounds__(128) k_batch_coarse32(const BatchCoarse* __restrict__ a,
-                                                        const int* __restrict__ vstart, int n) {
+                                                        const int* __restrict__ act, int N) {
     extern __shared__ double rs[];
-    batch_walk(a, vstart, n, [&](const BatchCoarse& A, VB vb) {
+    batch_walk(a, act, N, [&](const BatchCoarse& A, VB vb) {
         const MgLevel32 L = A.L;
         coarse_solve32(vb, L, A.X, A.N, A.status, A.S, rs);
     });
@@ -662,23 +665,26 @@ int batch_blocks_coarse(const BatchCoarse& a) {
 void launch_batch_flags(PcgScalars* const* S, int n, int* out, cudaStream_t s) {
     k_batch_flags<<<1, 256, 0, s>>>(S, n, out);
 }
-void launch_batch_update32(const BatchUpdate* a, const int* vstart, int n, cudaStream_t s) {
-    k_batch_update32<<<BATCH_GRID, RED_THREADS, 0, s>>>(a, vstart, n);
+void launch_batch_compact(const BatchCompact* jobs, int njobs, cudaStream_t s) {
+    k_batch_compact<<<(njobs + 31) / 32, 32, 0, s>>>(jobs, njobs);
 }
-void launch_batch_direction32(const BatchDirection* a, const int* vstart, int n, cudaStream_t s) {
-    k_batch_direction32<<<BATCH_GRID, RED_THREADS, 0, s>>>(a, vstart, n);
+void launch_batch_update32(const BatchUpdate* a, const int* act, int N, cudaStream_t s) {
+    k_batch_update32<<<BATCH_GRID, RED_THREADS, 0, s>>>(a, act, N);
 }
-void launch_batch_restrict32(const BatchRestrict* a, const int* vstart, int n, int stage, cudaStream_t s) {
-    k_batch_restrict32<<<BATCH_GRID, 256, 0, s>>>(a, vstart, n, stage);
+void launch_batch_direction32(const BatchDirection* a, const int* act, int N, cudaStream_t s) {
+    k_batch_direction32<<<BATCH_GRID, RED_THREADS, 0, s>>>(a, act, N);
 }
-void launch_batch_prolong32(const BatchProlong* a, const int* vstart, int n, cudaStream_t s) {
-    k_batch_prolong32<<<BATCH_GRID, 256, 0, s>>>(a, vstart, n);
+void launch_batch_restrict32(const BatchRestrict* a, const int* act, int N, int stage, cudaStream_t s) {
+    k_batch_restrict32<<<BATCH_GRID, 256, 0, s>>>(a, act, N, stage);
 }
-void launch_batch_prolong0_32(const BatchProlong0* a, const int* vstart, int n, cudaStream_t s) {
-    k_batch_prolong0_32<<<BATCH_GRID, RED_THREADS, 0, s>>>(a, vstart, n);
+void launch_batch_prolong32(const BatchProlong* a, const int* act, int N, cudaStream_t s) {
+    k_batch_prolong32<<<BATCH_GRID, 256, 0, s>>>(a, act, N);
 }
-void launch_batch_coarse32(const BatchCoarse* a, const int* vstart, int n, int max_n, cudaStream_t s) {
-    k_batch_coarse32<<<2 * BATCH_GRID, 128, (size_t)(max_n > 0 ? max_n : 1) * sizeof(double), s>>>(a, vstart, n);
+void launch_batch_prolong0_32(const BatchProlong0* a, const int* act, int N, cudaStream_t s) {
+    k_batch_prolong0_32<<<BATCH_GRID, RED_THREADS, 0, s>>>(a, act, N);
+}
+void launch_batch_coarse32(const BatchCoarse* a, const int* act, int N, int max_n, cudaStream_t s) {
+    k_batch_coarse32<<<2 * BATCH_GRID, 128, (size_t)(max_n > 0 ? max_n : 1) * sizeof(double), s>>>(a, act, N);
 }
 
 void launch_nodes_to32(const Grid& g, const double* a, float* b, cudaStream_t s) {

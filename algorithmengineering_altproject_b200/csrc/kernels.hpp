@@ -298,18 +298,24 @@ bool launch_matvec32_fused(int mode, const Grid& g, const ModalKe& kh, const Mod
                            RedSlot dot, PcgScalars* S, int* err, cudaStream_t s);
 
 // ---- batched launches (batch.cu): one persistent launch runs the logical launches of many instances of
-// uneven size.  Each takes a device array of per-instance arguments and vstart[0..n], the prefix sum of the
-// instances' logical block counts (each instance's count is the grid of its own launch, so its arithmetic and
-// reduction order are those of that launch); instances whose inner solve is done (S->done) skip their blocks.
-struct BatchMatvec {      // the PCG product K(E)p with p.Ap (TMA tile shapes; maps in global memory)
-    Grid g;
-    ModalTiling t;
+// uneven size.  Each takes a device array of the N instances' arguments and `act`, the instances still
+// iterating: act[0] = their count n, act[1 .. n] their positions in the argument array, act[1+N .. 1+N+n]
+// the prefix sum of their logical block counts (an instance's count is the grid of its own launch, so its
+// arithmetic and reduction order are those of that launch).  launch_batch_compact rebuilds `act` from the
+// instances' done flags between iterations; instances that finish inside an iteration skip their blocks there
+// (S->done), as their own launches would.
+struct BatchMatvec {      // K(E)u in the TMA tile shapes (maps in global memory) with the epilogue of `mode`:
+    Grid g;               // 0 the PCG product with p.Ap; 1 / 2 the Standard cycle's fused residual / correction
+    ModalTiling t;        // (launch_matvec32_fused)
     const uint8_t* mask;
     float* y;
     RedSlot dot;
     PcgScalars* S;
     const CUtensorMap* umap;
     const CUtensorMap* emap;
+    const float* rv;      // modes 1, 2: r
+    const float* rd;      // mode 2: 1/D
+    float omega;          // mode 2: Jacobi weight
 };
 struct BatchUpdate {      // r -= alpha Ap with |r|^2
     int64_t NNp;
@@ -331,6 +337,7 @@ struct BatchRestrict {    // restriction Lf -> Lc: span 4 x pass rf -> a1 then y
     float* a1;
     float* rc;
     PcgScalars* S;
+    int normalize;        // 1: the Adapted cycle's weighted average; 0: the Standard cycle's P^T
 };
 struct BatchProlong {     // prolongation + smoothing on a level above the finest
     MgLevel32 Lc, Lf;
@@ -352,25 +359,62 @@ struct BatchCoarse {      // coarsest-level solve
     const int* status;
     PcgScalars* S;
 };
+// the Standard V-cycle's level steps (FP32): op 0 x = w r / D, op 1 kx <- r - kx, op 2 x += w (r - kx) / D
+struct BatchLevelOp {
+    MgLevel32 L;
+    const float* r;
+    float* kx;
+    float* x;
+    float w;
+    PcgScalars* S;
+};
+struct BatchProlongAdd {  // xo = xi + P xc
+    MgLevel32 Lc, Lf;
+    const float* xc;
+    const float* xi;
+    float* xo;
+    PcgScalars* S;
+};
+struct BatchLevelMatvec { // y = K_l x from the level's FP32 element matrices
+    MgLevel32 L;
+    const float* Kel;
+    const float* x;
+    float* y;
+    PcgScalars* S;
+};
+int batch_blocks_level_op(const BatchLevelOp& a);
+int batch_blocks_prolong_add(const BatchProlongAdd& a);
+int batch_blocks_level_matvec(const BatchLevelMatvec& a);
+void launch_batch_level_op32(const BatchLevelOp* a, const int* act, int N, int op, cudaStream_t s);
+void launch_batch_prolong_add32(const BatchProlongAdd* a, const int* act, int N, cudaStream_t s);
+void launch_batch_level_matvec32(const BatchLevelMatvec* a, const int* act, int N, cudaStream_t s);
+
+struct BatchCompact {     // one launch list's compaction: act from the done flags of its N instances
+    PcgScalars* const* S;   // per position
+    const int* blocks;      // per position
+    int N;
+    int* act;
+};
 // logical block counts of one instance's own launches
 int batch_blocks_update();
 int batch_blocks_restrict(const BatchRestrict& a, int stage);   // stage 0: x or x-y-z pass, 1: y-z pass (0 if none)
 int batch_blocks_prolong(const BatchProlong& a);
 int batch_blocks_prolong0();
 int batch_blocks_coarse(const BatchCoarse& a);
-// the launches (a, vstart on the device; n instances; total = vstart[n] logical blocks)
+// the launches (a, act on the device; N instances in the list)
 void launch_batch_flags(PcgScalars* const* S, int n, int* out, cudaStream_t s);   // out[i] = S[i]->done
-void launch_batch_update32(const BatchUpdate* a, const int* vstart, int n, cudaStream_t s);
-void launch_batch_direction32(const BatchDirection* a, const int* vstart, int n, cudaStream_t s);
-void launch_batch_restrict32(const BatchRestrict* a, const int* vstart, int n, int stage, cudaStream_t s);
-void launch_batch_prolong32(const BatchProlong* a, const int* vstart, int n, cudaStream_t s);
-void launch_batch_prolong0_32(const BatchProlong0* a, const int* vstart, int n, cudaStream_t s);
-void launch_batch_coarse32(const BatchCoarse* a, const int* vstart, int n, int max_n, cudaStream_t s);
+void launch_batch_compact(const BatchCompact* jobs, int njobs, cudaStream_t s);
+void launch_batch_update32(const BatchUpdate* a, const int* act, int N, cudaStream_t s);
+void launch_batch_direction32(const BatchDirection* a, const int* act, int N, cudaStream_t s);
+void launch_batch_restrict32(const BatchRestrict* a, const int* act, int N, int stage, cudaStream_t s);
+void launch_batch_prolong32(const BatchProlong* a, const int* act, int N, cudaStream_t s);
+void launch_batch_prolong0_32(const BatchProlong0* a, const int* act, int N, cudaStream_t s);
+void launch_batch_coarse32(const BatchCoarse* a, const int* act, int N, int max_n, cudaStream_t s);
 // the batched PCG product: variant = the members' common TMA tile shape; false when it has no batched form
 bool modal_batched_available(int variant);
 int modal_batched_grid(int variant, int dev, int* grid);
-bool launch_batch_matvec32(int variant, const BatchMatvec* a, const int* vstart, int n, const ModalKe& kh, int grid,
-                           int* err, cudaStream_t s);
+bool launch_batch_matvec32(int variant, int mode, const BatchMatvec* a, const int* act, int N, const ModalKe& kh,
+                           int grid, int* err, cudaStream_t s);
 // the tensor maps of one instance's PCG product (p and E images); false when they cannot be encoded
 bool modal_tensor_maps_for(int variant, const Grid& g, const float* u, const float* E, CUtensorMap* umap,
                            CUtensorMap* emap);

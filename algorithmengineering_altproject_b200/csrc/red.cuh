@@ -78,4 +78,22 @@ __device__ __forceinline__ int batch_instance(const int* __restrict__ vstart, in
     return lo;
 }
 
+// A persistent grid walks the (instance, logical block) list of the active instances (act, kernels.hpp):
+// logical block v is block v - vs[k] of the k-th active instance, k = batch_instance(vs, n, v), in a launch of
+// vs[k+1] - vs[k] blocks.  The body runs as in that instance's own launch; the barrier between items keeps
+// shared scratch from being overwritten early.
+template <class A, class F>
+__device__ __forceinline__ void batch_walk(const A* __restrict__ a, const int* __restrict__ act, int N, F&& f) {
+    const int n = __ldg(act);
+    const int* __restrict__ pos = act + 1;
+    const int* __restrict__ vs = act + 1 + N;
+    const int total = __ldg(vs + n);
+    for (int v = blockIdx.x; v < total; v += gridDim.x) {
+        const int k = batch_instance(vs, n, v);
+        const int v0 = __ldg(vs + k);
+        f(a[__ldg(pos + k)], VB{v - v0, __ldg(vs + k + 1) - v0});
+        __syncthreads();
+    }
+}
+
 }  // namespace t3d

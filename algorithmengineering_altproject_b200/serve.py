@@ -2,10 +2,12 @@
 
 Requests (grid dims, volume fraction, load case, passive voids, OC iteration count; or a TopVoxel design
 domain, `DesignRequest.from_topvoxel`) are admitted in arrival order as soon as a slot and the HBM budget
-allow: each admitted request gets its own device
-context (model, MG hierarchy, density, warm-start displacement and filter state stay resident for all
-its OC iterations) and its own CUDA stream, and runs on a worker thread, so the kernels of all
-admitted requests overlap on the device while later arrivals wait.  The projected footprint of a
+allow: each admitted request gets its own device context (model, MG hierarchy, density, warm-start
+displacement and filter state stay resident for all its OC iterations).  With the batched engine (the
+default of the command line) an admitted request is initialised on a worker thread and then joins the
+one t3d batch that steps every request in flight together -- each kernel of the inner PCG iteration one
+launch for all of them -- leaving it when its iterations are done; with the streams engine each request
+runs its own loop on its own stream and the kernels of all admitted requests overlap on the device.  The projected footprint of a
 request is bytes-per-node (learned from the contexts created so far, per precision) times its padded
 node count, with a margin; a request that alone exceeds the budget is rejected.
 
@@ -30,8 +32,8 @@ import numpy as np
 # request threads start at once, and their first launches should not race the module loader.
 os.environ.setdefault("CUDA_MODULE_LOADING", "EAGER")
 
-from . import (T3D_COARSE_FULL, T3D_FP64, T3D_MIXED, T3D_SUM_FP64, Problem, ProblemSpec, T3DError,  # noqa: E402
-               topvoxel_info)
+from . import (T3D_BATCH_TILE, T3D_COARSE_FULL, T3D_FP64, T3D_MIXED, T3D_SUM_FP64, Batch, Problem,  # noqa: E402
+               ProblemSpec, T3DError, topvoxel_info)
 
 # bytes per padded grid node of a context, before the first context of a precision is measured
 DEFAULT_BYTES_PER_NODE = {T3D_FP64: 900.0, T3D_MIXED: 1100.0}
@@ -108,12 +110,24 @@ class DesignResult:
 class DesignServer:
     """Admits DesignRequests against an HBM budget and runs them concurrently on one GPU."""
 
-    def __init__(self, device=0, hbm_budget=160e9, max_active=8, precision=T3D_MIXED, **params):
+    def __init__(self, device=0, hbm_budget=160e9, max_active=8, precision=T3D_MIXED, engine="streams", **params):
+        """engine "streams": every admitted request runs its own design loop on its own context and stream;
+        "batched" (mixed precision): admitted requests are initialised alone, then join one t3d batch that
+        steps all of them together -- one launch per kernel of the inner PCG iteration for every request in
+        flight -- and leave it when their iterations are done (requests with several load cases, which the
+        batch does not take, run alone)."""
+        if engine not in ("streams", "batched"):
+            raise ValueError("engine must be 'streams' or 'batched'")
+        if engine == "batched" and precision != T3D_MIXED:
+            raise ValueError("the batched engine runs the mixed-precision form")
         self.device = device
         self.budget = float(hbm_budget)
         self.max_active = int(max_active)
         self.precision = precision
+        self.engine = engine
         self.params = dict(params)
+        if engine == "batched":
+            self.params["matvec32_tile"] = T3D_BATCH_TILE
         # arbitrary request grids: the full Galerkin coarsest operator (the reference's corner-sub-block
         # assembly is kept only for its own cantilever, where it is the parity target)
         self.params.setdefault("mg_coarse_assembly", T3D_COARSE_FULL)
@@ -126,6 +140,12 @@ class DesignServer:
         self._threads = []
         self._create_lock = threading.Lock()   # context creation (allocations, tile autotuning) one at a time
         self._warm = False
+        self._joining = []          # batched engine: initialised requests waiting to join the batch
+        self._engine_closed = False
+        self._engine_thread = None
+        if engine == "batched":
+            self._engine_thread = threading.Thread(target=self._engine, daemon=True)
+            self._engine_thread.start()
         self._dispatcher = threading.Thread(target=self._dispatch, daemon=True)
         self._dispatcher.start()
 
@@ -156,6 +176,11 @@ class DesignServer:
         self._dispatcher.join()
         for t in self._threads:
             t.join()
+        if self._engine_thread is not None:   # after the workers: every request has joined the batch or ended
+            with self._cv:
+                self._engine_closed = True
+                self._cv.notify_all()
+            self._engine_thread.join()
 
     def __enter__(self):
         return self
@@ -199,31 +224,98 @@ class DesignServer:
         res = DesignResult(req)
         res.admitted = time.perf_counter()
         try:
+            if self.engine == "batched" and getattr(req, "load_cases", 1) == 1 and req.iters > 0:
+                P = self._create(req)
+                try:
+                    res.c_solid = P.design_init(req.V0)
+                except BaseException:
+                    P.close()
+                    raise
+                with self._cv:                     # the engine steps it from here on and finishes the request
+                    self._joining.append((P, req, res, fut, need))
+                    self._cv.notify_all()
+                return
             self._execute(req, res)
         except T3DError as e:
             res.error = str(e)
         except Exception as e:   # any other failure is reported on the request, never lost in the worker
             res.error = "%s: %s" % (type(e).__name__, e)
-        finally:
-            res.finished = time.perf_counter()
-            with self._cv:
-                self._active -= 1
-                self._reserved -= need
-                self._cv.notify_all()
-            fut.set_result(res)
+        self._finish(res, fut, need)
 
-    def _execute(self, req, res):
-        """Runs one request to completion on its own context (and stream)."""
+    def _finish(self, res, fut, need):
+        res.finished = time.perf_counter()
+        with self._cv:
+            self._active -= 1
+            self._reserved -= need
+            self._cv.notify_all()
+        fut.set_result(res)
+
+    def _engine(self):
+        """The batched engine: one design iteration of every request in the batch per step; initialised
+        requests join between steps, finished ones leave (their context released and closed)."""
+        B = None
+        live = []                                  # (Problem, request, result, future, need), batch order
+        try:
+            B = Batch.open(self.device)
+            while True:
+                with self._cv:
+                    while not self._joining and not live and not self._engine_closed:
+                        self._cv.wait()
+                    if not self._joining and not live:
+                        return
+                    joining, self._joining = self._joining, []
+                for item in joining:
+                    try:
+                        B.adopt(item[0])
+                        live.append(item)
+                    except T3DError as e:
+                        item[0].close()
+                        item[2].error = str(e)
+                        self._finish(item[2], item[3], item[4])
+                if not live:
+                    continue
+                try:
+                    recs = B.design_step()
+                except Exception as e:             # the step failed for the whole batch: end every request in it
+                    for k in range(len(live) - 1, -1, -1):
+                        P, _, res, fut, need = live.pop(k)
+                        B.release(k).close()
+                        res.error = "%s: %s" % (type(e).__name__, e)
+                        self._finish(res, fut, need)
+                    continue
+                for (P, req, res, fut, need), r in zip(live, recs):
+                    res.objectives.append(r["obj"])
+                    res.pcg_iters.append(r["pcg_iters"])
+                for k in range(len(live) - 1, -1, -1):
+                    P, req, res, fut, need = live[k]
+                    if len(res.objectives) < req.iters:
+                        continue
+                    live.pop(k)
+                    P = B.release(k)
+                    if req.keep_density:
+                        res.density = P.density()
+                    P.close()
+                    self._finish(res, fut, need)
+        finally:
+            if B is not None:
+                B.close()
+
+    def _create(self, req):
         kw = dict(device=self.device, precision=self.precision, oc_sum_order=T3D_SUM_FP64, **self.params)
         with self._create_lock:
             if getattr(req, "topvoxel", None):
                 P = Problem.from_topvoxel(req.topvoxel, **kw)
             else:
                 P = Problem(req.nely, req.nelx, req.nelz, problem=req.spec(), **kw)
+        with self._cv:   # learn the footprint per node from the real allocation (single-case problems)
+            if getattr(req, "load_cases", 1) == 1:
+                self._bpn[self.precision] = max(self._bpn[self.precision], P.device_bytes / P.nn)
+        return P
+
+    def _execute(self, req, res):
+        """Runs one request to completion on its own context (and stream)."""
+        P = self._create(req)
         try:
-            with self._cv:   # learn the footprint per node from the real allocation (single-case problems)
-                if getattr(req, "load_cases", 1) == 1:
-                    self._bpn[self.precision] = max(self._bpn[self.precision], P.device_bytes / P.nn)
             res.c_solid = P.design_init(req.V0)
             for _ in range(req.iters):
                 r = P.design_step()
@@ -321,6 +413,9 @@ def main():
     ap.add_argument("--max-elements", type=float, default=16e6)
     ap.add_argument("--seed", type=int, default=20251203)
     ap.add_argument("--sequential-fp64", action="store_true", help="also run the same requests one at a time in FP64")
+    ap.add_argument("--engine", default="batched", choices=["batched", "streams"],
+                    help="batched: requests in flight stepped together in one t3d batch; streams: one context and "
+                         "stream per request")
     a = ap.parse_args()
     def workload(srv):
         rng = np.random.default_rng(a.seed)
@@ -328,9 +423,10 @@ def main():
             return run_batch(srv, rng, a.batch, a.iters)
         return run_poisson(srv, rng, a.rate, a.requests, a.iters, a.median, a.max_elements)
 
-    with DesignServer(hbm_budget=a.budget_gb * 1e9, max_active=a.max_active, precision=T3D_MIXED) as srv:
+    with DesignServer(hbm_budget=a.budget_gb * 1e9, max_active=a.max_active, precision=T3D_MIXED,
+                      engine=a.engine) as srv:
         res, wall = workload(srv)
-    out = {"mode": ("batch of %d instances" % a.batch) if a.batch else "Poisson arrivals",
+    out = {"mode": ("batch of %d instances" % a.batch) if a.batch else "Poisson arrivals", "engine": a.engine,
            "precision": "mixed", "rate_per_s": None if a.batch else a.rate, "iters": a.iters,
            "max_active": a.max_active, "budget_gb": a.budget_gb, **summary(res, wall)}
     if a.sequential_fp64:

@@ -3,7 +3,7 @@ sensitivities -> PDE filter -> OC) on the reference's cantilever.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--config c2]
                     [--precision mixed|fp64] [--regime converged|reference] [--compare-steps S]
-                    [--kernels-only --reps R --tile T]
+                    [--kernels-only --reps R --tile T] [--batch N --batch-iters K]
 
 `serving` (N=1, after the timed region) runs the request loop (serve.py) on Poisson arrivals at 0.5 and 8
 requests/s and the same requests one at a time in FP64: designs/s and p50/p95/p99 latency.
@@ -85,6 +85,10 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--serve-requests", type=int, default=8,
                     help="requests per arrival rate in the serving sample (0 = no serving sample)")
+    ap.add_argument("--batch", type=int, default=0,
+                    help="batched-designs mode: this many seed-drawn instances stepped together (t3d_batch), "
+                         "against the same designs run one at a time in mixed precision and in plain FP64")
+    ap.add_argument("--batch-iters", type=int, default=10, help="design iterations per instance in --batch mode")
     return ap.parse_args()
 
 
@@ -281,35 +285,115 @@ SERVE_SEED = 20251203
 SERVE_ITERS = 40
 
 
-def serving_sample(dev, n):
+def serving_sample(dev, n, regime):
     """designs/s and p50/p95/p99 end-to-end latency of the request loop (serve.DesignServer: admission by
     projected HBM footprint, concurrent contexts on their own streams) for n requests at each rate, and of the
     same requests served one at a time in FP64."""
     import algorithmengineering_altproject_b200 as t3d
     from algorithmengineering_altproject_b200 import serve
 
-    def run(rate, precision, max_active):
-        with serve.DesignServer(device=dev, hbm_budget=160e9, max_active=max_active, precision=precision) as srv:
+    def run(rate, precision, max_active, engine="streams"):
+        with serve.DesignServer(device=dev, hbm_budget=160e9, max_active=max_active, precision=precision,
+                                engine=engine, **regime_kw(t3d, regime)) as srv:
             res, wall = serve.run_poisson(srv, np.random.default_rng(SERVE_SEED), rate, n, SERVE_ITERS)
         s = serve.summary(res, wall)
         s["elements"] = int(sum(r.request.nelx * r.request.nely * r.request.nelz for r in res))
         return {"rate_per_s": rate, **s}
 
     out = {"requests_per_rate": n, "iters_per_request": SERVE_ITERS, "seed": SERVE_SEED, "budget_gb": 160,
-           "max_active": 8, "precision": "mixed",
+           "max_active": 16, "precision": "mixed", "regime": REGIMES[regime]["desc"],
+           "engine": "batched: requests in flight stepped together in one t3d batch, joining and leaving between "
+                     "design iterations",
            "note": "p99 of %d requests is their maximum latency; latency = arrival to result" % n,
-           "rates": [run(r, t3d.T3D_MIXED, 8) for r in SERVE_RATES]}
+           "rates": [run(r, t3d.T3D_MIXED, 16, "batched") for r in SERVE_RATES]}
+    out["streams_engine"] = run(SERVE_RATES[-1], t3d.T3D_MIXED, 8)
     out["sequential_fp64"] = run(SERVE_RATES[0], t3d.T3D_FP64, 1)
     return out
 
 
-def problem_kw(t3d, cfg, regime, precision, dev, tile=0):
+def run_batch_mode(args):
+    """The batched workload: --batch instances drawn with the serving seed (nelx a multiple of 8 in [32, 192],
+    nely and nelz nelx/2 scaled by U(0.5, 1), V0 ~ U(0.06, 0.30), the three load cases, 0-3 void ellipsoids),
+    --batch-iters design iterations each, timed three ways on the same designs: all instances stepped
+    together (t3d_batch: one launch per PCG kernel for all), one at a time in mixed precision (the same
+    parameters, so the same results), and one at a time in plain FP64.  Times are wall clock around the design
+    iterations (creation and the solid-domain solve excluded), synchronised; designs/s = design iterations/s
+    divided by the 40 OC iterations of a design."""
+    import torch
+    import algorithmengineering_altproject_b200 as t3d
+    from algorithmengineering_altproject_b200 import serve
+    dev = dist_env()[2]
+    torch.cuda.set_device(dev)
+    rng = np.random.default_rng(SERVE_SEED)
+    reqs = [serve.draw_instance(rng, iters=args.batch_iters) for _ in range(args.batch)]
+    dims = [(q.nely, q.nelx, q.nelz) for q in reqs]
+    common = dict(device=dev, oc_sum_order=t3d.T3D_SUM_FP64, mg_coarse_assembly=t3d.T3D_COARSE_FULL,
+                  **regime_kw(t3d, args.regime))
+    K = args.batch_iters
+    t0 = time.perf_counter()
+    B = t3d.Batch(dims, problems=[q.spec() for q in reqs], **common)
+    t_create = time.perf_counter() - t0
+    B.design_init([q.V0 for q in reqs])
+    torch.cuda.synchronize(dev)
+    l0 = B.info()
+    t0 = time.perf_counter()
+    brecs = [B.design_step() for _ in range(K)]
+    torch.cuda.synchronize(dev)
+    t_batch = time.perf_counter() - t0
+    info = B.info()
+    bobj = [[r[i]["obj"] for r in brecs] for i in range(len(reqs))]
+    B.close()
+
+    def alone(precision, **kw):
+        total, objs = 0.0, []
+        for q in reqs:
+            P = t3d.Problem(q.nely, q.nelx, q.nelz, problem=q.spec(), precision=precision, **common, **kw)
+            P.design_init(q.V0)
+            torch.cuda.synchronize(dev)
+            t0 = time.perf_counter()
+            objs.append([P.design_step()["obj"] for _ in range(K)])
+            torch.cuda.synchronize(dev)
+            total += time.perf_counter() - t0
+            P.close()
+        return total, objs
+
+    t_mixed, mobj = alone(t3d.T3D_MIXED, matvec32_tile=t3d.T3D_BATCH_TILE)
+    t_fp64, fobj = alone(t3d.T3D_FP64)
+    its = len(reqs) * K
+    rate = lambda t: its / t
+    worst = max(abs(f - b) / abs(f) for fo, bo in zip(fobj, bobj) for f, b in zip(fo, bo))
+    print(json.dumps({
+        "mode": "batched designs", "instances": len(reqs), "design_iters_each": K,
+        "elements_total": int(sum(a * b * c for a, b, c in dims)),
+        "elements_median": float(np.median([a * b * c for a, b, c in dims])),
+        "design_iters_per_s": {"batched": rate(t_batch), "sequential_mixed": rate(t_mixed),
+                               "sequential_fp64": rate(t_fp64)},
+        "designs_per_s_at_40_iters": {"batched": rate(t_batch) / 40, "sequential_mixed": rate(t_mixed) / 40,
+                                      "sequential_fp64": rate(t_fp64) / 40},
+        "speedup_vs_sequential_fp64": t_fp64 / t_batch, "speedup_vs_sequential_mixed": t_mixed / t_batch,
+        "batched_equals_solo_mixed": bobj == mobj,
+        "max_compliance_rel_err_vs_fp64": worst,
+        "batched_launches": info["batched_launches"] - l0["batched_launches"],
+        "member_launches": info["member_launches"] - l0["member_launches"],
+        "kernels_per_batched_pcg_iteration": info["kernels_per_iteration"],
+        "logical_blocks_per_batched_pcg_iteration": info["blocks_per_iteration"],
+        "arena_bytes": info["arena_bytes"], "create_s": t_create,
+        "regime": REGIMES[args.regime]["desc"],
+        "params": "mixed precision, full Galerkin coarsest, FP64 OC sum",
+        "data": "synthetic (seed-drawn instances; no dataset involved)"}), flush=True)
+    return 0
+
+
+def regime_kw(t3d, regime):
     R = REGIMES[regime]
+    return dict(mg_vcycle=t3d.T3D_VCYCLE_STANDARD if R["mg_vcycle"] == "standard" else t3d.T3D_VCYCLE_ADAPTED,
+                mg_rebuild_period=R["mg_rebuild_period"], cg_tol=R["cg_tol"], cg_max_it=R["cg_max_it"])
+
+
+def problem_kw(t3d, cfg, regime, precision, dev, tile=0):
     return dict(device=dev, mg_max_levels=cfg["max_levels"], oc_sum_order=t3d.T3D_SUM_FP64,
-                precision=t3d.T3D_MIXED if precision == "mixed" else t3d.T3D_FP64,
-                mg_vcycle=t3d.T3D_VCYCLE_STANDARD if R["mg_vcycle"] == "standard" else t3d.T3D_VCYCLE_ADAPTED,
-                mg_rebuild_period=R["mg_rebuild_period"], cg_tol=R["cg_tol"], cg_max_it=R["cg_max_it"],
-                matvec32_tile=tile)
+                precision=t3d.T3D_MIXED if precision == "mixed" else t3d.T3D_FP64, matvec32_tile=tile,
+                **regime_kw(t3d, regime))
 
 
 def matvec_roofline(P, mixed, mv_ms):
@@ -533,7 +617,7 @@ def run_b200(args):
     if rank == 0:
         if args.serve_requests > 0 and world == 1 and mixed:
             try:
-                line["serving"] = serving_sample(dev, args.serve_requests)
+                line["serving"] = serving_sample(dev, args.serve_requests, regime)
             except Exception as e:  # reported beside the headline, never required for it
                 line["serving"] = {"unavailable": "%s: %s" % (type(e).__name__, e)}
         print(json.dumps(line), flush=True)
@@ -549,6 +633,9 @@ def main():
         return run_reference_arm(args)
     if args.kernels_only:
         return run_kernels_only(args)
+    if args.batch > 0:
+        os.environ.setdefault("CUDA_MODULE_LOADING", "EAGER")
+        return run_batch_mode(args)
     return run_b200(args)
 
 

@@ -235,6 +235,15 @@ int  t3d_batch_create(int n, const int* dims, const t3d_params* params, const t3
                       struct t3d_batch** out);
 /* member i's context (owned by the batch; use it for queries such as t3d_get_density, not t3d_destroy) */
 int  t3d_batch_member(struct t3d_batch* b, int i, struct t3d_context** out);
+/* Continuous batching (a request loop): an empty batch on `device`; t3d_batch_adopt moves a context created
+ * and initialised alone (t3d_create_problem with the member rules above and matvec32_tile = T3D_BATCH_TILE,
+ * then t3d_design_init) into the batch, appended as the last member, from the next t3d_batch_design_step on;
+ * t3d_batch_release takes member i out again (later members move down by one) and hands its context back to
+ * the caller, who destroys it.  Members created by t3d_batch_create live in the batch's arena and cannot be
+ * released. */
+int  t3d_batch_open(int device, struct t3d_batch** out);
+int  t3d_batch_adopt(struct t3d_batch* b, struct t3d_context* ctx);
+int  t3d_batch_release(struct t3d_batch* b, int i, struct t3d_context** out);
 /* t3d_design_init of every member: V0[n] in, c_solid[n] out (may be NULL) */
 int  t3d_batch_design_init(struct t3d_batch* b, const float* V0, double* c_solid);
 /* one design iteration of every member: recs[n] */

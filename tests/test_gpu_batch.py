@@ -39,10 +39,17 @@ def same_records(a, b):
         assert a[key] == b[key], (key, a[key], b[key])
 
 
-def test_batch_members_equal_their_solo_runs():
+# the reference's solver (Adapted V-cycle, tol 1e-3) and the converged regime (Standard V-cycle rebuilt every
+# iteration, tol 1e-6)
+REGIMES = {"adapted": dict(), "standard": dict(mg_vcycle=1, mg_rebuild_period=1, cg_tol=1e-6, cg_max_it=2000)}
+
+
+@pytest.mark.parametrize("regime", sorted(REGIMES))
+def test_batch_members_equal_their_solo_runs(regime):
     import algorithmengineering_altproject_b200 as t3d
     steps = 3
-    B = t3d.Batch([c["dims"] for c in CASES], problems=[spec(t3d, c) for c in CASES], **COMMON)
+    R = REGIMES[regime]
+    B = t3d.Batch([c["dims"] for c in CASES], problems=[spec(t3d, c) for c in CASES], **COMMON, **R)
     info = B.info()
     assert info["members"] == len(CASES) and info["arena_bytes"] > 0
     assert all(m.device_bytes > 0 for m in B.members)
@@ -56,7 +63,7 @@ def test_batch_members_equal_their_solo_runs():
     assert 5 <= info["kernels_per_iteration"] <= 20
     assert info["batched_launches"] > 0
     for i, c in enumerate(CASES):
-        cs1, recs1, x1, u1 = run_alone(t3d, c, steps)
+        cs1, recs1, x1, u1 = run_alone(t3d, c, steps, **R)
         assert cs[i] == cs1
         for k in range(steps):
             same_records(brecs[k][i], recs1[k])
@@ -85,5 +92,58 @@ def test_batch_member_budgets_and_masks():
 
 def test_batch_rejects_members_it_cannot_batch():
     import algorithmengineering_altproject_b200 as t3d
-    with pytest.raises(t3d.T3DError, match="Adapted"):
-        t3d.Batch([(16, 32, 16)], mg_vcycle=t3d.T3D_VCYCLE_STANDARD)
+    with pytest.raises(t3d.T3DError, match="one V-cycle"):
+        t3d.Batch([(16, 32, 16), (16, 32, 16)], member_params=[dict(), dict(mg_vcycle=t3d.T3D_VCYCLE_STANDARD)])
+    with pytest.raises(t3d.T3DError, match="T3D_MIXED"):
+        P = t3d.Problem(16, 32, 16, matvec32_tile=t3d.T3D_BATCH_TILE)   # FP64
+        P.design_init(0.2)
+        B = t3d.Batch.open()
+        try:
+            B.adopt(P)
+        finally:
+            B.close()
+            P.close()
+
+
+def test_members_join_and_leave_between_steps():
+    """Continuous batching: contexts created and initialised alone join an open batch (adopt) and leave it
+    (release) between design iterations; each still equals its solo run."""
+    import algorithmengineering_altproject_b200 as t3d
+    cases = CASES[:3]
+
+    def make(c):
+        P = t3d.Problem(*c["dims"], problem=spec(t3d, c), precision=t3d.T3D_MIXED,
+                        matvec32_tile=t3d.T3D_BATCH_TILE, **COMMON)
+        P.design_init(c["V0"])
+        return P
+
+    B = t3d.Batch.open()
+    assert B.design_step() == []                     # an empty batch steps nothing
+    got = {0: [], 1: [], 2: []}
+    B.adopt(make(cases[0]))
+    B.adopt(make(cases[1]))
+    for r, k in zip(B.design_step(), (0, 1)):
+        got[k].append(r)
+    B.adopt(make(cases[2]))                           # joins at the second step
+    for r, k in zip(B.design_step(), (0, 1, 2)):
+        got[k].append(r)
+    P0 = B.release(0)                                 # leaves after two steps
+    x0 = P0.density()
+    P0.close()
+    for r, k in zip(B.design_step(), (1, 2)):
+        got[k].append(r)
+    x = {1: B.members[0].density(), 2: B.members[1].density(), 0: x0}
+    B.close()
+    for k, c in enumerate(cases):
+        _, recs1, x1, _ = run_alone(t3d, c, len(got[k]))
+        for a, b in zip(got[k], recs1):
+            same_records(a, b)
+        np.testing.assert_array_equal(x[k], x1)
+
+
+def test_arena_members_cannot_be_released():
+    import algorithmengineering_altproject_b200 as t3d
+    B = t3d.Batch([CASES[3]["dims"]], **COMMON)
+    with pytest.raises(t3d.T3DError, match="arena"):
+        B.release(0)
+    B.close()

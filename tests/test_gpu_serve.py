@@ -60,3 +60,29 @@ def test_topvoxel_requests_in_the_mix(tmp_path):
         assert a.c_solid == m.c_solid and a.objectives == m.objectives and a.pcg_iters == m.pcg_iters
         np.testing.assert_array_equal(a.density, m.density)
     assert len(alone[0].objectives) == 3 and all(np.isfinite(alone[0].objectives))
+
+
+def test_batched_engine_results_equal_results_alone():
+    """The batched engine (requests initialised alone, then stepped together in one t3d batch, joining and
+    leaving between design iterations): every request's results equal its run alone with the batch's tile
+    shape, exactly.  A two-load-case TopVoxel request, which the batch does not take, runs beside it alone."""
+    from algorithmengineering_altproject_b200 import T3D_BATCH_TILE
+    from algorithmengineering_altproject_b200.serve import DesignRequest, DesignServer
+
+    def reqs():
+        r = _requests()
+        r[0].iters, r[2].iters = 5, 2     # leave the batch at different steps
+        r.append(DesignRequest(8, 32, 8, 0.15, load_case=2, iters=4, rid=3, keep_density=True))
+        return r
+
+    with DesignServer(max_active=1, matvec32_tile=T3D_BATCH_TILE) as srv:
+        alone = [srv.submit(r).result() for r in reqs()]
+    with DesignServer(max_active=4, engine="batched") as srv:
+        futs = [srv.submit(r) for r in reqs()]
+        mixed = [f.result() for f in futs]
+    for a, m in zip(alone, mixed):
+        assert a.error is None and m.error is None, (a.error, m.error)
+        assert a.c_solid == m.c_solid
+        assert a.objectives == m.objectives and a.pcg_iters == m.pcg_iters
+        assert len(m.objectives) == m.request.iters
+        np.testing.assert_array_equal(a.density, m.density)
