@@ -148,6 +148,10 @@ _SIGS = {
     "t3d_batch_release": (C.c_int, [_BATCH, C.c_int, C.POINTER(_CTX)]),
     "t3d_batch_design_init": (C.c_int, [_BATCH, _f32p, _f64p]),
     "t3d_batch_design_step": (C.c_int, [_BATCH, C.POINTER(IterRecord)]),
+    "t3d_batch_run": (C.c_int, [_BATCH, C.POINTER(C.c_int), C.POINTER(IterRecord)]),
+    "t3d_batch_submit": (C.c_int, [_BATCH, _CTX, C.c_int]),
+    "t3d_batch_collect": (C.c_int, [_BATCH, C.c_int, C.POINTER(_CTX), C.POINTER(IterRecord), C.c_int,
+                                    C.POINTER(C.c_int), C.POINTER(C.c_int)]),
     "t3d_batch_info": (C.c_int, [_BATCH, C.POINTER(C.c_int64)]),
     "t3d_batch_destroy": (C.c_int, [_BATCH]),
 }
@@ -553,6 +557,45 @@ class Batch:
         _check(self._lib.t3d_batch_design_step(self._h, recs))
         return [recs[i].as_dict() for i in range(self.n)]
 
+    def run(self, steps):
+        """steps[i] design iterations of member i, members advancing independently (only their inner solves
+        share the batched launches); returns each member's list of records"""
+        steps = [int(k) for k in steps]
+        st = (C.c_int * self.n)(*steps)
+        recs = (IterRecord * max(1, sum(steps)))()
+        _check(self._lib.t3d_batch_run(self._h, st, recs))
+        out, k = [], 0
+        for n in steps:
+            out.append([recs[k + j].as_dict() for j in range(n)])
+            k += n
+        return out
+
+    def submit(self, problem, steps):
+        """Submitted work (a batch from Batch.open()): `problem` (created alone with precision T3D_MIXED and
+        matvec32_tile=T3D_BATCH_TILE, design_init done) runs `steps` design iterations in the batch from now
+        on; collect() hands it back when done."""
+        _check(self._lib.t3d_batch_submit(self._h, problem._h, int(steps)))
+        problem._owned = False
+        self._submitted = getattr(self, "_submitted", {})
+        self._submitted[problem._h.value if hasattr(problem._h, "value") else problem._h] = (problem, int(steps))
+
+    def collect(self, timeout_ms=100):
+        """(problem, records, error or None) of a finished submission, or None when none finished within the
+        timeout; the problem is the caller's again (close it)."""
+        c = _CTX()
+        nrec, status = C.c_int(), C.c_int()
+        pending = getattr(self, "_submitted", {})
+        cap = max([k for _, k in pending.values()] + [1])
+        recs = (IterRecord * cap)()
+        _check(self._lib.t3d_batch_collect(self._h, int(timeout_ms), C.byref(c), recs, cap, C.byref(nrec),
+                                           C.byref(status)))
+        if not c.value:
+            return None
+        problem, _ = pending.pop(c.value)
+        problem._owned = True
+        err = None if status.value == T3D_OK else self._lib.t3d_last_error().decode()
+        return problem, [recs[i].as_dict() for i in range(nrec.value)], err
+
     def info(self):
         v = (C.c_int64 * 6)()
         _check(self._lib.t3d_batch_info(self._h, v))
@@ -564,6 +607,8 @@ class Batch:
         if getattr(self, "_h", None):
             for m in self.members:
                 m._h = None
+            for p, _ in getattr(self, "_submitted", {}).values():   # destroyed with the batch
+                p._h = None
             self._lib.t3d_batch_destroy(self._h)
             self._h = None
 

@@ -20,8 +20,12 @@
 // in lock step: one true-residual pass for the members still iterating, one batched inner solve, one
 // accumulation, and again, each member with its own stop test and iteration budget.
 #include <atomic>
+#include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <memory>
+#include <mutex>
 #include <thread>
 
 #include "context.hpp"
@@ -43,6 +47,19 @@ struct LaunchList {      // one batched launch: per-instance arguments and the a
 
 }  // namespace
 
+struct Job {
+    t3d_context* c = nullptr;
+    int steps = 0;
+    bool release = false;               // submitted: leaves the batch when finished
+    std::vector<t3d_iter_record> recs;
+    int rc = T3D_OK;
+    std::string err;
+    int phase = 0;                      // 0 own work, 1 inner solve requested, 2 in the batched solve, 3 solved
+    PcgScalars init{};
+    bool started = false, finished = false;
+    std::thread th;
+};
+
 struct Batch {
     int dev = 0;
     std::vector<t3d_context*> m;
@@ -57,8 +74,8 @@ struct Batch {
     LaunchList rs0[8], rs1[8], pr[8], lop[8], lmv[8], pa[8];
     int maxL = 0, coarse_max = 0;
     CUtensorMap* maps = nullptr;
-    std::vector<BatchCompact> jobs;   // one per launch list
-    BatchCompact* djobs = nullptr;
+    std::vector<BatchCompact> compact;   // one compaction job per launch list
+    BatchCompact* dcompact = nullptr;
     PcgScalars** dS = nullptr;
     int* dflags = nullptr;
     int* err = nullptr;
@@ -71,6 +88,15 @@ struct Batch {
     int64_t iter_blocks = 0;
     int n_arena = 0;             // members 0 .. n_arena-1 live in the arena (created with the batch)
     bool dirty = true;           // membership changed: the launch lists and the graph are rebuilt before use
+    // the engine (batch.cu "the engine"): jobs, their handshake with the scheduler, submitted work
+    std::mutex mu;
+    std::condition_variable cv;
+    std::vector<std::unique_ptr<Job>> jobs;   // running or finished, not yet collected
+    std::vector<std::unique_ptr<Job>> incoming;   // submitted, not yet members
+    std::thread sched;           // the scheduler thread of submitted work
+    bool stop = false;
+    bool failed = false;
+    std::string fail_msg;
 
     template <class T>
     int dalloc(T** p, size_t n) {
@@ -95,8 +121,8 @@ struct Batch {
         hS = nullptr;
         hscal = nullptr;
         maps = nullptr;
-        jobs.clear();
-        djobs = nullptr;
+        compact.clear();
+        dcompact = nullptr;
         dS = nullptr;
         dflags = nullptr;
         err = nullptr;
@@ -149,7 +175,7 @@ int make_list(Batch* B, const std::vector<T>& a, const std::vector<int>& blocks,
     T3D_CUDA_OK(cudaMemcpy(db, blocks.data(), blocks.size() * sizeof(int), cudaMemcpyHostToDevice));
     T3D_CUDA_OK(cudaMemcpy(dS, S.data(), S.size() * sizeof(PcgScalars*), cudaMemcpyHostToDevice));
     L->args = da;
-    B->jobs.push_back(BatchCompact{dS, db, N, L->act});
+    B->compact.push_back(BatchCompact{dS, db, N, L->act});
     return T3D_OK;
 }
 
@@ -319,8 +345,9 @@ static int batch_lists(Batch* B) {
     }
     std::vector<PcgScalars*> S;
     for (const t3d_context* c : B->m) S.push_back(c->S32);
-    CHECK(B->dalloc(&B->djobs, B->jobs.size()));
-    T3D_CUDA_OK(cudaMemcpy(B->djobs, B->jobs.data(), B->jobs.size() * sizeof(BatchCompact), cudaMemcpyHostToDevice));
+    CHECK(B->dalloc(&B->dcompact, B->compact.size()));
+    T3D_CUDA_OK(cudaMemcpy(B->dcompact, B->compact.data(), B->compact.size() * sizeof(BatchCompact),
+                           cudaMemcpyHostToDevice));
     B->iter_kernels += 1;   // the compaction
     CHECK(B->dalloc(&B->dS, S.size()));
     T3D_CUDA_OK(cudaMemcpy(B->dS, S.data(), S.size() * sizeof(PcgScalars*), cudaMemcpyHostToDevice));
@@ -435,7 +462,7 @@ static void batch_iteration(Batch* B) {
     batch_vcycle(B);
     launch_batch_direction32(args_of<BatchDirection>(B->dir), B->dir.act, B->dir.n, B->st);
     // members whose solve ended in this iteration (their last step applied above) leave the work lists
-    launch_batch_compact(B->djobs, (int)B->jobs.size(), B->st);
+    launch_batch_compact(B->dcompact, (int)B->compact.size(), B->st);
 }
 
 static int batch_graph(Batch* B) {
@@ -452,149 +479,278 @@ static int batch_graph(Batch* B) {
 
 // While the batch stream runs the members' solve, every member context issues its own launches there too (its
 // stream is idle: the host synchronised it before); restored on exit.
-struct OnBatchStream {
-    Batch* B;
-    std::vector<cudaStream_t> own;
-    explicit OnBatchStream(Batch* b) : B(b) {
-        for (t3d_context* c : B->m) {
-            own.push_back(c->st);
-            c->st = B->st;
-        }
-    }
-    ~OnBatchStream() {
-        for (size_t i = 0; i < B->m.size(); ++i) B->m[i]->st = own[i];
-    }
-};
+// ------------------------------------------------------------------ the engine
+//
+// Members advance independently.  Each job (a member and a number of design iterations) runs on its own host
+// thread and stream: SIMP, MG rebuild, the FP64 defect-correction loop (true residual, stop test,
+// accumulation) and compliance, sensitivities, filter and OC.  Its inner FP32 MG-PCG is handed to the
+// scheduler, which owns the batch stream: between chunks it starts the requested inner solves (scalars, the
+// first V-cycle, p = z), then replays the graph of batched iterations for every member whose inner solve is
+// running, and hands each finished one back to its thread.  A member's scalars are written only by the
+// scheduler, between chunks, so the batched kernels never see them change inside a chunk; outside its inner
+// solves a member's scalars say done and the batched launches skip it.
 
-// mixed_solve (context.cu) for every member in lock step: the FP64 true residual and stop test per member,
-// the FP32 inner MG-PCG of all members still iterating in batched launches (inner target max(stop,
-// 1e-5 |r64|), at most the member's remaining budget), then u64 += d32.  iters[i]: the member's inner
-// iterations, or its cg_max_it when the budget ran out unconverged.
-static int batch_solve(Batch* B, int* iters) {
-    const int n = (int)B->m.size();
-    CHECK(batch_graph(B));
-    OnBatchStream on(B);
-    std::vector<double> stop((size_t)n), rn((size_t)n);
-    std::vector<int> budget((size_t)n), used((size_t)n, 0), outer((size_t)n, 0);
-    std::vector<char> conv((size_t)n, 0), active((size_t)n, 1);
-    for (int i = 0; i < n; ++i) {
-        t3d_context* c = B->m[i];
-        launch_cells_to32(c->g, c->E, c->E32, B->st);
-        launch_dot(c->g, 3, c->b, c->b, c->slot[3], c->scal + 5, B->st);
-        c->launches += 2;
-        T3D_CUDA_OK(cudaMemcpyAsync(B->hscal + i, c->scal + 5, sizeof(double), cudaMemcpyDeviceToHost, B->st));
+namespace {
+
+// one inner solve through the scheduler: blocks until the batched iterations of this member have ended
+int request_inner(Batch* B, Job* J, const PcgScalars& init) {
+    std::unique_lock<std::mutex> lk(B->mu);
+    J->init = init;
+    J->phase = 1;
+    B->cv.notify_all();
+    B->cv.wait(lk, [&] { return J->phase == 3 || B->failed; });
+    if (J->phase != 3) return set_error(T3D_ERR_CUDA, "batched inner solve: " + B->fail_msg);
+    J->phase = 0;
+    return T3D_OK;
+}
+
+// mixed_solve (context.cu) with the inner solve batched: same stop test, inner target max(stop, 1e-5 |r64|) and
+// budget, so the same iterates.  *iters: inner iterations, or cg_max_it when the budget ran out unconverged.
+int job_solve(Batch* B, Job* J, int* iters) {
+    t3d_context* c = J->c;
+    const Grid& g = c->g;
+    const double tol = (double)c->prm.cg_tol;
+    const int maxit = c->prm.cg_max_it;
+    launch_cells_to32(g, c->E, c->E32, c->st);
+    launch_dot(g, 3, c->b, c->b, c->slot[3], c->scal + 5, c->st);
+    c->launches += 2;
+    T3D_CUDA_OK(cudaMemcpyAsync(c->scal_h + 5, c->scal + 5, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CHECK(sync(c));
+    const double nb = std::sqrt(c->scal_h[5]);
+    const double stop = (1.0e-30 < nb ? nb : 1.0e-30) * tol;
+    int budget = maxit, used = 0, outer = 0;
+    bool converged = false;
+    for (; outer < BATCH_MAX_OUTER; ++outer) {
+        c->launches += 1 + matvec64(c, c->u, c->Ap, RedSlot{nullptr, nullptr}, nullptr);
+        launch_mixed_residual(g, c->b, c->Ap, c->r32, c->d32, c->slot[3], c->scal + 6, c->st);
+        CHECK(launch_check("mixed residual"));
+        T3D_CUDA_OK(cudaMemcpyAsync(c->scal_h + 6, c->scal + 6, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+        CHECK(sync(c));
+        const double rn = std::sqrt(c->scal_h[6]);
+        if (rn < stop) {
+            converged = true;
+            break;
+        }
+        if (budget <= 0) break;
+        PcgScalars init{};
+        init.stop = std::max(stop, 1e-5 * rn);
+        init.tol = tol;
+        init.first = 1;
+        init.maxit = budget;
+        CHECK(request_inner(B, J, init));
+        launch_mixed_accumulate(g, c->u, c->d32, c->st);
+        c->launches += 1;
+        T3D_CUDA_OK(cudaMemcpyAsync(c->S_h, c->S32, sizeof(PcgScalars), cudaMemcpyDeviceToHost, c->st));
+        CHECK(sync(c));
+        used += c->S_h->it;
+        budget -= c->S_h->it;
     }
-    T3D_CUDA_OK(cudaStreamSynchronize(B->st));
-    for (int i = 0; i < n; ++i) {
-        const double nb = std::sqrt(B->hscal[i]);
-        stop[(size_t)i] = (1.0e-30 < nb ? nb : 1.0e-30) * (double)B->m[i]->prm.cg_tol;
-        budget[(size_t)i] = B->m[i]->prm.cg_max_it;
-    }
-    for (int pass = 0; pass < BATCH_MAX_OUTER; ++pass) {
-        for (int i = 0; i < n; ++i) {
-            if (!active[(size_t)i]) continue;
-            t3d_context* c = B->m[i];
-            c->launches += 1 + matvec64(c, c->u, c->Ap, RedSlot{nullptr, nullptr}, nullptr);
-            launch_mixed_residual(c->g, c->b, c->Ap, c->r32, c->d32, c->slot[3], c->scal + 6, B->st);
-            T3D_CUDA_OK(cudaMemcpyAsync(B->hscal + i, c->scal + 6, sizeof(double), cudaMemcpyDeviceToHost, B->st));
-        }
-        CHECK(launch_check("batched residual"));
-        T3D_CUDA_OK(cudaStreamSynchronize(B->st));
-        bool any = false;
-        for (int i = 0; i < n; ++i) {
-            if (!active[(size_t)i]) continue;
-            rn[(size_t)i] = std::sqrt(B->hscal[i]);
-            if (rn[(size_t)i] < stop[(size_t)i]) {
-                conv[(size_t)i] = 1;
-                active[(size_t)i] = 0;
-            } else if (budget[(size_t)i] <= 0) {
-                active[(size_t)i] = 0;
-            } else {
-                any = true;
-                ++outer[(size_t)i];
-            }
-        }
-        if (!any) break;
-        // per-member inner-solve scalars; members not iterating are masked (done, nothing left to apply)
-        for (int i = 0; i < n; ++i) {
-            PcgScalars& h = B->hS[i];
-            std::memset(&h, 0, sizeof h);
-            if (active[(size_t)i]) {
-                h.stop = std::max(stop[(size_t)i], 1e-5 * rn[(size_t)i]);
-                h.tol = (double)B->m[i]->prm.cg_tol;
-                h.first = 1;
-                h.maxit = budget[(size_t)i];
-            } else {
-                h.done = 1;
-            }
-            T3D_CUDA_OK(cudaMemcpyAsync(B->m[i]->S32, &h, sizeof h, cudaMemcpyHostToDevice, B->st));
-        }
-        launch_batch_compact(B->djobs, (int)B->jobs.size(), B->st);   // the members iterating in this pass
-        batch_vcycle(B);   // z = M r for them
-        B->launches += B->iter_kernels - 3;
-        for (int i = 0; i < n; ++i)
-            if (active[(size_t)i]) {
-                const t3d_context* c = B->m[i];
-                T3D_CUDA_OK(cudaMemcpyAsync(c->p32, c->z32, 3 * c->g.NNp * sizeof(float), cudaMemcpyDeviceToDevice,
-                                            B->st));
-            }
-        int longest = 0;
-        for (int i = 0; i < n; ++i)
-            if (active[(size_t)i]) longest = std::max(longest, budget[(size_t)i]);
-        for (int chunk = 0;; ++chunk) {
-            T3D_CUDA_OK(cudaGraphLaunch(B->graph, B->st));
-            B->launches += (int64_t)BATCH_CHUNK * B->iter_kernels + 1;
-            launch_batch_flags(B->dS, n, B->dflags, B->st);
-            T3D_CUDA_OK(cudaMemcpyAsync(B->hflags, B->dflags, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, B->st));
-            T3D_CUDA_OK(cudaStreamSynchronize(B->st));
-            bool all = true;
-            for (int i = 0; i < n; ++i) all = all && B->hflags[i] != 0;
-            if (all) break;
-            // every member stops by its own budget on the device (PcgScalars::maxit); this bound never binds
-            if ((int64_t)(chunk + 1) * BATCH_CHUNK > (int64_t)longest + BATCH_CHUNK)
-                return set_error(T3D_ERR_NUMERIC, "batched inner solve did not stop within its budget");
-        }
-        for (int i = 0; i < n; ++i) {
-            if (!active[(size_t)i]) continue;
-            t3d_context* c = B->m[i];
-            launch_mixed_accumulate(c->g, c->u, c->d32, B->st);
+    c->last_outer = outer;
+    *iters = converged ? used : maxit;
+    return T3D_OK;
+}
+
+void job_main(Batch* B, Job* J) {
+    cudaSetDevice(B->dev);
+    t3d_context* c = J->c;
+    int rc = T3D_OK;
+    for (int k = 0; k < J->steps && rc == T3D_OK; ++k) {
+        rc = design_pre(c);
+        int its = 0;
+        if (rc == T3D_OK) rc = job_solve(B, J, &its);
+        if (rc == T3D_OK) {
+            launch_compliance64(c->g, c->Ke, c->E, c->u, c->ce, c->slot[0], c->scal + 0, c->st);
             c->launches += 1;
-            T3D_CUDA_OK(cudaMemcpyAsync(B->hS + i, c->S32, sizeof(PcgScalars), cudaMemcpyDeviceToHost, B->st));
+            t3d_iter_record r{};
+            rc = design_post(c, its, &r);
+            if (rc == T3D_OK) J->recs.push_back(r);
         }
+    }
+    std::lock_guard<std::mutex> lk(B->mu);
+    J->rc = rc;
+    if (rc != T3D_OK) J->err = t3d_last_error();
+    J->finished = true;
+    B->cv.notify_all();
+}
+
+int member_index(const Batch* B, const t3d_context* c) {
+    for (size_t i = 0; i < B->m.size(); ++i)
+        if (B->m[i] == c) return (int)i;
+    return -1;
+}
+
+// the scheduler's start of one member's inner solve (solve loop of mixed_solve: scalars, z = M r, p = z), issued
+// on the batch stream with the member's own kernels
+int start_inner(Batch* B, Job* J) {
+    t3d_context* c = J->c;
+    T3D_CUDA_OK(cudaMemcpyAsync(c->S32, &J->init, sizeof(PcgScalars), cudaMemcpyHostToDevice, B->st));
+    const cudaStream_t own = c->st;
+    c->st = B->st;
+    const int rc = member_vcycle32(c, c->r32, c->z32, c->S32, c->slot[2]);
+    c->st = own;
+    CHECK(rc);
+    T3D_CUDA_OK(cudaMemcpyAsync(c->p32, c->z32, 3 * c->g.NNp * sizeof(float), cudaMemcpyDeviceToDevice, B->st));
+    return launch_check("batched solve start");
+}
+
+}  // namespace
+
+// masks member c out of the batched launches until its first inner solve starts
+static int mask_member(Batch* B, t3d_context* c) {
+    PcgScalars h{};
+    h.done = 1;
+    T3D_CUDA_OK(cudaMemcpyAsync(c->S32, &h, sizeof h, cudaMemcpyHostToDevice, B->st));
+    return T3D_OK;
+}
+
+// The scheduler.  Between chunks: adds submitted members (and starts their threads) and drops finished
+// submitted ones, rebuilds the launch lists and the graph when membership changed, starts the requested
+// inner solves, then replays one chunk for the members solving and hands the finished ones back to their
+// threads.  Returns when every job has finished (`submitted` false: the jobs of t3d_batch_run) or, for
+// submitted work, once stop is set and nothing is left to run.
+static int schedule(Batch* B, bool submitted) {
+    for (;;) {
+        std::vector<Job*> starting, adding, dropping;
+        bool solving = false;
+        {
+            std::unique_lock<std::mutex> lk(B->mu);
+            auto any = [&](auto pred) {
+                for (auto& j : B->jobs)
+                    if (pred(*j)) return true;
+                return false;
+            };
+            auto done = [&] {
+                const bool running = any([](const Job& j) { return !j.finished; });
+                return submitted ? (B->stop && !running && B->incoming.empty()) : !running;
+            };
+            auto work = [&] {
+                return any([](const Job& j) { return j.phase == 1 || j.phase == 2; }) || !B->incoming.empty() ||
+                       any([&](const Job& j) { return j.finished && j.release && member_index(B, j.c) >= 0; }) ||
+                       done();
+            };
+            B->cv.wait(lk, work);
+            if (!any([](const Job& j) { return j.phase == 1 || j.phase == 2; }) && B->incoming.empty() &&
+                !any([&](const Job& j) { return j.finished && j.release && member_index(B, j.c) >= 0; }) && done())
+                return T3D_OK;
+            for (auto& j : B->incoming) {
+                adding.push_back(j.get());
+                B->jobs.push_back(std::move(j));
+            }
+            B->incoming.clear();
+            for (auto& j : B->jobs) {
+                if (j->finished && j->release && member_index(B, j->c) >= 0) dropping.push_back(j.get());
+                if (j->phase == 1) {
+                    j->phase = 2;
+                    starting.push_back(j.get());
+                }
+                solving = solving || j->phase == 2;
+            }
+        }
+        // membership
+        for (Job* J : dropping) {
+            if (J->th.joinable()) J->th.join();
+            B->m.erase(B->m.begin() + member_index(B, J->c));
+            B->dirty = true;
+        }
+        for (Job* J : adding) {
+            B->m.push_back(J->c);
+            int rc = batch_members_check(B);
+            if (rc == T3D_OK) rc = mask_member(B, J->c);
+            if (rc != T3D_OK) {
+                B->m.pop_back();
+                std::lock_guard<std::mutex> lk(B->mu);
+                J->rc = rc;
+                J->err = t3d_last_error();
+                J->finished = true;
+                continue;
+            }
+            if (B->m.size() == 1) B->kh = J->c->kh;
+            B->dirty = true;
+            J->started = true;
+            J->th = std::thread(job_main, B, J);
+        }
+        if (!dropping.empty()) {
+            std::lock_guard<std::mutex> lk(B->mu);
+            B->cv.notify_all();   // finished submitted jobs are now collectable
+        }
+        if (B->dirty) CHECK(batch_lists(B));
+        for (Job* J : starting) CHECK(start_inner(B, J));
+        if (!solving) continue;
+        CHECK(batch_graph(B));
+        launch_batch_compact(B->dcompact, (int)B->compact.size(), B->st);   // the members solving in this chunk
+        T3D_CUDA_OK(cudaGraphLaunch(B->graph, B->st));
+        B->launches += (int64_t)BATCH_CHUNK * B->iter_kernels + 2;
+        const int n = (int)B->m.size();
+        launch_batch_flags(B->dS, n, B->dflags, B->st);
+        T3D_CUDA_OK(cudaMemcpyAsync(B->hflags, B->dflags, (size_t)n * sizeof(int), cudaMemcpyDeviceToHost, B->st));
         T3D_CUDA_OK(cudaStreamSynchronize(B->st));
-        for (int i = 0; i < n; ++i) {
-            if (!active[(size_t)i]) continue;
-            used[(size_t)i] += B->hS[i].it;
-            budget[(size_t)i] -= B->hS[i].it;
+        std::lock_guard<std::mutex> lk(B->mu);
+        for (auto& j : B->jobs) {
+            if (j->phase != 2) continue;
+            const int i = member_index(B, j->c);
+            if (i >= 0 && B->hflags[i]) j->phase = 3;
         }
+        B->cv.notify_all();
     }
-    for (int i = 0; i < n; ++i) {
-        iters[i] = conv[(size_t)i] ? used[(size_t)i] : B->m[i]->prm.cg_max_it;
-        B->m[i]->last_outer = outer[(size_t)i];
-    }
+}
+
+static void fail(Batch* B, int rc) {
+    std::lock_guard<std::mutex> lk(B->mu);
+    B->failed = true;
+    B->fail_msg = t3d_last_error();
+    (void)rc;
+    B->cv.notify_all();
+}
+
+static int check_batch_tma(Batch* B) {
+    if (!B->err) return T3D_OK;
     int e = 0;
     T3D_CUDA_OK(cudaMemcpy(&e, B->err, sizeof(int), cudaMemcpyDeviceToHost));
     if (e) return set_error(T3D_ERR_CUDA, "batched TMA-staged K(E)p: an mbarrier wait timed out");
     return T3D_OK;
 }
 
-static int batch_design_step(Batch* B, t3d_iter_record* recs) {
+// steps[i] design iterations of member i, every member on its own thread, the inner solves batched;
+// recs: the members' records one after another (steps[0] of member 0, then member 1's, ...)
+static int batch_run(Batch* B, const int* steps, t3d_iter_record* recs) {
+    if (B->sched.joinable()) return set_error(T3D_ERR_INVALID, "the batch is serving submitted work");
     if (B->m.empty()) return T3D_OK;
     if (B->dirty) CHECK(batch_lists(B));
-    CHECK(for_members(B, [&](int i) -> int {
-        t3d_context* c = B->m[i];
-        CHECK(design_pre(c));
-        T3D_CUDA_OK(cudaStreamSynchronize(c->st));
-        return T3D_OK;
-    }));
-    std::vector<int> its(B->m.size(), 0);
-    CHECK(batch_solve(B, its.data()));
-    return for_members(B, [&](int i) -> int {
-        t3d_context* c = B->m[i];
-        launch_compliance64(c->g, c->Ke, c->E, c->u, c->ce, c->slot[0], c->scal + 0, c->st);
-        c->launches += 1;
-        return design_post(c, its[(size_t)i], recs ? recs + i : nullptr);
-    });
+    for (t3d_context* c : B->m) CHECK(mask_member(B, c));
+    T3D_CUDA_OK(cudaStreamSynchronize(B->st));
+    for (t3d_context* c : B->m) {
+        std::unique_ptr<Job> J(new Job());
+        J->c = c;
+        J->steps = steps ? steps[B->jobs.size()] : 1;
+        B->jobs.push_back(std::move(J));
+    }
+    for (auto& J : B->jobs) {
+        J->started = true;
+        J->th = std::thread(job_main, B, J.get());
+    }
+    int rc = schedule(B, false);
+    if (rc != T3D_OK) fail(B, rc);
+    for (auto& J : B->jobs)
+        if (J->th.joinable()) J->th.join();
+    std::string msg;
+    int jrc = T3D_OK;
+    size_t k = 0;
+    for (size_t i = 0; i < B->jobs.size(); ++i) {
+        Job& J = *B->jobs[i];
+        if (J.rc != T3D_OK && jrc == T3D_OK) {
+            jrc = J.rc;
+            msg = "batch member " + std::to_string(i) + ": " + J.err;
+        }
+        if (recs)
+            for (const t3d_iter_record& r : J.recs) recs[k++] = r;
+    }
+    B->jobs.clear();
+    const bool failed = B->failed;
+    B->failed = false;
+    if (rc != T3D_OK) return rc;
+    if (failed) return set_error(T3D_ERR_CUDA, B->fail_msg);
+    if (jrc != T3D_OK) return set_error(jrc, msg);
+    return check_batch_tma(B);
 }
 
 }  // namespace t3d
@@ -636,6 +792,7 @@ int t3d_batch_open(int device, t3d_batch** out) {
 
 int t3d_batch_adopt(t3d_batch* b, t3d_context* ctx) {
     if (!b || !ctx) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    if (b->sched.joinable()) return t3d::set_error(T3D_ERR_INVALID, "the batch is serving submitted work");
     if (!ctx->design_ready) return t3d::set_error(T3D_ERR_INVALID, "t3d_design_init not called on the context");
     for (const t3d_context* c : b->m)
         if (c == ctx) return t3d::set_error(T3D_ERR_INVALID, "context is already a batch member");
@@ -655,6 +812,7 @@ int t3d_batch_adopt(t3d_batch* b, t3d_context* ctx) {
 int t3d_batch_release(t3d_batch* b, int i, t3d_context** out) {
     if (!b || !out || i < 0 || i >= (int)b->m.size()) return t3d::set_error(T3D_ERR_INVALID, "bad batch member");
     if (i < b->n_arena) return t3d::set_error(T3D_ERR_INVALID, "member lives in the batch arena");
+    if (b->sched.joinable()) return t3d::set_error(T3D_ERR_INVALID, "the batch is serving submitted work");
     if (cudaSetDevice(b->dev) != cudaSuccess) return t3d::set_error(T3D_ERR_CUDA, "cudaSetDevice failed");
     if (cudaStreamSynchronize(b->st) != cudaSuccess) return t3d::set_error(T3D_ERR_CUDA, "batch stream failed");
     *out = b->m[(size_t)i];
@@ -680,7 +838,75 @@ int t3d_batch_design_init(t3d_batch* b, const float* V0, double* c_solid) {
 int t3d_batch_design_step(t3d_batch* b, t3d_iter_record* recs) {
     if (!b) return t3d::set_error(T3D_ERR_INVALID, "null batch");
     if (cudaSetDevice(b->dev) != cudaSuccess) return t3d::set_error(T3D_ERR_CUDA, "cudaSetDevice failed");
-    return t3d::batch_design_step(b, recs);
+    return t3d::batch_run(b, nullptr, recs);
+}
+
+int t3d_batch_run(t3d_batch* b, const int* steps, t3d_iter_record* recs) {
+    if (!b || !steps) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    for (size_t i = 0; i < b->m.size(); ++i)
+        if (steps[i] < 0) return t3d::set_error(T3D_ERR_INVALID, "negative step count");
+    if (cudaSetDevice(b->dev) != cudaSuccess) return t3d::set_error(T3D_ERR_CUDA, "cudaSetDevice failed");
+    return t3d::batch_run(b, steps, recs);
+}
+
+int t3d_batch_submit(t3d_batch* b, t3d_context* ctx, int steps) {
+    if (!b || !ctx || steps < 0) return t3d::set_error(T3D_ERR_INVALID, "bad argument");
+    if (!ctx->design_ready) return t3d::set_error(T3D_ERR_INVALID, "t3d_design_init not called on the context");
+    if (ctx->dev != b->dev) return t3d::set_error(T3D_ERR_INVALID, "context is on another device");
+    std::lock_guard<std::mutex> lk(b->mu);
+    if (b->stop) return t3d::set_error(T3D_ERR_INVALID, "the batch is shutting down");
+    if (!b->sched.joinable() && !b->m.empty())
+        return t3d::set_error(T3D_ERR_INVALID, "submitted work needs a batch without members (t3d_batch_open)");
+    std::unique_ptr<t3d::Job> J(new t3d::Job());
+    J->c = ctx;
+    J->steps = steps;
+    J->release = true;
+    b->incoming.push_back(std::move(J));
+    if (!b->sched.joinable()) {
+        t3d::Batch* B = b;
+        b->sched = std::thread([B] {
+            cudaSetDevice(B->dev);
+            const int rc = t3d::schedule(B, true);
+            if (rc != T3D_OK) t3d::fail(B, rc);
+        });
+    }
+    b->cv.notify_all();
+    return T3D_OK;
+}
+
+int t3d_batch_collect(t3d_batch* b, int timeout_ms, t3d_context** ctx, t3d_iter_record* recs, int cap, int* nrec,
+                      int* status) {
+    if (!b || !ctx || !nrec || !status) return t3d::set_error(T3D_ERR_INVALID, "null argument");
+    *ctx = nullptr;
+    *nrec = 0;
+    *status = T3D_OK;
+    std::unique_lock<std::mutex> lk(b->mu);
+    auto ready = [&]() -> int {
+        for (size_t i = 0; i < b->jobs.size(); ++i) {
+            const t3d::Job& J = *b->jobs[i];
+            if (J.release && J.finished && t3d::member_index(b, J.c) < 0) return (int)i;
+        }
+        return -1;
+    };
+    int k = ready();
+    if (k < 0 && !b->failed)
+        b->cv.wait_for(lk, std::chrono::milliseconds(timeout_ms > 0 ? timeout_ms : 0),
+                       [&] { return (k = ready()) >= 0 || b->failed; });
+    if (k < 0) {
+        if (b->failed) return t3d::set_error(T3D_ERR_CUDA, "batch scheduler: " + b->fail_msg);
+        return T3D_OK;   // nothing finished yet
+    }
+    std::unique_ptr<t3d::Job> J = std::move(b->jobs[(size_t)k]);
+    b->jobs.erase(b->jobs.begin() + k);
+    lk.unlock();
+    if (J->th.joinable()) J->th.join();
+    *ctx = J->c;
+    const int n = std::min<int>(cap, (int)J->recs.size());
+    for (int i = 0; i < n && recs; ++i) recs[i] = J->recs[(size_t)i];
+    *nrec = n;
+    *status = J->rc;
+    if (J->rc != T3D_OK) t3d::set_error(J->rc, J->err);
+    return T3D_OK;
 }
 
 int t3d_batch_info(t3d_batch* b, int64_t* info) {
@@ -697,6 +923,20 @@ int t3d_batch_info(t3d_batch* b, int64_t* info) {
 }
 
 int t3d_batch_destroy(t3d_batch* b) {
+    if (!b) return T3D_OK;
+    if (b->sched.joinable()) {   // submitted work: let the running jobs finish, then stop the scheduler
+        {
+            std::lock_guard<std::mutex> lk(b->mu);
+            b->stop = true;
+            b->cv.notify_all();
+        }
+        b->sched.join();
+        for (auto& J : b->jobs) {
+            if (J->th.joinable()) J->th.join();
+            if (t3d::member_index(b, J->c) < 0) delete J->c;   // finished and released, never collected
+        }
+        for (auto& J : b->incoming) delete J->c;
+    }
     delete b;
     return T3D_OK;
 }

@@ -857,6 +857,11 @@ static void vcycle32(Context* c, const float* r, float* z, PcgScalars* S, RedSlo
     launch_prolong_smooth0_32(c->lv32[1], c->lv32[0], c->lv32[1].x, r, z, c->prm.mg_weight, dot, S, c->st);
 }
 
+int member_vcycle32(Context* c, const float* r, float* z, PcgScalars* S, RedSlot dot) {
+    vcycle32(c, r, z, S, dot);
+    return launch_check("V-cycle");
+}
+
 static void pcg32_iteration(Context* c) {
     c->launches += 2;
     matvec32(c, c->p32, c->Ap32, c->slot[0], c->S32);

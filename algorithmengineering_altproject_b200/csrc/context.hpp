@@ -171,6 +171,8 @@ int design_init(Context* c, float V0, double* Csolid);
 // K(E) u = b with the compliance into c->scal[0] ... design_post (objective, sensitivities, filter, OC, record)
 int design_pre(Context* c);
 int design_post(Context* c, int pcg_iters, t3d_iter_record* rec);
+// z = M r: one FP32 V-cycle of the mixed-precision inner solve (either cycle) on c->st
+int member_vcycle32(Context* c, const float* r, float* z, PcgScalars* S, RedSlot dot);
 
 }  // namespace t3d
 

@@ -251,54 +251,44 @@ class DesignServer:
         fut.set_result(res)
 
     def _engine(self):
-        """The batched engine: one design iteration of every request in the batch per step; initialised
-        requests join between steps, finished ones leave (their context released and closed)."""
-        B = None
-        live = []                                  # (Problem, request, result, future, need), batch order
+        """The batched engine: requests initialised on their worker threads are submitted to one t3d batch,
+        where each advances on its own (host thread and stream) and only the inner PCG solves share the
+        batched launches; finished ones come back through collect()."""
+        B = Batch.open(self.device)
+        live = {}                                  # problem handle -> (request, result, future, need)
         try:
-            B = Batch.open(self.device)
             while True:
                 with self._cv:
-                    while not self._joining and not live and not self._engine_closed:
-                        self._cv.wait()
-                    if not self._joining and not live:
-                        return
                     joining, self._joining = self._joining, []
-                for item in joining:
+                    closing = self._engine_closed
+                for P, req, res, fut, need in joining:
                     try:
-                        B.adopt(item[0])
-                        live.append(item)
+                        B.submit(P, req.iters)
+                        live[P._h.value] = (req, res, fut, need)
                     except T3DError as e:
-                        item[0].close()
-                        item[2].error = str(e)
-                        self._finish(item[2], item[3], item[4])
-                if not live:
-                    continue
-                try:
-                    recs = B.design_step()
-                except Exception as e:             # the step failed for the whole batch: end every request in it
-                    for k in range(len(live) - 1, -1, -1):
-                        P, _, res, fut, need = live.pop(k)
-                        B.release(k).close()
-                        res.error = "%s: %s" % (type(e).__name__, e)
+                        P.close()
+                        res.error = str(e)
                         self._finish(res, fut, need)
+                if not live:
+                    if closing and not joining:
+                        return
+                    with self._cv:
+                        self._cv.wait_for(lambda: self._joining or self._engine_closed, timeout=0.5)
                     continue
-                for (P, req, res, fut, need), r in zip(live, recs):
-                    res.objectives.append(r["obj"])
-                    res.pcg_iters.append(r["pcg_iters"])
-                for k in range(len(live) - 1, -1, -1):
-                    P, req, res, fut, need = live[k]
-                    if len(res.objectives) < req.iters:
-                        continue
-                    live.pop(k)
-                    P = B.release(k)
-                    if req.keep_density:
-                        res.density = P.density()
-                    P.close()
-                    self._finish(res, fut, need)
+                got = B.collect(50)
+                if got is None:
+                    continue
+                P, recs, err = got
+                req, res, fut, need = live.pop(P._h.value)
+                res.objectives = [r["obj"] for r in recs]
+                res.pcg_iters = [r["pcg_iters"] for r in recs]
+                res.error = err
+                if req.keep_density and err is None:
+                    res.density = P.density()
+                P.close()
+                self._finish(res, fut, need)
         finally:
-            if B is not None:
-                B.close()
+            B.close()
 
     def _create(self, req):
         kw = dict(device=self.device, precision=self.precision, oc_sum_order=T3D_SUM_FP64, **self.params)

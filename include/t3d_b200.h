@@ -248,6 +248,19 @@ int  t3d_batch_release(struct t3d_batch* b, int i, struct t3d_context** out);
 int  t3d_batch_design_init(struct t3d_batch* b, const float* V0, double* c_solid);
 /* one design iteration of every member: recs[n] */
 int  t3d_batch_design_step(struct t3d_batch* b, t3d_iter_record* recs);
+/* steps[i] design iterations of member i; recs receives member 0's records, then member 1's, ... (sum of
+ * steps).  Members advance independently (each on its own host thread and stream); only their inner solves
+ * share the batched launches, so a member with a short solve does not wait for one with a long solve. */
+int  t3d_batch_run(struct t3d_batch* b, const int* steps, t3d_iter_record* recs);
+/* Submitted work (a request loop), on a batch from t3d_batch_open: t3d_batch_submit hands over a context
+ * created and initialised alone (t3d_design_init) to run `steps` design iterations in the batch, starting at
+ * once; t3d_batch_collect waits up to timeout_ms for a finished one and returns its context (the caller's
+ * again: destroy it), its records (up to cap) and its status in *status (*ctx NULL: none finished yet).
+ * t3d_batch_destroy waits for submitted work still running.  While submitted work exists, t3d_batch_run,
+ * t3d_batch_design_step, t3d_batch_adopt and t3d_batch_release are refused. */
+int  t3d_batch_submit(struct t3d_batch* b, struct t3d_context* ctx, int steps);
+int  t3d_batch_collect(struct t3d_batch* b, int timeout_ms, struct t3d_context** ctx, t3d_iter_record* recs, int cap,
+                       int* nrec, int* status);
 /* info[0] arena bytes, [1] members, [2] batched kernel launches so far, [3] kernels of one batched PCG
  * iteration, [4] logical blocks of one batched PCG iteration, [5] member kernels launched so far */
 int  t3d_batch_info(struct t3d_batch* b, int64_t* info);

@@ -60,7 +60,7 @@ def test_batch_members_equal_their_solo_runs(regime):
     info = B.info()
     B.close()
     # one launch per kernel of the PCG iteration for all members: far fewer than the members' own launches
-    assert 5 <= info["kernels_per_iteration"] <= 20
+    assert 5 <= info["kernels_per_iteration"] <= 40
     assert info["batched_launches"] > 0
     for i, c in enumerate(CASES):
         cs1, recs1, x1, u1 = run_alone(t3d, c, steps, **R)
@@ -147,3 +147,56 @@ def test_arena_members_cannot_be_released():
     with pytest.raises(t3d.T3DError, match="arena"):
         B.release(0)
     B.close()
+
+
+def test_run_with_uneven_step_counts():
+    """t3d_batch_run: members run different numbers of design iterations, each advancing on its own; every
+    member equals its solo run."""
+    import algorithmengineering_altproject_b200 as t3d
+    cases = CASES[:3]
+    steps = [2, 4, 1]
+    R = REGIMES["standard"]
+    B = t3d.Batch([c["dims"] for c in cases], problems=[spec(t3d, c) for c in cases], **COMMON, **R)
+    B.design_init([c["V0"] for c in cases])
+    recs = B.run(steps)
+    x = [m.density() for m in B.members]
+    B.close()
+    for i, c in enumerate(cases):
+        assert len(recs[i]) == steps[i]
+        _, recs1, x1, _ = run_alone(t3d, c, steps[i], **R)
+        for a, b in zip(recs[i], recs1):
+            same_records(a, b)
+        np.testing.assert_array_equal(x[i], x1)
+
+
+def test_submitted_work_is_collected_with_solo_results():
+    """Submitted work (the request loop's engine): contexts initialised alone are submitted with their own
+    iteration counts and collected when done; results equal the solo runs."""
+    import algorithmengineering_altproject_b200 as t3d
+    cases = CASES
+    steps = [3, 1, 2, 4]
+    B = t3d.Batch.open()
+    subs = {}
+    for i, c in enumerate(cases):
+        P = t3d.Problem(*c["dims"], problem=spec(t3d, c), precision=t3d.T3D_MIXED,
+                        matvec32_tile=t3d.T3D_BATCH_TILE, **COMMON)
+        P.design_init(c["V0"])
+        B.submit(P, steps[i])
+        subs[id(P)] = i
+    got = {}
+    while len(got) < len(cases):
+        r = B.collect(1000)
+        if r is None:
+            continue
+        P, recs, err = r
+        assert err is None, err
+        got[subs[id(P)]] = (recs, P.density())
+        P.close()
+    B.close()
+    for i, c in enumerate(cases):
+        recs, x = got[i]
+        assert len(recs) == steps[i]
+        _, recs1, x1, _ = run_alone(t3d, c, steps[i])
+        for a, b in zip(recs, recs1):
+            same_records(a, b)
+        np.testing.assert_array_equal(x, x1)
