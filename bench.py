@@ -333,7 +333,7 @@ def run_batch_mode(args):
     t0 = time.perf_counter()
     B = t3d.Batch(dims, problems=[q.spec() for q in reqs], **common)
     t_create = time.perf_counter() - t0
-    B.design_init([q.V0 for q in reqs])
+    bcs = B.design_init([q.V0 for q in reqs])
     torch.cuda.synchronize(dev)
     l0 = B.info()
     t0 = time.perf_counter()
@@ -342,13 +342,14 @@ def run_batch_mode(args):
     t_batch = time.perf_counter() - t0
     info = B.info()
     bobj = np.array([[r["obj"] for r in brecs[i]] for i in range(len(reqs))])
+    bits = np.array([[r["pcg_iters"] for r in brecs[i]] for i in range(len(reqs))])
     B.close()
 
     def alone(precision, **kw):
-        total, objs, its = 0.0, [], []
+        total, objs, its, css = 0.0, [], [], []
         for q in reqs:
             P = t3d.Problem(q.nely, q.nelx, q.nelz, problem=q.spec(), precision=precision, **common, **kw)
-            P.design_init(q.V0)
+            css.append(P.design_init(q.V0))
             torch.cuda.synchronize(dev)
             t0 = time.perf_counter()
             recs = [P.design_step() for _ in range(K)]
@@ -357,10 +358,10 @@ def run_batch_mode(args):
             objs.append([r["obj"] for r in recs])
             its.append([r["pcg_iters"] for r in recs])
             P.close()
-        return total, np.array(objs), np.array(its)
+        return total, np.array(objs), np.array(its), np.array(css)
 
-    t_mixed, mobj, _ = alone(t3d.T3D_MIXED, matvec32_tile=t3d.T3D_BATCH_TILE)
-    t_fp64, fobj, fits = alone(t3d.T3D_FP64)
+    t_mixed, mobj, mits, mcs = alone(t3d.T3D_MIXED, matvec32_tile=t3d.T3D_BATCH_TILE)
+    t_fp64, fobj, fits, _ = alone(t3d.T3D_FP64)
     # the same designs through the request loop's streams engine (one context and stream each, 12 in flight, all
     # submitted at once): wall time to the last result with K iterations each minus the same with none (creation
     # and the solid-domain solve), so that like the other arms it counts the design iterations only
@@ -380,7 +381,11 @@ def run_batch_mode(args):
     its = len(reqs) * K
     rate = lambda t: its / t
     # bit-identity with the solo runs (NaN-aware), and the compliance error against FP64 per instance
-    mismatch = [k for k in range(len(reqs)) if not np.array_equal(bobj[k], mobj[k], equal_nan=True)]
+    mismatch = [k for k in range(len(reqs)) if not np.array_equal(bobj[k], mobj[k], equal_nan=True)
+                or bcs[k] != mcs[k]]
+    mismatch_detail = [{"instance": k, "dims": list(dims[k]), "c_solid": [repr(bcs[k]), repr(mcs[k])],
+                        "obj_batched": [repr(v) for v in bobj[k]], "obj_solo": [repr(v) for v in mobj[k]],
+                        "pcg_batched": bits[k].tolist(), "pcg_solo": mits[k].tolist()} for k in mismatch]
     with np.errstate(divide="ignore", invalid="ignore"):
         rel = np.nanmax(np.abs(fobj - bobj) / np.abs(fobj), axis=1)
     capped = [k for k in range(len(reqs)) if (fits[k] >= REGIMES[args.regime]["cg_max_it"]).any()]
@@ -400,7 +405,7 @@ def run_batch_mode(args):
         "designs_per_s_at_40_iters": {"batched": rate(t_batch) / 40, "sequential_mixed": rate(t_mixed) / 40,
                                       "sequential_fp64": rate(t_fp64) / 40},
         "speedup_vs_sequential_fp64": t_fp64 / t_batch, "speedup_vs_sequential_mixed": t_mixed / t_batch,
-        "batched_equals_solo_mixed": not mismatch, "instances_differing_from_solo": mismatch,
+        "batched_equals_solo_mixed": not mismatch, "instances_differing_from_solo": mismatch_detail,
         "compliance_rel_err_vs_fp64": worst,
         "batched_launches": info["batched_launches"] - l0["batched_launches"],
         "member_launches": info["member_launches"] - l0["member_launches"],
