@@ -3,8 +3,8 @@
 //
 // Layout.  The members' buffers are carved from one device arena (sized by a first, counting creation of each
 // member).  Each member keeps its own context -- grid, MG hierarchy, FP32/FP64 vectors, reduction slots and
-// scalars -- so everything outside the inner solve runs per member on the member's stream, in parallel host
-// threads (SIMP, MG rebuild, compliance, sensitivities, filter, OC).
+// scalars -- so everything outside the inner solve runs per member on the member's own host thread and stream
+// (SIMP, MG rebuild, the FP64 defect correction, compliance, sensitivities, filter, OC): see "the engine".
 //
 // Work list.  Every kernel of the FP32 MG-PCG iteration is one persistent launch over (instance, logical
 // block) items (kernels.hpp, "batched launches"): the logical blocks of an instance are the blocks of the
@@ -16,9 +16,8 @@
 // captured once in a CUDA graph and replayed; the host polls the members' done flags (gathered into one
 // array) after each replay.
 //
-// The FP64 defect-correction loop around the inner solve (mixed_solve in context.cu) is run for all members
-// in lock step: one true-residual pass for the members still iterating, one batched inner solve, one
-// accumulation, and again, each member with its own stop test and iteration budget.
+// The FP64 defect-correction loop around each inner solve is the single-design one (mixed_solve in context.cu),
+// run by the member's thread, so members do not wait for one another between inner solves.
 #include <atomic>
 #include <chrono>
 #include <cmath>

@@ -9,6 +9,8 @@
 // matrices of the coarse levels (FP32 images of the FP64 set-up), and K_0 = the modal FP32 K(E) of the moduli
 // the hierarchy was built from.  Level 0's vectors are pitched (Grid::px rows, MgLevel32::pitch/cs); the
 // coarse levels' are not.  Every kernel skips its work once S->done (the inner PCG converged).
+#include <type_traits>
+
 #include "kernels.hpp"
 #include "red.cuh"
 
@@ -30,11 +32,111 @@ __device__ __forceinline__ int64_t vidx(const MgLevel32& L, int64_t n) {
     return (n / nnx) * L.pitch + n % nnx;
 }
 
+template <class V>
+__device__ __forceinline__ float& lane_of(V& v, int k) {
+    return reinterpret_cast<float*>(&v)[k];
+}
+template <class V>
+__device__ __forceinline__ float lane_of(const V& v, int k) {
+    return reinterpret_cast<const float*>(&v)[k];
+}
+
+// x = w r / D on the pitched finest level: 4 consecutive row entries per thread (16-byte loads and stores of the
+// pitched vectors; the row's pads past x = nx stay zero).  Same arithmetic per DOF as the generic loop.
+__device__ __forceinline__ void jacobi_init0_32(VB vb, const MgLevel32& L, const float* __restrict__ r,
+                                               float* __restrict__ x, float w) {
+    const int fnx = L.nx + 1, q4 = L.pitch >> 2;
+    const int64_t rows = (int64_t)(L.ny + 1) * (L.nz + 1), per_c = rows * q4;
+    for (int64_t t = (int64_t)vb.b * blockDim.x + threadIdx.x; t < 3 * per_c; t += (int64_t)vb.n * blockDim.x) {
+        const int c = (int)(t / per_c);
+        const int64_t rt = t - c * per_c, row = rt / q4;
+        const int x0 = 4 * (int)(rt - row * q4);
+        const int64_t i = c * L.cs + row * L.pitch + x0;
+        const float4 rv = *reinterpret_cast<const float4*>(r + i), dv = *reinterpret_cast<const float4*>(L.diag + i);
+        float4 o = make_float4(0.f, 0.f, 0.f, 0.f);
+        const uint8_t* mk = L.mask + row * fnx;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int fx = x0 + k;
+            if (fx < fnx && !((mk[fx] >> c) & 1)) lane_of(o, k) = (w * lane_of(rv, k)) * lane_of(dv, k);
+        }
+        *reinterpret_cast<float4*>(x + i) = o;
+    }
+}
+
+// xo = xi + P xc on the pitched finest level.  A thread takes a run of SP consecutive fine nodes of one row that
+// share one coarse cell (fine x = SP j + k; the row's last node, x = nx, clamped to the last coarse cell, is a run
+// of its own): the cell's 8 corners are loaded once for the run and its nodes move as one SP-wide vector.
+// Consecutive threads take consecutive runs across row ends.  Same weights and accumulation order per node as
+// the generic loop of prolong_add32.
+template <int SP>
+__device__ __forceinline__ void prolong_add0_32(VB vb, const MgLevel32& Lc, const MgLevel32& Lf,
+                                                const float* __restrict__ xc, const float* xi, float* xo) {
+    using V = typename std::conditional<SP == 4, float4, float2>::type;
+    const int fnx = Lf.nx + 1, fny = Lf.ny + 1, cnx = Lc.nx + 1, cny = Lc.ny + 1;
+    const int runs = Lc.nx + 1;   // Lf.nx = SP Lc.nx: Lc.nx runs of SP nodes and the last node
+    const int64_t total = (int64_t)runs * fny * (Lf.nz + 1);
+    for (int64_t t = (int64_t)vb.b * blockDim.x + threadIdx.x; t < total; t += (int64_t)vb.n * blockDim.x) {
+        const int64_t row = t / runs;
+        const int j = (int)(t - row * runs);
+        const int fz = (int)(row / fny), fy = (int)(row - (int64_t)fz * fny);
+        const bool last = j == Lc.nx;
+        const int cx = last ? Lc.nx - 1 : j;
+        int cy = fy / SP, cz = fz / SP;
+        if (cy >= Lc.ny) cy = Lc.ny - 1;
+        if (cz >= Lc.nz) cz = Lc.nz - 1;
+        float X[3][8];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int A = 0; A < 8; ++A)
+                X[c][A] = xc[c * Lc.cs + ((int64_t)(cz + corner_dz(A)) * cny + cy + corner_dy(A)) * cnx + cx +
+                             corner_dx(A)];
+        const uint8_t* mk = Lf.mask + row * fnx;
+        if (last) {   // x = nx: one node
+            const int fx = Lf.nx, m = mk[fx];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                float p = 0.0f;
+#pragma unroll
+                for (int A = 0; A < 8; ++A)
+                    p = fmaf(tri_wf(SP, fx - cx * SP, fy - cy * SP, fz - cz * SP, A), X[c][A], p);
+                const int64_t i = c * Lf.cs + row * Lf.pitch + fx;
+                xo[i] = ((m >> c) & 1) ? 0.0f : xi[i] + p;
+            }
+            continue;
+        }
+        const int64_t rb = row * Lf.pitch + SP * j;
+        int m[SP];
+#pragma unroll
+        for (int k = 0; k < SP; ++k) m[k] = mk[SP * j + k];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const V v = *reinterpret_cast<const V*>(xi + c * Lf.cs + rb);
+            V o;
+#pragma unroll
+            for (int k = 0; k < SP; ++k) {
+                const int fx = SP * j + k;
+                float p = 0.0f;
+#pragma unroll
+                for (int A = 0; A < 8; ++A)
+                    p = fmaf(tri_wf(SP, fx - cx * SP, fy - cy * SP, fz - cz * SP, A), X[c][A], p);
+                lane_of(o, k) = ((m[k] >> c) & 1) ? 0.0f : lane_of(v, k) + p;
+            }
+            *reinterpret_cast<V*>(xo + c * Lf.cs + rb) = o;
+        }
+    }
+}
+
 // x = w r / D
 // (kernel bodies take the logical block VB, so that the batched launches below run them unchanged)
 __device__ __forceinline__ void jacobi_init32(VB vb, const MgLevel32& L, const float* __restrict__ r,
                                               float* __restrict__ x, float w, const PcgScalars* S) {
     if (S->done) return;
+    if (L.pitch != L.nx + 1) {   // the pitched finest level
+        jacobi_init0_32(vb, L, r, x, w);
+        return;
+    }
     for (int64_t n = (int64_t)vb.b * blockDim.x + threadIdx.x; n < L.nn; n += (int64_t)vb.n * blockDim.x) {
         const int m = L.mask[n];
         const int64_t v = vidx(L, n);
@@ -93,6 +195,11 @@ __device__ __forceinline__ void prolong_add32(VB vb, const MgLevel32& Lc, const 
                                               const float* __restrict__ xc, const float* xi, float* xo,
                                               const PcgScalars* S) {
     if (S->done) return;
+    if (Lf.pitch != Lf.nx + 1 && (Lc.span == 2 || Lc.span == 4) && Lf.nx == Lc.span * Lc.nx) {   // pitched level 0
+        if (Lc.span == 4) prolong_add0_32<4>(vb, Lc, Lf, xc, xi, xo);
+        else prolong_add0_32<2>(vb, Lc, Lf, xc, xi, xo);
+        return;
+    }
     const int s = Lc.span;
     const int fnx = Lf.nx + 1, fny = Lf.ny + 1, cnx = Lc.nx + 1, cny = Lc.ny + 1;
     for (int64_t n = (int64_t)vb.b * blockDim.x + threadIdx.x; n < Lf.nn; n += (int64_t)vb.n * blockDim.x) {

@@ -442,12 +442,19 @@ __global__ void __launch_bounds__(RED_THREADS) k_prolong_smooth0_32(MgLevel32 Lc
     prolong_smooth0_32<SP>(vb_real(), Lc, Lf, xc, r, z, w, dot, S, sh);
 }
 
-// coarsest level: FP64 inverse applied to the FP32 residual in FP64, or the Jacobi fallback
+// coarsest level: FP64 inverse applied to the FP32 residual in FP64, or the Jacobi fallback.  Dense form: a block
+// of COARSE_THREADS computes 32 outputs, its warps splitting the inner index into contiguous ranges (loads of X
+// coalesced across the 32 outputs), then warp 0 adds the warps' partial sums in warp order.
+constexpr int COARSE_THREADS = 256, COARSE_WARPS = COARSE_THREADS / 32;
+__host__ __device__ inline int coarse_blocks(int N, int64_t nn) {
+    return N > 0 ? (N + 31) / 32 : (int)(nn + COARSE_THREADS - 1) / COARSE_THREADS;
+}
 __device__ __forceinline__ void coarse_solve32(VB vb, const MgLevel32& L, const double* __restrict__ X, int N,
-                                               const int* __restrict__ status, const PcgScalars* S, double* rs) {
+                                               const int* __restrict__ status, const PcgScalars* S, double* rs,
+                                               double* part) {
     if (S->done) return;
     const int64_t nn = L.nn;
-    if (*status != 1) {
+    if (N == 0 || *status != 1) {
         for (int64_t n = (int64_t)vb.b * blockDim.x + threadIdx.x; n < nn; n += (int64_t)vb.n * blockDim.x) {
             const int m = L.mask[n];
             for (int c = 0; c < 3; ++c)
@@ -457,17 +464,25 @@ __device__ __forceinline__ void coarse_solve32(VB vb, const MgLevel32& L, const 
     }
     for (int j = threadIdx.x; j < N; j += blockDim.x) rs[j] = (double)L.r[(j % 3) * nn + j / 3];
     __syncthreads();
-    const int i = vb.b * blockDim.x + threadIdx.x;
-    if (i >= N) return;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int i = vb.b * 32 + lane;
+    const int per = (N + COARSE_WARPS - 1) / COARSE_WARPS, j0 = w * per, j1 = min(N, j0 + per);
     double acc = 0.0;
-    for (int j = 0; j < N; ++j) acc = fma(X[(int64_t)j * N + i], rs[j], acc);
-    const int ni = i / 3, ci = i % 3;
-    L.x[ci * nn + ni] = ((L.mask[ni] >> ci) & 1) ? 0.0f : (float)acc;
+    if (i < N)
+        for (int j = j0; j < j1; ++j) acc = fma(X[(int64_t)j * N + i], rs[j], acc);
+    part[w * 32 + lane] = acc;
+    __syncthreads();
+    if (w == 0 && i < N) {
+        double t = 0.0;
+        for (int k = 0; k < COARSE_WARPS; ++k) t += part[k * 32 + lane];
+        const int ni = i / 3, ci = i % 3;
+        L.x[ci * nn + ni] = ((L.mask[ni] >> ci) & 1) ? 0.0f : (float)t;
+    }
 }
-__global__ void __launch_bounds__(128) k_coarse_solve32(MgLevel32 L, const double* __restrict__ X, int N,
-                                                        const int* __restrict__ status, const PcgScalars* S) {
+__global__ void __launch_bounds__(COARSE_THREADS) k_coarse_solve32(MgLevel32 L, const double* __restrict__ X, int N,
+                                                                   const int* __restrict__ status, const PcgScalars* S) {
     extern __shared__ double rs[];
-    coarse_solve32(vb_real(), L, X, N, status, S, rs);
+    coarse_solve32(vb_real(), L, X, N, status, S, rs, rs + (N > 0 ? N : 0));
 }
 
 // ---------------------------------------------------------------- PCG vector steps in FP32
@@ -627,12 +642,12 @@ __global__ void __launch_bounds__(RED_THREADS) k_batch_prolong0_32(const BatchPr
     });
 }
 
-__global__ void __launch_bounds__(128) k_batch_coarse32(const BatchCoarse* __restrict__ a,
-                                                        const int* __restrict__ act, int N) {
+__global__ void __launch_bounds__(COARSE_THREADS) k_batch_coarse32(const BatchCoarse* __restrict__ a,
+                                                                   const int* __restrict__ act, int N, int max_n) {
     extern __shared__ double rs[];
     batch_walk(a, act, N, [&](const BatchCoarse& A, VB vb) {
         const MgLevel32 L = A.L;
-        coarse_solve32(vb, L, A.X, A.N, A.status, A.S, rs);
+        coarse_solve32(vb, L, A.X, A.N, A.status, A.S, rs, rs + max_n);
     });
 }
 
@@ -658,10 +673,7 @@ int batch_blocks_restrict(const BatchRestrict& a, int stage) {
     return stage == 0 ? (int)blocks_for(Lc.nn, 256) : 0;
 }
 int batch_blocks_prolong(const BatchProlong& a) { return (int)blocks_for(a.Lf.nn, 256); }
-int batch_blocks_coarse(const BatchCoarse& a) {
-    const int64_t work = a.N > 0 ? a.N : a.L.nn;
-    return (int)std::max<int64_t>(1, (work + 127) / 128);
-}
+int batch_blocks_coarse(const BatchCoarse& a) { return std::max(1, coarse_blocks(a.N, a.L.nn)); }
 void launch_batch_flags(PcgScalars* const* S, int n, int* out, cudaStream_t s) {
     k_batch_flags<<<1, 256, 0, s>>>(S, n, out);
 }
@@ -684,7 +696,9 @@ void launch_batch_prolong0_32(const BatchProlong0* a, const int* act, int N, cud
     k_batch_prolong0_32<<<BATCH_GRID, RED_THREADS, 0, s>>>(a, act, N);
 }
 void launch_batch_coarse32(const BatchCoarse* a, const int* act, int N, int max_n, cudaStream_t s) {
-    k_batch_coarse32<<<2 * BATCH_GRID, 128, (size_t)(max_n > 0 ? max_n : 1) * sizeof(double), s>>>(a, act, N);
+    const int mn = max_n > 0 ? max_n : 0;
+    k_batch_coarse32<<<BATCH_GRID, COARSE_THREADS, (size_t)(mn + 32 * COARSE_WARPS) * sizeof(double), s>>>(a, act, N,
+                                                                                                           mn);
 }
 
 void launch_nodes_to32(const Grid& g, const double* a, float* b, cudaStream_t s) {
@@ -737,9 +751,9 @@ void launch_prolong_smooth0_32(const MgLevel32& Lc, const MgLevel32& Lf, const f
 }
 void launch_coarse_solve32(const MgLevel32& L, const double* X, int N, const int* status, const PcgScalars* S,
                            cudaStream_t s) {
-    const int64_t work = N > 0 ? N : L.nn;
-    const unsigned blocks = (unsigned)((work + 127) / 128 > 0 ? (work + 127) / 128 : 1);
-    k_coarse_solve32<<<blocks, 128, (size_t)(N > 0 ? N : 1) * sizeof(double), s>>>(L, X, N, status, S);
+    const unsigned blocks = (unsigned)std::max(1, coarse_blocks(N, L.nn));
+    k_coarse_solve32<<<blocks, COARSE_THREADS, (size_t)((N > 0 ? N : 0) + 32 * COARSE_WARPS) * sizeof(double), s>>>(
+        L, X, N, status, S);
 }
 void launch_pcg_update32(const Grid& g, float* x, float* r, const float* p, const float* Ap, RedSlot red,
                          PcgScalars* S, cudaStream_t s) {
