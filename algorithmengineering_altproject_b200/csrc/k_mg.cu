@@ -398,16 +398,21 @@ __global__ void k_coarse_assemble(MgLevel Lc, const double* __restrict__ Kce, do
 __global__ void __launch_bounds__(1024) k_cholesky(const double* __restrict__ A, double* __restrict__ LT,
                                                    double* __restrict__ Lrow, int N, int* status) {
     __shared__ int fail;
+    extern __shared__ double colj[];   // column j of the factor (N doubles)
     if (threadIdx.x == 0) fail = 0;
     for (int64_t t = threadIdx.x; t < (int64_t)N * N; t += blockDim.x) {
         const int jj = (int)(t / N), ii = (int)(t % N);   // LT[jj][ii] = A[ii][jj] (lower)
         LT[t] = ii >= jj ? A[(int64_t)ii * N + jj] : 0.0;
     }
     __syncthreads();
+    // Right-looking: when column j is reached, LT holds in its rows i >= j the entry A_ij minus the products
+    // L_ik L_jk of the earlier columns, subtracted one at a time in increasing k -- the very sequence of the
+    // left-looking sum s = A_ij - L_i0 L_j0 - L_i1 L_j1 - ... (coarsest.cpp:24-58), so the factor is the same
+    // bit for bit; the trailing updates of all later columns run in parallel.
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     for (int j = 0; j < N; ++j) {
         if (threadIdx.x == 0) {
-            double s = LT[(int64_t)j * N + j];
-            for (int k = 0; k < j; ++k) s = s - LT[(int64_t)k * N + j] * LT[(int64_t)k * N + j];
+            const double s = LT[(int64_t)j * N + j];
             if (s <= 0.0) fail = 1;
             else LT[(int64_t)j * N + j] = sqrt(s);
         }
@@ -415,9 +420,23 @@ __global__ void __launch_bounds__(1024) k_cholesky(const double* __restrict__ A,
         if (fail) break;
         const double ljj = LT[(int64_t)j * N + j];
         for (int i = j + 1 + threadIdx.x; i < N; i += blockDim.x) {
-            double s = LT[(int64_t)j * N + i];
-            for (int k = 0; k < j; ++k) s = s - LT[(int64_t)k * N + i] * LT[(int64_t)k * N + j];
-            LT[(int64_t)j * N + i] = s / ljj;
+            const double v = LT[(int64_t)j * N + i] / ljj;
+            LT[(int64_t)j * N + i] = v;
+            colj[i] = v;
+        }
+        __syncthreads();
+        for (int m = j + 1 + warp; m < N; m += nwarps) {   // column m, rows i >= m: subtract L_ij L_mj
+            const double lmj = colj[m];
+            double* __restrict__ Wm = LT + (int64_t)m * N;
+            int i = m + lane;
+            for (; i + 96 < N; i += 128) {   // four independent updates in flight per thread
+                const double w0 = Wm[i], w1 = Wm[i + 32], w2 = Wm[i + 64], w3 = Wm[i + 96];
+                Wm[i] = w0 - colj[i] * lmj;
+                Wm[i + 32] = w1 - colj[i + 32] * lmj;
+                Wm[i + 64] = w2 - colj[i + 64] * lmj;
+                Wm[i + 96] = w3 - colj[i + 96] * lmj;
+            }
+            for (; i < N; i += 32) Wm[i] = Wm[i] - colj[i] * lmj;
         }
         __syncthreads();
     }
@@ -529,7 +548,7 @@ void launch_coarse_assemble(const MgLevel& Lc, const double* Kce, double* Kc, cu
     k_coarse_assemble<<<blocks_for(N * N, 256), 256, 0, s>>>(Lc, Kce, Kc);
 }
 void launch_cholesky(const double* A, double* LT, double* Lrow, int N, int* status, cudaStream_t s) {
-    k_cholesky<<<1, 1024, 0, s>>>(A, LT, Lrow, N, status);
+    k_cholesky<<<1, 1024, (size_t)(N > 0 ? N : 1) * sizeof(double), s>>>(A, LT, Lrow, N, status);
 }
 void launch_coarse_inverse(const double* Lrow, int N, const int* status, double* X, cudaStream_t s) {
     const size_t smem = (size_t)N * INV_COLS * sizeof(double);   // N <= 1000: at most 128 KB

@@ -92,15 +92,23 @@ __device__ __forceinline__ void prolong_add0_32(VB vb, const MgLevel32& Lc, cons
             for (int A = 0; A < 8; ++A)
                 X[c][A] = xc[c * Lc.cs + ((int64_t)(cz + corner_dz(A)) * cny + cy + corner_dy(A)) * cnx + cx +
                              corner_dx(A)];
+        // the weights tri_wf(...) = w_x w_y w_z are products of multiples of 1/SP (SP = 2, 4): exact in any
+        // order, so w_y w_z is formed once per run and w_x per node, giving the same values bit for bit
+        constexpr float is = 1.0f / (float)SP;
+        const int ry = fy - cy * SP, rz = fz - cz * SP;
+        float wyz[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            wyz[q] = ((q & 1) ? ry * is : (SP - ry) * is) * ((q & 2) ? rz * is : (SP - rz) * is);
         const uint8_t* mk = Lf.mask + row * fnx;
-        if (last) {   // x = nx: one node
+        if (last) {   // x = nx: one node, all weight on the cell's upper x corners
             const int fx = Lf.nx, m = mk[fx];
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
                 float p = 0.0f;
 #pragma unroll
                 for (int A = 0; A < 8; ++A)
-                    p = fmaf(tri_wf(SP, fx - cx * SP, fy - cy * SP, fz - cz * SP, A), X[c][A], p);
+                    p = fmaf((corner_dx(A) ? 1.0f : 0.0f) * wyz[corner_dy(A) + 2 * corner_dz(A)], X[c][A], p);
                 const int64_t i = c * Lf.cs + row * Lf.pitch + fx;
                 xo[i] = ((m >> c) & 1) ? 0.0f : xi[i] + p;
             }
@@ -108,19 +116,23 @@ __device__ __forceinline__ void prolong_add0_32(VB vb, const MgLevel32& Lc, cons
         }
         const int64_t rb = row * Lf.pitch + SP * j;
         int m[SP];
+        float w[SP][8];
 #pragma unroll
-        for (int k = 0; k < SP; ++k) m[k] = mk[SP * j + k];
+        for (int k = 0; k < SP; ++k) {
+            m[k] = mk[SP * j + k];
+#pragma unroll
+            for (int A = 0; A < 8; ++A)
+                w[k][A] = (corner_dx(A) ? k * is : (SP - k) * is) * wyz[corner_dy(A) + 2 * corner_dz(A)];
+        }
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             const V v = *reinterpret_cast<const V*>(xi + c * Lf.cs + rb);
             V o;
 #pragma unroll
             for (int k = 0; k < SP; ++k) {
-                const int fx = SP * j + k;
                 float p = 0.0f;
 #pragma unroll
-                for (int A = 0; A < 8; ++A)
-                    p = fmaf(tri_wf(SP, fx - cx * SP, fy - cy * SP, fz - cz * SP, A), X[c][A], p);
+                for (int A = 0; A < 8; ++A) p = fmaf(w[k][A], X[c][A], p);
                 lane_of(o, k) = ((m[k] >> c) & 1) ? 0.0f : lane_of(v, k) + p;
             }
             *reinterpret_cast<V*>(xo + c * Lf.cs + rb) = o;

@@ -110,3 +110,31 @@ def test_every_modal_tile_shape_gives_identical_results(dims):
         np.testing.assert_array_equal(y, ref, err_msg="tile shape %d %s" % (v, shapes[-1]))
         P.close()
     assert len(shapes) >= 6 and any(s[3] == 2 for s in shapes), shapes   # the TMA-staged shapes are among them
+
+
+@pytest.mark.parametrize("dims", [(17, 40, 23), (30, 60, 30)])
+def test_every_tma_tile_shape_gives_the_same_standard_vcycle(dims):
+    """The Standard V-cycle fuses its level-0 residual and correction into the TMA-staged K(E)u (epilogue modes
+    1 and 2): every TMA shape gives the same z bit for bit."""
+    import algorithmengineering_altproject_b200 as t3d
+    rng = np.random.default_rng(5)
+    ref, seen = None, 0
+    for v in range(64):
+        try:
+            P = t3d.Problem(*dims, precision=t3d.T3D_MIXED, mg_vcycle=t3d.T3D_VCYCLE_STANDARD, matvec32_tile=v + 1)
+        except t3d.T3DError:
+            break
+        if P.info().matvec32_tile[3] < 2:
+            P.close()
+            continue
+        if ref is None:
+            E = np.where(rng.random(P.ne) < 0.5, 1e-9, rng.uniform(0.01, 1.0, P.ne))
+            r = rng.standard_normal(P.nf)
+        P.make_diagonal_preconditioner_from_static(E)
+        z = P.vcycle32(r)
+        if ref is None:
+            ref = z
+        np.testing.assert_array_equal(z, ref, err_msg="tile shape %d" % v)
+        seen += 1
+        P.close()
+    assert seen >= 4
