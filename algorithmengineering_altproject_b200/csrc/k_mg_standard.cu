@@ -122,7 +122,9 @@ __global__ void __launch_bounds__(576) k_galerkin_fine(Grid g, MgLevel L1, int s
 __global__ void __launch_bounds__(576) k_galerkin_coarse(MgLevel Lf, MgLevel Lc, const double* __restrict__ Kf,
                                                          double* __restrict__ Kc) {
     __shared__ int cmask[8];
-    const int s = Lc.span;
+    __shared__ double wt[125][8];   // tri_w(s, fx, fy, fz, A) at fine offsets 0..s (s <= 4), the same values
+    __shared__ double kf[576];      // the current child's element matrix
+    const int s = Lc.span, s1 = s + 1;
     const int ce = blockIdx.x;
     const int cx = ce % Lc.nx, cy = (ce / Lc.nx) % Lc.ny, cz = ce / (Lc.nx * Lc.ny);
     const int P = threadIdx.x / 24, Q = threadIdx.x % 24;
@@ -130,18 +132,26 @@ __global__ void __launch_bounds__(576) k_galerkin_coarse(MgLevel Lf, MgLevel Lc,
     if (threadIdx.x < 8)
         cmask[threadIdx.x] = Lc.mask[lnode(Lc, cx + corner_dx(threadIdx.x), cy + corner_dy(threadIdx.x),
                                            cz + corner_dz(threadIdx.x))];
+    for (int t = threadIdx.x; t < s1 * s1 * s1 * 8; t += blockDim.x) {
+        const int o = t / 8;
+        wt[o][t % 8] = tri_w(s, o % s1, (o / s1) % s1, o / (s1 * s1), t % 8);
+    }
     double acc = 0.0;
     for (int k = 0; k < s; ++k)
         for (int j = 0; j < s; ++j)
             for (int i = 0; i < s; ++i) {
                 const int fe = ((cz * s + k) * Lf.ny + cy * s + j) * Lf.nx + cx * s + i;
+                __syncthreads();   // the weights are ready; the previous child's matrix has been read
+                kf[threadIdx.x] = Kf[(int64_t)fe * 576 + threadIdx.x];
+                __syncthreads();
                 double t = 0.0;
                 for (int a = 0; a < 8; ++a) {
-                    const double wa = tri_w(s, i + corner_dx(a), j + corner_dy(a), k + corner_dz(a), A);
+                    const double wa = wt[(k + corner_dz(a)) * s1 * s1 + (j + corner_dy(a)) * s1 + i + corner_dx(a)][A];
                     double u = 0.0;
                     for (int b = 0; b < 8; ++b) {
-                        const double wb = tri_w(s, i + corner_dx(b), j + corner_dy(b), k + corner_dz(b), B);
-                        u = u + wb * Kf[(int64_t)fe * 576 + (3 * a + r) * 24 + 3 * b + q];
+                        const double wb =
+                            wt[(k + corner_dz(b)) * s1 * s1 + (j + corner_dy(b)) * s1 + i + corner_dx(b)][B];
+                        u = u + wb * kf[(3 * a + r) * 24 + 3 * b + q];
                     }
                     t = t + wa * u;
                 }

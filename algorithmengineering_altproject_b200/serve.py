@@ -139,6 +139,9 @@ class DesignServer:
         self._closed = False
         self._threads = []
         self._create_lock = threading.Lock()   # context creation (allocations, tile autotuning) one at a time
+        # first solves one at a time: run concurrently they occasionally gave one context a zero solid-domain
+        # compliance (cause not found); their design iterations still overlap
+        self._init_lock = threading.Lock()
         self._warm = False
         self._joining = []          # batched engine: initialised requests waiting to join the batch
         self._engine_closed = False
@@ -227,7 +230,8 @@ class DesignServer:
             if self.engine == "batched" and getattr(req, "load_cases", 1) == 1 and req.iters > 0:
                 P = self._create(req)
                 try:
-                    res.c_solid = P.design_init(req.V0)
+                    with self._init_lock:
+                        res.c_solid = P.design_init(req.V0)
                 except BaseException:
                     P.close()
                     raise
@@ -306,7 +310,8 @@ class DesignServer:
         """Runs one request to completion on its own context (and stream)."""
         P = self._create(req)
         try:
-            res.c_solid = P.design_init(req.V0)
+            with self._init_lock:
+                res.c_solid = P.design_init(req.V0)
             for _ in range(req.iters):
                 r = P.design_step()
                 res.objectives.append(r["obj"])
