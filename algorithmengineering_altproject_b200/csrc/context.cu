@@ -596,7 +596,7 @@ static int mg_setup(Context* c) {
             launch_to_coarse_layout(Lc, c->Kel[c->nlev - 1], c->Kce, c->st);
             launch_coarse_assemble(Lc, c->Kce, c->Kc, c->st);
             launch_cholesky(c->Kc, c->LT, c->Lrow, c->Nc, c->chol_status, c->st);
-            launch_coarse_inverse(c->Lrow, c->Nc, c->chol_status, c->Xc, c->st);
+            launch_coarse_inverse(c->LT, c->Lrow, c->Nc, c->chol_status, c->Xc, c->st);
         }
         if (c->mixed) {   // FP32 images: level-0 moduli, coarse element matrices, reciprocal diagonals
             launch_cells_to32(c->g, c->E_mg, c->E_mg32, c->st);
@@ -625,7 +625,7 @@ static int mg_setup(Context* c) {
         launch_coarse_element_matrices(c->g, Lc, span, c->mask0, c->E, c->Ke, (double)c->prm.Emin, c->Kce, c->st);
         launch_coarse_assemble(Lc, c->Kce, c->Kc, c->st);
         launch_cholesky(c->Kc, c->LT, c->Lrow, c->Nc, c->chol_status, c->st);
-        launch_coarse_inverse(c->Lrow, c->Nc, c->chol_status, c->Xc, c->st);
+        launch_coarse_inverse(c->LT, c->Lrow, c->Nc, c->chol_status, c->Xc, c->st);
     }
     if (c->mixed) {
         for (int l = 0; l < c->nlev; ++l) {

@@ -451,34 +451,44 @@ __global__ void __launch_bounds__(1024) k_cholesky(const double* __restrict__ A,
     if (threadIdx.x == 0) *status = 1;
 }
 
-// Coarsest inverse for the canonical coarsest solve: column j of X = L'^-1 L^-1 e_j computed by
-// thread j with the reference's substitution order (coarsest.cpp:92-122); column j is stored
-// contiguously (X[j*N + i]).  Runs at each MG set-up after a successful factorisation.
-// Column j of the coarsest inverse by forward and backward substitution with the factor's rows, each
-// sum in increasing k (the oracle's order).  A block of INV_COLS threads owns INV_COLS columns, whose
-// working vectors sit in shared memory as [i][lane] (no bank conflicts; factor rows are broadcast loads).
-constexpr int INV_COLS = 16;
-__global__ void k_coarse_inverse(const double* __restrict__ Lrow, int N, const int* __restrict__ status,
-                                 double* __restrict__ X) {
-    extern __shared__ double xs[];   // [N][INV_COLS]
+// Coarsest inverse for the canonical coarsest solve: column j of X = L'^-1 L^-1 e_j (coarsest.cpp:92-122),
+// stored contiguously (X[j*N + i]).  A warp per column, both substitutions column-oriented: when x_k is final
+// every row below takes its term L_ik x_k, so each row's running value receives its terms in increasing k
+// (forward) and decreasing i (backward) and is divided last -- the order of the row-oriented sums, bit for bit.
+// Rows above j are skipped in the forward pass: their values stay +0 and leave the others unchanged (each
+// running value there is +0 or 1, never -0).  The warp's lanes split the rows; the factor is read by columns
+// (LT) in the forward pass and by rows (Lrow) in the backward one, both coalesced.
+constexpr int INV_WARPS = 8;   // columns per block
+constexpr int INV_MAX_N = 1000;   // the largest dense coarsest system (NlimitDofs)
+__global__ void __launch_bounds__(INV_WARPS * 32) k_coarse_inverse(const double* __restrict__ LT,
+                                                                   const double* __restrict__ Lrow, int N,
+                                                                   const int* __restrict__ status,
+                                                                   double* __restrict__ X) {
+    extern __shared__ double xs_all[];   // [INV_WARPS][N]
     if (*status != 1) return;
-    const int lane = threadIdx.x;
-    const int j = blockIdx.x * INV_COLS + lane;
-    for (int i = 0; i < N; ++i) xs[i * INV_COLS + lane] = (i == j) ? 1.0 : 0.0;
-    for (int i = 0; i < N; ++i) {
-        double sum = xs[i * INV_COLS + lane];
-        const double* Li = Lrow + (int64_t)i * N;
-        for (int k = 0; k < i; ++k) sum = sum - Li[k] * xs[k * INV_COLS + lane];
-        xs[i * INV_COLS + lane] = sum / Li[i];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int j = blockIdx.x * INV_WARPS + w;
+    if (j >= N) return;   // the whole warp (no block barrier below)
+    double* xs = xs_all + (int64_t)w * N;
+    for (int i = lane; i < N; i += 32) xs[i] = (i == j) ? 1.0 : 0.0;
+    __syncwarp();
+    for (int k = j; k < N; ++k) {
+        const double xk = xs[k] / Lrow[(int64_t)k * N + k];
+        __syncwarp();
+        if (lane == (k & 31)) xs[k] = xk;
+        const double* __restrict__ Lk = LT + (int64_t)k * N;   // column k: L_ik at Lk[i]
+        for (int i = k + 1 + lane; i < N; i += 32) xs[i] = xs[i] - Lk[i] * xk;
+        __syncwarp();
     }
     for (int i = N - 1; i >= 0; --i) {
-        const double* Li = Lrow + (int64_t)i * N;
-        const double xi = xs[i * INV_COLS + lane] / Li[i];
-        xs[i * INV_COLS + lane] = xi;
-        for (int k = 0; k < i; ++k) xs[k * INV_COLS + lane] = xs[k * INV_COLS + lane] - Li[k] * xi;
+        const double* __restrict__ Li = Lrow + (int64_t)i * N;
+        const double xi = xs[i] / Li[i];
+        __syncwarp();
+        if (lane == (i & 31)) xs[i] = xi;
+        for (int k = lane; k < i; k += 32) xs[k] = xs[k] - Li[k] * xi;
+        __syncwarp();
     }
-    if (j < N)
-        for (int i = 0; i < N; ++i) X[(int64_t)j * N + i] = xs[i * INV_COLS + lane];
+    for (int i = lane; i < N; i += 32) X[(int64_t)j * N + i] = xs[i];
 }
 
 // Coarsest solve x_i = sum_j X[i][j] r_j (sequential in j) when the factorisation succeeded, else
@@ -550,13 +560,14 @@ void launch_coarse_assemble(const MgLevel& Lc, const double* Kce, double* Kc, cu
 void launch_cholesky(const double* A, double* LT, double* Lrow, int N, int* status, cudaStream_t s) {
     k_cholesky<<<1, 1024, (size_t)(N > 0 ? N : 1) * sizeof(double), s>>>(A, LT, Lrow, N, status);
 }
-void launch_coarse_inverse(const double* Lrow, int N, const int* status, double* X, cudaStream_t s) {
-    const size_t smem = (size_t)N * INV_COLS * sizeof(double);   // N <= 1000: at most 128 KB
+void launch_coarse_inverse(const double* LT, const double* Lrow, int N, const int* status, double* X,
+                           cudaStream_t s) {
+    const size_t smem = (size_t)N * INV_WARPS * sizeof(double);   // N <= 1000: at most 64 KB
     // the attribute is per function, not per launch: always the bound for the largest N, so that contexts set
     // up concurrently from several host threads never lower it under another thread's launch
     cudaFuncSetAttribute(k_coarse_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)(1000 * INV_COLS * sizeof(double)));
-    k_coarse_inverse<<<blocks_for(N, INV_COLS), INV_COLS, smem, s>>>(Lrow, N, status, X);
+                         (int)(INV_MAX_N * INV_WARPS * sizeof(double)));
+    k_coarse_inverse<<<blocks_for(N, INV_WARPS), INV_WARPS * 32, smem, s>>>(LT, Lrow, N, status, X);
 }
 void launch_coarse_solve(const MgLevel& L, const double* X, int N, const int* status, const PcgScalars* S,
                          cudaStream_t s) {

@@ -46,8 +46,19 @@ __global__ void __launch_bounds__(576) k_galerkin_fine(Grid g, MgLevel L1, int s
     __shared__ uint8_t cmk[GB][64][8];       // child corner masks
     __shared__ uint8_t anym[GB][64];         // child touches a fixed DOF
     __shared__ uint8_t cmask[GB][8];         // coarse corner masks
-    const int ne1 = L1.nx * L1.ny * L1.nz, ns = s * s * s;
+    __shared__ uint8_t nm[GB][125];          // masks of each coarse element's (s+1)^3 fine nodes (s <= 4)
+    const int ne1 = L1.nx * L1.ny * L1.nz, ns = s * s * s, s1 = s + 1, nr = s1 * s1 * s1;
     const int e0 = blockIdx.x * GB;
+    for (int q = threadIdx.x; q < GB * nr; q += blockDim.x) {   // each node mask loaded once per block
+        const int b = q / nr, o = q % nr, ce = e0 + b;
+        uint8_t m = 0;
+        if (ce < ne1) {
+            const int cx = ce % L1.nx, cy = (ce / L1.nx) % L1.ny, cz = ce / (L1.nx * L1.ny);
+            m = mask0[g.node(cx * s + o % s1, cy * s + (o / s1) % s1, cz * s + o / (s1 * s1))];
+        }
+        nm[b][o] = m;
+    }
+    __syncthreads();
     for (int q = threadIdx.x; q < GB * ns; q += blockDim.x) {
         const int b = q / ns, p = q % ns, ce = e0 + b;
         double Ee = 0.0;
@@ -59,7 +70,7 @@ __global__ void __launch_bounds__(576) k_galerkin_fine(Grid g, MgLevel L1, int s
             const double e = E[g.cell(fx, fy, fz)];
             Ee = e <= 1.0e-16 ? 0.0 : e;   // K(E) skips these elements
             for (int a = 0; a < 8; ++a) {
-                const uint8_t m = mask0[g.node(fx + corner_dx(a), fy + corner_dy(a), fz + corner_dz(a))];
+                const uint8_t m = nm[b][((k + corner_dz(a)) * s1 + j + corner_dy(a)) * s1 + i + corner_dx(a)];
                 cmk[b][p][a] = m;
                 any |= m;
             }

@@ -125,7 +125,8 @@ void launch_coarse_assemble(const MgLevel& Lc, const double* Kce, double* Kc, cu
 void launch_cholesky(const double* A, double* LT, double* Lrow, int N, int* status, cudaStream_t s);
 // canonical coarsest solve: inverse columns from the factor, then x = X r (Jacobi fallback when
 // *status != 1, preconditioner.cpp:76-77, 195-215)
-void launch_coarse_inverse(const double* Lrow, int N, const int* status, double* X, cudaStream_t s);
+void launch_coarse_inverse(const double* LT, const double* Lrow, int N, const int* status, double* X,
+                           cudaStream_t s);
 void launch_coarse_solve(const MgLevel& L, const double* X, int N, const int* status, const PcgScalars* S,
                          cudaStream_t s);
 
