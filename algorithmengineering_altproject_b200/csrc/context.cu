@@ -577,7 +577,7 @@ static int download_cells_f32(Context* c, const float* cells, float* h) {
 // ------------------------------------------------------------------ multigrid
 // make_diagonal_preconditioner_from_static for the moduli in c->E (preconditioner.cpp:38-79)
 static int mg_setup(Context* c) {
-    c->launches += 1 + (c->nlev - 1) + (c->Nc ? 4 : 0);
+    c->launches += 1 + (c->nlev - 1) + (c->Nc ? 3 : 0);
     launch_diag0(c->g, c->Ke, c->E, c->mask0, c->lv[0].diag, c->st);
     if (c->standard) {   // Galerkin element matrices and their diagonals on every coarse level
         // the cycle's level-0 operator is K(E) of these moduli, so that a hierarchy kept between rebuilds
@@ -595,7 +595,7 @@ static int mg_setup(Context* c) {
             const MgLevel& Lc = c->lv[c->nlev - 1];
             launch_to_coarse_layout(Lc, c->Kel[c->nlev - 1], c->Kce, c->st);
             launch_coarse_assemble(Lc, c->Kce, c->Kc, c->st);
-            launch_cholesky(c->Kc, c->LT, c->Lrow, c->Nc, c->chol_status, c->st);
+            c->launches += launch_cholesky(c->Kc, c->LT, c->Lrow, c->Nc, c->chol_status, c->st);
             launch_coarse_inverse(c->LT, c->Lrow, c->Nc, c->chol_status, c->Xc, c->st);
         }
         if (c->mixed) {   // FP32 images: level-0 moduli, coarse element matrices, reciprocal diagonals
@@ -624,7 +624,7 @@ static int mg_setup(Context* c) {
         if (c->prm.mg_coarse_assembly == T3D_COARSE_FULL) span = c->g.nx / Lc.nx;
         launch_coarse_element_matrices(c->g, Lc, span, c->mask0, c->E, c->Ke, (double)c->prm.Emin, c->Kce, c->st);
         launch_coarse_assemble(Lc, c->Kce, c->Kc, c->st);
-        launch_cholesky(c->Kc, c->LT, c->Lrow, c->Nc, c->chol_status, c->st);
+        c->launches += launch_cholesky(c->Kc, c->LT, c->Lrow, c->Nc, c->chol_status, c->st);
         launch_coarse_inverse(c->LT, c->Lrow, c->Nc, c->chol_status, c->Xc, c->st);
     }
     if (c->mixed) {

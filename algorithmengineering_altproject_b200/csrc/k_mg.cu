@@ -392,51 +392,56 @@ __global__ void k_coarse_assemble(MgLevel Lc, const double* __restrict__ Kce, do
     Kc[t] = v;
 }
 
-// Left-looking Cholesky of the lower triangle with the row-oriented sums of coarsest.cpp:13-35:
+// Cholesky of the lower triangle with the row-oriented sums of coarsest.cpp:13-35:
 // L_ij = (A_ij - sum_{k<j} L_ik L_jk) / L_jj, L_jj = sqrt(A_jj - sum_{k<j} L_jk^2), sums in k order.
-// One CTA; columns in turn, rows of a column in parallel.  *status = 1 on success, 0 if not SPD.
-__global__ void __launch_bounds__(1024) k_cholesky(const double* __restrict__ A, double* __restrict__ LT,
-                                                   double* __restrict__ Lrow, int N, int* status) {
+// Factor column j is LT[j*N + i] = L_ij.  Blocked right-looking: when column j is reached, LT holds in its rows
+// i >= j the entry A_ij minus the products L_ik L_jk of the earlier columns, subtracted one at a time in
+// increasing k -- the very sequence of the left-looking sum s = A_ij - L_i0 L_j0 - L_i1 L_j1 - ...
+// (coarsest.cpp:24-58), so the factor is the same bit for bit.  Panels of CHOL_NB columns are factored by one
+// CTA in shared memory; the panel's products are then subtracted from all later columns, in increasing k, by
+// a grid of 32x32 tiles.  *status = 1 on success, 0 if not SPD (a non-positive pivot).
+constexpr int CHOL_NB = 32;                  // panel width
+constexpr int CHOL_SMEM_DOUBLES = 25600;     // panel bound: CHOL_NB x N doubles for N <= 800 (200 KB)
+constexpr int CHOL_TILE = 32;
+
+// LT = the lower triangle of A, transposed (column j contiguous); *status = 1
+__global__ void k_chol_init(const double* __restrict__ A, double* __restrict__ LT, int N, int* status) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t == 0) *status = 1;
+    if (t >= (int64_t)N * N) return;
+    const int jj = (int)(t / N), ii = (int)(t % N);   // LT[jj][ii] = A[ii][jj] (lower)
+    LT[t] = ii >= jj ? A[(int64_t)ii * N + jj] : 0.0;
+}
+
+// columns [k0, k1) of the factor, rows [k0, N): pan[c * R + o] = LT[(k0 + c) * N + k0 + o], R = N - k0
+__global__ void __launch_bounds__(1024) k_chol_panel(double* __restrict__ LT, int N, int k0, int k1, int* status) {
+    extern __shared__ double pan[];
     __shared__ int fail;
-    extern __shared__ double colj[];   // column j of the factor (N doubles)
-    if (threadIdx.x == 0) fail = 0;
-    for (int64_t t = threadIdx.x; t < (int64_t)N * N; t += blockDim.x) {
-        const int jj = (int)(t / N), ii = (int)(t % N);   // LT[jj][ii] = A[ii][jj] (lower)
-        LT[t] = ii >= jj ? A[(int64_t)ii * N + jj] : 0.0;
+    if (*status == 0) return;   // an earlier panel failed (the same value for every thread)
+    const int R = N - k0, W = k1 - k0;
+    for (int t = threadIdx.x; t < W * R; t += blockDim.x) {
+        const int c = t / R, o = t - c * R;
+        pan[t] = LT[(int64_t)(k0 + c) * N + k0 + o];
     }
+    if (threadIdx.x == 0) fail = 0;
     __syncthreads();
-    // Right-looking: when column j is reached, LT holds in its rows i >= j the entry A_ij minus the products
-    // L_ik L_jk of the earlier columns, subtracted one at a time in increasing k -- the very sequence of the
-    // left-looking sum s = A_ij - L_i0 L_j0 - L_i1 L_j1 - ... (coarsest.cpp:24-58), so the factor is the same
-    // bit for bit; the trailing updates of all later columns run in parallel.
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    for (int j = 0; j < N; ++j) {
+    for (int c = 0; c < W; ++c) {
+        double* col = pan + c * R;   // column j = k0 + c; its row i at col[i - k0]
         if (threadIdx.x == 0) {
-            const double s = LT[(int64_t)j * N + j];
+            const double s = col[c];
             if (s <= 0.0) fail = 1;
-            else LT[(int64_t)j * N + j] = sqrt(s);
+            else col[c] = sqrt(s);
         }
         __syncthreads();
         if (fail) break;
-        const double ljj = LT[(int64_t)j * N + j];
-        for (int i = j + 1 + threadIdx.x; i < N; i += blockDim.x) {
-            const double v = LT[(int64_t)j * N + i] / ljj;
-            LT[(int64_t)j * N + i] = v;
-            colj[i] = v;
-        }
+        const double ljj = col[c];
+        for (int o = c + 1 + threadIdx.x; o < R; o += blockDim.x) col[o] = col[o] / ljj;
         __syncthreads();
-        for (int m = j + 1 + warp; m < N; m += nwarps) {   // column m, rows i >= m: subtract L_ij L_mj
-            const double lmj = colj[m];
-            double* __restrict__ Wm = LT + (int64_t)m * N;
-            int i = m + lane;
-            for (; i + 96 < N; i += 128) {   // four independent updates in flight per thread
-                const double w0 = Wm[i], w1 = Wm[i + 32], w2 = Wm[i + 64], w3 = Wm[i + 96];
-                Wm[i] = w0 - colj[i] * lmj;
-                Wm[i + 32] = w1 - colj[i + 32] * lmj;
-                Wm[i + 64] = w2 - colj[i + 64] * lmj;
-                Wm[i + 96] = w3 - colj[i + 96] * lmj;
-            }
-            for (; i < N; i += 32) Wm[i] = Wm[i] - colj[i] * lmj;
+        // the panel's later columns m = k0 + d, rows i >= m: subtract L_ij L_mj
+        const int rest = W - c - 1;
+        for (int t = threadIdx.x; t < rest * R; t += blockDim.x) {
+            const int d = c + 1 + t / R, o = t % R;
+            if (o >= d) pan[d * R + o] = pan[d * R + o] - col[o] * col[d];
         }
         __syncthreads();
     }
@@ -444,11 +449,49 @@ __global__ void __launch_bounds__(1024) k_cholesky(const double* __restrict__ A,
         if (threadIdx.x == 0) *status = 0;
         return;
     }
-    for (int64_t t = threadIdx.x; t < (int64_t)N * N; t += blockDim.x) {
-        const int ii = (int)(t / N), jj = (int)(t % N);
-        Lrow[t] = jj <= ii ? LT[(int64_t)jj * N + ii] : 0.0;
+    for (int t = threadIdx.x; t < W * R; t += blockDim.x) {
+        const int c = t / R, o = t - c * R;
+        LT[(int64_t)(k0 + c) * N + k0 + o] = pan[t];
     }
-    if (threadIdx.x == 0) *status = 1;
+}
+
+// columns m >= k1, rows i >= m: subtract L_ij L_mj for the panel's columns j = k0..k1-1 in increasing j.
+// Block t is the lower-triangular tile (bm <= bi) of 32 columns m and 32 rows i.
+__global__ void __launch_bounds__(256) k_chol_trailing(double* __restrict__ LT, int N, int k0, int k1,
+                                                       const int* status) {
+    __shared__ double Pm[CHOL_NB][CHOL_TILE], Pi[CHOL_NB][CHOL_TILE];
+    if (*status == 0) return;
+    const int t = blockIdx.x;
+    int bi = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+    while ((bi + 1) * (bi + 2) / 2 <= t) ++bi;
+    while (bi * (bi + 1) / 2 > t) --bi;
+    const int bm = t - bi * (bi + 1) / 2;
+    const int m0 = k1 + bm * CHOL_TILE, i0 = k1 + bi * CHOL_TILE, W = k1 - k0;
+    for (int q = threadIdx.x; q < W * CHOL_TILE; q += blockDim.x) {
+        const int c = q / CHOL_TILE, x = q % CHOL_TILE;
+        const double* Lj = LT + (int64_t)(k0 + c) * N;
+        Pm[c][x] = m0 + x < N ? Lj[m0 + x] : 0.0;
+        Pi[c][x] = i0 + x < N ? Lj[i0 + x] : 0.0;
+    }
+    __syncthreads();
+    const int x = threadIdx.x % CHOL_TILE, y = threadIdx.x / CHOL_TILE;
+    const int i = i0 + x;
+    for (int u = y; u < CHOL_TILE; u += blockDim.x / CHOL_TILE) {
+        const int m = m0 + u;
+        if (m >= N || i >= N || i < m) continue;
+        double* w = LT + (int64_t)m * N + i;
+        double v = *w;
+        for (int c = 0; c < W; ++c) v = v - Pi[c][x] * Pm[c][u];
+        *w = v;
+    }
+}
+
+// Lrow = the factor by rows (Lrow[i*N + j] = L_ij, 0 above the diagonal), written only on success
+__global__ void k_chol_rows(const double* __restrict__ LT, double* __restrict__ Lrow, int N, const int* status) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)N * N || *status == 0) return;
+    const int ii = (int)(t / N), jj = (int)(t % N);
+    Lrow[t] = jj <= ii ? LT[(int64_t)jj * N + ii] : 0.0;
 }
 
 // Coarsest inverse for the canonical coarsest solve: column j of X = L'^-1 L^-1 e_j (coarsest.cpp:92-122),
@@ -557,8 +600,25 @@ void launch_coarse_assemble(const MgLevel& Lc, const double* Kce, double* Kc, cu
     const int64_t N = 3 * Lc.nn;
     k_coarse_assemble<<<blocks_for(N * N, 256), 256, 0, s>>>(Lc, Kce, Kc);
 }
-void launch_cholesky(const double* A, double* LT, double* Lrow, int N, int* status, cudaStream_t s) {
-    k_cholesky<<<1, 1024, (size_t)(N > 0 ? N : 1) * sizeof(double), s>>>(A, LT, Lrow, N, status);
+int launch_cholesky(const double* A, double* LT, double* Lrow, int N, int* status, cudaStream_t s) {
+    const int64_t NN = (int64_t)N * N;
+    k_chol_init<<<std::max(1u, blocks_for(NN, 256)), 256, 0, s>>>(A, LT, N, status);
+    int launches = 1;
+    if (N <= 0) return launches;
+    const int nb = std::max(1, std::min(CHOL_NB, CHOL_SMEM_DOUBLES / N));
+    // the attribute is per function, not per launch: always the bound, so that contexts set up concurrently
+    // from several host threads never lower it under another thread's launch
+    cudaFuncSetAttribute(k_chol_panel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(CHOL_SMEM_DOUBLES * sizeof(double)));
+    for (int k0 = 0; k0 < N; k0 += nb) {
+        const int k1 = std::min(k0 + nb, N);
+        k_chol_panel<<<1, 1024, (size_t)(k1 - k0) * (N - k0) * sizeof(double), s>>>(LT, N, k0, k1, status);
+        const int T = (N - k1 + CHOL_TILE - 1) / CHOL_TILE;
+        if (T > 0) k_chol_trailing<<<T * (T + 1) / 2, 256, 0, s>>>(LT, N, k0, k1, status);
+        launches += T > 0 ? 2 : 1;
+    }
+    k_chol_rows<<<blocks_for(NN, 256), 256, 0, s>>>(LT, Lrow, N, status);
+    return launches + 1;
 }
 void launch_coarse_inverse(const double* LT, const double* Lrow, int N, const int* status, double* X,
                            cudaStream_t s) {

@@ -37,18 +37,24 @@ __device__ __forceinline__ int lnode(const MgLevel& L, int x, int y, int z) {
 // level-1 element matrices from the finest grid: one CTA (576 threads, thread = entry (P, Q)) per GB
 // consecutive coarse elements (cz*ny1 + cy)*nx1 + cx, so that each G_pos entry is read once per batch;
 // children are summed in position order, masked ones by the explicit product
-constexpr int GB = 8;
-__global__ void __launch_bounds__(576) k_galerkin_fine(Grid g, MgLevel L1, int s, const double* __restrict__ E,
+constexpr int GB = 16;
+
+__global__ void __launch_bounds__(576, 1) k_galerkin_fine(Grid g, MgLevel L1, int s, const double* __restrict__ E,
                                                        const uint8_t* __restrict__ mask0,
                                                        const double* __restrict__ Gpos,
                                                        const double* __restrict__ Keg, double* __restrict__ Kel) {
-    __shared__ double Ec[GB][64];            // child moduli (0: skipped), s^3 <= 64
-    __shared__ uint8_t cmk[GB][64][8];       // child corner masks
-    __shared__ uint8_t anym[GB][64];         // child touches a fixed DOF
-    __shared__ uint8_t cmask[GB][8];         // coarse corner masks
-    __shared__ uint8_t nm[GB][125];          // masks of each coarse element's (s+1)^3 fine nodes (s <= 4)
+    __shared__ __align__(16) double Ec[64][GB];   // child moduli by position (0: skipped), s^3 <= 64
+    __shared__ uint8_t cmk[GB][64][8];            // child corner masks
+    __shared__ uint8_t anym[GB][64];              // child touches a fixed DOF
+    __shared__ uint8_t cmask[GB][8];              // coarse corner masks
+    __shared__ uint8_t nm[GB][125];               // masks of each coarse element's (s+1)^3 fine nodes (s <= 4)
+    __shared__ double wt[125][8];                 // tri_w(s, fx, fy, fz, A) at fine offsets 0..s: the same values
+    __shared__ double kg[576];                    // the fine element stiffness
+    __shared__ double us[576];                    // a masked child's inner sums u(a; r, B, q)
+    __shared__ int masked;                        // some child of the batch touches a fixed DOF
     const int ne1 = L1.nx * L1.ny * L1.nz, ns = s * s * s, s1 = s + 1, nr = s1 * s1 * s1;
     const int e0 = blockIdx.x * GB;
+    if (threadIdx.x == 0) masked = 0;
     for (int q = threadIdx.x; q < GB * nr; q += blockDim.x) {   // each node mask loaded once per block
         const int b = q / nr, o = q % nr, ce = e0 + b;
         uint8_t m = 0;
@@ -58,6 +64,11 @@ __global__ void __launch_bounds__(576) k_galerkin_fine(Grid g, MgLevel L1, int s
         }
         nm[b][o] = m;
     }
+    for (int t = threadIdx.x; t < nr * 8; t += blockDim.x) {
+        const int o = t / 8;
+        wt[o][t % 8] = tri_w(s, o % s1, (o / s1) % s1, o / (s1 * s1), t % 8);
+    }
+    kg[threadIdx.x] = Keg[threadIdx.x];
     __syncthreads();
     for (int q = threadIdx.x; q < GB * ns; q += blockDim.x) {
         const int b = q / ns, p = q % ns, ce = e0 + b;
@@ -75,8 +86,9 @@ __global__ void __launch_bounds__(576) k_galerkin_fine(Grid g, MgLevel L1, int s
                 any |= m;
             }
         }
-        Ec[b][p] = Ee;
+        Ec[p][b] = Ee;
         anym[b][p] = any;
+        if (any && Ee != 0.0) masked = 1;
     }
     for (int q = threadIdx.x; q < GB * 8; q += blockDim.x) {
         const int b = q / 8, A = q % 8, ce = e0 + b;
@@ -90,32 +102,67 @@ __global__ void __launch_bounds__(576) k_galerkin_fine(Grid g, MgLevel L1, int s
     __syncthreads();
     const int P = threadIdx.x / 24, Q = threadIdx.x % 24;
     const int A = P / 3, r = P % 3, B = Q / 3, q = Q % 3;
+    const double* __restrict__ gcol = Gpos + threadIdx.x;
     double acc[GB];
 #pragma unroll
     for (int b = 0; b < GB; ++b) acc[b] = 0.0;
-    for (int p = 0; p < ns; ++p) {
-        const double gp = Gpos[p * 576 + threadIdx.x];
-        const int i = p % s, j = (p / s) % s, k = p / (s * s);
+    if (!masked) {
+        // Every child is plain: acc_b += E_bp G_p[t] for all b in position order.  A skipped child (E_bp = 0)
+        // adds +-0, which leaves acc unchanged (acc starts at +0 and a sum never turns into -0), so the sums are
+        // those of the per-child test below.  The next four children's G_pos entries load while four are summed.
+        double gn[4];
 #pragma unroll
-        for (int b = 0; b < GB; ++b) {
-            const double Ee = Ec[b][p];
-            if (Ee == 0.0) continue;
-            if (!anym[b][p]) {
-                acc[b] = acc[b] + Ee * gp;
-            } else {   // sum_{a,b'} w_aA w_b'B M_ar M_b'q E Ke[3a+r][3b'+q]
-                double t = 0.0;
-                for (int a = 0; a < 8; ++a) {
-                    if ((cmk[b][p][a] >> r) & 1) continue;
-                    const double wa = tri_w(s, i + corner_dx(a), j + corner_dy(a), k + corner_dz(a), A);
+        for (int v = 0; v < 4; ++v) gn[v] = gcol[v * 576];   // ns = s^3 is 8 or 64
+        for (int p0 = 0; p0 < ns; p0 += 4) {
+            double gc[4];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) gc[v] = gn[v];
+            if (p0 + 4 < ns) {
+#pragma unroll
+                for (int v = 0; v < 4; ++v) gn[v] = gcol[(p0 + 4 + v) * 576];
+            }
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                const double2* e2 = reinterpret_cast<const double2*>(&Ec[p0 + v][0]);
+#pragma unroll
+                for (int h = 0; h < GB / 2; ++h) {
+                    const double2 e = e2[h];
+                    acc[2 * h] = acc[2 * h] + e.x * gc[v];
+                    acc[2 * h + 1] = acc[2 * h + 1] + e.y * gc[v];
+                }
+            }
+        }
+    } else {
+        for (int p = 0; p < ns; ++p) {
+            const double gp = gcol[p * 576];
+            const int i = p % s, j = (p / s) % s, k = p / (s * s);
+#pragma unroll
+            for (int b = 0; b < GB; ++b) {
+                const double Ee = Ec[p][b];
+                if (Ee == 0.0) continue;
+                if (!anym[b][p]) {
+                    acc[b] = acc[b] + Ee * gp;
+                } else {   // sum_{a,c} w_aA w_cB M_ar M_cq E Ke[3a+r][3c+q]
+                    // the inner sums u(a; r, B, q) = sum_c w_cB M_cq Ke[3a+r][3c+q] do not depend on A: thread
+                    // (3a+r, Q) forms its own once into us, and the outer sum over a reads them (the same terms in
+                    // the same order as summing u inside the loop over a).  The branch is the same for the block.
                     double u = 0.0;
                     for (int c = 0; c < 8; ++c) {
                         if ((cmk[b][p][c] >> q) & 1) continue;
-                        const double wc = tri_w(s, i + corner_dx(c), j + corner_dy(c), k + corner_dz(c), B);
-                        u = u + wc * Keg[(3 * a + r) * 24 + 3 * c + q];
+                        const double wc = wt[((k + corner_dz(c)) * s1 + j + corner_dy(c)) * s1 + i + corner_dx(c)][B];
+                        u = u + wc * kg[(3 * A + r) * 24 + 3 * c + q];
                     }
-                    t = t + wa * u;
+                    us[threadIdx.x] = u;
+                    __syncthreads();
+                    double t = 0.0;
+                    for (int a = 0; a < 8; ++a) {
+                        if ((cmk[b][p][a] >> r) & 1) continue;
+                        const double wa = wt[((k + corner_dz(a)) * s1 + j + corner_dy(a)) * s1 + i + corner_dx(a)][A];
+                        t = t + wa * us[(3 * a + r) * 24 + Q];
+                    }
+                    acc[b] = acc[b] + Ee * t;
+                    __syncthreads();   // us is rewritten by the next masked child
                 }
-                acc[b] = acc[b] + Ee * t;
             }
         }
     }
@@ -135,6 +182,7 @@ __global__ void __launch_bounds__(576) k_galerkin_coarse(MgLevel Lf, MgLevel Lc,
     __shared__ int cmask[8];
     __shared__ double wt[125][8];   // tri_w(s, fx, fy, fz, A) at fine offsets 0..s (s <= 4), the same values
     __shared__ double kf[576];      // the current child's element matrix
+    __shared__ double us[576];      // its inner sums u(a; r, B, q), entry (3a+r)*24 + 3B+q
     const int s = Lc.span, s1 = s + 1;
     const int ce = blockIdx.x;
     const int cx = ce % Lc.nx, cy = (ce / Lc.nx) % Lc.ny, cz = ce / (Lc.nx * Lc.ny);
@@ -147,28 +195,36 @@ __global__ void __launch_bounds__(576) k_galerkin_coarse(MgLevel Lf, MgLevel Lc,
         const int o = t / 8;
         wt[o][t % 8] = tri_w(s, o % s1, (o / s1) % s1, o / (s1 * s1), t % 8);
     }
+    // t = sum_a w_aA u(a; r, B, q) with u(a; r, B, q) = sum_b w_bB K_c[3a+r][3b+q]: u does not depend on A, so
+    // thread (3a+r, Q) forms its own once per child into us and the sum over a reads them -- the same terms in
+    // the same order as summing u inside the loop over a.  The next child's matrix entry loads meanwhile.
+    const int ns = s * s * s;
+    auto child = [&](int p) {
+        const int i = p % s, j = (p / s) % s, k = p / (s * s);
+        return ((int64_t)((cz * s + k) * Lf.ny + cy * s + j) * Lf.nx + cx * s + i) * 576 + threadIdx.x;
+    };
+    double knext = Kf[child(0)];
     double acc = 0.0;
-    for (int k = 0; k < s; ++k)
-        for (int j = 0; j < s; ++j)
-            for (int i = 0; i < s; ++i) {
-                const int fe = ((cz * s + k) * Lf.ny + cy * s + j) * Lf.nx + cx * s + i;
-                __syncthreads();   // the weights are ready; the previous child's matrix has been read
-                kf[threadIdx.x] = Kf[(int64_t)fe * 576 + threadIdx.x];
-                __syncthreads();
-                double t = 0.0;
-                for (int a = 0; a < 8; ++a) {
-                    const double wa = wt[(k + corner_dz(a)) * s1 * s1 + (j + corner_dy(a)) * s1 + i + corner_dx(a)][A];
-                    double u = 0.0;
-                    for (int b = 0; b < 8; ++b) {
-                        const double wb =
-                            wt[(k + corner_dz(b)) * s1 * s1 + (j + corner_dy(b)) * s1 + i + corner_dx(b)][B];
-                        u = u + wb * kf[(3 * a + r) * 24 + 3 * b + q];
-                    }
-                    t = t + wa * u;
-                }
-                acc = acc + t;
-            }
-    __syncthreads();
+    for (int p = 0; p < ns; ++p) {
+        const int i = p % s, j = (p / s) % s, k = p / (s * s);
+        kf[threadIdx.x] = knext;
+        __syncthreads();   // kf is complete (and the weights ready)
+        if (p + 1 < ns) knext = Kf[child(p + 1)];
+        double u = 0.0;
+        for (int b = 0; b < 8; ++b) {
+            const double wb = wt[(k + corner_dz(b)) * s1 * s1 + (j + corner_dy(b)) * s1 + i + corner_dx(b)][B];
+            u = u + wb * kf[(3 * A + r) * 24 + 3 * b + q];
+        }
+        us[threadIdx.x] = u;
+        __syncthreads();   // us is complete
+        double t = 0.0;
+        for (int a = 0; a < 8; ++a) {
+            const double wa = wt[(k + corner_dz(a)) * s1 * s1 + (j + corner_dy(a)) * s1 + i + corner_dx(a)][A];
+            t = t + wa * us[(3 * a + r) * 24 + Q];
+        }
+        acc = acc + t;
+        __syncthreads();   // kf and us are rewritten by the next child
+    }
     if (((cmask[A] >> r) & 1) || ((cmask[B] >> q) & 1)) acc = 0.0;
     Kc[(int64_t)ce * 576 + threadIdx.x] = acc;
 }

@@ -122,7 +122,8 @@ void launch_prolong_smooth0(const MgLevel& Lc, const MgLevel& Lf, const double* 
 void launch_coarse_element_matrices(const Grid& g0, const MgLevel& Lc, int span, const uint8_t* mask0, const double* E,
                                     const double* Ke, double emin, double* Kce, cudaStream_t s);
 void launch_coarse_assemble(const MgLevel& Lc, const double* Kce, double* Kc, cudaStream_t s);
-void launch_cholesky(const double* A, double* LT, double* Lrow, int N, int* status, cudaStream_t s);
+// returns the number of kernels it launched
+int launch_cholesky(const double* A, double* LT, double* Lrow, int N, int* status, cudaStream_t s);
 // canonical coarsest solve: inverse columns from the factor, then x = X r (Jacobi fallback when
 // *status != 1, preconditioner.cpp:76-77, 195-215)
 void launch_coarse_inverse(const double* LT, const double* Lrow, int N, const int* status, double* X,

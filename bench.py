@@ -35,6 +35,7 @@ import statistics
 import subprocess
 import sys
 import time
+import warnings
 
 import numpy as np
 
@@ -386,15 +387,23 @@ def run_batch_mode(args):
     mismatch_detail = [{"instance": k, "dims": list(dims[k]), "c_solid": [repr(bcs[k]), repr(mcs[k])],
                         "obj_batched": [repr(v) for v in bobj[k]], "obj_solo": [repr(v) for v in mobj[k]],
                         "pcg_batched": bits[k].tolist(), "pcg_solo": mits[k].tolist()} for k in mismatch]
-    with np.errstate(divide="ignore", invalid="ignore"):
+    with np.errstate(divide="ignore", invalid="ignore"), warnings.catch_warnings():
+        warnings.simplefilter("ignore", RuntimeWarning)   # an all-NaN row (a singular domain) gives NaN
         rel = np.nanmax(np.abs(fobj - bobj) / np.abs(fobj), axis=1)
     capped = [k for k in range(len(reqs)) if (fits[k] >= REGIMES[args.regime]["cg_max_it"]).any()]
-    order = np.argsort(-np.nan_to_num(rel, nan=np.inf))
-    worst = {"max": float(rel[order[0]]), "median": float(np.nanmedian(rel)),
-             "instances_over_1e-6": int(np.sum(~(rel <= 1e-6))),
-             "top": [{"instance": int(k), "dims": list(dims[k]), "rel_err": float(rel[k]),
-                      "fp64_pcg_capped": int(k) in capped} for k in order[:3]],
-             "fp64_solves_at_the_iteration_cap": len(capped)}
+    # the error is stated over the instances whose FP64 solves all converged; an instance whose FP64 solve
+    # stopped at the iteration cap (a singular domain) has no converged solution to compare with
+    conv = np.array([k for k in range(len(reqs)) if k not in capped], dtype=np.int64)
+    rc = rel[conv] if conv.size else np.array([np.nan])
+    order = conv[np.argsort(-np.nan_to_num(rc, nan=np.inf))] if conv.size else conv
+    worst = {"over": "instances whose FP64 solves converged", "instances": int(conv.size),
+             "max": float(np.nanmax(rc)) if np.isfinite(rc).any() else None,
+             "median": float(np.nanmedian(rc)) if np.isfinite(rc).any() else None,
+             "instances_over_1e-6": int(np.sum(~(rc <= 1e-6))),
+             "top": [{"instance": int(k), "dims": list(dims[k]), "rel_err": float(rel[k])} for k in order[:3]],
+             "fp64_solves_at_the_iteration_cap": [{"instance": k, "dims": list(dims[k]),
+                                                   "rel_err": None if not np.isfinite(rel[k]) else float(rel[k])}
+                                                  for k in capped]}
     print(json.dumps({
         "mode": "batched designs", "instances": len(reqs), "design_iters_each": K,
         "elements_total": int(sum(a * b * c for a, b, c in dims)),
