@@ -85,6 +85,14 @@ __device__ __forceinline__ void prolong_add0_32(VB vb, const MgLevel32& Lc, cons
         int cy = fy / SP, cz = fz / SP;
         if (cy >= Lc.ny) cy = Lc.ny - 1;
         if (cz >= Lc.nz) cz = Lc.nz - 1;
+        // the run's fine rows are loaded first, so that their HBM reads and the coarse corners' L2 reads are in
+        // flight together (xo may be xi: every read of the run precedes its writes, as before)
+        const int64_t rb = row * Lf.pitch + SP * j;
+        V v[3];
+        if (!last) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) v[c] = *reinterpret_cast<const V*>(xi + c * Lf.cs + rb);
+        }
         float X[3][8];
 #pragma unroll
         for (int c = 0; c < 3; ++c)
@@ -114,7 +122,6 @@ __device__ __forceinline__ void prolong_add0_32(VB vb, const MgLevel32& Lc, cons
             }
             continue;
         }
-        const int64_t rb = row * Lf.pitch + SP * j;
         int m[SP];
         float w[SP][8];
 #pragma unroll
@@ -126,14 +133,13 @@ __device__ __forceinline__ void prolong_add0_32(VB vb, const MgLevel32& Lc, cons
         }
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            const V v = *reinterpret_cast<const V*>(xi + c * Lf.cs + rb);
             V o;
 #pragma unroll
             for (int k = 0; k < SP; ++k) {
                 float p = 0.0f;
 #pragma unroll
                 for (int A = 0; A < 8; ++A) p = fmaf(w[k][A], X[c][A], p);
-                lane_of(o, k) = ((m[k] >> c) & 1) ? 0.0f : lane_of(v, k) + p;
+                lane_of(o, k) = ((m[k] >> c) & 1) ? 0.0f : lane_of(v[c], k) + p;
             }
             *reinterpret_cast<V*>(xo + c * Lf.cs + rb) = o;
         }

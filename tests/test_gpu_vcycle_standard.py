@@ -236,3 +236,25 @@ def test_set_ke_invalidates_the_hierarchy():
         P.make_diagonal_preconditioner_from_static(E)
         assert np.all(np.isfinite(P.vcycle(np.ones(P.nf))))
         P.close()
+
+
+def test_coarsest_factor_failure_in_a_later_panel():
+    # moduli zero in the upper half of the grid: the coarsest Galerkin matrix (8x4x4 cells) has zero rows from the
+    # first free node of coarse layer z = 3 on (DOF 408 of 675, panel 12 of the blocked factor), so the factor
+    # reports failure
+    # (the coarse solve falls back to Jacobi, preconditioner.cpp:195-215) and the V-cycle stays finite; a
+    # later set-up with valid moduli factors again
+    import algorithmengineering_altproject_b200 as t3d
+    P = t3d.Problem(32, 64, 32, mg_vcycle=t3d.T3D_VCYCLE_STANDARD, mg_max_levels=3)
+    assert P.coarse_n == 675
+    nx, ny, nz = P.res
+    cz = P.ele_map_back().astype(np.int64) // (nx * ny)
+    P.make_diagonal_preconditioner_from_static(np.where(cz < nz // 2, 1.0, 0.0))
+    assert P.info().coarse_cholesky_ok == 0
+    r = np.random.default_rng(5).standard_normal(P.nf)
+    assert np.all(np.isfinite(P.vcycle(r)))
+    P.make_diagonal_preconditioner_from_static(np.ones(P.ne))
+    assert P.info().coarse_cholesky_ok == 1
+    z = P.vcycle(r)
+    assert np.all(np.isfinite(z)) and float(r @ z) > 0.0
+    P.close()
